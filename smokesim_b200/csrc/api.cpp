@@ -1,0 +1,775 @@
+// api.cpp - the C ABI of libsmokesim.so (include/smokesim.h).
+//
+// Host orchestration of the smoke step: the order of run_physics_step
+// (common/physics/physics.c:72-101), the recursive V-cycle of
+// common/physics/grid.c:177-209, the emitter clock of
+// update_emitters_status.comp and the rigid obstacles of obstacle_update.comp
+// (both tiny, run on the host), and device memory ownership.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "ss_internal.h"
+
+using namespace ss;
+
+namespace ss {
+
+static thread_local std::string g_err;
+
+int set_error(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+int check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return SS_OK;
+    return set_error(e == cudaErrorMemoryAllocation ? SS_E_OOM : SS_E_CUDA,
+                     std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+StepConsts make_consts(const ss_sim* s, const ss_params* p) {
+    StepConsts c{};
+    c.dt = p->time_step;
+    c.rho = p->density;
+    c.t_amb = p->t_ambient;
+    c.alpha = p->t_weight_coeff;
+    c.beta = p->t_temp_coeff;
+    c.eps = p->vorticity_confinement;
+    for (int d = 0; d < 3; ++d) c.wind[d] = p->wind[d];
+    c.cfl = c.dt / s->h;
+    c.rho_h = c.rho * s->h;
+    c.dt_h = c.dt * s->h;
+    c.k_upd = -c.dt / (c.rho * s->h);
+    c.vort_k = s->h;
+    return c;
+}
+
+}  // namespace ss
+
+#define TRY(x)                 \
+    do {                       \
+        int _rc = (x);         \
+        if (_rc != SS_OK) return _rc; \
+    } while (0)
+#define CU(x, what) TRY(check_cuda((x), what))
+
+static cudaStream_t as_stream(void* st) { return (cudaStream_t)st; }
+
+static int dalloc(void** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return check_cuda(e, "cudaMalloc");
+    return SS_OK;
+}
+
+static void free_sim(ss_sim* s) {
+    if (!s) return;
+    for (int d = 0; d < 3; ++d)
+        for (int b = 0; b < 2; ++b) cudaFree(s->vel[d][b]);
+    for (int b = 0; b < 2; ++b) { cudaFree(s->dens[b]); cudaFree(s->temp[b]); }
+    cudaFree(s->solid);
+    cudaFree(s->flags);
+    for (int d = 0; d < 3; ++d) cudaFree(s->svel[d]);
+    for (int l = 0; l < s->levels; ++l) { cudaFree(s->p[l]); cudaFree(s->r[l]); cudaFree(s->alpha[l]); }
+    cudaFree(s->div0);
+    if (s->div0r != s->div0) cudaFree(s->div0r);
+    cudaFree(s->vort);
+    cudaFree(s->red.partial);
+    cudaFree(s->red.out);
+    if (s->red.host) cudaFreeHost(s->red.host);
+    cudaFree(s->d_em);
+    cudaFree(s->d_ob);
+    cudaFree(s->d_bx);
+    delete s;
+}
+
+static bool finite_params(const ss_params* p) {
+    const float v[] = {p->time_step, p->density, p->t_ambient, p->t_weight_coeff, p->t_temp_coeff,
+                       p->vorticity_confinement, p->wind[0], p->wind[1], p->wind[2], p->current_time};
+    for (float x : v)
+        if (!isfinite(x)) return false;
+    return isfinite(p->mg.tol);
+}
+
+static int check_params(const ss_sim* s, const ss_params* p) {
+    if (!s || !p) return set_error(SS_E_INVALID, "NULL handle or params");
+    if (!finite_params(p)) return set_error(SS_E_NONFINITE, "non-finite parameter");
+    if (!(p->time_step > 0.f) || !(p->density > 0.f)) return set_error(SS_E_INVALID, "time_step and density must be > 0");
+    if (p->mg.n_pre < 0 || p->mg.n_post < 0 || p->mg.n_coarse < 0 || p->mg.n_vcycles < 0 || p->mg.tol < 0)
+        return set_error(SS_E_INVALID, "negative multigrid schedule entry");
+    if (p->mg.precision != SS_PREC_FP32 && p->mg.precision != SS_PREC_MIXED)
+        return set_error(SS_E_INVALID, "unknown precision mode");
+    return SS_OK;
+}
+
+extern "C" {
+
+int ss_abi_version(void) { return SS_ABI_VERSION; }
+
+const char* ss_strerror(int status) {
+    switch (status) {
+    case SS_OK: return "ok";
+    case SS_E_INVALID: return "invalid argument";
+    case SS_E_CUDA: return "CUDA error";
+    case SS_E_OOM: return "out of memory";
+    case SS_E_NOT_CONVERGED: return "pressure solve did not reach the tolerance";
+    case SS_E_NONFINITE: return "non-finite input";
+    case SS_E_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+    }
+}
+
+const char* ss_last_error_message(void) { return g_err.c_str(); }
+
+void ss_default_params(ss_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    // reference get_default_p_settings (common/physics/physics.c:7-20)
+    p->time_step = 1.0f / 120.0f;
+    p->density = 1.0f;
+    p->t_ambient = 293.0f;
+    p->t_temp_coeff = 1.0f;
+    p->t_weight_coeff = 0.07f;
+    p->vorticity_confinement = 1.0f;
+    p->stage_mask = SS_STAGE_ALL;
+    p->collect_stats = 0;
+    // reference v_cycle schedule (common/physics/grid.c:177-190)
+    p->mg.n_pre = 16;
+    p->mg.n_post = 16;
+    p->mg.n_coarse = 80;
+    p->mg.n_vcycles = 1;
+    p->mg.tol = 0.0;
+    p->mg.ref_quirks = 1;
+    p->mg.precision = SS_PREC_FP32;
+}
+
+int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
+    if (!d || !out) return set_error(SS_E_INVALID, "NULL desc or out");
+    *out = nullptr;
+    if (d->dim != 2 && d->dim != 3) return set_error(SS_E_INVALID, "dim must be 2 or 3");
+    const int nz = d->dim == 2 ? 1 : d->n[2];
+    if (d->n[0] < 3 || d->n[1] < 3 || nz < 1 || (d->dim == 3 && nz < 3))
+        return set_error(SS_E_INVALID, "grid must have at least 3 cells per axis");
+    if (d->dim == 2 && d->n[2] != 1) return set_error(SS_E_INVALID, "2D grids need n[2] == 1");
+    const double cells = (double)(d->n[0] + 1) * (d->n[1] + 1) * (nz + 1);
+    if (cells >= 2147483647.0) return set_error(SS_E_INVALID, "grid too large (face arrays must index in 31 bits)");
+    if (!(d->cell_size > 0.f) || !isfinite(d->cell_size)) return set_error(SS_E_INVALID, "cell_size must be > 0");
+    if (d->density_channels != 1 && d->density_channels != 3) return set_error(SS_E_INVALID, "density_channels must be 1 or 3");
+    if (!isfinite(d->t_ambient)) return set_error(SS_E_NONFINITE, "t_ambient");
+    cudaStream_t st = as_stream(stream);
+
+    ss_sim* s = new ss_sim();
+    s->dim = d->dim;
+    s->nx = d->n[0]; s->ny = d->n[1]; s->nz = nz;
+    s->nch = d->density_channels;
+    s->enclosed = d->enclosed ? 1 : 0;
+    s->min_coarse = d->min_coarse > 0 ? d->min_coarse : 4;
+    s->h = d->cell_size;
+    s->t_amb0 = d->t_ambient;
+    s->ncell = (size_t)s->nx * s->ny * s->nz;
+    s->nv[0] = (size_t)(s->nx + 1) * s->ny * s->nz;
+    s->nv[1] = (size_t)s->nx * (s->ny + 1) * s->nz;
+    s->nv[2] = s->dim == 3 ? (size_t)s->nx * s->ny * (s->nz + 1) : 0;
+
+    // pyramid: reference gen_grid_pressure_solve_textures3d (3d/grid3d.c:45-68)
+    // with the smallest level dimension as a parameter
+    int dims[3] = {s->nx, s->ny, s->nz};
+    int lv = 0;
+    while (lv < SS_MAX_LEVELS) {
+        bool ok = dims[0] >= s->min_coarse && dims[1] >= s->min_coarse && (s->dim == 2 || dims[2] >= s->min_coarse);
+        if (!ok) break;
+        s->lv[lv].n[0] = dims[0]; s->lv[lv].n[1] = dims[1]; s->lv[lv].n[2] = s->dim == 2 ? 1 : dims[2];
+        dims[0] /= 2; dims[1] /= 2; if (s->dim == 3) dims[2] /= 2;
+        ++lv;
+    }
+    if (lv == 0) {
+        s->lv[0].n[0] = s->nx; s->lv[0].n[1] = s->ny; s->lv[0].n[2] = s->nz;
+        lv = 1;
+    }
+    s->levels = lv;
+    for (int l = 0; l < lv; ++l) {
+        s->lv[l].h = s->h * (float)(1 << l);
+        s->lv[l].hh = s->lv[l].h * s->lv[l].h;
+    }
+
+    int rc = SS_OK;
+    auto A = [&](void** p, size_t bytes) { if (rc == SS_OK) rc = dalloc(p, bytes); };
+    for (int dd = 0; dd < s->dim; ++dd)
+        for (int b = 0; b < 2; ++b) A((void**)&s->vel[dd][b], s->nv[dd] * sizeof(float));
+    for (int b = 0; b < 2; ++b) {
+        A((void**)&s->dens[b], s->ncell * s->nch * sizeof(float));
+        A((void**)&s->temp[b], s->ncell * sizeof(float));
+    }
+    A((void**)&s->solid, s->ncell);
+    A((void**)&s->flags, s->ncell);
+    for (int l = 0; l < lv; ++l) {
+        const size_t n = (size_t)s->lv[l].n[0] * s->lv[l].n[1] * s->lv[l].n[2];
+        A((void**)&s->p[l], n * sizeof(float));
+        A((void**)&s->r[l], n * sizeof(float));
+        if (l > 0) A((void**)&s->alpha[l], n * sizeof(float));
+    }
+    A((void**)&s->div0, s->ncell * sizeof(float));
+    if (s->enclosed) s->div0r = s->div0;
+    else A((void**)&s->div0r, s->ncell * sizeof(float));
+    A((void**)&s->vort, s->ncell * (s->dim == 3 ? 3 : 1) * sizeof(float));
+    s->red.max_blocks = (int)(((s->nx + 32) / 32 + 1) * ((s->ny + 8) / 8 + 1) * (size_t)(s->nz + 1));
+    A((void**)&s->red.partial, (size_t)s->red.max_blocks * sizeof(double));
+    A((void**)&s->red.out, SLOT_COUNT * sizeof(double));
+    if (rc == SS_OK) {
+        cudaError_t e = cudaMallocHost((void**)&s->red.host, SLOT_COUNT * sizeof(double));
+        if (e != cudaSuccess) rc = check_cuda(e, "cudaMallocHost");
+    }
+    if (rc != SS_OK) {
+        free_sim(s);
+        return rc;
+    }
+    // initial state: velocities and pressure 0, smoke (0, 0, 0, t_ambient)
+    for (int dd = 0; dd < s->dim; ++dd)
+        for (int b = 0; b < 2; ++b) rc = rc ? rc : check_cuda(cudaMemsetAsync(s->vel[dd][b], 0, s->nv[dd] * 4, st), "memset");
+    for (int b = 0; b < 2; ++b) {
+        if (!rc) rc = check_cuda(cudaMemsetAsync(s->dens[b], 0, s->ncell * s->nch * 4, st), "memset");
+        if (!rc) rc = launch_fill(s->temp[b], s->ncell, s->t_amb0, st);
+    }
+    for (int l = 0; l < lv && !rc; ++l) {
+        const size_t n = (size_t)s->lv[l].n[0] * s->lv[l].n[1] * s->lv[l].n[2];
+        rc = check_cuda(cudaMemsetAsync(s->p[l], 0, n * 4, st), "memset");
+        if (!rc) rc = check_cuda(cudaMemsetAsync(s->r[l], 0, n * 4, st), "memset");
+    }
+    if (!rc) rc = check_cuda(cudaMemsetAsync(s->div0, 0, s->ncell * 4, st), "memset");
+    if (!rc && s->div0r != s->div0) rc = check_cuda(cudaMemsetAsync(s->div0r, 0, s->ncell * 4, st), "memset");
+    if (!rc) rc = ss_set_scene(s, nullptr, 0, nullptr, 0, nullptr, 0, stream);
+    if (!rc) rc = check_cuda(cudaStreamSynchronize(st), "create sync");
+    if (rc) {
+        free_sim(s);
+        return rc;
+    }
+    *out = s;
+    return SS_OK;
+}
+
+int ss_destroy(ss_sim* s) {
+    if (!s) return set_error(SS_E_INVALID, "NULL handle");
+    cudaDeviceSynchronize();
+    free_sim(s);
+    return SS_OK;
+}
+
+int ss_get_desc(const ss_sim* s, ss_desc* out, int* levels, int level_sizes[][3]) {
+    if (!s) return set_error(SS_E_INVALID, "NULL handle");
+    if (out) {
+        out->dim = s->dim;
+        out->n[0] = s->nx; out->n[1] = s->ny; out->n[2] = s->nz;
+        out->cell_size = s->h;
+        out->density_channels = s->nch;
+        out->enclosed = s->enclosed;
+        out->min_coarse = s->min_coarse;
+        out->t_ambient = s->t_amb0;
+    }
+    if (levels) *levels = s->levels;
+    if (level_sizes)
+        for (int l = 0; l < s->levels; ++l)
+            for (int d = 0; d < 3; ++d) level_sizes[l][d] = s->lv[l].n[d];
+    return SS_OK;
+}
+
+// ------------------------------------------------------------------- scene
+static int upload_array(void** dptr, int* cap, const void* host, size_t elem, int n, cudaStream_t st) {
+    if (n > *cap) {
+        cudaFree(*dptr);
+        *dptr = nullptr;
+        TRY(dalloc(dptr, elem * (size_t)n));
+        *cap = n;
+    }
+    if (n > 0) CU(cudaMemcpyAsync(*dptr, host, elem * (size_t)n, cudaMemcpyHostToDevice, st), "scene upload");
+    return SS_OK;
+}
+
+static bool scene_moving(const ss_sim* s) {
+    for (const ss_obstacle& o : s->ob)
+        if (o.anchored != 1.f) return true;
+    return false;
+}
+
+static int rasterize_solid(ss_sim* s, cudaStream_t st) {
+    // solid velocity channels only when some obstacle or box can carry one
+    bool need = false;
+    for (const ss_obstacle& o : s->ob)
+        if ((o.velocity[0] != 0.f || o.velocity[1] != 0.f || o.velocity[2] != 0.f) && o.anchored != 1.f) need = true;
+    for (const ss_box& b : s->bx)
+        if ((b.velocity[0] != 0.f || b.velocity[1] != 0.f || b.velocity[2] != 0.f) && b.anchored != 1.f) need = true;
+    if (scene_moving(s)) need = true;
+    if (need && !s->svel[0]) {
+        for (int d = 0; d < s->dim; ++d) TRY(dalloc((void**)&s->svel[d], s->ncell * sizeof(float)));
+    }
+    s->svel_active = need ? 1 : 0;
+    TRY(upload_array((void**)&s->d_ob, &s->cap_ob, s->ob.data(), sizeof(ss_obstacle), (int)s->ob.size(), st));
+    TRY(upload_array((void**)&s->d_bx, &s->cap_bx, s->bx.data(), sizeof(ss_box), (int)s->bx.size(), st));
+    TRY(launch_rasterize(s, st));
+    TRY(launch_flags(s, st));
+    TRY(launch_solid_pyramid(s, st));
+    return SS_OK;
+}
+
+int ss_set_scene(ss_sim* s, const ss_emitter* em, int ne, const ss_obstacle* ob, int no, const ss_box* bx, int nb,
+                 void* stream) {
+    if (!s) return set_error(SS_E_INVALID, "NULL handle");
+    if (ne < 0 || no < 0 || nb < 0 || ne > SS_MAX_EMITTERS || no > SS_MAX_OBSTACLES || nb > SS_MAX_BOXES)
+        return set_error(SS_E_INVALID, "scene object count out of range");
+    if ((ne && !em) || (no && !ob) || (nb && !bx)) return set_error(SS_E_INVALID, "NULL scene array");
+    for (int i = 0; i < ne; ++i) {
+        const ss_emitter& e = em[i];
+        const float v[] = {e.pos[0], e.pos[1], e.pos[2], e.radius, e.density[0], e.density[1], e.density[2],
+                           e.temperature, e.velocity[0], e.velocity[1], e.velocity[2]};
+        for (float x : v)
+            if (!isfinite(x)) return set_error(SS_E_NONFINITE, "non-finite emitter field");
+    }
+    for (int i = 0; i < no; ++i) {
+        const ss_obstacle& o = ob[i];
+        const float v[] = {o.pos[0], o.pos[1], o.pos[2], o.radius, o.velocity[0], o.velocity[1], o.velocity[2], o.anchored};
+        for (float x : v)
+            if (!isfinite(x)) return set_error(SS_E_NONFINITE, "non-finite obstacle field");
+    }
+    for (int i = 0; i < nb; ++i) {
+        const ss_box& b = bx[i];
+        const float v[] = {b.lo[0], b.lo[1], b.lo[2], b.hi[0], b.hi[1], b.hi[2], b.velocity[0], b.velocity[1], b.velocity[2], b.anchored};
+        for (float x : v)
+            if (!isfinite(x)) return set_error(SS_E_NONFINITE, "non-finite box field");
+    }
+    cudaStream_t st = as_stream(stream);
+    s->em.assign(em, em + ne);
+    s->ob.assign(ob, ob + no);
+    s->bx.assign(bx, bx + nb);
+    TRY(upload_array((void**)&s->d_em, &s->cap_em, s->em.data(), sizeof(ss_emitter), ne, st));
+    TRY(rasterize_solid(s, st));
+    CU(cudaStreamSynchronize(st), "set_scene sync");
+    return SS_OK;
+}
+
+int ss_get_scene(ss_sim* s, ss_emitter* em, int ne, ss_obstacle* ob, int no) {
+    if (!s) return set_error(SS_E_INVALID, "NULL handle");
+    if (em) std::copy_n(s->em.begin(), std::min<size_t>((size_t)std::max(ne, 0), s->em.size()), em);
+    if (ob) std::copy_n(s->ob.begin(), std::min<size_t>((size_t)std::max(no, 0), s->ob.size()), ob);
+    return SS_OK;
+}
+
+// reference update_emitters_status (shaders3d/compute/update_emitters_status.comp:49-59)
+static void emitters_status(ss_sim* s, float current_time) {
+    for (ss_emitter& e : s->em) {
+        if (e.emit == 1 && e.delay != 0) {
+            e.emit = 0;
+            e.last_emit = (int)current_time;
+            continue;
+        }
+        if (current_time - (float)e.last_emit >= (float)e.delay) e.emit = 1;
+    }
+}
+
+// reference obstacle_update (shaders3d/compute/obstacle_update.comp:51-135):
+// gravity, wall bounce 0.999, push-out against the input positions, damping.
+static void obstacles_update(ss_sim* s, float dt) {
+    const int n = (int)s->ob.size();
+    if (n == 0) return;
+    const std::vector<ss_obstacle> in = s->ob;
+    const bool d3 = s->dim == 3;
+    const int nd = d3 ? 3 : 2;
+    const float maxb[3] = {(float)s->nx, (float)s->ny, (float)s->nz};
+    for (int i = 0; i < n; ++i) {
+        float pos[3] = {in[i].pos[0], in[i].pos[1], d3 ? in[i].pos[2] : 0.f};
+        float vel[3] = {in[i].velocity[0], in[i].velocity[1], d3 ? in[i].velocity[2] : 0.f};
+        const float r = in[i].radius, anchored = in[i].anchored, movable = 1.f - anchored;
+        if (!(anchored == 1.f)) {
+            vel[1] = vel[1] + -9.81f * dt * movable;
+            vel[0] = vel[0] + 0.f * dt * movable;
+            if (d3) vel[2] = vel[2] + 0.f * dt * movable;
+            for (int c = 0; c < nd; ++c) pos[c] = pos[c] + vel[c] * dt * movable;
+            const float B = 0.999f;
+            for (int c = 0; c < nd; ++c) {
+                if (pos[c] - r < 0.f) { pos[c] = 0.f + r; vel[c] *= -B; }
+                if (pos[c] + r > maxb[c]) { pos[c] = maxb[c] - r; vel[c] *= -B; }
+            }
+            for (int j = 0; j < n; ++j) {
+                if (j == i) continue;
+                const float dd[3] = {pos[0] - in[j].pos[0], pos[1] - in[j].pos[1], d3 ? pos[2] - in[j].pos[2] : 0.f};
+                const float dist = d3 ? sqrtf(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]) : sqrtf(dd[0] * dd[0] + dd[1] * dd[1]);
+                const float min_dist = r + in[j].radius;
+                if (dist < min_dist && dist > 0.0001f) {
+                    const float nn[3] = {dd[0] / dist, dd[1] / dist, dd[2] / dist};
+                    for (int c = 0; c < nd; ++c) pos[c] += nn[c] * (min_dist - dist) * 0.5f * movable;
+                    const float rv[3] = {vel[0] - in[j].velocity[0], vel[1] - in[j].velocity[1],
+                                         d3 ? vel[2] - in[j].velocity[2] : 0.f};
+                    const float vn = d3 ? rv[0] * nn[0] + rv[1] * nn[1] + rv[2] * nn[2] : rv[0] * nn[0] + rv[1] * nn[1];
+                    if (vn < 0.f)
+                        for (int c = 0; c < nd; ++c) vel[c] -= vn * nn[c] * movable;
+                }
+            }
+        }
+        s->ob[i].pos[0] = pos[0]; s->ob[i].pos[1] = pos[1];
+        if (d3) s->ob[i].pos[2] = pos[2];
+        s->ob[i].velocity[0] = vel[0] * 0.999f;
+        s->ob[i].velocity[1] = vel[1] * 0.999f;
+        if (d3) s->ob[i].velocity[2] = vel[2] * 0.999f;
+    }
+}
+
+// ------------------------------------------------------------------- fields
+static int field_buffer(ss_sim* s, int f, float** ptr, size_t* count) {
+    switch (f) {
+    case SS_FIELD_VX: *ptr = s->vel[0][s->vi[0]]; *count = s->nv[0]; return SS_OK;
+    case SS_FIELD_VY: *ptr = s->vel[1][s->vi[1]]; *count = s->nv[1]; return SS_OK;
+    case SS_FIELD_VZ:
+        if (s->dim != 3) return set_error(SS_E_INVALID, "2D grid has no w");
+        *ptr = s->vel[2][s->vi[2]]; *count = s->nv[2]; return SS_OK;
+    case SS_FIELD_DENSITY: *ptr = s->dens[s->si]; *count = s->ncell * s->nch; return SS_OK;
+    case SS_FIELD_TEMPERATURE: *ptr = s->temp[s->si]; *count = s->ncell; return SS_OK;
+    case SS_FIELD_PRESSURE: *ptr = s->p[0]; *count = s->ncell; return SS_OK;
+    case SS_FIELD_DIVERGENCE: *ptr = s->div0; *count = s->ncell; return SS_OK;
+    default: return set_error(SS_E_INVALID, "unknown field");
+    }
+}
+
+int ss_set_field(ss_sim* s, int f, const float* host, size_t count, void* stream) {
+    if (!s || !host) return set_error(SS_E_INVALID, "NULL argument");
+    if (f == SS_FIELD_SOLID || f == SS_FIELD_DIVERGENCE) return set_error(SS_E_INVALID, "field is read only (use ss_set_scene)");
+    float* d;
+    size_t n;
+    TRY(field_buffer(s, f, &d, &n));
+    if (count != n) return set_error(SS_E_INVALID, "element count does not match the field");
+    for (size_t i = 0; i < n; ++i)
+        if (!isfinite(host[i])) return set_error(SS_E_NONFINITE, "non-finite value in field data");
+    cudaStream_t st = as_stream(stream);
+    CU(cudaMemcpyAsync(d, host, n * sizeof(float), cudaMemcpyHostToDevice, st), "set_field");
+    CU(cudaStreamSynchronize(st), "set_field sync");
+    return SS_OK;
+}
+
+int ss_get_field(ss_sim* s, int f, float* host, size_t count, void* stream) {
+    if (!s || !host) return set_error(SS_E_INVALID, "NULL argument");
+    cudaStream_t st = as_stream(stream);
+    if (f == SS_FIELD_SOLID) {
+        if (count != s->ncell) return set_error(SS_E_INVALID, "element count does not match the field");
+        std::vector<uint8_t> tmp(s->ncell);
+        CU(cudaMemcpyAsync(tmp.data(), s->solid, s->ncell, cudaMemcpyDeviceToHost, st), "get_field");
+        CU(cudaStreamSynchronize(st), "get_field sync");
+        for (size_t i = 0; i < s->ncell; ++i) host[i] = tmp[i] ? 1.f : 0.f;
+        return SS_OK;
+    }
+    if (f == SS_FIELD_DIVERGENCE) {
+        CU(cudaMemsetAsync(s->div0, 0, s->ncell * sizeof(float), st), "memset");
+        TRY(launch_divergence(s, true, -1, st));
+    }
+    float* d;
+    size_t n;
+    TRY(field_buffer(s, f, &d, &n));
+    if (count != n) return set_error(SS_E_INVALID, "element count does not match the field");
+    CU(cudaMemcpyAsync(host, d, n * sizeof(float), cudaMemcpyDeviceToHost, st), "get_field");
+    CU(cudaStreamSynchronize(st), "get_field sync");
+    return SS_OK;
+}
+
+int ss_field_device_ptr(ss_sim* s, int f, void** dptr, size_t* count) {
+    if (!s || !dptr) return set_error(SS_E_INVALID, "NULL argument");
+    if (f == SS_FIELD_SOLID) {
+        *dptr = s->solid;
+        if (count) *count = s->ncell;
+        return SS_OK;
+    }
+    float* d;
+    size_t n;
+    TRY(field_buffer(s, f, &d, &n));
+    *dptr = d;
+    if (count) *count = n;
+    return SS_OK;
+}
+
+int ss_clear_grid(ss_sim* s, float t_ambient, void* stream) {
+    if (!s) return set_error(SS_E_INVALID, "NULL handle");
+    if (!isfinite(t_ambient)) return set_error(SS_E_NONFINITE, "t_ambient");
+    cudaStream_t st = as_stream(stream);
+    // reference clear_grid3d (3d/grid3d.c:164-183)
+    for (int d = 0; d < s->dim; ++d)
+        for (int b = 0; b < 2; ++b) CU(cudaMemsetAsync(s->vel[d][b], 0, s->nv[d] * 4, st), "memset");
+    for (int b = 0; b < 2; ++b) {
+        CU(cudaMemsetAsync(s->dens[b], 0, s->ncell * s->nch * 4, st), "memset");
+        TRY(launch_fill(s->temp[b], s->ncell, t_ambient, st));
+    }
+    for (int l = 0; l < s->levels; ++l) {
+        const size_t n = (size_t)s->lv[l].n[0] * s->lv[l].n[1] * s->lv[l].n[2];
+        CU(cudaMemsetAsync(s->p[l], 0, n * 4, st), "memset");
+    }
+    CU(cudaStreamSynchronize(st), "clear sync");
+    return SS_OK;
+}
+
+int ss_get_level(ss_sim* s, int L, int what, float* host, size_t count, void* stream) {
+    if (!s || !host) return set_error(SS_E_INVALID, "NULL argument");
+    if (L < 0 || L >= s->levels) return set_error(SS_E_INVALID, "level out of range");
+    const size_t n = (size_t)s->lv[L].n[0] * s->lv[L].n[1] * s->lv[L].n[2];
+    if (count != n) return set_error(SS_E_INVALID, "element count does not match the level");
+    cudaStream_t st = as_stream(stream);
+    if (what == SS_LEVEL_FLUID_WEIGHT) {
+        std::vector<float> tmp(n);
+        if (L == 0) {
+            std::vector<uint8_t> sb(n);
+            CU(cudaMemcpyAsync(sb.data(), s->solid, n, cudaMemcpyDeviceToHost, st), "get_level");
+            CU(cudaStreamSynchronize(st), "sync");
+            for (size_t i = 0; i < n; ++i) host[i] = sb[i] ? 0.f : 1.f;
+        } else {
+            CU(cudaMemcpyAsync(tmp.data(), s->alpha[L], n * 4, cudaMemcpyDeviceToHost, st), "get_level");
+            CU(cudaStreamSynchronize(st), "sync");
+            for (size_t i = 0; i < n; ++i) host[i] = 1.f - tmp[i];
+        }
+        return SS_OK;
+    }
+    float* d = what == SS_LEVEL_PRESSURE ? s->p[L] : what == SS_LEVEL_RESIDUAL ? s->r[L] : nullptr;
+    if (!d) return set_error(SS_E_INVALID, "unknown level array");
+    CU(cudaMemcpyAsync(host, d, n * 4, cudaMemcpyDeviceToHost, st), "get_level");
+    CU(cudaStreamSynchronize(st), "sync");
+    return SS_OK;
+}
+
+int ss_set_level(ss_sim* s, int L, int what, const float* host, size_t count, void* stream) {
+    if (!s || !host) return set_error(SS_E_INVALID, "NULL argument");
+    if (L < 0 || L >= s->levels) return set_error(SS_E_INVALID, "level out of range");
+    const size_t n = (size_t)s->lv[L].n[0] * s->lv[L].n[1] * s->lv[L].n[2];
+    if (count != n) return set_error(SS_E_INVALID, "element count does not match the level");
+    float* d = what == SS_LEVEL_PRESSURE ? s->p[L] : what == SS_LEVEL_RESIDUAL ? s->r[L] : nullptr;
+    if (!d) return set_error(SS_E_INVALID, "level array is read only");
+    cudaStream_t st = as_stream(stream);
+    CU(cudaMemcpyAsync(d, host, n * 4, cudaMemcpyHostToDevice, st), "set_level");
+    CU(cudaStreamSynchronize(st), "sync");
+    return SS_OK;
+}
+
+// ------------------------------------------------------------------ solver
+static int v_cycle_rec(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int L, cudaStream_t st) {
+    const int q = mg.ref_quirks;
+    if (L == s->levels - 1) return launch_smooth(s, c, L, mg.n_coarse, q, st);
+    TRY(launch_smooth(s, c, L, mg.n_pre, q, st));
+    // residual written in place only where the reference's post-smoother reads it
+    TRY(launch_residual(s, c, L, q && L > 0, true, q, st));
+    const size_t nc = (size_t)s->lv[L + 1].n[0] * s->lv[L + 1].n[1] * s->lv[L + 1].n[2];
+    CU(cudaMemsetAsync(s->p[L + 1], 0, nc * sizeof(float), st), "clear coarse p");
+    TRY(v_cycle_rec(s, c, mg, L + 1, st));
+    TRY(launch_prolong(s, L, st));
+    return launch_smooth(s, c, L, mg.n_post, q, st);
+}
+
+static int read_slots(ss_sim* s, cudaStream_t st) {
+    CU(cudaMemcpyAsync(s->red.host, s->red.out, SLOT_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st), "slots");
+    CU(cudaStreamSynchronize(st), "slots sync");
+    return SS_OK;
+}
+
+static int ensure_pyramid(ss_sim* s, cudaStream_t st) {
+    if (s->pyramid_dirty) TRY(launch_solid_pyramid(s, st));
+    return SS_OK;
+}
+
+// multigrid_pressure_solve (common/physics/grid.c:173-175)
+static int pressure_solve(ss_sim* s, const ss_params* p, const StepConsts& c, cudaStream_t st) {
+    const ss_mg_schedule& mg = p->mg;
+    const bool tol_mode = mg.tol > 0.0;
+    const bool stats = p->collect_stats || tol_mode;
+    TRY(ensure_pyramid(s, st));
+    TRY(launch_divergence(s, true, stats ? SLOT_DIV_BEFORE : -1, st));
+    const int cap = mg.n_vcycles > 0 ? mg.n_vcycles : 1;
+    int done = 0;
+    bool conv = true;
+    if (!tol_mode) {
+        for (; done < cap; ++done) TRY(v_cycle_rec(s, c, mg, 0, st));
+        if (stats) TRY(launch_projected_residual_norm(s, c, SLOT_RESIDUAL, st));
+        if (stats) {
+            TRY(read_slots(s, st));
+            s->st.div_before = sqrt(s->red.host[SLOT_DIV_BEFORE]);
+            s->st.residual = sqrt(s->red.host[SLOT_RESIDUAL]);
+        }
+    } else {
+        TRY(launch_projected_residual_norm(s, c, SLOT_RESIDUAL, st));
+        TRY(read_slots(s, st));
+        const double db = sqrt(s->red.host[SLOT_DIV_BEFORE]);
+        double res = sqrt(s->red.host[SLOT_RESIDUAL]);
+        while (done < cap && !(res <= mg.tol * db)) {
+            TRY(v_cycle_rec(s, c, mg, 0, st));
+            ++done;
+            TRY(launch_projected_residual_norm(s, c, SLOT_RESIDUAL, st));
+            TRY(read_slots(s, st));
+            res = sqrt(s->red.host[SLOT_RESIDUAL]);
+        }
+        conv = res <= mg.tol * db;
+        s->st.div_before = db;
+        s->st.residual = res;
+    }
+    s->st.vcycles = done;
+    s->st.converged = conv ? 1 : 0;
+    return SS_OK;
+}
+
+static int do_step(ss_sim* s, const ss_params* p, cudaStream_t st) {
+    const StepConsts c = make_consts(s, p);
+    const int m = p->stage_mask;
+    if (m & SS_STAGE_HANDLE_EMITTERS) {
+        emitters_status(s, p->current_time);
+        TRY(upload_array((void**)&s->d_em, &s->cap_em, s->em.data(), sizeof(ss_emitter), (int)s->em.size(), st));
+        TRY(launch_emitters(s, c, st));
+    }
+    if (m & SS_STAGE_ADVECT_VELOCITIES) {
+        TRY(launch_advect_velocities(s, c, (m & SS_STAGE_APPLY_BUOYANCY) != 0, st));
+    } else if (m & SS_STAGE_APPLY_BUOYANCY) {
+        TRY(launch_buoyancy(s, c, st));
+    }
+    if (m & SS_STAGE_APPLY_VORTICITY) TRY(launch_vorticity(s, c, st));
+    if (m & SS_STAGE_RESOLVE_PRESSURE) TRY(pressure_solve(s, p, c, st));
+    if (m & SS_STAGE_UPDATE_VELOCITIES) {
+        TRY(launch_update_velocities(s, c, st));
+        if ((m & SS_STAGE_RESOLVE_PRESSURE) && (p->collect_stats || p->mg.tol > 0.0)) {
+            TRY(launch_divergence(s, false, SLOT_DIV_AFTER, st));
+            TRY(read_slots(s, st));
+            s->st.div_after = sqrt(s->red.host[SLOT_DIV_AFTER]);
+            s->st.rel_div = s->st.div_before > 0 ? s->st.div_after / s->st.div_before : 0.0;
+        }
+    }
+    if (m & SS_STAGE_ADVECT_SMOKE) TRY(launch_advect_smoke(s, c, st));
+    if (m & SS_STAGE_OBSTACLES) {
+        if (scene_moving(s)) {
+            obstacles_update(s, p->time_step);
+            TRY(rasterize_solid(s, st));
+        } else {
+            obstacles_update(s, p->time_step);  // anchored: only the stored velocity decays
+        }
+    }
+    s->st.steps += 1;
+    return SS_OK;
+}
+
+int ss_run_physics_step(ss_sim* s, const ss_params* p, int nsteps, void* stream) {
+    TRY(check_params(s, p));
+    if (nsteps < 0) return set_error(SS_E_INVALID, "nsteps < 0");
+    cudaStream_t st = as_stream(stream);
+    s->st.steps = 0;
+    s->nlaunch = 0;
+    for (int i = 0; i < nsteps; ++i) TRY(do_step(s, p, st));
+    s->st.kernel_launches = s->nlaunch;
+    CU(cudaGetLastError(), "step");
+    if (p->mg.tol > 0.0 && (p->stage_mask & SS_STAGE_RESOLVE_PRESSURE) && !s->st.converged)
+        return set_error(SS_E_NOT_CONVERGED, "V-cycle cap reached before the divergence tolerance");
+    return SS_OK;
+}
+
+int ss_get_stats(ss_sim* s, ss_stats* out) {
+    if (!s || !out) return set_error(SS_E_INVALID, "NULL argument");
+    *out = s->st;
+    return SS_OK;
+}
+
+// ------------------------------------------------------------ single stages
+int ss_update_emitters_status(ss_sim* s, const ss_params* p, void* stream) {
+    TRY(check_params(s, p));
+    emitters_status(s, p->current_time);
+    return upload_array((void**)&s->d_em, &s->cap_em, s->em.data(), sizeof(ss_emitter), (int)s->em.size(), as_stream(stream));
+}
+
+int ss_handle_emitters(ss_sim* s, const ss_params* p, void* stream) {
+    TRY(check_params(s, p));
+    cudaStream_t st = as_stream(stream);
+    TRY(upload_array((void**)&s->d_em, &s->cap_em, s->em.data(), sizeof(ss_emitter), (int)s->em.size(), st));
+    return launch_emitters(s, make_consts(s, p), st);
+}
+
+int ss_advect_velocities(ss_sim* s, const ss_params* p, void* stream) {
+    TRY(check_params(s, p));
+    return launch_advect_velocities(s, make_consts(s, p), false, as_stream(stream));
+}
+
+int ss_apply_buoyancy(ss_sim* s, const ss_params* p, void* stream) {
+    TRY(check_params(s, p));
+    return launch_buoyancy(s, make_consts(s, p), as_stream(stream));
+}
+
+int ss_apply_vorticity(ss_sim* s, const ss_params* p, void* stream) {
+    TRY(check_params(s, p));
+    return launch_vorticity(s, make_consts(s, p), as_stream(stream));
+}
+
+int ss_multigrid_pressure_solve(ss_sim* s, const ss_params* p, void* stream) {
+    TRY(check_params(s, p));
+    cudaStream_t st = as_stream(stream);
+    TRY(pressure_solve(s, p, make_consts(s, p), st));
+    if (p->mg.tol > 0.0 && !s->st.converged)
+        return set_error(SS_E_NOT_CONVERGED, "V-cycle cap reached before the divergence tolerance");
+    return SS_OK;
+}
+
+int ss_v_cycle(ss_sim* s, const ss_params* p, int level, void* stream) {
+    TRY(check_params(s, p));
+    if (level < 0 || level >= s->levels) return set_error(SS_E_INVALID, "level out of range");
+    cudaStream_t st = as_stream(stream);
+    TRY(ensure_pyramid(s, st));
+    if (level == 0) TRY(launch_divergence(s, true, -1, st));
+    return v_cycle_rec(s, make_consts(s, p), p->mg, level, st);
+}
+
+int ss_smooth(ss_sim* s, const ss_params* p, int level, int iterations, void* stream) {
+    TRY(check_params(s, p));
+    if (level < 0 || level >= s->levels || iterations < 0) return set_error(SS_E_INVALID, "level/iterations out of range");
+    cudaStream_t st = as_stream(stream);
+    TRY(ensure_pyramid(s, st));
+    if (level == 0) TRY(launch_divergence(s, true, -1, st));
+    return launch_smooth(s, make_consts(s, p), level, iterations, p->mg.ref_quirks, st);
+}
+
+int ss_compute_residual(ss_sim* s, const ss_params* p, int level, void* stream) {
+    TRY(check_params(s, p));
+    if (level < 0 || level >= s->levels) return set_error(SS_E_INVALID, "level out of range");
+    cudaStream_t st = as_stream(stream);
+    TRY(ensure_pyramid(s, st));
+    if (level == 0) TRY(launch_divergence(s, true, -1, st));
+    return launch_residual(s, make_consts(s, p), level, true, false, p->mg.ref_quirks, st);
+}
+
+int ss_compute_restrict(ss_sim* s, const ss_params* p, int level, void* stream) {
+    TRY(check_params(s, p));
+    if (level < 0 || level + 1 >= s->levels) return set_error(SS_E_INVALID, "level out of range");
+    cudaStream_t st = as_stream(stream);
+    TRY(ensure_pyramid(s, st));
+    return launch_restrict(s, level, st);
+}
+
+int ss_prolong_and_add(ss_sim* s, const ss_params* p, int level, void* stream) {
+    TRY(check_params(s, p));
+    if (level < 0 || level >= s->levels) return set_error(SS_E_INVALID, "level out of range");
+    return launch_prolong(s, level, as_stream(stream));
+}
+
+int ss_update_velocities(ss_sim* s, const ss_params* p, void* stream) {
+    TRY(check_params(s, p));
+    return launch_update_velocities(s, make_consts(s, p), as_stream(stream));
+}
+
+int ss_advect_smoke(ss_sim* s, const ss_params* p, void* stream) {
+    TRY(check_params(s, p));
+    return launch_advect_smoke(s, make_consts(s, p), as_stream(stream));
+}
+
+int ss_obstacle_update_step(ss_sim* s, const ss_params* p, void* stream) {
+    TRY(check_params(s, p));
+    obstacles_update(s, p->time_step);
+    if (scene_moving(s)) TRY(rasterize_solid(s, as_stream(stream)));
+    return SS_OK;
+}
+
+int ss_update_solid_map(ss_sim* s, void* stream) {
+    if (!s) return set_error(SS_E_INVALID, "NULL handle");
+    return rasterize_solid(s, as_stream(stream));
+}
+
+int ss_init_solid_map(ss_sim* s, void* stream) {
+    if (!s) return set_error(SS_E_INVALID, "NULL handle");
+    return rasterize_solid(s, as_stream(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,587 @@
+// k_fluid.cu - per-cell / per-face stages of the smoke step.
+//
+// Each kernel restates one or more reference compute shaders; the shader is
+// cited at the kernel.  Velocities are read from the current ping-pong buffer
+// and written to the other one (the reference's texture/image pairs,
+// 3d/grid3d.c:104-162), smoke likewise.
+#include "common.cuh"
+#include "ss_internal.h"
+
+namespace ss {
+
+struct FluidArgs {
+    int nx, ny, nz, nch;
+    const float* u;
+    const float* v;
+    const float* w;
+    float* uo;
+    float* vo;
+    float* wo;
+    const uint8_t* flags;
+    const float* dens;
+    const float* temp;
+    float* dens_o;
+    float* temp_o;
+    const float* sv0;
+    const float* sv1;
+    const float* sv2;
+    StepConsts c;
+};
+
+static FluidArgs fluid_args(ss_sim* s, const StepConsts& c) {
+    FluidArgs a;
+    a.nx = s->nx; a.ny = s->ny; a.nz = s->nz; a.nch = s->nch;
+    a.u = s->vel[0][s->vi[0]]; a.v = s->vel[1][s->vi[1]]; a.w = s->dim == 3 ? s->vel[2][s->vi[2]] : nullptr;
+    a.uo = s->vel[0][1 - s->vi[0]]; a.vo = s->vel[1][1 - s->vi[1]];
+    a.wo = s->dim == 3 ? s->vel[2][1 - s->vi[2]] : nullptr;
+    a.flags = s->flags;
+    a.dens = s->dens[s->si]; a.temp = s->temp[s->si];
+    a.dens_o = s->dens[1 - s->si]; a.temp_o = s->temp[1 - s->si];
+    a.sv0 = s->svel_active ? s->svel[0] : nullptr;
+    a.sv1 = s->svel_active ? s->svel[1] : nullptr;
+    a.sv2 = s->svel_active ? s->svel[2] : nullptr;
+    a.c = c;
+    return a;
+}
+
+SS_D bool solid_oob1(const uint8_t* __restrict__ f, int x, int y, int z, int nx, int ny, int nz) {
+    if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return true;
+    return f[idx3(x, y, z, nx, ny)] & F_SOLID;
+}
+SS_D bool solid_oob0(const uint8_t* __restrict__ f, int x, int y, int z, int nx, int ny, int nz) {
+    if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return false;
+    return f[idx3(x, y, z, nx, ny)] & F_SOLID;
+}
+
+static inline dim3 grid_for(int ax, int ay, int az, dim3 b) {
+    return dim3((ax + b.x - 1) / b.x, (ay + b.y - 1) / b.y, (az + b.z - 1) / b.z);
+}
+
+// ------------------------------------------------------------------ emitters
+// handle_emitters (shaders3d/compute/handle_emitters.comp:49-76; 2D :47-74) on
+// the bounding box of the active emitters, in place, plus the face-velocity
+// extension.  Emitters are applied in array order, like the shader's loop.
+template <int DIM>
+__global__ void k_emitters(FluidArgs a, const ss_emitter* __restrict__ em, int ne, int lox, int loy, int loz,
+                           int ex, int ey, int ez, float* __restrict__ dens, float* __restrict__ temp,
+                           float* __restrict__ u, float* __restrict__ v, float* __restrict__ w) {
+    int x = lox + blockIdx.x * blockDim.x + threadIdx.x;
+    int y = loy + blockIdx.y * blockDim.y + threadIdx.y;
+    int z = loz + blockIdx.z * blockDim.z + threadIdx.z;
+    if (x >= lox + ex || y >= loy + ey || z >= loz + ez) return;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const float dt = a.c.dt;
+    if (x < nx && y < ny && z < nz) {
+        const int c = idx3(x, y, z, nx, ny);
+        const size_t ncell = (size_t)nx * ny * nz;
+        float sm[3] = {0.f, 0.f, 0.f};
+        for (int ch = 0; ch < a.nch; ++ch) sm[ch] = dens[ch * ncell + c];
+        float t = temp[c];
+        bool hit = false;
+        for (int k = 0; k < ne; ++k) {
+            const ss_emitter& e = em[k];
+            if (!(e.emit > 0)) continue;
+            float dx = (float)x - e.pos[0], dy = (float)y - e.pos[1];
+            float d2 = dx * dx + dy * dy;
+            if constexpr (DIM == 3) { float dz = (float)z - e.pos[2]; d2 = d2 + dz * dz; }
+            float dist = sqrtf(d2);
+            float rad = e.radius;
+            if (dist < rad) {
+                float falloff;
+                if (e.falloff > 0) {
+                    float tt = (dist - rad) / (0.f - rad);
+                    tt = clampt(tt, 0.f, 1.f);
+                    falloff = tt * tt * (3.f - 2.f * tt);
+                } else {
+                    falloff = 1.f;
+                }
+                for (int ch = 0; ch < a.nch; ++ch) sm[ch] = sm[ch] + e.density[ch] * falloff * dt;
+                t = t + e.temperature * falloff * dt;
+                hit = true;
+            }
+        }
+        if (hit) {
+            for (int ch = 0; ch < a.nch; ++ch) dens[ch * ncell + c] = sm[ch];
+            temp[c] = t;
+        }
+    }
+#pragma unroll
+    for (int comp = 0; comp < DIM; ++comp) {
+        int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        float val = 0.f;
+        bool hit = false;
+        for (int k = 0; k < ne; ++k) {
+            const ss_emitter& e = em[k];
+            if (!(e.emit > 0 && e.set_velocity)) continue;
+            float dx = (float)x - e.pos[0], dy = (float)y - e.pos[1];
+            float d2 = dx * dx + dy * dy;
+            if constexpr (DIM == 3) { float dz = (float)z - e.pos[2]; d2 = d2 + dz * dz; }
+            if (sqrtf(d2) < e.radius) { val = e.velocity[comp]; hit = true; }
+        }
+        if (hit) {
+            float* dst = comp == 0 ? u : comp == 1 ? v : w;
+            dst[idx3(x, y, z, ax, ay)] = val;
+        }
+    }
+}
+
+int launch_emitters(ss_sim* s, const StepConsts& c, cudaStream_t st) {
+    // bounding box (cells and faces) of the active emitters
+    int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-1, -1, -1};
+    int active = 0;
+    for (const ss_emitter& e : s->em) {
+        if (!(e.emit > 0)) continue;
+        ++active;
+        for (int d = 0; d < s->dim; ++d) {
+            int a = (int)floorf(e.pos[d] - e.radius) - 1, b = (int)ceilf(e.pos[d] + e.radius) + 2;
+            lo[d] = lo[d] < a ? lo[d] : a;
+            hi[d] = hi[d] > b ? hi[d] : b;
+        }
+    }
+    if (!active) return SS_OK;
+    if (s->dim == 2) { lo[2] = 0; hi[2] = 1; }
+    const int ext[3] = {s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1};
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = lo[d] < 0 ? 0 : lo[d];
+        hi[d] = hi[d] > ext[d] ? ext[d] : hi[d];
+        if (hi[d] <= lo[d]) return SS_OK;
+    }
+    FluidArgs a = fluid_args(s, c);
+    dim3 b(32, 4, 1);
+    dim3 g = grid_for(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], b);
+    float* u = s->vel[0][s->vi[0]];
+    float* v = s->vel[1][s->vi[1]];
+    float* w = s->dim == 3 ? s->vel[2][s->vi[2]] : nullptr;
+    if (s->dim == 3)
+        k_emitters<3><<<g, b, 0, st>>>(a, s->d_em, (int)s->em.size(), lo[0], lo[1], lo[2], hi[0] - lo[0],
+                                       hi[1] - lo[1], hi[2] - lo[2], s->dens[s->si], s->temp[s->si], u, v, w);
+    else
+        k_emitters<2><<<g, b, 0, st>>>(a, s->d_em, (int)s->em.size(), lo[0], lo[1], lo[2], hi[0] - lo[0],
+                                       hi[1] - lo[1], hi[2] - lo[2], s->dens[s->si], s->temp[s->si], u, v, w);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_emitters");
+}
+
+// ------------------------------------------------------- velocity advection
+// advect_vx / advect_vy / advect_vz (shaders3d/compute/advect_vx.comp:54-77,
+// advect_vy.comp:55-79, advect_vz.comp:55-78; 2D advect_vx.comp:50-73,
+// advect_vy.comp:51-75).  With BUOY, apply_buoyancy (apply_buoyancy.comp:39-52)
+// is fused into the y faces: a y face touching solid (out of grid = fluid)
+// keeps the value the reference's write buffer holds there, which after the
+// advection swap is the pre-advection velocity.
+template <int DIM, bool BUOY>
+__global__ void __launch_bounds__(256) k_advect_velocity(FluidArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const float cfl = a.c.cfl;
+#pragma unroll
+    for (int comp = 0; comp < DIM; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        const float* __restrict__ src = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
+        float* __restrict__ dst = comp == 0 ? a.uo : comp == 1 ? a.vo : a.wo;
+        const int i = idx3(x, y, z, ax, ay);
+        const int id = comp == 0 ? x : comp == 1 ? y : z;
+        float out;
+        if (id == 0 && a.c.wind[comp] != 0.f) {
+            out = a.c.wind[comp];
+        } else if (solid_oob1(a.flags, x, y, z, nx, ny, nz) ||
+                   solid_oob1(a.flags, x - (comp == 0), y - (comp == 1), z - (comp == 2), nx, ny, nz)) {
+            out = 0.f;
+        } else {
+            const float gx = (float)x + (comp == 0 ? 0.f : 0.5f);
+            const float gy = (float)y + (comp == 1 ? 0.f : 0.5f);
+            const float gz = DIM == 3 ? (float)z + (comp == 2 ? 0.f : 0.5f) : 0.f;
+            float vel[3];
+            interp_velocity<DIM>(a.u, a.v, a.w, nx, ny, nz, gx, gy, gz, vel);
+            const float bx = gx - vel[0] * cfl, by = gy - vel[1] * cfl, bz = gz - vel[2] * cfl;
+            out = sample_border<DIM>(src, ax, ay, az, bx - (comp == 0 ? 0.f : 0.5f), by - (comp == 1 ? 0.f : 0.5f),
+                                     bz - (comp == 2 ? 0.f : 0.5f), 0.f);
+        }
+        if constexpr (BUOY) {
+            if (comp == 1) {
+                if (solid_oob0(a.flags, x, y, z, nx, ny, nz) || solid_oob0(a.flags, x, y - 1, z, nx, ny, nz)) {
+                    out = __ldg(src + i);
+                } else {
+                    const Taps t = make_taps<DIM>(nx, ny, nz, (float)x, (float)y - 0.5f, (float)z);
+                    const size_t ncell = (size_t)nx * ny * nz;
+                    float total = sample_taps<DIM>(a.dens, nx, ny, nz, t, 0.f);
+                    if (a.nch == 3) {
+                        total = total + sample_taps<DIM>(a.dens + ncell, nx, ny, nz, t, 0.f);
+                        total = total + sample_taps<DIM>(a.dens + 2 * ncell, nx, ny, nz, t, 0.f);
+                    }
+                    const float T = sample_taps<DIM>(a.temp, nx, ny, nz, t, a.c.t_amb);
+                    const float buoy = -a.c.alpha * total + a.c.beta * (T - a.c.t_amb);
+                    out = out + buoy * a.c.dt;
+                }
+            }
+        }
+        dst[i] = out;
+    }
+}
+
+int launch_advect_velocities(ss_sim* s, const StepConsts& c, bool fuse_buoyancy, cudaStream_t st) {
+    FluidArgs a = fluid_args(s, c);
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, b);
+    if (s->dim == 3) {
+        if (fuse_buoyancy) k_advect_velocity<3, true><<<g, b, 0, st>>>(a);
+        else k_advect_velocity<3, false><<<g, b, 0, st>>>(a);
+    } else {
+        if (fuse_buoyancy) k_advect_velocity<2, true><<<g, b, 0, st>>>(a);
+        else k_advect_velocity<2, false><<<g, b, 0, st>>>(a);
+    }
+    for (int d = 0; d < s->dim; ++d) s->vi[d] ^= 1;
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_advect_velocity");
+}
+
+// ----------------------------------------------------------------- buoyancy
+// apply_buoyancy (shaders3d/compute/apply_buoyancy.comp:39-52; 2D :37-50) as a
+// stand-alone stage: faces touching solid are not written.
+template <int DIM>
+__global__ void k_buoyancy(FluidArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    if (x >= nx || y >= ny + 1 || z >= nz) return;
+    if (solid_oob0(a.flags, x, y, z, nx, ny, nz) || solid_oob0(a.flags, x, y - 1, z, nx, ny, nz)) return;
+    const Taps t = make_taps<DIM>(nx, ny, nz, (float)x, (float)y - 0.5f, (float)z);
+    const size_t ncell = (size_t)nx * ny * nz;
+    float total = sample_taps<DIM>(a.dens, nx, ny, nz, t, 0.f);
+    if (a.nch == 3) {
+        total = total + sample_taps<DIM>(a.dens + ncell, nx, ny, nz, t, 0.f);
+        total = total + sample_taps<DIM>(a.dens + 2 * ncell, nx, ny, nz, t, 0.f);
+    }
+    const float T = sample_taps<DIM>(a.temp, nx, ny, nz, t, a.c.t_amb);
+    const float buoy = -a.c.alpha * total + a.c.beta * (T - a.c.t_amb);
+    const int i = idx3(x, y, z, nx, ny + 1);
+    a.vo[i] = a.v[i] + buoy * a.c.dt;
+}
+
+int launch_buoyancy(ss_sim* s, const StepConsts& c, cudaStream_t st) {
+    FluidArgs a = fluid_args(s, c);
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for(s->nx, s->ny + 1, s->nz, b);
+    if (s->dim == 3) k_buoyancy<3><<<g, b, 0, st>>>(a);
+    else k_buoyancy<2><<<g, b, 0, st>>>(a);
+    s->vi[1] ^= 1;
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_buoyancy");
+}
+
+// ---------------------------------------------------------------- vorticity
+// calculate_vorticity (shaders3d/compute/calculate_vorticity.comp:59-84; 2D
+// :51-69).  Velocity fetches outside the face arrays read 0.
+template <int DIM>
+__global__ void k_vorticity(FluidArgs a, float* __restrict__ vort) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    if (x >= nx || y >= ny || z >= nz) return;
+    const int c = idx3(x, y, z, nx, ny);
+    const size_t ncell = (size_t)nx * ny * nz;
+    const float two_h = 2.f * a.c.vort_k;
+    if (a.flags[c] & F_SOLID) {
+        vort[c] = 0.f;
+        if constexpr (DIM == 3) { vort[ncell + c] = 0.f; vort[2 * ncell + c] = 0.f; }
+        return;
+    }
+    const float* u = a.u;
+    const float* v = a.v;
+    const float* w = a.w;
+#define CCX(X, Y, Z) ((fetch_b(u, nx + 1, ny, nz, X, Y, Z, 0.f) + fetch_b(u, nx + 1, ny, nz, (X) + 1, Y, Z, 0.f)) * 0.5f)
+#define CCY(X, Y, Z) ((fetch_b(v, nx, ny + 1, nz, X, Y, Z, 0.f) + fetch_b(v, nx, ny + 1, nz, X, (Y) + 1, Z, 0.f)) * 0.5f)
+#define CCZ(X, Y, Z) ((fetch_b(w, nx, ny, nz + 1, X, Y, Z, 0.f) + fetch_b(w, nx, ny, nz + 1, X, Y, (Z) + 1, 0.f)) * 0.5f)
+    if constexpr (DIM == 2) {
+        const float z1 = CCY(x + 1, y, 0) - CCY(x - 1, y, 0);
+        const float z2 = CCX(x, y + 1, 0) - CCX(x, y - 1, 0);
+        vort[c] = (z1 - z2) / two_h;
+    } else {
+        const float x1 = CCZ(x, y + 1, z) - CCZ(x, y - 1, z);
+        const float x2 = CCY(x, y, z + 1) - CCY(x, y, z - 1);
+        const float y1 = CCX(x, y, z + 1) - CCX(x, y, z - 1);
+        const float y2 = CCZ(x + 1, y, z) - CCZ(x - 1, y, z);
+        const float z1 = CCY(x + 1, y, z) - CCY(x - 1, y, z);
+        const float z2 = CCX(x, y + 1, z) - CCX(x, y - 1, z);
+        vort[c] = (x1 - x2) / two_h;
+        vort[ncell + c] = (y1 - y2) / two_h;
+        vort[2 * ncell + c] = (z1 - z2) / two_h;
+    }
+#undef CCX
+#undef CCY
+#undef CCZ
+}
+
+template <int DIM>
+SS_D float vmag(const float* __restrict__ vort, int x, int y, int z, int nx, int ny, int nz) {
+    if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return 0.f;
+    const int c = idx3(x, y, z, nx, ny);
+    if constexpr (DIM == 2) {
+        return fabsf(__ldg(vort + c));
+    } else {
+        const size_t n = (size_t)nx * ny * nz;
+        const float o0 = __ldg(vort + c), o1 = __ldg(vort + n + c), o2 = __ldg(vort + 2 * n + c);
+        return sqrtf(o0 * o0 + o1 * o1 + o2 * o2);
+    }
+}
+
+// apply_vorticity_x/y/z (shaders3d/compute/apply_vorticity_x.comp:43-63 and
+// siblings; 2D apply_vorticity_x.comp:41-60, apply_vorticity_y.comp:41-60).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_apply_vorticity(FluidArgs a, const float* __restrict__ vort) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const float two_h = 2.f * a.c.vort_k, eps = 1e-20f;
+    const size_t ncell = (size_t)nx * ny * nz;
+    // the force of cell (x,y,z) is shared by its three faces of the same index
+    float f[3] = {0.f, 0.f, 0.f};
+    bool have = false;
+#pragma unroll
+    for (int comp = 0; comp < DIM; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        if (!have) {
+            const float dx = vmag<DIM>(vort, x + 1, y, z, nx, ny, nz) - vmag<DIM>(vort, x - 1, y, z, nx, ny, nz);
+            const float dy = vmag<DIM>(vort, x, y + 1, z, nx, ny, nz) - vmag<DIM>(vort, x, y - 1, z, nx, ny, nz);
+            const bool in = x < nx && y < ny && z < nz;
+            const int c = in ? idx3(x, y, z, nx, ny) : 0;
+            if constexpr (DIM == 3) {
+                const float dz = vmag<DIM>(vort, x, y, z + 1, nx, ny, nz) - vmag<DIM>(vort, x, y, z - 1, nx, ny, nz);
+                const float gx = dx / two_h, gy = dy / two_h, gz = dz / two_h;
+                const float len = sqrtf(gx * gx + gy * gy + gz * gz) + eps;
+                const float nxv = gx / len, nyv = gy / len, nzv = gz / len;
+                const float o0 = in ? __ldg(vort + c) : 0.f;
+                const float o1 = in ? __ldg(vort + ncell + c) : 0.f;
+                const float o2 = in ? __ldg(vort + 2 * ncell + c) : 0.f;
+                f[0] = nyv * o2 - o1 * nzv;
+                f[1] = nzv * o0 - o2 * nxv;
+                f[2] = nxv * o1 - o0 * nyv;
+            } else {
+                const float gx = dx / two_h, gy = dy / two_h;
+                const float len = sqrtf(gx * gx + gy * gy) + eps;
+                const float nxv = gx / len, nyv = gy / len;
+                const float o0 = in ? __ldg(vort + c) : 0.f;
+                f[0] = -nyv * o0;
+                f[1] = -nxv * o0;
+            }
+            have = true;
+        }
+        const float* __restrict__ src = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
+        float* __restrict__ dst = comp == 0 ? a.uo : comp == 1 ? a.vo : a.wo;
+        const int i = idx3(x, y, z, ax, ay);
+        dst[i] = __ldg(src + i) + (f[comp] * 0.5f * a.c.eps * a.c.vort_k * a.c.dt) / a.c.rho;
+    }
+}
+
+int launch_vorticity(ss_sim* s, const StepConsts& c, cudaStream_t st) {
+    FluidArgs a = fluid_args(s, c);
+    a.c.vort_k = s->h;
+    dim3 b(32, 8, 1);
+    dim3 gc = grid_for(s->nx, s->ny, s->nz, b);
+    dim3 gf = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, b);
+    if (s->dim == 3) {
+        k_vorticity<3><<<gc, b, 0, st>>>(a, s->vort);
+        k_apply_vorticity<3><<<gf, b, 0, st>>>(a, s->vort);
+    } else {
+        k_vorticity<2><<<gc, b, 0, st>>>(a, s->vort);
+        k_apply_vorticity<2><<<gf, b, 0, st>>>(a, s->vort);
+    }
+    for (int d = 0; d < s->dim; ++d) s->vi[d] ^= 1;
+    s->nlaunch += 2;
+    return check_cuda(cudaGetLastError(), "k_vorticity");
+}
+
+// -------------------------------------------------------- projection update
+// update_vx/vy/vz (shaders3d/compute/update_vx.comp:45-62 and siblings; 2D
+// :43-60): faces touching solid (out of grid = fluid) take the solid map's
+// velocity of cell idx (0 outside the grid).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const float* __restrict__ p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const bool in = x < nx && y < ny && z < nz;
+    const float pc = in ? __ldg(p + idx3(x, y, z, nx, ny)) : 0.f;
+    const bool sc = in && (a.flags[idx3(x, y, z, nx, ny)] & F_SOLID);
+#pragma unroll
+    for (int comp = 0; comp < DIM; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        const int xm = x - (comp == 0), ym = y - (comp == 1), zm = z - (comp == 2);
+        const float* __restrict__ src = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
+        float* __restrict__ dst = comp == 0 ? a.uo : comp == 1 ? a.vo : a.wo;
+        const int i = idx3(x, y, z, ax, ay);
+        if (sc || solid_oob0(a.flags, xm, ym, zm, nx, ny, nz)) {
+            const float* sv = comp == 0 ? a.sv0 : comp == 1 ? a.sv1 : a.sv2;
+            dst[i] = (in && sv) ? sv[idx3(x, y, z, nx, ny)] : 0.f;
+            continue;
+        }
+        const float plo = (xm < 0 || ym < 0 || zm < 0) ? 0.f : __ldg(p + idx3(xm, ym, zm, nx, ny));
+        dst[i] = __ldg(src + i) + a.c.k_upd * (pc - plo);
+    }
+}
+
+int launch_update_velocities(ss_sim* s, const StepConsts& c, cudaStream_t st) {
+    FluidArgs a = fluid_args(s, c);
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, b);
+    if (s->dim == 3) k_update_velocity<3><<<g, b, 0, st>>>(a, s->p[0]);
+    else k_update_velocity<2><<<g, b, 0, st>>>(a, s->p[0]);
+    for (int d = 0; d < s->dim; ++d) s->vi[d] ^= 1;
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_update_velocity");
+}
+
+// ------------------------------------------------------------ smoke advection
+// advect_smoke (shaders3d/compute/advect_smoke.comp:55-72; 2D :51-68).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    if (x >= nx || y >= ny || z >= nz) return;
+    const int c = idx3(x, y, z, nx, ny);
+    const size_t ncell = (size_t)nx * ny * nz;
+    if (a.flags[c] & F_SOLID) {
+        for (int ch = 0; ch < a.nch; ++ch) a.dens_o[ch * ncell + c] = 0.f;
+        a.temp_o[c] = a.c.t_amb;
+        return;
+    }
+    const float gx = (float)x + 0.5f, gy = (float)y + 0.5f, gz = DIM == 3 ? (float)z + 0.5f : 0.f;
+    float vel[3];
+    interp_velocity<DIM>(a.u, a.v, a.w, nx, ny, nz, gx, gy, gz, vel);
+    const float cfl = a.c.cfl;
+    const float bx = gx - vel[0] * cfl, by = gy - vel[1] * cfl, bz = gz - vel[2] * cfl;
+    const Taps t = make_taps<DIM>(nx, ny, nz, bx - 0.5f, by - 0.5f, bz - 0.5f);
+    for (int ch = 0; ch < a.nch; ++ch) a.dens_o[ch * ncell + c] = sample_taps<DIM>(a.dens + ch * ncell, nx, ny, nz, t, 0.f);
+    a.temp_o[c] = sample_taps<DIM>(a.temp, nx, ny, nz, t, a.c.t_amb);
+}
+
+int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st) {
+    FluidArgs a = fluid_args(s, c);
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for(s->nx, s->ny, s->nz, b);
+    if (s->dim == 3) k_advect_smoke<3><<<g, b, 0, st>>>(a);
+    else k_advect_smoke<2><<<g, b, 0, st>>>(a);
+    s->si ^= 1;
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_advect_smoke");
+}
+
+// ---------------------------------------------------------------- divergence
+// Level-0 divergence with solid-velocity substitution, the delta_v of
+// smooth.comp:105-113 (out of grid = fluid) and, for open domains, of
+// compute_residual.comp:116-124 (out of grid = solid, velocity 0).  Optional
+// FP64 sum of squares over fluid cells into per-block partials.
+SS_D double block_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __shared__ double warp_part[32];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    if ((tid & 31) == 0) warp_part[tid >> 5] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (tid < 32) {
+        r = tid < (nthreads + 31) / 32 ? warp_part[tid] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    return r;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restrict__ div0, float* __restrict__ div0r,
+                                                    double* __restrict__ partial) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    double acc = 0.0;
+    if (x < nx && y < ny && z < nz) {
+        const int c = idx3(x, y, z, nx, ny);
+        const uint8_t fl = a.flags[c];
+        if (!(fl & F_SOLID)) {
+            const bool sv = a.sv0 != nullptr;
+            const float v_top = (fl & F_TOP) ? (sv ? a.sv1[c + nx] : 0.f) : __ldg(a.v + idx3(x, y + 1, z, nx, ny + 1));
+            const float v_bottom = (fl & F_BOTTOM) ? (sv ? a.sv1[c - nx] : 0.f) : __ldg(a.v + idx3(x, y, z, nx, ny + 1));
+            const float v_right = (fl & F_RIGHT) ? (sv ? a.sv0[c + 1] : 0.f) : __ldg(a.u + idx3(x + 1, y, z, nx + 1, ny));
+            const float v_left = (fl & F_LEFT) ? (sv ? a.sv0[c - 1] : 0.f) : __ldg(a.u + idx3(x, y, z, nx + 1, ny));
+            float d = v_right - v_left + v_top - v_bottom;
+            float v_front = 0.f, v_back = 0.f;
+            if constexpr (DIM == 3) {
+                const int pl = nx * ny;
+                v_front = (fl & F_FRONT) ? (sv ? a.sv2[c + pl] : 0.f) : __ldg(a.w + idx3(x, y, z + 1, nx, ny));
+                v_back = (fl & F_BACK) ? (sv ? a.sv2[c - pl] : 0.f) : __ldg(a.w + idx3(x, y, z, nx, ny));
+                d = d + v_front - v_back;
+            }
+            if (div0) div0[c] = d;
+            if (div0r) {
+                // residual rule: out-of-grid neighbours are solid with velocity 0
+                const float rt = y + 1 >= ny ? 0.f : v_top, rb = y == 0 ? 0.f : v_bottom;
+                const float rr = x + 1 >= nx ? 0.f : v_right, rl = x == 0 ? 0.f : v_left;
+                float dr = rr - rl + rt - rb;
+                if constexpr (DIM == 3) {
+                    const float rf = z + 1 >= nz ? 0.f : v_front, rk = z == 0 ? 0.f : v_back;
+                    dr = dr + rf - rk;
+                }
+                div0r[c] = dr;
+            }
+            acc = (double)d * (double)d;
+        }
+    }
+    if (partial) {
+        const double bs = block_sum(acc);
+        if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0)
+            partial[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = bs;
+    }
+}
+
+int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st) {
+    StepConsts c{};
+    FluidArgs a = fluid_args(s, c);
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for(s->nx, s->ny, s->nz, b);
+    const int nblocks = (int)(g.x * g.y * g.z);
+    float* d0 = write ? s->div0 : nullptr;
+    float* d0r = (write && s->div0r != s->div0) ? s->div0r : nullptr;
+    double* part = slot >= 0 ? s->red.partial : nullptr;
+    if (s->dim == 3) k_divergence<3><<<g, b, 0, st>>>(a, d0, d0r, part);
+    else k_divergence<2><<<g, b, 0, st>>>(a, d0, d0r, part);
+    s->nlaunch += 1;
+    int rc = check_cuda(cudaGetLastError(), "k_divergence");
+    if (rc || slot < 0) return rc;
+    return launch_reduce_final(s, nblocks, slot, st);
+}
+
+// Fixed-order final sum of the per-block partials (deterministic).
+__global__ void k_reduce_final(const double* __restrict__ partial, int n, double* __restrict__ out, int slot) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+    __shared__ double sh[1024];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[slot] = sh[0];
+}
+
+int launch_reduce_final(ss_sim* s, int nblocks, int slot, cudaStream_t st) {
+    k_reduce_final<<<1, 1024, 0, st>>>(s->red.partial, nblocks, s->red.out, slot);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_reduce_final");
+}
+
+}  // namespace ss

@@ -1,0 +1,464 @@
+// k_mg.cu - multigrid pressure projection kernels.
+//
+// Reference: the recursive V-cycle of common/physics/grid.c:173-266 over the
+// pressure / residual / solid pyramid of 3d/grid3d.c:45-68, with the shaders
+// of shaders{2,3}d/compute/pressure_solve/.  Level 0 reads the solid map as a
+// flag byte and its right-hand side from the precomputed divergence (the
+// reference recomputes it from the velocities in every sweep); coarse levels
+// read the FP16-rounded solid fraction alpha (the reference stores the solid
+// pyramid as RGBA16F images).
+#include "common.cuh"
+#include "ss_internal.h"
+
+namespace ss {
+
+struct MGArgs {
+    float* __restrict__ p;
+    float* __restrict__ r;          // level right-hand side / residual (L >= 1)
+    const float* __restrict__ alpha;  // L >= 1
+    const uint8_t* __restrict__ flags;  // L == 0
+    const float* __restrict__ div0;   // L == 0, smoother rule
+    const float* __restrict__ div0r;  // L == 0, residual rule
+    int nx, ny, nz;
+    float oobA;     // solid fraction read for out-of-grid neighbours (0 = open, 1 = wall)
+    float hh;       // h_L^2
+    float rho_h;    // rho * h   (L == 0 smoother)
+    float dt;
+    float rho;
+    float dt_h;     // dt * h    (L == 0 residual)
+};
+
+// Out-of-grid rule: ref_quirks keeps the reference's smoother (open, p = 0) /
+// residual (wall) mismatch; the corrected mode uses the physical rule of the
+// grid (wall when enclosed, open otherwise) in both operators.
+static float smooth_oob(const ss_sim* s, int quirks) { return quirks ? 0.f : (s->enclosed ? 1.f : 0.f); }
+static float resid_oob(const ss_sim* s, int quirks) { return quirks ? 1.f : (s->enclosed ? 1.f : 0.f); }
+
+static MGArgs mg_args(ss_sim* s, const StepConsts& c, int L, float oobA) {
+    MGArgs a;
+    a.oobA = oobA;
+    a.p = s->p[L];
+    a.r = s->r[L];
+    a.alpha = L > 0 ? s->alpha[L] : nullptr;
+    a.flags = s->flags;
+    a.div0 = oobA != 0.f ? s->div0r : s->div0;   // level-0 right-hand side under the chosen rule
+    a.div0r = a.div0;
+    a.nx = s->lv[L].n[0]; a.ny = s->lv[L].n[1]; a.nz = s->lv[L].n[2];
+    a.hh = s->lv[L].hh;
+    a.rho_h = c.rho_h;
+    a.dt = c.dt;
+    a.rho = c.rho;
+    a.dt_h = c.dt_h;
+    return a;
+}
+
+// ------------------------------------------------------------------ smoother
+// smooth.comp:79-136 (2D :74-123): red-black Gauss-Seidel in place; solid
+// cells and cells without fluid neighbours are skipped; out of grid = fluid
+// with p = 0.
+template <int DIM, bool L0>
+SS_D void smooth_cell(const MGArgs& a, int x, int y, int z) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int c = idx3(x, y, z, nx, ny);
+    float f_top, f_bottom, f_right, f_left, f_front = 0.f, f_back = 0.f;
+    if constexpr (L0) {
+        const uint8_t fl = a.flags[c];
+        if (fl & F_SOLID) return;
+        const float fo = 1.f - a.oobA;
+        f_top = (fl & F_TOP) ? 0.f : (y + 1 < ny ? 1.f : fo);
+        f_bottom = (fl & F_BOTTOM) ? 0.f : (y > 0 ? 1.f : fo);
+        f_right = (fl & F_RIGHT) ? 0.f : (x + 1 < nx ? 1.f : fo);
+        f_left = (fl & F_LEFT) ? 0.f : (x > 0 ? 1.f : fo);
+        if constexpr (DIM == 3) {
+            f_front = (fl & F_FRONT) ? 0.f : (z + 1 < nz ? 1.f : fo);
+            f_back = (fl & F_BACK) ? 0.f : (z > 0 ? 1.f : fo);
+        }
+    } else {
+        if (a.alpha[c] >= 1.f) return;
+        f_top = 1.f - (y + 1 < ny ? a.alpha[c + nx] : a.oobA);
+        f_bottom = 1.f - (y > 0 ? a.alpha[c - nx] : a.oobA);
+        f_right = 1.f - (x + 1 < nx ? a.alpha[c + 1] : a.oobA);
+        f_left = 1.f - (x > 0 ? a.alpha[c - 1] : a.oobA);
+        if constexpr (DIM == 3) {
+            f_front = 1.f - (z + 1 < nz ? a.alpha[c + nx * ny] : a.oobA);
+            f_back = 1.f - (z > 0 ? a.alpha[c - nx * ny] : a.oobA);
+        }
+    }
+    float f_sum = f_top + f_bottom + f_right + f_left;
+    if constexpr (DIM == 3) f_sum = f_sum + f_front + f_back;
+    if (f_sum == 0.f) return;
+    const float* P = a.p;
+    const float p_top = y + 1 < ny ? P[c + nx] : 0.f;
+    const float p_bottom = y > 0 ? P[c - nx] : 0.f;
+    const float p_right = x + 1 < nx ? P[c + 1] : 0.f;
+    const float p_left = x > 0 ? P[c - 1] : 0.f;
+    float p_sum = p_top * f_top + p_bottom * f_bottom;
+    p_sum = p_sum + p_right * f_right;
+    p_sum = p_sum + p_left * f_left;
+    if constexpr (DIM == 3) {
+        const float p_front = z + 1 < nz ? P[c + nx * ny] : 0.f;
+        const float p_back = z > 0 ? P[c - nx * ny] : 0.f;
+        p_sum = p_sum + p_front * f_front;
+        p_sum = p_sum + p_back * f_back;
+    }
+    float pn;
+    if constexpr (L0) pn = (p_sum - a.rho_h * a.div0[c] / a.dt) / f_sum;
+    else pn = (p_sum - a.r[c] * a.hh) / f_sum;
+    a.p[c] = pn;
+}
+
+template <int DIM, bool L0>
+__global__ void __launch_bounds__(256) k_smooth(MGArgs a, int parity) {
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((y + z + parity) & 1);
+    if (x >= a.nx || y >= a.ny || z >= a.nz) return;
+    smooth_cell<DIM, L0>(a, x, y, z);
+}
+
+static inline dim3 grid_for(int ax, int ay, int az, dim3 b) {
+    return dim3((ax + b.x - 1) / b.x, (ay + b.y - 1) / b.y, (az + b.z - 1) / b.z);
+}
+
+int launch_smooth(ss_sim* s, const StepConsts& c, int L, int iterations, int quirks, cudaStream_t st) {
+    MGArgs a = mg_args(s, c, L, smooth_oob(s, quirks));
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for((a.nx + 1) / 2, a.ny, a.nz, b);
+    for (int it = 0; it < 2 * iterations; ++it) {
+        const int parity = it & 1;
+        if (s->dim == 3) {
+            if (L == 0) k_smooth<3, true><<<g, b, 0, st>>>(a, parity);
+            else k_smooth<3, false><<<g, b, 0, st>>>(a, parity);
+        } else {
+            if (L == 0) k_smooth<2, true><<<g, b, 0, st>>>(a, parity);
+            else k_smooth<2, false><<<g, b, 0, st>>>(a, parity);
+        }
+    }
+    s->nlaunch += 2 * iterations;
+    return check_cuda(cudaGetLastError(), "k_smooth");
+}
+
+// ------------------------------------------------------------------ residual
+// compute_residual.comp:77-130 (2D :72-117): r = b - (sum_f p_nb - f_sum p)/h^2,
+// out of grid = solid; level 0 takes b = rho*div/(dt*h).
+template <int DIM, bool L0>
+SS_D float residual_cell(const MGArgs& a, int x, int y, int z) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int c = idx3(x, y, z, nx, ny);
+    float f_top, f_bottom, f_right, f_left, f_front = 0.f, f_back = 0.f;
+    if constexpr (L0) {
+        const uint8_t fl = a.flags[c];
+        if (fl & F_SOLID) return 0.f;
+        const float fo = 1.f - a.oobA;
+        f_top = (fl & F_TOP) ? 0.f : (y + 1 < ny ? 1.f : fo);
+        f_bottom = (fl & F_BOTTOM) ? 0.f : (y > 0 ? 1.f : fo);
+        f_right = (fl & F_RIGHT) ? 0.f : (x + 1 < nx ? 1.f : fo);
+        f_left = (fl & F_LEFT) ? 0.f : (x > 0 ? 1.f : fo);
+        if constexpr (DIM == 3) {
+            f_front = (fl & F_FRONT) ? 0.f : (z + 1 < nz ? 1.f : fo);
+            f_back = (fl & F_BACK) ? 0.f : (z > 0 ? 1.f : fo);
+        }
+    } else {
+        if (a.alpha[c] >= 1.f) return 0.f;
+        f_top = 1.f - (y + 1 < ny ? a.alpha[c + nx] : a.oobA);
+        f_bottom = 1.f - (y > 0 ? a.alpha[c - nx] : a.oobA);
+        f_right = 1.f - (x + 1 < nx ? a.alpha[c + 1] : a.oobA);
+        f_left = 1.f - (x > 0 ? a.alpha[c - 1] : a.oobA);
+        if constexpr (DIM == 3) {
+            f_front = 1.f - (z + 1 < nz ? a.alpha[c + nx * ny] : a.oobA);
+            f_back = 1.f - (z > 0 ? a.alpha[c - nx * ny] : a.oobA);
+        }
+    }
+    const float* P = a.p;
+    const float p_top = y + 1 < ny ? P[c + nx] : 0.f;
+    const float p_bottom = y > 0 ? P[c - nx] : 0.f;
+    const float p_right = x + 1 < nx ? P[c + 1] : 0.f;
+    const float p_left = x > 0 ? P[c - 1] : 0.f;
+    float p_sum = p_top * f_top + p_bottom * f_bottom;
+    p_sum = p_sum + p_right * f_right;
+    p_sum = p_sum + p_left * f_left;
+    float f_sum = f_top + f_bottom + f_right + f_left;
+    if constexpr (DIM == 3) {
+        const float p_front = z + 1 < nz ? P[c + nx * ny] : 0.f;
+        const float p_back = z > 0 ? P[c - nx * ny] : 0.f;
+        p_sum = p_sum + p_front * f_front;
+        p_sum = p_sum + p_back * f_back;
+        f_sum = f_sum + f_front + f_back;
+    }
+    float old;
+    if constexpr (L0) old = a.rho * a.div0r[c] / a.dt_h;
+    else old = a.r[c];
+    return old - (p_sum - f_sum * P[c]) / a.hh;
+}
+
+// One thread per coarse cell: residual of its 2^DIM children (written in place
+// when WRITE_FINE, the reference's in-place residual), then restrict_residual
+// (restrict_residual.comp:40-64, 2D :40-59) into the next level when
+// WRITE_COARSE.  The grid also covers the fine cells left over by odd sizes.
+template <int DIM, bool L0, bool WRITE_FINE, bool WRITE_COARSE>
+__global__ void __launch_bounds__(256) k_residual_restrict(MGArgs a, float* __restrict__ rc, int cx, int cy, int cz) {
+    const int X = blockIdx.x * blockDim.x + threadIdx.x;
+    const int Y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int Z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int x0 = 2 * X, y0 = 2 * Y, z0 = DIM == 3 ? 2 * Z : 0;
+    if (x0 >= nx || y0 >= ny || z0 >= nz) return;
+    float v[2][2][2];  // [dz][dy][dx]
+#pragma unroll
+    for (int dz = 0; dz < (DIM == 3 ? 2 : 1); ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) {
+                const int x = x0 + dx, y = y0 + dy, z = z0 + dz;
+                float res = 0.f;
+                if (x < nx && y < ny && z < nz) {
+                    res = residual_cell<DIM, L0>(a, x, y, z);
+                    if constexpr (WRITE_FINE) a.r[idx3(x, y, z, nx, ny)] = res;
+                }
+                v[dz][dy][dx] = res;
+            }
+    if constexpr (WRITE_COARSE) {
+        if (X < cx && Y < cy && Z < cz) {
+            float out;
+            if constexpr (DIM == 3) {
+                const float bottom = v[0][0][0] + v[1][0][0] + v[0][0][1] + v[1][0][1];
+                const float top = v[0][1][0] + v[1][1][0] + v[0][1][1] + v[1][1][1];
+                out = (bottom + top) / 8.f;
+            } else {
+                out = (v[0][0][0] + v[0][0][1] + v[0][1][0] + v[0][1][1]) / 4.f;
+            }
+            rc[idx3(X, Y, Z, cx, cy)] = out;
+        }
+    }
+}
+
+template <int DIM, bool L0>
+static void launch_rr(const MGArgs& a, float* rc, int cx, int cy, int cz, bool wf, bool wc, dim3 g, dim3 b,
+                      cudaStream_t st) {
+    if (wf && wc) k_residual_restrict<DIM, L0, true, true><<<g, b, 0, st>>>(a, rc, cx, cy, cz);
+    else if (wf) k_residual_restrict<DIM, L0, true, false><<<g, b, 0, st>>>(a, rc, cx, cy, cz);
+    else k_residual_restrict<DIM, L0, false, true><<<g, b, 0, st>>>(a, rc, cx, cy, cz);
+}
+
+int launch_residual(ss_sim* s, const StepConsts& c, int L, bool write_fine, bool write_coarse, int quirks,
+                    cudaStream_t st) {
+    if (!write_fine && !write_coarse) return SS_OK;
+    if (write_coarse && L + 1 >= s->levels) return set_error(SS_E_INVALID, "residual restriction below the coarsest level");
+    MGArgs a = mg_args(s, c, L, resid_oob(s, quirks));
+    const int cx = write_coarse ? s->lv[L + 1].n[0] : 0;
+    const int cy = write_coarse ? s->lv[L + 1].n[1] : 0;
+    const int cz = write_coarse ? s->lv[L + 1].n[2] : 0;
+    float* rc = write_coarse ? s->r[L + 1] : nullptr;
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for((a.nx + 1) / 2, (a.ny + 1) / 2, s->dim == 3 ? (a.nz + 1) / 2 : 1, b);
+    if (s->dim == 3) {
+        if (L == 0) launch_rr<3, true>(a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
+        else launch_rr<3, false>(a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
+    } else {
+        if (L == 0) launch_rr<2, true>(a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
+        else launch_rr<2, false>(a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
+    }
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_residual_restrict");
+}
+
+// restrict_residual alone (reads the in-place residual of level L)
+template <int DIM>
+__global__ void k_restrict(const float* __restrict__ rf, int fx, int fy, float* __restrict__ rc, int cx, int cy, int cz) {
+    const int X = blockIdx.x * blockDim.x + threadIdx.x;
+    const int Y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int Z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (X >= cx || Y >= cy || Z >= cz) return;
+    const int x = 2 * X, y = 2 * Y, z = 2 * Z;
+    float out;
+    if constexpr (DIM == 3) {
+        const float bottom = rf[idx3(x, y, z, fx, fy)] + rf[idx3(x, y, z + 1, fx, fy)] + rf[idx3(x + 1, y, z, fx, fy)] +
+                             rf[idx3(x + 1, y, z + 1, fx, fy)];
+        const float top = rf[idx3(x, y + 1, z, fx, fy)] + rf[idx3(x, y + 1, z + 1, fx, fy)] +
+                          rf[idx3(x + 1, y + 1, z, fx, fy)] + rf[idx3(x + 1, y + 1, z + 1, fx, fy)];
+        out = (bottom + top) / 8.f;
+    } else {
+        out = (rf[idx3(x, y, 0, fx, fy)] + rf[idx3(x + 1, y, 0, fx, fy)] + rf[idx3(x, y + 1, 0, fx, fy)] +
+               rf[idx3(x + 1, y + 1, 0, fx, fy)]) / 4.f;
+    }
+    rc[idx3(X, Y, Z, cx, cy)] = out;
+}
+
+int launch_restrict(ss_sim* s, int L, cudaStream_t st) {
+    if (L + 1 >= s->levels) return set_error(SS_E_INVALID, "restriction below the coarsest level");
+    const int* f = s->lv[L].n;
+    const int* cc = s->lv[L + 1].n;
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for(cc[0], cc[1], cc[2], b);
+    if (s->dim == 3) k_restrict<3><<<g, b, 0, st>>>(s->r[L], f[0], f[1], s->r[L + 1], cc[0], cc[1], cc[2]);
+    else k_restrict<2><<<g, b, 0, st>>>(s->r[L], f[0], f[1], s->r[L + 1], cc[0], cc[1], cc[2]);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_restrict");
+}
+
+// --------------------------------------------------------------- prolongation
+// prolong_pressure.comp:39-51: p_L += GL_LINEAR, CLAMP_TO_EDGE sample of
+// p_{L+1} at the fine cell centre, on every cell.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_prolong(float* __restrict__ p, int ax, int ay, int az,
+                                                 const float* __restrict__ pc, int cx, int cy, int cz) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (x >= ax || y >= ay || z >= az) return;
+    const float tx = (((float)x + 0.5f) / (float)ax) * (float)cx - 0.5f;
+    const float ty = (((float)y + 0.5f) / (float)ay) * (float)cy - 0.5f;
+    const float fx = floorf(tx), fy = floorf(ty);
+    const int x0 = (int)fx, y0 = (int)fy;
+    const float wx = tx - fx, wy = ty - fy;
+    const int xa = min(max(x0, 0), cx - 1), xb = min(max(x0 + 1, 0), cx - 1);
+    const int ya = min(max(y0, 0), cy - 1), yb = min(max(y0 + 1, 0), cy - 1);
+    float s;
+    if constexpr (DIM == 2) {
+        s = lerp_(lerp_(__ldg(pc + idx3(xa, ya, 0, cx, cy)), __ldg(pc + idx3(xb, ya, 0, cx, cy)), wx),
+                  lerp_(__ldg(pc + idx3(xa, yb, 0, cx, cy)), __ldg(pc + idx3(xb, yb, 0, cx, cy)), wx), wy);
+    } else {
+        const float tz = (((float)z + 0.5f) / (float)az) * (float)cz - 0.5f;
+        const float fz = floorf(tz);
+        const int z0 = (int)fz;
+        const float wz = tz - fz;
+        const int za = min(max(z0, 0), cz - 1), zb = min(max(z0 + 1, 0), cz - 1);
+        const float c0 = lerp_(lerp_(__ldg(pc + idx3(xa, ya, za, cx, cy)), __ldg(pc + idx3(xb, ya, za, cx, cy)), wx),
+                               lerp_(__ldg(pc + idx3(xa, yb, za, cx, cy)), __ldg(pc + idx3(xb, yb, za, cx, cy)), wx), wy);
+        const float c1 = lerp_(lerp_(__ldg(pc + idx3(xa, ya, zb, cx, cy)), __ldg(pc + idx3(xb, ya, zb, cx, cy)), wx),
+                               lerp_(__ldg(pc + idx3(xa, yb, zb, cx, cy)), __ldg(pc + idx3(xb, yb, zb, cx, cy)), wx), wy);
+        s = lerp_(c0, c1, wz);
+    }
+    const int i = idx3(x, y, z, ax, ay);
+    p[i] = p[i] + s;
+}
+
+int launch_prolong(ss_sim* s, int L, cudaStream_t st) {
+    const int next = L + 1 < s->levels ? L + 1 : s->levels - 1;
+    const int* f = s->lv[L].n;
+    const int* cc = s->lv[next].n;
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for(f[0], f[1], f[2], b);
+    if (s->dim == 3) k_prolong<3><<<g, b, 0, st>>>(s->p[L], f[0], f[1], f[2], s->p[next], cc[0], cc[1], cc[2]);
+    else k_prolong<2><<<g, b, 0, st>>>(s->p[L], f[0], f[1], f[2], s->p[next], cc[0], cc[1], cc[2]);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_prolong");
+}
+
+// -------------------------------------------------------------- solid pyramid
+// restrict_solid.comp:53-78 (2D :53-73): mean of the children, zeroed below
+// 0.5, stored as FP16.  Only the alpha channel feeds the coarse operators.
+template <int DIM, bool FROM_FLAGS>
+__global__ void k_restrict_alpha(const uint8_t* __restrict__ flags, const float* __restrict__ af, int fx, int fy,
+                                 float* __restrict__ ac, int cx, int cy, int cz) {
+    const int X = blockIdx.x * blockDim.x + threadIdx.x;
+    const int Y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int Z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (X >= cx || Y >= cy || Z >= cz) return;
+    const int x = 2 * X, y = 2 * Y, z = 2 * Z;
+    auto A = [&](int i, int j, int k) -> float {
+        const int q = idx3(i, j, k, fx, fy);
+        if constexpr (FROM_FLAGS) return (flags[q] & F_SOLID) ? 1.f : 0.f;
+        else return af[q];
+    };
+    float m;
+    if constexpr (DIM == 3) {
+        const float b = A(x, y, z) + A(x, y, z + 1) + A(x + 1, y, z) + A(x + 1, y, z + 1);
+        const float t = A(x, y + 1, z) + A(x, y + 1, z + 1) + A(x + 1, y + 1, z) + A(x + 1, y + 1, z + 1);
+        m = (b + t) / 8.f;
+    } else {
+        m = (A(x, y, 0) + A(x + 1, y, 0) + A(x, y + 1, 0) + A(x + 1, y + 1, 0)) / 4.f;
+    }
+    const float keep = m >= 0.5f ? 1.f : 0.f;
+    ac[idx3(X, Y, Z, cx, cy)] = round_half(m * keep);
+}
+
+int launch_solid_pyramid(ss_sim* s, cudaStream_t st) {
+    dim3 b(32, 8, 1);
+    for (int L = 0; L + 1 < s->levels; ++L) {
+        const int* f = s->lv[L].n;
+        const int* cc = s->lv[L + 1].n;
+        dim3 g = grid_for(cc[0], cc[1], cc[2], b);
+        if (s->dim == 3) {
+            if (L == 0) k_restrict_alpha<3, true><<<g, b, 0, st>>>(s->flags, nullptr, f[0], f[1], s->alpha[1], cc[0], cc[1], cc[2]);
+            else k_restrict_alpha<3, false><<<g, b, 0, st>>>(nullptr, s->alpha[L], f[0], f[1], s->alpha[L + 1], cc[0], cc[1], cc[2]);
+        } else {
+            if (L == 0) k_restrict_alpha<2, true><<<g, b, 0, st>>>(s->flags, nullptr, f[0], f[1], s->alpha[1], cc[0], cc[1], cc[2]);
+            else k_restrict_alpha<2, false><<<g, b, 0, st>>>(nullptr, s->alpha[L], f[0], f[1], s->alpha[L + 1], cc[0], cc[1], cc[2]);
+        }
+    }
+    s->pyramid_dirty = 0;
+    s->nlaunch += s->levels - 1;
+    return check_cuda(cudaGetLastError(), "k_restrict_alpha");
+}
+
+// ------------------------------------------------- projected residual (FP64)
+// R = div - (dt/(rho h)) (sum_f p_nb - f_sum p) over fluid cells, evaluated in
+// FP64 from the FP32 state: the divergence the projection would leave.
+SS_D double block_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __shared__ double warp_part[32];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    if ((tid & 31) == 0) warp_part[tid >> 5] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (tid < 32) {
+        r = tid < (nthreads + 31) / 32 ? warp_part[tid] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    return r;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_projected_residual(const float* __restrict__ p, const float* __restrict__ div0,
+                                                            const uint8_t* __restrict__ flags, int nx, int ny, int nz,
+                                                            double k, double* __restrict__ partial) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    double acc = 0.0;
+    if (x < nx && y < ny && z < nz) {
+        const int c = idx3(x, y, z, nx, ny);
+        const uint8_t fl = flags[c];
+        if (!(fl & F_SOLID)) {
+            double psum = 0.0, fsum = 0.0;
+            auto nb = [&](bool in, uint8_t bit, int off) {
+                const double f = in ? ((fl & bit) ? 0.0 : 1.0) : 1.0;
+                const double pn = in ? (double)p[c + off] : 0.0;
+                psum += f * pn;
+                fsum += f;
+            };
+            nb(y + 1 < ny, F_TOP, nx);
+            nb(y > 0, F_BOTTOM, -nx);
+            nb(x + 1 < nx, F_RIGHT, 1);
+            nb(x > 0, F_LEFT, -1);
+            if constexpr (DIM == 3) {
+                nb(z + 1 < nz, F_FRONT, nx * ny);
+                nb(z > 0, F_BACK, -nx * ny);
+            }
+            const double rr = (double)div0[c] - k * (psum - fsum * (double)p[c]);
+            acc = rr * rr;
+        }
+    }
+    const double bs = block_sum_d(acc);
+    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0)
+        partial[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = bs;
+}
+
+int launch_projected_residual_norm(ss_sim* s, const StepConsts& c, int slot, cudaStream_t st) {
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for(s->nx, s->ny, s->nz, b);
+    const double k = (double)c.dt / ((double)c.rho * (double)s->h);
+    if (s->dim == 3) k_projected_residual<3><<<g, b, 0, st>>>(s->p[0], s->div0, s->flags, s->nx, s->ny, s->nz, k, s->red.partial);
+    else k_projected_residual<2><<<g, b, 0, st>>>(s->p[0], s->div0, s->flags, s->nx, s->ny, s->nz, k, s->red.partial);
+    s->nlaunch += 1;
+    int rc = check_cuda(cudaGetLastError(), "k_projected_residual");
+    if (rc) return rc;
+    return launch_reduce_final(s, (int)(g.x * g.y * g.z), slot, st);
+}
+
+}  // namespace ss

@@ -1,0 +1,116 @@
+// ss_internal.h - device state of one grid and the kernel launchers.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/smokesim.h"
+
+namespace ss {
+
+struct Level {
+    int n[3];
+    float h;    // cell size of the level: h * 2^L
+    float hh;   // h*h
+};
+
+// Launch-time constants of a step (all derived on the host in FP32 exactly as
+// the oracle derives them).
+struct StepConsts {
+    float dt, rho, t_amb, alpha, beta, eps;
+    float wind[3];
+    float cfl;      // dt / h
+    float rho_h;    // rho * h       (smoother right-hand side)
+    float dt_h;     // dt * h        (residual right-hand side)
+    float k_upd;    // -dt / (rho*h) (projection update)
+    float vort_k;   // unused scaling helper
+};
+
+struct ReduceSlots {
+    double* partial;      // per-block partial sums (device scratch)
+    double* out;          // reduction results (device), SLOT_* below
+    double* host;         // pinned mirror of out
+    int max_blocks;
+};
+enum { SLOT_DIV_BEFORE = 0, SLOT_RESIDUAL = 1, SLOT_DIV_AFTER = 2, SLOT_COUNT = 8 };
+
+}  // namespace ss
+
+struct ss_sim {
+    int dim, nx, ny, nz, nch, enclosed, min_coarse;
+    float h, t_amb0;
+    size_t ncell, nv[3];
+
+    float* vel[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+    int vi[3] = {0, 0, 0};
+    float* dens[2] = {nullptr, nullptr};   // nch planes of ncell, channel-major
+    float* temp[2] = {nullptr, nullptr};
+    int si = 0;
+
+    uint8_t* solid = nullptr;      // level-0: 1 solid / 0 fluid (rasteriser output)
+    uint8_t* flags = nullptr;      // level-0 flag byte with neighbour bits
+    float* svel[3] = {nullptr, nullptr, nullptr};   // solid velocity (FP16-rounded); null = all zero
+    int svel_active = 0;
+
+    int levels = 0;
+    ss::Level lv[SS_MAX_LEVELS];
+    float* p[SS_MAX_LEVELS] = {};
+    float* r[SS_MAX_LEVELS] = {};
+    float* alpha[SS_MAX_LEVELS] = {};   // coarse solid fraction (L >= 1), FP16-rounded values
+    float* div0 = nullptr;              // level-0 divergence, smoother boundary rule
+    float* div0r = nullptr;             // residual boundary rule (== div0 when enclosed)
+    float* vort = nullptr;              // 3*ncell (2D: ncell) vorticity scratch
+    ss::ReduceSlots red{};
+
+    std::vector<ss_emitter> em;
+    std::vector<ss_obstacle> ob;
+    std::vector<ss_box> bx;
+    ss_emitter* d_em = nullptr;
+    ss_obstacle* d_ob = nullptr;
+    ss_box* d_bx = nullptr;
+    int cap_em = 0, cap_ob = 0, cap_bx = 0;
+    int pyramid_dirty = 1;
+
+    ss_stats st{};
+    long long nlaunch = 0;     // kernels launched since the counter was reset
+    cudaStream_t stream0 = nullptr;
+};
+
+namespace ss {
+
+// error helpers (api.cpp)
+int set_error(int code, const std::string& msg);
+int check_cuda(cudaError_t e, const char* what);
+
+StepConsts make_consts(const ss_sim* s, const ss_params* p);
+
+// ---- fluid kernels (k_fluid.cu) ----
+int launch_emitters(ss_sim* s, const StepConsts& c, cudaStream_t st);
+int launch_advect_velocities(ss_sim* s, const StepConsts& c, bool fuse_buoyancy, cudaStream_t st);
+int launch_buoyancy(ss_sim* s, const StepConsts& c, cudaStream_t st);
+int launch_vorticity(ss_sim* s, const StepConsts& c, cudaStream_t st);
+int launch_update_velocities(ss_sim* s, const StepConsts& c, cudaStream_t st);
+int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st);
+// divergence of the current velocities into div0 (+div0r); optional ||div||^2 into slot
+int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st);
+
+// ---- multigrid kernels (k_mg.cu) ----
+int launch_smooth(ss_sim* s, const StepConsts& c, int L, int iterations, int quirks, cudaStream_t st);
+int launch_residual(ss_sim* s, const StepConsts& c, int L, bool write_fine, bool write_coarse, int quirks,
+                    cudaStream_t st);
+int launch_restrict(ss_sim* s, int L, cudaStream_t st);
+int launch_prolong(ss_sim* s, int L, cudaStream_t st);
+int launch_projected_residual_norm(ss_sim* s, const StepConsts& c, int slot, cudaStream_t st);
+int launch_solid_pyramid(ss_sim* s, cudaStream_t st);
+
+// ---- scene kernels (k_scene.cu) ----
+int launch_rasterize(ss_sim* s, cudaStream_t st);
+int launch_flags(ss_sim* s, cudaStream_t st);
+int launch_fill(float* a, size_t n, float v, cudaStream_t st);
+
+// ---- reductions ----
+int launch_reduce_final(ss_sim* s, int nblocks, int slot, cudaStream_t st);
+
+}  // namespace ss
