@@ -226,6 +226,26 @@ int ss_obstacle_update_step(ss_sim* sim, const ss_params* params, void* stream);
 int ss_update_solid_map(ss_sim* sim, void* stream);                                  /* grid.c:164-171 */
 int ss_init_solid_map(ss_sim* sim, void* stream);                                    /* grid.c:147-154 */
 
+/* ---- allocation-free divergence norm ---------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc -
+ * a host application that hands out all device memory from its own fixed
+ * budget (a game engine or renderer with a VRAM cap), or a per-frame callback
+ * where an allocation would stall the frame - and that therefore cannot create
+ * an ss_sim.  Writes to *out_norm (device memory, one double) the L2 norm over
+ * fluid cells of the discrete divergence of the caller's MAC velocities u, v,
+ * w (device arrays in the layout above; w unused when dim == 2), where
+ * solid[c] != 0 marks solid cells (device, one byte per cell), solid
+ * neighbours' faces count as velocity 0 and out-of-grid neighbours as fluid:
+ * the quantity ss_stats.div_before reports when every obstacle is at rest.
+ * Allocates nothing: its scratch (16384 FP64 partial sums, 128 KiB) is a
+ * static device array that every GPU loading this library holds until exit.
+ * At most 67,108,864 cells; larger grids return SS_E_INVALID.  The first call
+ * on each device looks up that array's address (a one-time set-up); make that
+ * first call before any stream capture begins.  All calls share the scratch,
+ * so calls that overlap on the GPU (different streams, no ordering) race. */
+int ss_divergence_norm_noalloc(int dim, const int n[3], const float* u, const float* v, const float* w,
+                               const uint8_t* solid, double* out_norm, void* stream);
+
 /* Level data of the multigrid pyramid (pressure / residual), for tests. */
 enum ss_level_field { SS_LEVEL_PRESSURE = 0, SS_LEVEL_RESIDUAL = 1, SS_LEVEL_FLUID_WEIGHT = 2 };
 int ss_get_level(ss_sim* sim, int level, int what, float* host, size_t count, void* stream);

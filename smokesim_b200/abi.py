@@ -270,7 +270,7 @@ EXPORTED = [
     "ss_apply_vorticity", "ss_multigrid_pressure_solve", "ss_v_cycle", "ss_smooth",
     "ss_compute_residual", "ss_compute_restrict", "ss_prolong_and_add", "ss_update_velocities",
     "ss_advect_smoke", "ss_obstacle_update_step", "ss_update_solid_map", "ss_init_solid_map",
-    "ss_get_level", "ss_set_level",
+    "ss_get_level", "ss_set_level", "ss_divergence_norm_noalloc",
 ]
 
 
@@ -307,4 +307,5 @@ def _declare(L):
     L.ss_update_solid_map.argtypes = [vp, vp]
     L.ss_init_solid_map.argtypes = [vp, vp]
     L.ss_get_level.argtypes = [vp, i, i, fp, sz, vp]
+    L.ss_divergence_norm_noalloc.argtypes = [i, C.POINTER(C.c_int * 3), vp, vp, vp, vp, vp, vp]
     L.ss_set_level.argtypes = [vp, i, i, fp, sz, vp]
