@@ -196,6 +196,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
         s->lv[l].h = s->h * (float)(1 << l);
         s->lv[l].hh = s->lv[l].h * s->lv[l].h;
     }
+    s->bottom = bottom_start(s);
 
     int rc = SS_OK;
     auto A = [&](void** p, size_t bytes) { if (rc == SS_OK) rc = dalloc(p, bytes); };
@@ -548,6 +549,7 @@ int ss_set_level(ss_sim* s, int L, int what, const float* host, size_t count, vo
 // ------------------------------------------------------------------ solver
 static int v_cycle_rec(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int L, cudaStream_t st) {
     const int q = mg.ref_quirks;
+    if (L >= 1 && L >= s->bottom && L < s->levels) return launch_bottom(s, mg, L, st);
     if (L == s->levels - 1) return launch_smooth(s, c, L, mg.n_coarse, q, st);
     TRY(launch_smooth(s, c, L, mg.n_pre, q, st));
     // residual written in place only where the reference's post-smoother reads it

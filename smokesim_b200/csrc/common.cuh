@@ -130,6 +130,97 @@ SS_D void interp_velocity(const float* __restrict__ u, const float* __restrict__
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Specialised forms of sample_border at the points the kernels actually use.
+// At a MAC face or cell centre every texel-space coordinate is an integer or
+// an integer + 1/2, so each linear weight is exactly 0 or 0.5.  A weight-0
+// lerp a*(1-0) + b*0 equals a (for finite b), so skipping those taps gives the
+// same value as the generic 8-tap form; the remaining lerps are kept in the
+// generic x-then-y-then-z nesting.
+
+// value of a[x,y,z] or the border when out of range
+SS_D float at_b(const float* __restrict__ a, int ax, int ay, int az, int x, int y, int z) {
+    return fetch_b(a, ax, ay, az, x, y, z, 0.f);
+}
+
+// Velocity at the x face (i, j+1/2, k+1/2)
+template <int DIM>
+SS_D void vel_at_xface(const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+                       int nx, int ny, int nz, int i, int j, int k, float out[3]) {
+    out[0] = __ldg(u + idx3(i, j, k, nx + 1, ny));
+    // v at texel (i-1/2, j+1/2, k): x and y at 0.5
+    out[1] = lerp_(lerp_(at_b(v, nx, ny + 1, nz, i - 1, j, k), at_b(v, nx, ny + 1, nz, i, j, k), 0.5f),
+                   lerp_(at_b(v, nx, ny + 1, nz, i - 1, j + 1, k), at_b(v, nx, ny + 1, nz, i, j + 1, k), 0.5f), 0.5f);
+    if constexpr (DIM == 3) {
+        // w at texel (i-1/2, j, k+1/2): x and z at 0.5
+        out[2] = lerp_(lerp_(at_b(w, nx, ny, nz + 1, i - 1, j, k), at_b(w, nx, ny, nz + 1, i, j, k), 0.5f),
+                       lerp_(at_b(w, nx, ny, nz + 1, i - 1, j, k + 1), at_b(w, nx, ny, nz + 1, i, j, k + 1), 0.5f), 0.5f);
+    } else {
+        out[2] = 0.f;
+    }
+}
+
+// Velocity at the y face (i+1/2, j, k+1/2)
+template <int DIM>
+SS_D void vel_at_yface(const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+                       int nx, int ny, int nz, int i, int j, int k, float out[3]) {
+    // u at texel (i+1/2, j-1/2, k)
+    out[0] = lerp_(lerp_(at_b(u, nx + 1, ny, nz, i, j - 1, k), at_b(u, nx + 1, ny, nz, i + 1, j - 1, k), 0.5f),
+                   lerp_(at_b(u, nx + 1, ny, nz, i, j, k), at_b(u, nx + 1, ny, nz, i + 1, j, k), 0.5f), 0.5f);
+    out[1] = __ldg(v + idx3(i, j, k, nx, ny + 1));
+    if constexpr (DIM == 3) {
+        // w at texel (i, j-1/2, k+1/2): y and z at 0.5
+        out[2] = lerp_(lerp_(at_b(w, nx, ny, nz + 1, i, j - 1, k), at_b(w, nx, ny, nz + 1, i, j, k), 0.5f),
+                       lerp_(at_b(w, nx, ny, nz + 1, i, j - 1, k + 1), at_b(w, nx, ny, nz + 1, i, j, k + 1), 0.5f), 0.5f);
+    } else {
+        out[2] = 0.f;
+    }
+}
+
+// Velocity at the z face (i+1/2, j+1/2, k)
+SS_D void vel_at_zface(const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+                       int nx, int ny, int nz, int i, int j, int k, float out[3]) {
+    // u at texel (i+1/2, j, k-1/2): x and z at 0.5
+    out[0] = lerp_(lerp_(at_b(u, nx + 1, ny, nz, i, j, k - 1), at_b(u, nx + 1, ny, nz, i + 1, j, k - 1), 0.5f),
+                   lerp_(at_b(u, nx + 1, ny, nz, i, j, k), at_b(u, nx + 1, ny, nz, i + 1, j, k), 0.5f), 0.5f);
+    // v at texel (i, j+1/2, k-1/2): y and z at 0.5
+    out[1] = lerp_(lerp_(at_b(v, nx, ny + 1, nz, i, j, k - 1), at_b(v, nx, ny + 1, nz, i, j + 1, k - 1), 0.5f),
+                   lerp_(at_b(v, nx, ny + 1, nz, i, j, k), at_b(v, nx, ny + 1, nz, i, j + 1, k), 0.5f), 0.5f);
+    out[2] = __ldg(w + idx3(i, j, k, nx, ny));
+}
+
+// Velocity at the cell centre (i+1/2, j+1/2, k+1/2): each component is the
+// mean of the cell's two faces on its axis.
+template <int DIM>
+SS_D void vel_at_centre(const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+                        int nx, int ny, int nz, int i, int j, int k, float out[3]) {
+    out[0] = lerp_(__ldg(u + idx3(i, j, k, nx + 1, ny)), __ldg(u + idx3(i + 1, j, k, nx + 1, ny)), 0.5f);
+    out[1] = lerp_(__ldg(v + idx3(i, j, k, nx, ny + 1)), __ldg(v + idx3(i, j + 1, k, nx, ny + 1)), 0.5f);
+    if constexpr (DIM == 3) out[2] = lerp_(__ldg(w + idx3(i, j, k, nx, ny)), __ldg(w + idx3(i, j, k + 1, nx, ny)), 0.5f);
+    else out[2] = 0.f;
+}
+
+// Border sample with a branch-free interior fast path: when all taps are in
+// range one base address serves the 8 (4) loads.
+template <int DIM>
+SS_D float sample_taps_fast(const float* __restrict__ a, int ax, int ay, int az, const Taps& t, float border) {
+    const bool in = t.x0 >= 0 && t.x0 + 1 < ax && t.y0 >= 0 && t.y0 + 1 < ay &&
+                    (DIM == 2 || (t.z0 >= 0 && t.z0 + 1 < az));
+    if (!in) return sample_taps<DIM>(a, ax, ay, az, t, border);
+    const float* p = a + idx3(t.x0, t.y0, t.z0, ax, ay);
+    const float c00 = __ldg(p), c10 = __ldg(p + 1), c01 = __ldg(p + ax), c11 = __ldg(p + ax + 1);
+    if constexpr (DIM == 2) {
+        return lerp_(lerp_(c00, c10, t.wx), lerp_(c01, c11, t.wx), t.wy);
+    } else {
+        const int pl = ax * ay;
+        const float d00 = __ldg(p + pl), d10 = __ldg(p + pl + 1), d01 = __ldg(p + pl + ax), d11 = __ldg(p + pl + ax + 1);
+        const float c0 = lerp_(lerp_(c00, c10, t.wx), lerp_(c01, c11, t.wx), t.wy);
+        const float c1 = lerp_(lerp_(d00, d10, t.wx), lerp_(d01, d11, t.wx), t.wy);
+        return lerp_(c0, c1, t.wz);
+    }
+}
+
 SS_D float round_half(float x) { return __half2float(__float2half_rn(x)); }
 
 }  // namespace ss

@@ -170,6 +170,13 @@ int launch_emitters(ss_sim* s, const StepConsts& c, cudaStream_t st) {
 // is fused into the y faces: a y face touching solid (out of grid = fluid)
 // keeps the value the reference's write buffer holds there, which after the
 // advection swap is the pre-advection velocity.
+// mean of a cell array at the two cells either side of the y face (x, y, z):
+// texel (x, y-1/2, z), weights 0 / 0.5 / 0
+template <int DIM>
+SS_D float yface_mean(const float* __restrict__ a, int nx, int ny, int nz, int x, int y, int z, float border) {
+    return lerp_(fetch_b(a, nx, ny, nz, x, y - 1, z, border), fetch_b(a, nx, ny, nz, x, y, z, border), 0.5f);
+}
+
 template <int DIM, bool BUOY>
 __global__ void __launch_bounds__(256) k_advect_velocity(FluidArgs a) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -177,6 +184,8 @@ __global__ void __launch_bounds__(256) k_advect_velocity(FluidArgs a) {
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const float cfl = a.c.cfl;
+    // solid flags of this cell and of its -x, -y, -z neighbours (out of grid = solid)
+    const bool s_c = solid_oob1(a.flags, x, y, z, nx, ny, nz);
 #pragma unroll
     for (int comp = 0; comp < DIM; ++comp) {
         const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
@@ -188,32 +197,33 @@ __global__ void __launch_bounds__(256) k_advect_velocity(FluidArgs a) {
         float out;
         if (id == 0 && a.c.wind[comp] != 0.f) {
             out = a.c.wind[comp];
-        } else if (solid_oob1(a.flags, x, y, z, nx, ny, nz) ||
-                   solid_oob1(a.flags, x - (comp == 0), y - (comp == 1), z - (comp == 2), nx, ny, nz)) {
+        } else if (s_c || solid_oob1(a.flags, x - (comp == 0), y - (comp == 1), z - (comp == 2), nx, ny, nz)) {
             out = 0.f;
         } else {
+            float vel[3];
+            if (comp == 0) vel_at_xface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+            else if (comp == 1) vel_at_yface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+            else vel_at_zface(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
             const float gx = (float)x + (comp == 0 ? 0.f : 0.5f);
             const float gy = (float)y + (comp == 1 ? 0.f : 0.5f);
             const float gz = DIM == 3 ? (float)z + (comp == 2 ? 0.f : 0.5f) : 0.f;
-            float vel[3];
-            interp_velocity<DIM>(a.u, a.v, a.w, nx, ny, nz, gx, gy, gz, vel);
             const float bx = gx - vel[0] * cfl, by = gy - vel[1] * cfl, bz = gz - vel[2] * cfl;
-            out = sample_border<DIM>(src, ax, ay, az, bx - (comp == 0 ? 0.f : 0.5f), by - (comp == 1 ? 0.f : 0.5f),
-                                     bz - (comp == 2 ? 0.f : 0.5f), 0.f);
+            const Taps t = make_taps<DIM>(ax, ay, az, bx - (comp == 0 ? 0.f : 0.5f), by - (comp == 1 ? 0.f : 0.5f),
+                                          bz - (comp == 2 ? 0.f : 0.5f));
+            out = sample_taps_fast<DIM>(src, ax, ay, az, t, 0.f);
         }
         if constexpr (BUOY) {
             if (comp == 1) {
                 if (solid_oob0(a.flags, x, y, z, nx, ny, nz) || solid_oob0(a.flags, x, y - 1, z, nx, ny, nz)) {
                     out = __ldg(src + i);
                 } else {
-                    const Taps t = make_taps<DIM>(nx, ny, nz, (float)x, (float)y - 0.5f, (float)z);
                     const size_t ncell = (size_t)nx * ny * nz;
-                    float total = sample_taps<DIM>(a.dens, nx, ny, nz, t, 0.f);
+                    float total = yface_mean<DIM>(a.dens, nx, ny, nz, x, y, z, 0.f);
                     if (a.nch == 3) {
-                        total = total + sample_taps<DIM>(a.dens + ncell, nx, ny, nz, t, 0.f);
-                        total = total + sample_taps<DIM>(a.dens + 2 * ncell, nx, ny, nz, t, 0.f);
+                        total = total + yface_mean<DIM>(a.dens + ncell, nx, ny, nz, x, y, z, 0.f);
+                        total = total + yface_mean<DIM>(a.dens + 2 * ncell, nx, ny, nz, x, y, z, 0.f);
                     }
-                    const float T = sample_taps<DIM>(a.temp, nx, ny, nz, t, a.c.t_amb);
+                    const float T = yface_mean<DIM>(a.temp, nx, ny, nz, x, y, z, a.c.t_amb);
                     const float buoy = -a.c.alpha * total + a.c.beta * (T - a.c.t_amb);
                     out = out + buoy * a.c.dt;
                 }
@@ -250,14 +260,13 @@ __global__ void k_buoyancy(FluidArgs a) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     if (x >= nx || y >= ny + 1 || z >= nz) return;
     if (solid_oob0(a.flags, x, y, z, nx, ny, nz) || solid_oob0(a.flags, x, y - 1, z, nx, ny, nz)) return;
-    const Taps t = make_taps<DIM>(nx, ny, nz, (float)x, (float)y - 0.5f, (float)z);
     const size_t ncell = (size_t)nx * ny * nz;
-    float total = sample_taps<DIM>(a.dens, nx, ny, nz, t, 0.f);
+    float total = yface_mean<DIM>(a.dens, nx, ny, nz, x, y, z, 0.f);
     if (a.nch == 3) {
-        total = total + sample_taps<DIM>(a.dens + ncell, nx, ny, nz, t, 0.f);
-        total = total + sample_taps<DIM>(a.dens + 2 * ncell, nx, ny, nz, t, 0.f);
+        total = total + yface_mean<DIM>(a.dens + ncell, nx, ny, nz, x, y, z, 0.f);
+        total = total + yface_mean<DIM>(a.dens + 2 * ncell, nx, ny, nz, x, y, z, 0.f);
     }
-    const float T = sample_taps<DIM>(a.temp, nx, ny, nz, t, a.c.t_amb);
+    const float T = yface_mean<DIM>(a.temp, nx, ny, nz, x, y, z, a.c.t_amb);
     const float buoy = -a.c.alpha * total + a.c.beta * (T - a.c.t_amb);
     const int i = idx3(x, y, z, nx, ny + 1);
     a.vo[i] = a.v[i] + buoy * a.c.dt;
@@ -459,12 +468,13 @@ __global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a) {
     }
     const float gx = (float)x + 0.5f, gy = (float)y + 0.5f, gz = DIM == 3 ? (float)z + 0.5f : 0.f;
     float vel[3];
-    interp_velocity<DIM>(a.u, a.v, a.w, nx, ny, nz, gx, gy, gz, vel);
+    vel_at_centre<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
     const float cfl = a.c.cfl;
     const float bx = gx - vel[0] * cfl, by = gy - vel[1] * cfl, bz = gz - vel[2] * cfl;
     const Taps t = make_taps<DIM>(nx, ny, nz, bx - 0.5f, by - 0.5f, bz - 0.5f);
-    for (int ch = 0; ch < a.nch; ++ch) a.dens_o[ch * ncell + c] = sample_taps<DIM>(a.dens + ch * ncell, nx, ny, nz, t, 0.f);
-    a.temp_o[c] = sample_taps<DIM>(a.temp, nx, ny, nz, t, a.c.t_amb);
+    for (int ch = 0; ch < a.nch; ++ch)
+        a.dens_o[ch * ncell + c] = sample_taps_fast<DIM>(a.dens + ch * ncell, nx, ny, nz, t, 0.f);
+    a.temp_o[c] = sample_taps_fast<DIM>(a.temp, nx, ny, nz, t, a.c.t_amb);
 }
 
 int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st) {

@@ -461,4 +461,216 @@ int launch_projected_residual_norm(ss_sim* s, const StepConsts& c, int slot, cud
     return launch_reduce_final(s, (int)(g.x * g.y * g.z), slot, st);
 }
 
+
+// ------------------------------------------------------------- bottom solver
+// The lower part of the V-cycle (levels Lb..coarsest) in ONE thread block with
+// every array resident in shared memory.  It runs the same per-cell
+// operations as the per-level kernels above (smooth_cell, residual_cell, the
+// restriction sum order, the prolongation formula), so the result is
+// bit-identical to launching them level by level - without the
+// 2*(n_pre+n_post)+2 launches per level and 2*n_coarse launches on the
+// coarsest level, which are pure launch latency at these sizes.
+struct BottomLevel {
+    int n[3];
+    int off;        // offset of the level in the shared arrays
+    float hh;
+};
+struct BottomArgs {
+    int nlev;
+    BottomLevel lv[SS_MAX_LEVELS];
+    float* p[SS_MAX_LEVELS];
+    float* r[SS_MAX_LEVELS];
+    const float* alpha[SS_MAX_LEVELS];
+    int total;
+    int n_pre, n_post, n_coarse, quirks;
+    float oob_smooth, oob_resid;
+};
+
+SS_D MGArgs bottom_level(const BottomArgs& b, float* sp, float* sr, float* sa, int l, float oobA) {
+    MGArgs a;
+    a.p = sp + b.lv[l].off;
+    a.r = sr + b.lv[l].off;
+    a.alpha = sa + b.lv[l].off;
+    a.flags = nullptr;
+    a.div0 = nullptr;
+    a.div0r = nullptr;
+    a.nx = b.lv[l].n[0];
+    a.ny = b.lv[l].n[1];
+    a.nz = b.lv[l].n[2];
+    a.oobA = oobA;
+    a.hh = b.lv[l].hh;
+    a.rho_h = 0.f;
+    a.dt = 1.f;
+    a.rho = 1.f;
+    a.dt_h = 1.f;
+    return a;
+}
+
+template <int DIM>
+SS_D void bottom_smooth(const MGArgs& a, int iterations) {
+    const int n = a.nx * a.ny * a.nz;
+    for (int it = 0; it < 2 * iterations; ++it) {
+        const int parity = it & 1;
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+            const int x = c % a.nx, t = c / a.nx, y = t % a.ny, z = t / a.ny;
+            if (((x + y + z) & 1) != parity) continue;
+            smooth_cell<DIM, false>(a, x, y, z);
+        }
+        __syncthreads();
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(1024) k_bottom(BottomArgs b) {
+    extern __shared__ float sm[];
+    float* sp = sm;
+    float* sr = sm + b.total;
+    float* sa = sm + 2 * b.total;
+    for (int l = 0; l < b.nlev; ++l) {
+        const int n = b.lv[l].n[0] * b.lv[l].n[1] * b.lv[l].n[2];
+        const int o = b.lv[l].off;
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+            sp[o + c] = b.p[l][c];
+            sr[o + c] = b.r[l][c];
+            sa[o + c] = b.alpha[l][c];
+        }
+    }
+    __syncthreads();
+    // down: pre-smoothing, residual (in place only with the reference's rule) + restriction, clear next p
+    for (int l = 0; l + 1 < b.nlev; ++l) {
+        const MGArgs a = bottom_level(b, sp, sr, sa, l, b.oob_smooth);
+        bottom_smooth<DIM>(a, b.n_pre);
+        const MGArgs ar = bottom_level(b, sp, sr, sa, l, b.oob_resid);
+        const int cx = b.lv[l + 1].n[0], cy = b.lv[l + 1].n[1], cz = b.lv[l + 1].n[2];
+        const int hx = (a.nx + 1) / 2, hy = (a.ny + 1) / 2, hz = DIM == 3 ? (a.nz + 1) / 2 : 1;
+        float* rc = sr + b.lv[l + 1].off;
+        for (int q = threadIdx.x; q < hx * hy * hz; q += blockDim.x) {
+            const int X = q % hx, t = q / hx, Y = t % hy, Z = t / hy;
+            const int x0 = 2 * X, y0 = 2 * Y, z0 = DIM == 3 ? 2 * Z : 0;
+            float v[2][2][2];
+            for (int dz = 0; dz < (DIM == 3 ? 2 : 1); ++dz)
+                for (int dy = 0; dy < 2; ++dy)
+                    for (int dx = 0; dx < 2; ++dx) {
+                        const int x = x0 + dx, y = y0 + dy, z = z0 + dz;
+                        float res = 0.f;
+                        if (x < a.nx && y < a.ny && z < a.nz) {
+                            res = residual_cell<DIM, false>(ar, x, y, z);
+                            if (b.quirks) ar.r[idx3(x, y, z, a.nx, a.ny)] = res;
+                        }
+                        v[dz][dy][dx] = res;
+                    }
+            if (X < cx && Y < cy && Z < cz) {
+                float out;
+                if constexpr (DIM == 3) {
+                    const float bottom = v[0][0][0] + v[1][0][0] + v[0][0][1] + v[1][0][1];
+                    const float top = v[0][1][0] + v[1][1][0] + v[0][1][1] + v[1][1][1];
+                    out = (bottom + top) / 8.f;
+                } else {
+                    out = (v[0][0][0] + v[0][0][1] + v[0][1][0] + v[0][1][1]) / 4.f;
+                }
+                rc[idx3(X, Y, Z, cx, cy)] = out;
+            }
+        }
+        float* pc = sp + b.lv[l + 1].off;
+        for (int c = threadIdx.x; c < cx * cy * cz; c += blockDim.x) pc[c] = 0.f;
+        __syncthreads();
+    }
+    // coarsest level
+    bottom_smooth<DIM>(bottom_level(b, sp, sr, sa, b.nlev - 1, b.oob_smooth), b.n_coarse);
+    // up: prolongation + post-smoothing
+    for (int l = b.nlev - 2; l >= 0; --l) {
+        const MGArgs a = bottom_level(b, sp, sr, sa, l, b.oob_smooth);
+        const int cx = b.lv[l + 1].n[0], cy = b.lv[l + 1].n[1], cz = b.lv[l + 1].n[2];
+        const float* pc = sp + b.lv[l + 1].off;
+        const int ax = a.nx, ay = a.ny, az = a.nz;
+        for (int c = threadIdx.x; c < ax * ay * az; c += blockDim.x) {
+            const int x = c % ax, t = c / ax, y = t % ay, z = t / ay;
+            const float tx = (((float)x + 0.5f) / (float)ax) * (float)cx - 0.5f;
+            const float ty = (((float)y + 0.5f) / (float)ay) * (float)cy - 0.5f;
+            const float fx = floorf(tx), fy = floorf(ty);
+            const int x0 = (int)fx, y0 = (int)fy;
+            const float wx = tx - fx, wy = ty - fy;
+            const int xa = min(max(x0, 0), cx - 1), xb = min(max(x0 + 1, 0), cx - 1);
+            const int ya = min(max(y0, 0), cy - 1), yb = min(max(y0 + 1, 0), cy - 1);
+            float sv;
+            if constexpr (DIM == 2) {
+                sv = lerp_(lerp_(pc[idx3(xa, ya, 0, cx, cy)], pc[idx3(xb, ya, 0, cx, cy)], wx),
+                           lerp_(pc[idx3(xa, yb, 0, cx, cy)], pc[idx3(xb, yb, 0, cx, cy)], wx), wy);
+            } else {
+                const float tz = (((float)z + 0.5f) / (float)az) * (float)cz - 0.5f;
+                const float fz = floorf(tz);
+                const int z0 = (int)fz;
+                const float wz = tz - fz;
+                const int za = min(max(z0, 0), cz - 1), zb = min(max(z0 + 1, 0), cz - 1);
+                const float c0 = lerp_(lerp_(pc[idx3(xa, ya, za, cx, cy)], pc[idx3(xb, ya, za, cx, cy)], wx),
+                                       lerp_(pc[idx3(xa, yb, za, cx, cy)], pc[idx3(xb, yb, za, cx, cy)], wx), wy);
+                const float c1 = lerp_(lerp_(pc[idx3(xa, ya, zb, cx, cy)], pc[idx3(xb, ya, zb, cx, cy)], wx),
+                                       lerp_(pc[idx3(xa, yb, zb, cx, cy)], pc[idx3(xb, yb, zb, cx, cy)], wx), wy);
+                sv = lerp_(c0, c1, wz);
+            }
+            a.p[c] = a.p[c] + sv;
+        }
+        __syncthreads();
+        bottom_smooth<DIM>(a, b.n_post);
+    }
+    // write back every level (pressure and, with the in-place rule, residual)
+    for (int l = 0; l < b.nlev; ++l) {
+        const int n = b.lv[l].n[0] * b.lv[l].n[1] * b.lv[l].n[2];
+        const int o = b.lv[l].off;
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+            b.p[l][c] = sp[o + c];
+            b.r[l][c] = sr[o + c];
+        }
+    }
+}
+
+int bottom_start(const ss_sim* s) {
+    // finest level >= 1 from which the rest of the pyramid fits the block's shared memory
+    long long cum = 0;
+    int start = s->levels;
+    for (int l = s->levels - 1; l >= 1; --l) {
+        const long long n = (long long)s->lv[l].n[0] * s->lv[l].n[1] * s->lv[l].n[2];
+        if ((cum + n) * 12 > kBottomSmemBytes) break;
+        cum += n;
+        start = l;
+    }
+    return start;
+}
+
+int launch_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, cudaStream_t st) {
+    BottomArgs b{};
+    b.nlev = s->levels - L;
+    int off = 0;
+    for (int l = 0; l < b.nlev; ++l) {
+        const ss::Level& lv = s->lv[L + l];
+        b.lv[l].n[0] = lv.n[0]; b.lv[l].n[1] = lv.n[1]; b.lv[l].n[2] = lv.n[2];
+        b.lv[l].off = off;
+        b.lv[l].hh = lv.hh;
+        b.p[l] = s->p[L + l];
+        b.r[l] = s->r[L + l];
+        b.alpha[l] = s->alpha[L + l];
+        off += lv.n[0] * lv.n[1] * lv.n[2];
+    }
+    b.total = off;
+    b.n_pre = mg.n_pre; b.n_post = mg.n_post; b.n_coarse = mg.n_coarse;
+    b.quirks = mg.ref_quirks ? 1 : 0;
+    b.oob_smooth = smooth_oob(s, mg.ref_quirks);
+    b.oob_resid = resid_oob(s, mg.ref_quirks);
+    const size_t smem = (size_t)3 * off * sizeof(float);
+    if (smem > (size_t)kBottomSmemBytes) return set_error(SS_E_INVALID, "bottom levels exceed shared memory");
+    static bool attr_set[2] = {false, false};
+    const int di = s->dim == 3 ? 1 : 0;
+    if (!attr_set[di]) {
+        cudaError_t e = s->dim == 3
+            ? cudaFuncSetAttribute(k_bottom<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBytes)
+            : cudaFuncSetAttribute(k_bottom<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBytes);
+        if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute(k_bottom)");
+        attr_set[di] = true;
+    }
+    if (s->dim == 3) k_bottom<3><<<1, 1024, smem, st>>>(b);
+    else k_bottom<2><<<1, 1024, smem, st>>>(b);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_bottom");
+}
+
 }  // namespace ss

@@ -55,6 +55,7 @@ struct ss_sim {
     int svel_active = 0;
 
     int levels = 0;
+    int bottom = 0;            // first level solved by the single-block bottom kernel (== levels: none)
     ss::Level lv[SS_MAX_LEVELS];
     float* p[SS_MAX_LEVELS] = {};
     float* r[SS_MAX_LEVELS] = {};
@@ -104,6 +105,10 @@ int launch_restrict(ss_sim* s, int L, cudaStream_t st);
 int launch_prolong(ss_sim* s, int L, cudaStream_t st);
 int launch_projected_residual_norm(ss_sim* s, const StepConsts& c, int slot, cudaStream_t st);
 int launch_solid_pyramid(ss_sim* s, cudaStream_t st);
+// levels Lb..coarsest of the V-cycle in one thread block (shared memory)
+constexpr int kBottomSmemBytes = 160 * 1024;
+int bottom_start(const ss_sim* s);
+int launch_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, cudaStream_t st);
 
 // ---- scene kernels (k_scene.cu) ----
 int launch_rasterize(ss_sim* s, cudaStream_t st);
