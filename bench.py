@@ -242,7 +242,8 @@ def main():
                "h2d_bytes_per_step": C.sizeof(abi.Emitter) * len(sc["emitters"]),
                "d2h_bytes_per_step": 8 * 8}
 
-        # roofline of the dominant kernel: the level-0 red-black smoother.
+        # roofline of the dominant kernel: the level-0 red-black smoother
+        # (k_rb_smooth, one colour per launch on the colour-split arrays).
         # 13 B/cell per red+black sweep (read/write p, read rhs, read flag).
         reps = 10
         sim.smooth(p, 0, 1)
@@ -265,7 +266,7 @@ def main():
             pass
         peak = float(peaks.get("hbm_gbs", 6650.0))
         achieved = alg_bytes / (launch_ms / 1e3) / 1e9
-        roofline = {"kernel": "k_smooth<3,L0> (one colour of a red-black sweep, 256^3)", "bound": "hbm",
+        roofline = {"kernel": "k_rb_smooth<3> (one colour of a level-0 red-black sweep, 256^3)", "bound": "hbm",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": launch_ms, "traffic": None}

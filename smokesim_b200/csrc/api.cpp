@@ -75,16 +75,24 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->solid);
     cudaFree(s->flags);
     for (int d = 0; d < 3; ++d) cudaFree(s->svel[d]);
-    for (int l = 0; l < s->levels; ++l) { cudaFree(s->p[l]); cudaFree(s->r[l]); cudaFree(s->alpha[l]); }
+    for (int l = 0; l < s->levels; ++l) {
+        cudaFree(s->p[l]); cudaFree(s->r[l]); cudaFree(s->alpha[l]);
+        cudaFree(s->p_alt[l]); cudaFree(s->r_alt[l]);
+    }
     cudaFree(s->div0);
     if (s->div0r != s->div0) cudaFree(s->div0r);
     cudaFree(s->vort);
+    cudaFree(s->rhs_s);
+    cudaFree(s->fmask);
+    cudaFree(s->rb_mask);
+    cudaFree(s->rhs_r);
     cudaFree(s->red.partial);
     cudaFree(s->red.out);
     if (s->red.host) cudaFreeHost(s->red.host);
     cudaFree(s->d_em);
     cudaFree(s->d_ob);
     cudaFree(s->d_bx);
+    cudaFree(s->d_err);
     delete s;
 }
 
@@ -212,15 +220,24 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
         const size_t n = (size_t)s->lv[l].n[0] * s->lv[l].n[1] * s->lv[l].n[2];
         A((void**)&s->p[l], n * sizeof(float));
         A((void**)&s->r[l], n * sizeof(float));
+        if (l < s->bottom || l == 0) A((void**)&s->p_alt[l], n * sizeof(float));
         if (l > 0) A((void**)&s->alpha[l], n * sizeof(float));
+        if (l > 0 && l < s->bottom) A((void**)&s->r_alt[l], n * sizeof(float));
     }
     A((void**)&s->div0, s->ncell * sizeof(float));
     if (s->enclosed) s->div0r = s->div0;
     else A((void**)&s->div0r, s->ncell * sizeof(float));
     A((void**)&s->vort, s->ncell * (s->dim == 3 ? 3 : 1) * sizeof(float));
+    if (s->nx % 2 == 0 && s->levels > 1) {   // colour-split level 0 (k_rb.cu)
+        A((void**)&s->rhs_s, s->ncell * sizeof(float));
+        A((void**)&s->rhs_r, s->ncell * sizeof(float));
+        A((void**)&s->fmask, s->ncell);
+        A((void**)&s->rb_mask, s->ncell);
+    }
     s->red.max_blocks = (int)(((s->nx + 32) / 32 + 1) * ((s->ny + 8) / 8 + 1) * (size_t)(s->nz + 1));
     A((void**)&s->red.partial, (size_t)s->red.max_blocks * sizeof(double));
     A((void**)&s->red.out, SLOT_COUNT * sizeof(double));
+    A((void**)&s->d_err, sizeof(int));
     if (rc == SS_OK) {
         cudaError_t e = cudaMallocHost((void**)&s->red.host, SLOT_COUNT * sizeof(double));
         if (e != cudaSuccess) rc = check_cuda(e, "cudaMallocHost");
@@ -241,6 +258,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
         rc = check_cuda(cudaMemsetAsync(s->p[l], 0, n * 4, st), "memset");
         if (!rc) rc = check_cuda(cudaMemsetAsync(s->r[l], 0, n * 4, st), "memset");
     }
+    if (!rc) rc = check_cuda(cudaMemsetAsync(s->d_err, 0, sizeof(int), st), "memset");
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->div0, 0, s->ncell * 4, st), "memset");
     if (!rc && s->div0r != s->div0) rc = check_cuda(cudaMemsetAsync(s->div0r, 0, s->ncell * 4, st), "memset");
     if (!rc) rc = ss_set_scene(s, nullptr, 0, nullptr, 0, nullptr, 0, stream);
@@ -312,6 +330,7 @@ static int rasterize_solid(ss_sim* s, cudaStream_t st) {
     TRY(upload_array((void**)&s->d_bx, &s->cap_bx, s->bx.data(), sizeof(ss_box), (int)s->bx.size(), st));
     TRY(launch_rasterize(s, st));
     TRY(launch_flags(s, st));
+    if (s->rb_mask) TRY(launch_rb_split_mask(s, st));
     TRY(launch_solid_pyramid(s, st));
     return SS_OK;
 }
@@ -547,24 +566,47 @@ int ss_set_level(ss_sim* s, int L, int what, const float* host, size_t count, vo
 }
 
 // ------------------------------------------------------------------ solver
+// v_cycle (common/physics/grid.c:177-209).  Levels from s->bottom down run in
+// one single-block launch; above it every red-black sweep is one tiled launch,
+// the last pre-smoothing sweep carrying the residual + restriction and the
+// first post-smoothing sweep the prolongation.
 static int v_cycle_rec(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int L, cudaStream_t st) {
     const int q = mg.ref_quirks;
+    if (L == 0 && s->rb_active) {
+        // level 0 on the colour-split arrays; residual + restriction fused
+        TRY(launch_rb_sweep(s, mg.n_pre, st));
+        TRY(launch_rb_residual_restrict(s, st));
+        const size_t nc = (size_t)s->lv[1].n[0] * s->lv[1].n[1] * s->lv[1].n[2];
+        CU(cudaMemsetAsync(s->p[1], 0, nc * sizeof(float), st), "clear coarse p");
+        TRY(v_cycle_rec(s, c, mg, 1, st));
+        TRY(launch_rb_prolong(s, st));
+        return launch_rb_sweep(s, mg.n_post, st);
+    }
     if (L >= 1 && L >= s->bottom && L < s->levels) return launch_bottom(s, mg, L, st);
     if (L == s->levels - 1) return launch_smooth(s, c, L, mg.n_coarse, q, st);
-    TRY(launch_smooth(s, c, L, mg.n_pre, q, st));
+    for (int i = 0; i < mg.n_pre; ++i) TRY(launch_rbgs_sweep(s, c, L, q, false, i == mg.n_pre - 1, st));
     // residual written in place only where the reference's post-smoother reads it
-    TRY(launch_residual(s, c, L, q && L > 0, true, q, st));
+    if (mg.n_pre == 0) TRY(launch_residual(s, c, L, q && L > 0, true, q, st));
     const size_t nc = (size_t)s->lv[L + 1].n[0] * s->lv[L + 1].n[1] * s->lv[L + 1].n[2];
     CU(cudaMemsetAsync(s->p[L + 1], 0, nc * sizeof(float), st), "clear coarse p");
     TRY(v_cycle_rec(s, c, mg, L + 1, st));
-    TRY(launch_prolong(s, L, st));
-    return launch_smooth(s, c, L, mg.n_post, q, st);
+    if (mg.n_post == 0) return launch_prolong(s, L, st);
+    for (int i = 0; i < mg.n_post; ++i) TRY(launch_rbgs_sweep(s, c, L, q, i == 0, false, st));
+    return SS_OK;
+}
+
+static int check_device_error(ss_sim* s, cudaStream_t st) {
+    int err = 0;
+    CU(cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "error word");
+    CU(cudaStreamSynchronize(st), "error word sync");
+    if (err) return set_error(SS_E_CUDA, "a kernel gave up waiting for its tile loads (bounded barrier wait)");
+    return SS_OK;
 }
 
 static int read_slots(ss_sim* s, cudaStream_t st) {
     CU(cudaMemcpyAsync(s->red.host, s->red.out, SLOT_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st), "slots");
     CU(cudaStreamSynchronize(st), "slots sync");
-    return SS_OK;
+    return check_device_error(s, st);
 }
 
 static int ensure_pyramid(ss_sim* s, cudaStream_t st) {
@@ -578,12 +620,29 @@ static int pressure_solve(ss_sim* s, const ss_params* p, const StepConsts& c, cu
     const bool tol_mode = mg.tol > 0.0;
     const bool stats = p->collect_stats || tol_mode;
     TRY(ensure_pyramid(s, st));
-    TRY(launch_divergence(s, true, stats ? SLOT_DIV_BEFORE : -1, st));
+    TRY(launch_divergence(s, true, stats ? SLOT_DIV_BEFORE : -1, st, &c, mg.ref_quirks));
     const int cap = mg.n_vcycles > 0 ? mg.n_vcycles : 1;
     int done = 0;
     bool conv = true;
+    const bool rb = rb_supported(s, mg.ref_quirks);
+    auto cycle = [&]() -> int {
+        if (rb) TRY(launch_rb_convert(s, true, st));
+        s->rb_active = rb ? 1 : 0;
+        int rc = v_cycle_rec(s, c, mg, 0, st);
+        s->rb_active = 0;
+        if (rc) return rc;
+        if (rb) TRY(launch_rb_convert(s, false, st));
+        return SS_OK;
+    };
     if (!tol_mode) {
-        for (; done < cap; ++done) TRY(v_cycle_rec(s, c, mg, 0, st));
+        if (rb) TRY(launch_rb_convert(s, true, st));
+        s->rb_active = rb ? 1 : 0;
+        for (; done < cap; ++done) {
+            int rc = v_cycle_rec(s, c, mg, 0, st);
+            if (rc) { s->rb_active = 0; return rc; }
+        }
+        s->rb_active = 0;
+        if (rb) TRY(launch_rb_convert(s, false, st));
         if (stats) TRY(launch_projected_residual_norm(s, c, SLOT_RESIDUAL, st));
         if (stats) {
             TRY(read_slots(s, st));
@@ -596,7 +655,7 @@ static int pressure_solve(ss_sim* s, const ss_params* p, const StepConsts& c, cu
         const double db = sqrt(s->red.host[SLOT_DIV_BEFORE]);
         double res = sqrt(s->red.host[SLOT_RESIDUAL]);
         while (done < cap && !(res <= mg.tol * db)) {
-            TRY(v_cycle_rec(s, c, mg, 0, st));
+            TRY(cycle());
             ++done;
             TRY(launch_projected_residual_norm(s, c, SLOT_RESIDUAL, st));
             TRY(read_slots(s, st));
@@ -665,7 +724,7 @@ int ss_run_physics_step(ss_sim* s, const ss_params* p, int nsteps, void* stream)
 int ss_get_stats(ss_sim* s, ss_stats* out) {
     if (!s || !out) return set_error(SS_E_INVALID, "NULL argument");
     *out = s->st;
-    return SS_OK;
+    return check_device_error(s, nullptr);
 }
 
 // ------------------------------------------------------------ single stages
@@ -711,8 +770,17 @@ int ss_v_cycle(ss_sim* s, const ss_params* p, int level, void* stream) {
     if (level < 0 || level >= s->levels) return set_error(SS_E_INVALID, "level out of range");
     cudaStream_t st = as_stream(stream);
     TRY(ensure_pyramid(s, st));
-    if (level == 0) TRY(launch_divergence(s, true, -1, st));
-    return v_cycle_rec(s, make_consts(s, p), p->mg, level, st);
+    const StepConsts c = make_consts(s, p);
+    if (level != 0) return v_cycle_rec(s, c, p->mg, level, st);
+    TRY(launch_divergence(s, true, -1, st, &c, p->mg.ref_quirks));
+    const bool rb = rb_supported(s, p->mg.ref_quirks);
+    if (rb) TRY(launch_rb_convert(s, true, st));
+    s->rb_active = rb ? 1 : 0;
+    const int rc = v_cycle_rec(s, c, p->mg, 0, st);
+    s->rb_active = 0;
+    if (rc) return rc;
+    if (rb) TRY(launch_rb_convert(s, false, st));
+    return SS_OK;
 }
 
 int ss_smooth(ss_sim* s, const ss_params* p, int level, int iterations, void* stream) {
@@ -720,8 +788,16 @@ int ss_smooth(ss_sim* s, const ss_params* p, int level, int iterations, void* st
     if (level < 0 || level >= s->levels || iterations < 0) return set_error(SS_E_INVALID, "level/iterations out of range");
     cudaStream_t st = as_stream(stream);
     TRY(ensure_pyramid(s, st));
+    const StepConsts c = make_consts(s, p);
+    if (level == 0 && rb_supported(s, p->mg.ref_quirks)) {
+        // the colour-split sweeps the V-cycle uses (same values)
+        TRY(launch_divergence(s, true, -1, st, &c, p->mg.ref_quirks));
+        TRY(launch_rb_convert(s, true, st));
+        TRY(launch_rb_sweep(s, iterations, st));
+        return launch_rb_convert(s, false, st);
+    }
     if (level == 0) TRY(launch_divergence(s, true, -1, st));
-    return launch_smooth(s, make_consts(s, p), level, iterations, p->mg.ref_quirks, st);
+    return launch_smooth(s, c, level, iterations, p->mg.ref_quirks, st);
 }
 
 int ss_compute_residual(ss_sim* s, const ss_params* p, int level, void* stream) {

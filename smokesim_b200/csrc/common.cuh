@@ -223,4 +223,36 @@ SS_D float sample_taps_fast(const float* __restrict__ a, int ax, int ay, int az,
 
 SS_D float round_half(float x) { return __half2float(__float2half_rn(x)); }
 
+// a / f for an integer count f in 1..6, value-identical to the IEEE quotient
+// (the same value; -0 may come back as +0): q0 = a*RN(1/f) followed by one
+// residual correction with fused multiply-adds, verified exhaustively against
+// IEEE division over every finite float a for f = 1..5 (tests/division_check.c).
+// For f = 6 it divides a/2 by 3, exact except where a/2 is subnormal, which
+// takes the IEEE path.
+SS_D float div_by_count(float a, int f) {
+    if (f == 6) {
+        if (fabsf(a) < 7.52316385e-37f) return a / 6.f;
+        a = a * 0.5f;
+        f = 3;
+    }
+    const float y = f == 1 ? 1.f : f == 2 ? 0.5f : f == 3 ? (1.0f / 3.0f) : f == 4 ? 0.25f : (1.0f / 5.0f);
+    const float q0 = __fmul_rn(a, y);
+    const float r = __fmaf_rn(-(float)f, q0, a);
+    return __fmaf_rn(r, y, q0);
+}
+
+// Fluid mask byte of a level-0 cell: bit 0 the cell is fluid, bits 1-6 the
+// +y,-y,+x,-x,+z,-z neighbour is fluid (out of grid: fluid on an open grid,
+// solid on an enclosed one).  Zero - the TMA fill outside the grid - reads as
+// "not fluid", so tile kernels need no bounds checks.
+enum : uint8_t {
+    M_FLUID = 1u << 0,
+    M_TOP = 1u << 1,
+    M_BOTTOM = 1u << 2,
+    M_RIGHT = 1u << 3,
+    M_LEFT = 1u << 4,
+    M_FRONT = 1u << 5,
+    M_BACK = 1u << 6,
+};
+
 }  // namespace ss

@@ -510,9 +510,28 @@ SS_D double block_sum(double v) {
     return r;
 }
 
+// position of cell (x,y,z) in the colour-split level-0 arrays (k_rb.cu): the
+// colour-(x+y+z)&1 half, row-major with nx/2 entries per row (nx even)
+SS_D int rb_slot(int x, int y, int z, int nx, int ny, int nz) {
+    const int half = nx >> 1;
+    return (((x + y + z) & 1) ? half * ny * nz : 0) + (z * ny + y) * half + (x >> 1);
+}
+
+// Optional level-0 right-hand sides of the pressure operators, computed once
+// per solve with the operations the reference evaluates in every sweep:
+// rhs_s = rho*h*div/dt (smooth.comp:129), rhs_r = rho*div/(dt*h)
+// (compute_residual.comp:124), each with its out-of-grid rule, stored
+// colour-split for the level-0 kernels of k_rb.cu.
+struct RhsOut {
+    float* rhs_s;
+    float* rhs_r;
+    float rho_h, dt, rho, dt_h;
+    int s_solid, r_solid;   // out-of-grid neighbours count as solid in the smoother / residual
+};
+
 template <int DIM>
 __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restrict__ div0, float* __restrict__ div0r,
-                                                    double* __restrict__ partial) {
+                                                    double* __restrict__ partial, RhsOut ro) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -536,7 +555,7 @@ __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restri
                 d = d + v_front - v_back;
             }
             if (div0) div0[c] = d;
-            if (div0r) {
+            if (div0r || ro.rhs_s) {
                 // residual rule: out-of-grid neighbours are solid with velocity 0
                 const float rt = y + 1 >= ny ? 0.f : v_top, rb = y == 0 ? 0.f : v_bottom;
                 const float rr = x + 1 >= nx ? 0.f : v_right, rl = x == 0 ? 0.f : v_left;
@@ -545,9 +564,18 @@ __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restri
                     const float rf = z + 1 >= nz ? 0.f : v_front, rk = z == 0 ? 0.f : v_back;
                     dr = dr + rf - rk;
                 }
-                div0r[c] = dr;
+                if (div0r) div0r[c] = dr;
+                if (ro.rhs_s) {
+                    const int q = rb_slot(x, y, z, nx, ny, nz);
+                    ro.rhs_s[q] = ro.rho_h * (ro.s_solid ? dr : d) / ro.dt;
+                    ro.rhs_r[q] = ro.rho * (ro.r_solid ? dr : d) / ro.dt_h;
+                }
             }
             acc = (double)d * (double)d;
+        } else if (ro.rhs_s) {
+            const int q = rb_slot(x, y, z, nx, ny, nz);
+            ro.rhs_s[q] = 0.f;
+            ro.rhs_r[q] = 0.f;
         }
     }
     if (partial) {
@@ -557,17 +585,25 @@ __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restri
     }
 }
 
-int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st) {
+int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st, const StepConsts* sc, int quirks) {
     StepConsts c{};
     FluidArgs a = fluid_args(s, c);
+    RhsOut ro{};
+    if (write && sc && quirks >= 0 && rb_supported(s, quirks)) {
+        ro.rhs_s = s->rhs_s;
+        ro.rhs_r = s->rhs_r;
+        ro.rho_h = sc->rho_h; ro.dt = sc->dt; ro.rho = sc->rho; ro.dt_h = sc->dt_h;
+        ro.s_solid = quirks ? 0 : s->enclosed;
+        ro.r_solid = quirks ? 1 : s->enclosed;
+    }
     dim3 b(32, 8, 1);
     dim3 g = grid_for(s->nx, s->ny, s->nz, b);
     const int nblocks = (int)(g.x * g.y * g.z);
     float* d0 = write ? s->div0 : nullptr;
     float* d0r = (write && s->div0r != s->div0) ? s->div0r : nullptr;
     double* part = slot >= 0 ? s->red.partial : nullptr;
-    if (s->dim == 3) k_divergence<3><<<g, b, 0, st>>>(a, d0, d0r, part);
-    else k_divergence<2><<<g, b, 0, st>>>(a, d0, d0r, part);
+    if (s->dim == 3) k_divergence<3><<<g, b, 0, st>>>(a, d0, d0r, part, ro);
+    else k_divergence<2><<<g, b, 0, st>>>(a, d0, d0r, part, ro);
     s->nlaunch += 1;
     int rc = check_cuda(cudaGetLastError(), "k_divergence");
     if (rc || slot < 0) return rc;

@@ -506,18 +506,44 @@ SS_D MGArgs bottom_level(const BottomArgs& b, float* sp, float* sr, float* sa, i
     return a;
 }
 
+// Red-black sweeps of one small level.  Each thread's cells (at most
+// kBottomCells) and their colours are decoded once, outside the sweep loop;
+// a level small enough for two cells per thread of fewer warps runs on those
+// warps only, synchronised by a named barrier.
+constexpr int kBottomCells = 4;
 template <int DIM>
 SS_D void bottom_smooth(const MGArgs& a, int iterations) {
     const int n = a.nx * a.ny * a.nz;
-    for (int it = 0; it < 2 * iterations; ++it) {
-        const int parity = it & 1;
-        for (int c = threadIdx.x; c < n; c += blockDim.x) {
-            const int x = c % a.nx, t = c / a.nx, y = t % a.ny, z = t / a.ny;
-            if (((x + y + z) & 1) != parity) continue;
-            smooth_cell<DIM, false>(a, x, y, z);
+    int nt = blockDim.x;
+    while (nt > 128 && (n + nt / 2 - 1) / (nt / 2) <= 2) nt /= 2;
+    if ((int)threadIdx.x < nt) {
+        int cx[kBottomCells], cy[kBottomCells], cz[kBottomCells], col[kBottomCells];
+        int k = 0;
+        for (int c = threadIdx.x; c < n && k < kBottomCells; c += nt, ++k) {
+            cx[k] = c % a.nx;
+            const int t = c / a.nx;
+            cy[k] = t % a.ny;
+            cz[k] = t / a.ny;
+            col[k] = (cx[k] + cy[k] + cz[k]) & 1;
         }
-        __syncthreads();
+        const bool fits = (n + nt - 1) / nt <= kBottomCells;
+        for (int it = 0; it < 2 * iterations; ++it) {
+            const int parity = it & 1;
+            if (fits) {
+                for (int q = 0; q < k; ++q)
+                    if (col[q] == parity) smooth_cell<DIM, false>(a, cx[q], cy[q], cz[q]);
+            } else {
+                for (int c = threadIdx.x; c < n; c += nt) {
+                    const int x = c % a.nx, t = c / a.nx, y = t % a.ny, z = t / a.ny;
+                    if (((x + y + z) & 1) != parity) continue;
+                    smooth_cell<DIM, false>(a, x, y, z);
+                }
+            }
+            if (nt == (int)blockDim.x) __syncthreads();
+            else asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
+        }
     }
+    __syncthreads();
 }
 
 template <int DIM>

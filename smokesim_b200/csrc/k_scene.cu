@@ -57,7 +57,8 @@ __global__ void k_rasterize(uint8_t* __restrict__ solid, float* __restrict__ sv0
 
 // flag byte: bit 0 own solid, bits 1-6 neighbours (+y,-y,+x,-x,+z,-z), out of grid = fluid
 template <int DIM>
-__global__ void k_flags(const uint8_t* __restrict__ solid, uint8_t* __restrict__ flags, int nx, int ny, int nz) {
+__global__ void k_flags(const uint8_t* __restrict__ solid, uint8_t* __restrict__ flags, uint8_t* __restrict__ fmask,
+                        int nx, int ny, int nz, int enclosed) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -73,6 +74,19 @@ __global__ void k_flags(const uint8_t* __restrict__ solid, uint8_t* __restrict__
         if (z > 0 && solid[c - nx * ny]) f |= F_BACK;
     }
     flags[c] = f;
+    if (fmask) {
+        const uint8_t oob = enclosed ? 0 : 1;   // out-of-grid neighbour fluid on an open grid
+        uint8_t m = solid[c] ? 0 : M_FLUID;
+        m |= (y + 1 < ny ? !solid[c + nx] : oob) ? M_TOP : 0;
+        m |= (y > 0 ? !solid[c - nx] : oob) ? M_BOTTOM : 0;
+        m |= (x + 1 < nx ? !solid[c + 1] : oob) ? M_RIGHT : 0;
+        m |= (x > 0 ? !solid[c - 1] : oob) ? M_LEFT : 0;
+        if constexpr (DIM == 3) {
+            m |= (z + 1 < nz ? !solid[c + nx * ny] : oob) ? M_FRONT : 0;
+            m |= (z > 0 ? !solid[c - nx * ny] : oob) ? M_BACK : 0;
+        }
+        fmask[c] = m;
+    }
 }
 
 static inline dim3 grid_for(int ax, int ay, int az, dim3 b) {
@@ -98,8 +112,8 @@ int launch_rasterize(ss_sim* s, cudaStream_t st) {
 int launch_flags(ss_sim* s, cudaStream_t st) {
     dim3 b(32, 8, 1);
     dim3 g = grid_for(s->nx, s->ny, s->nz, b);
-    if (s->dim == 3) k_flags<3><<<g, b, 0, st>>>(s->solid, s->flags, s->nx, s->ny, s->nz);
-    else k_flags<2><<<g, b, 0, st>>>(s->solid, s->flags, s->nx, s->ny, s->nz);
+    if (s->dim == 3) k_flags<3><<<g, b, 0, st>>>(s->solid, s->flags, s->fmask, s->nx, s->ny, s->nz, s->enclosed);
+    else k_flags<2><<<g, b, 0, st>>>(s->solid, s->flags, s->fmask, s->nx, s->ny, s->nz, s->enclosed);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_flags");
 }

@@ -1,5 +1,6 @@
 // ss_internal.h - device state of one grid and the kernel launchers.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -36,6 +37,14 @@ struct ReduceSlots {
 };
 enum { SLOT_DIV_BEFORE = 0, SLOT_RESIDUAL = 1, SLOT_DIV_AFTER = 2, SLOT_COUNT = 8 };
 
+struct TensorMapEntry {
+    CUtensorMap map;
+    const void* ptr;
+    bool bytes;
+    int dims[3];
+    int box[3];
+};
+
 }  // namespace ss
 
 struct ss_sim {
@@ -51,6 +60,7 @@ struct ss_sim {
 
     uint8_t* solid = nullptr;      // level-0: 1 solid / 0 fluid (rasteriser output)
     uint8_t* flags = nullptr;      // level-0 flag byte with neighbour bits
+    uint8_t* fmask = nullptr;      // level-0 fluid mask (M_* bits); null when nx is odd
     float* svel[3] = {nullptr, nullptr, nullptr};   // solid velocity (FP16-rounded); null = all zero
     int svel_active = 0;
 
@@ -59,10 +69,15 @@ struct ss_sim {
     ss::Level lv[SS_MAX_LEVELS];
     float* p[SS_MAX_LEVELS] = {};
     float* r[SS_MAX_LEVELS] = {};
+    float* p_alt[SS_MAX_LEVELS] = {};   // second buffer of the tiled sweep (p_in -> p_out)
+    float* r_alt[SS_MAX_LEVELS] = {};   // second buffer of the fused in-place residual (L >= 1)
     float* alpha[SS_MAX_LEVELS] = {};   // coarse solid fraction (L >= 1), FP16-rounded values
     float* div0 = nullptr;              // level-0 divergence, smoother boundary rule
     float* div0r = nullptr;             // residual boundary rule (== div0 when enclosed)
     float* vort = nullptr;              // 3*ncell (2D: ncell) vorticity scratch
+    float* rhs_s = nullptr;             // level-0 rho*h*div/dt of the current solve, colour-split (k_rb.cu)
+    float* rhs_r = nullptr;             // level-0 rho*div/(dt*h) of the current solve, colour-split
+    uint8_t* rb_mask = nullptr;         // colour-split copy of fmask
     ss::ReduceSlots red{};
 
     std::vector<ss_emitter> em;
@@ -76,6 +91,10 @@ struct ss_sim {
 
     ss_stats st{};
     long long nlaunch = 0;     // kernels launched since the counter was reset
+    int* d_err = nullptr;      // device error word: bit 0 = a bounded barrier wait gave up
+    int use_tma = 1;           // TMA tile loads in the coarse-level sweeps where the layout allows
+    int rb_active = 0;         // level-0 pressure currently lives colour-split in p_alt[0]
+    std::vector<ss::TensorMapEntry> tmaps;
     cudaStream_t stream0 = nullptr;
 };
 
@@ -95,7 +114,9 @@ int launch_vorticity(ss_sim* s, const StepConsts& c, cudaStream_t st);
 int launch_update_velocities(ss_sim* s, const StepConsts& c, cudaStream_t st);
 int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st);
 // divergence of the current velocities into div0 (+div0r); optional ||div||^2 into slot
-int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st);
+// with sc and quirks >= 0 also the level-0 right-hand sides rhs_s / rhs_r of that boundary rule
+int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st, const StepConsts* sc = nullptr,
+                      int quirks = -1);
 
 // ---- multigrid kernels (k_mg.cu) ----
 int launch_smooth(ss_sim* s, const StepConsts& c, int L, int iterations, int quirks, cudaStream_t st);
@@ -109,6 +130,19 @@ int launch_solid_pyramid(ss_sim* s, cudaStream_t st);
 constexpr int kBottomSmemBytes = 160 * 1024;
 int bottom_start(const ss_sim* s);
 int launch_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, cudaStream_t st);
+// one red-black sweep per launch, tiled in shared memory (k_rbgs.cu)
+int launch_rbgs_sweep(ss_sim* s, const StepConsts& c, int L, int quirks, bool prolong, bool resid,
+                      cudaStream_t st);
+// the same sweep with the tile fetched by TMA (k_rbgs_tma.cu); 3D, nx % 16 == 0
+bool tma_sweep_supported(const ss_sim* s, int L);
+int launch_rbgs_sweep_tma(ss_sim* s, const StepConsts& c, int L, int quirks, bool resid, cudaStream_t st);
+// level 0 on colour-split arrays during a solve (k_rb.cu)
+bool rb_supported(const ss_sim* s, int quirks);
+int launch_rb_convert(ss_sim* s, bool split, cudaStream_t st);
+int launch_rb_split_mask(ss_sim* s, cudaStream_t st);
+int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st);
+int launch_rb_residual_restrict(ss_sim* s, cudaStream_t st);
+int launch_rb_prolong(ss_sim* s, cudaStream_t st);
 
 // ---- scene kernels (k_scene.cu) ----
 int launch_rasterize(ss_sim* s, cudaStream_t st);

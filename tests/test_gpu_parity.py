@@ -241,3 +241,35 @@ def test_workload_scene_steps(workload):
         g.step(sc["params"])
         o.step(sc["params"])
     assert_same(g, o, dim, workload)
+
+
+# Grids whose level-0 (and, for the last one, level-1) row pitch is a multiple
+# of 16 bytes of flags: the red-black sweeps fetch their tiles with TMA there.
+TMA_GRIDS = [
+    ("3d_tma", 3, (32, 24, 20), 1, 1, 4),
+    ("3d_tma_open_rgb", 3, (48, 32, 36), 3, 0, 4),
+    ("3d_tma_l1", 3, (64, 48, 48), 1, 1, 8),
+]
+
+
+@pytest.mark.parametrize("name,dim,n,nch,enc,mc", TMA_GRIDS)
+@pytest.mark.parametrize("quirks", [1, 0])
+def test_v_cycle_bitwise_tma(name, dim, n, nch, enc, mc, quirks):
+    g, o = make_pair(dim, n, nch, enc, seed=13, min_coarse=mc)
+    p = scene.workload_params(ref_quirks=quirks, n_pre=2, n_post=2, n_coarse=12)
+    for _ in range(2):
+        g.v_cycle(p, 0)
+        o.v_cycle(0, p)
+    for L in range(g.levels):
+        assert np.array_equal(g.get_level(L, abi.LEVEL_PRESSURE), o.get_level(L, abi.LEVEL_PRESSURE)), f"p L{L}"
+        assert np.array_equal(g.get_level(L, abi.LEVEL_RESIDUAL), o.get_level(L, abi.LEVEL_RESIDUAL)) or L == 0, f"r L{L}"
+
+
+@pytest.mark.parametrize("name,dim,n,nch,enc,mc", TMA_GRIDS)
+def test_full_step_bitwise_tma(name, dim, n, nch, enc, mc):
+    g, o = make_pair(dim, n, nch, enc, seed=17, min_coarse=mc, t_amb=0.1)
+    p = scene.workload_params(t_ambient=0.1, n_coarse=20, n_pre=3, n_post=1)
+    for k in range(2):
+        g.step(p)
+        o.step(p)
+        assert_same(g, o, dim, f"tma full step {k}")
