@@ -85,6 +85,7 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->rhs_s);
     cudaFree(s->fmask);
     cudaFree(s->rb_mask);
+    cudaFree(s->rb_pw);
     cudaFree(s->rhs_r);
     cudaFree(s->red.partial);
     cudaFree(s->red.out);
@@ -261,6 +262,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->d_err, 0, sizeof(int), st), "memset");
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->div0, 0, s->ncell * 4, st), "memset");
     if (!rc && s->div0r != s->div0) rc = check_cuda(cudaMemsetAsync(s->div0r, 0, s->ncell * 4, st), "memset");
+    if (!rc && s->rb_mask) rc = rb_init_vector_paths(s, st);
     if (!rc) rc = ss_set_scene(s, nullptr, 0, nullptr, 0, nullptr, 0, stream);
     if (!rc) rc = check_cuda(cudaStreamSynchronize(st), "create sync");
     if (rc) {

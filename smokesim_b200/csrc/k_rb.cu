@@ -13,6 +13,9 @@
 // 77-130 (value-identical; fluid mask with select instead of p*f, the division
 // by the fluid-neighbour count through div_by_count, right-hand sides
 // precomputed with the reference's operations by k_divergence).
+#include <cmath>
+#include <vector>
+
 #include "common.cuh"
 #include "ss_internal.h"
 
@@ -169,6 +172,231 @@ __global__ void __launch_bounds__(256) k_rb_prolong(float* __restrict__ p_red, f
     dst[i] = dst[i] + s;
 }
 
+// ------------------------------------------------------------------ 4 cells per thread
+// With nx % 8 == 0 every colour row holds a whole number of float4 quads, so
+// a thread takes four consecutive same-colour cells of a row: one float4 of
+// each neighbouring row of the other colour, one of its own row plus one
+// scalar for the row-end neighbour, a float4 of right-hand sides and the four
+// mask bytes in one word.  Same values as the one-cell kernels above: the
+// neighbour sum keeps the order +y, -y, +x, -x, +z, -z and selects 0 for a
+// non-fluid or out-of-grid neighbour.
+SS_D float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+SS_D float f4(const float4& v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, const float* __restrict__ po,
+                                                    const float* __restrict__ rhs_c, const uint8_t* __restrict__ mask_c,
+                                                    RBLevel g, int colour) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (q >= (g.half >> 2) || y >= g.ny) return;
+    const int xh0 = q << 2;
+    const int i = (z * g.ny + y) * g.half + xh0;
+    const uint32_t m4 = __ldg(reinterpret_cast<const uint32_t*>(mask_c + i));
+    if ((m4 & 0x01010101u) == 0) return;
+    const int par = (y + z + colour) & 1;   // x = 2*xh + par
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 pt = y + 1 < g.ny ? ldg4(po + i + g.half) : zero;
+    const float4 pb = y > 0 ? ldg4(po + i - g.half) : zero;
+    const float4 pm = ldg4(po + i);
+    float4 pf = zero, pk = zero;
+    if constexpr (DIM == 3) {
+        const int pl = g.ny * g.half;
+        if (z + 1 < g.nz) pf = ldg4(po + i + pl);
+        if (z > 0) pk = ldg4(po + i - pl);
+    }
+    // row-end neighbour: left of the first cell (par 0) or right of the last (par 1)
+    const float extra = par == 0 ? (xh0 > 0 ? __ldg(po + i - 1) : 0.f) : (xh0 + 4 < g.half ? __ldg(po + i + 4) : 0.f);
+    const float4 rhs = ldg4(rhs_c + i);
+    float out[4];
+    bool wr[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t m = (m4 >> (8 * k)) & 0xFFu;
+        const int fs = __popc(m & 0x7Eu);
+        wr[k] = (m & M_FLUID) && fs != 0;
+        const float left = par ? f4(pm, k) : (k ? f4(pm, k - 1) : extra);
+        const float right = par ? (k < 3 ? f4(pm, k + 1) : extra) : f4(pm, k);
+        float sum = ((m & M_TOP) ? f4(pt, k) : 0.f) + ((m & M_BOTTOM) ? f4(pb, k) : 0.f);
+        sum = sum + ((m & M_RIGHT) ? right : 0.f);
+        sum = sum + ((m & M_LEFT) ? left : 0.f);
+        if constexpr (DIM == 3) {
+            sum = sum + ((m & M_FRONT) ? f4(pf, k) : 0.f);
+            sum = sum + ((m & M_BACK) ? f4(pk, k) : 0.f);
+        }
+        out[k] = wr[k] ? div_by_count(sum - f4(rhs, k), fs) : 0.f;
+    }
+    if (wr[0] && wr[1] && wr[2] && wr[3]) {
+        *reinterpret_cast<float4*>(pc + i) = make_float4(out[0], out[1], out[2], out[3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (wr[k]) pc[i + k] = out[k];
+    }
+}
+
+// Residual of the fine cells under four consecutive coarse cells of a row,
+// restricted: per fine row the even-x cells sit in one colour array and the
+// odd-x cells in the other, both at the coarse x index.
+template <int DIM, bool POW2>
+__global__ void __launch_bounds__(256) k_rb_residual_restrict4(const float* __restrict__ p_red, const float* __restrict__ p_black,
+                                                               const float* __restrict__ rr_red, const float* __restrict__ rr_black,
+                                                               const uint8_t* __restrict__ m_red, const uint8_t* __restrict__ m_black,
+                                                               RBLevel g, float* __restrict__ rc, int cx, int cy,
+                                                               float hh, float inv_hh) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int Y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int Z = blockIdx.z;
+    if (q >= (cx >> 2) || Y >= cy) return;
+    const int X0 = q << 2;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int pl = g.ny * g.half;
+    float v[2][2][2][4];   // [dz][dy][dx][k]
+#pragma unroll
+    for (int dz = 0; dz < (DIM == 3 ? 2 : 1); ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy) {
+            const int y = 2 * Y + dy, z = DIM == 3 ? 2 * Z + dz : 0;
+            const int c0 = (y + z) & 1;   // colour of the even-x cells of this row
+            const float* A0 = c0 ? p_black : p_red;
+            const float* A1 = c0 ? p_red : p_black;
+            const int i = (z * g.ny + y) * g.half + X0;
+            // own row: even cells in A0, odd cells in A1; neighbouring rows swap
+            const float4 e_m = ldg4(A0 + i), o_m = ldg4(A1 + i);
+            const bool up = y + 1 < g.ny, dn = y > 0;
+            const float4 e_t = up ? ldg4(A1 + i + g.half) : zero, o_t = up ? ldg4(A0 + i + g.half) : zero;
+            const float4 e_b = dn ? ldg4(A1 + i - g.half) : zero, o_b = dn ? ldg4(A0 + i - g.half) : zero;
+            float4 e_f = zero, o_f = zero, e_k = zero, o_k = zero;
+            if constexpr (DIM == 3) {
+                if (z + 1 < g.nz) { e_f = ldg4(A1 + i + pl); o_f = ldg4(A0 + i + pl); }
+                if (z > 0) { e_k = ldg4(A1 + i - pl); o_k = ldg4(A0 + i - pl); }
+            }
+            const float o_left = X0 > 0 ? __ldg(A1 + i - 1) : 0.f;            // x = 2*X0 - 1
+            const float e_right = X0 + 4 < g.half ? __ldg(A0 + i + 4) : 0.f;   // x = 2*X0 + 8
+            const uint32_t me = __ldg(reinterpret_cast<const uint32_t*>((c0 ? m_black : m_red) + i));
+            const uint32_t mo = __ldg(reinterpret_cast<const uint32_t*>((c0 ? m_red : m_black) + i));
+            const float4 re = ldg4((c0 ? rr_black : rr_red) + i);
+            const float4 ro = ldg4((c0 ? rr_red : rr_black) + i);
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const uint32_t m = ((dx ? mo : me) >> (8 * k)) & 0xFFu;
+                    float res = 0.f;
+                    if (m & M_FLUID) {
+                        float top, bot, left, right, front = 0.f, back = 0.f, own, rr;
+                        if (dx == 0) {
+                            top = f4(e_t, k); bot = f4(e_b, k);
+                            left = k ? f4(o_m, k - 1) : o_left;
+                            right = f4(o_m, k);
+                            if constexpr (DIM == 3) { front = f4(e_f, k); back = f4(e_k, k); }
+                            own = f4(e_m, k); rr = f4(re, k);
+                        } else {
+                            top = f4(o_t, k); bot = f4(o_b, k);
+                            left = f4(e_m, k);
+                            right = k < 3 ? f4(e_m, k + 1) : e_right;
+                            if constexpr (DIM == 3) { front = f4(o_f, k); back = f4(o_k, k); }
+                            own = f4(o_m, k); rr = f4(ro, k);
+                        }
+                        float sum = ((m & M_TOP) ? top : 0.f) + ((m & M_BOTTOM) ? bot : 0.f);
+                        sum = sum + ((m & M_RIGHT) ? right : 0.f);
+                        sum = sum + ((m & M_LEFT) ? left : 0.f);
+                        if constexpr (DIM == 3) {
+                            sum = sum + ((m & M_FRONT) ? front : 0.f);
+                            sum = sum + ((m & M_BACK) ? back : 0.f);
+                        }
+                        const float f_sum = (float)__popc(m & 0x7Eu);
+                        const float lap = sum - f_sum * own;
+                        res = rr - (POW2 ? lap * inv_hh : lap / hh);
+                    }
+                    v[dz][dy][dx][k] = res;
+                }
+        }
+    float out[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if constexpr (DIM == 3) {
+            const float bottom = v[0][0][0][k] + v[1][0][0][k] + v[0][0][1][k] + v[1][0][1][k];
+            const float top = v[0][1][0][k] + v[1][1][0][k] + v[0][1][1][k] + v[1][1][1][k];
+            out[k] = (bottom + top) / 8.f;
+        } else {
+            out[k] = (v[0][0][0][k] + v[0][0][1][k] + v[0][1][0][k] + v[0][1][1][k]) / 4.f;
+        }
+    }
+    *reinterpret_cast<float4*>(rc + (Z * cy + Y) * cx + X0) = make_float4(out[0], out[1], out[2], out[3]);
+}
+
+// prolong_pressure.comp:39-51 for the fine cells under four consecutive
+// coarse cells of a row; interpolation weights come from per-axis tables
+// computed with the same float expression as k_rb_prolong (whose lower
+// coarse index is x/2 - 1 + (x & 1), checked on the host when the tables are
+// made).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_rb_prolong4(float* __restrict__ p_red, float* __restrict__ p_black, RBLevel g,
+                                                     const float* __restrict__ pc, int cx, int cy, int cz,
+                                                     const float* __restrict__ pw) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int Y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int Z = blockIdx.z;
+    if (q >= (cx >> 2) || Y >= cy) return;
+    const int X0 = q << 2;
+    const float* wxt = pw;
+    const float* wyt = pw + g.nx;
+    const float* wzt = pw + g.nx + g.ny;
+    const int Ys[3] = {max(Y - 1, 0), Y, min(Y + 1, cy - 1)};
+    const int Zs[3] = {max(Z - 1, 0), Z, min(Z + 1, cz - 1)};
+    const int xl = max(X0 - 1, 0), xr = min(X0 + 4, cx - 1);
+    float wx[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) wx[j] = __ldg(wxt + 2 * X0 + j);
+#pragma unroll
+    for (int ez = 0; ez < (DIM == 3 ? 2 : 1); ++ez) {
+        const int z = DIM == 3 ? 2 * Z + ez : 0;
+        const float wz = DIM == 3 ? __ldg(wzt + z) : 0.f;
+        float R[2][3][6];   // [plane za/zb][row Y-1..Y+1][x X0-1..X0+4]
+#pragma unroll
+        for (int pz = 0; pz < (DIM == 3 ? 2 : 1); ++pz)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int base = ((DIM == 3 ? Zs[ez + pz] : 0) * cy + Ys[r]) * cx;
+                const float4 c = ldg4(pc + base + X0);
+                R[pz][r][0] = __ldg(pc + base + xl);
+                R[pz][r][1] = c.x; R[pz][r][2] = c.y; R[pz][r][3] = c.z; R[pz][r][4] = c.w;
+                R[pz][r][5] = __ldg(pc + base + xr);
+            }
+#pragma unroll
+        for (int ey = 0; ey < 2; ++ey) {
+            const int y = 2 * Y + ey;
+            const float wy = __ldg(wyt + y);
+            float se[4], so[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int lo = k + e, hi = k + e + 1;
+                    const float w = wx[2 * k + e];
+                    float sv = lerp_(lerp_(R[0][ey][lo], R[0][ey][hi], w), lerp_(R[0][ey + 1][lo], R[0][ey + 1][hi], w), wy);
+                    if constexpr (DIM == 3) {
+                        const float c1 = lerp_(lerp_(R[1][ey][lo], R[1][ey][hi], w), lerp_(R[1][ey + 1][lo], R[1][ey + 1][hi], w), wy);
+                        sv = lerp_(sv, c1, wz);
+                    }
+                    (e ? so : se)[k] = sv;
+                }
+            const int c0 = (y + z) & 1;
+            float* E = c0 ? p_black : p_red;
+            float* O = c0 ? p_red : p_black;
+            const int i = (z * g.ny + y) * g.half + X0;
+            float4 a = *reinterpret_cast<const float4*>(E + i);
+            a.x = a.x + se[0]; a.y = a.y + se[1]; a.z = a.z + se[2]; a.w = a.w + se[3];
+            *reinterpret_cast<float4*>(E + i) = a;
+            float4 b = *reinterpret_cast<const float4*>(O + i);
+            b.x = b.x + so[0]; b.y = b.y + so[1]; b.z = b.z + so[2]; b.w = b.w + so[3];
+            *reinterpret_cast<float4*>(O + i) = b;
+        }
+    }
+}
+
 // ------------------------------------------------------------------ host
 // 256-thread blocks over rows of length n: n threads (rounded up to a warp)
 // along x, the rest of the block on successive rows
@@ -217,11 +445,16 @@ int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st) {
     const float* rhs[2] = {s->rhs_s, s->rhs_s + h};
     const uint8_t* mask[2] = {s->rb_mask, s->rb_mask + h};
     dim3 b, gr;
-    row_launch(g.half, g.ny, g.nz, b, gr);
+    row_launch(s->rb_vec ? g.half / 4 : g.half, g.ny, g.nz, b, gr);
     for (int it = 0; it < iterations; ++it)
         for (int c = 0; c < 2; ++c) {
-            if (s->dim == 3) k_rb_smooth<3><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
-            else k_rb_smooth<2><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
+            if (s->rb_vec) {
+                if (s->dim == 3) k_rb_smooth4<3><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
+                else k_rb_smooth4<2><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
+            } else {
+                if (s->dim == 3) k_rb_smooth<3><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
+                else k_rb_smooth<2><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
+            }
         }
     s->nlaunch += 2 * iterations;
     return check_cuda(cudaGetLastError(), "k_rb_smooth");
@@ -240,10 +473,24 @@ int launch_rb_residual_restrict(ss_sim* s, cudaStream_t st) {
     const float hh = s->lv[0].hh;
     const bool p2 = pow2f(hh);
     dim3 b, gr;
-    row_launch(cx, cy, cz, b, gr);
     const float* pr = s->p_alt[0];
     const float* pb = pr + h;
     const float* rr = s->rhs_r;
+    if (s->rb_vec) {
+        row_launch(cx / 4, cy, cz, b, gr);
+        const uint8_t* mr = s->rb_mask;
+        const uint8_t* mb = s->rb_mask + h;
+        if (s->dim == 3) {
+            if (p2) k_rb_residual_restrict4<3, true><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, s->r[1], cx, cy, hh, 1.f / hh);
+            else k_rb_residual_restrict4<3, false><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, s->r[1], cx, cy, hh, 0.f);
+        } else {
+            if (p2) k_rb_residual_restrict4<2, true><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, s->r[1], cx, cy, hh, 1.f / hh);
+            else k_rb_residual_restrict4<2, false><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, s->r[1], cx, cy, hh, 0.f);
+        }
+        s->nlaunch += 1;
+        return check_cuda(cudaGetLastError(), "k_rb_residual_restrict4");
+    }
+    row_launch(cx, cy, cz, b, gr);
     if (s->dim == 3) {
         if (p2) k_rb_residual_restrict<3, true><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, s->rb_mask, s->rb_mask + h, g, s->r[1], cx, cy, cz, hh, 1.f / hh);
         else k_rb_residual_restrict<3, false><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, s->rb_mask, s->rb_mask + h, g, s->r[1], cx, cy, cz, hh, 0.f);
@@ -259,11 +506,56 @@ int launch_rb_prolong(ss_sim* s, cudaStream_t st) {
     const RBLevel g = rb_level(s);
     const size_t h = s->ncell / 2;
     const int cx = s->lv[1].n[0], cy = s->lv[1].n[1], cz = s->lv[1].n[2];
+    if (s->rb_prolong_vec) {
+        dim3 b, gr;
+        row_launch(cx / 4, cy, cz, b, gr);
+        if (s->dim == 3) k_rb_prolong4<3><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, s->p[1], cx, cy, cz, s->rb_pw);
+        else k_rb_prolong4<2><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, s->p[1], cx, cy, cz, s->rb_pw);
+        s->nlaunch += 1;
+        return check_cuda(cudaGetLastError(), "k_rb_prolong4");
+    }
     dim3 b(128), gr((g.nx + 127) / 128, g.ny, g.nz);
     if (s->dim == 3) k_rb_prolong<3><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, s->p[1], cx, cy, cz);
     else k_rb_prolong<2><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, s->p[1], cx, cy, cz);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_rb_prolong");
+}
+
+// Per-axis weight of the fine cell's coarse interpolation, the float
+// expression of k_rb_prolong; returns false when the lower coarse index does
+// not follow x/2 - 1 + (x & 1) (clamped) on this axis.
+static bool prolong_axis_table(int n, int c, float* w) {
+    if (n != 2 * c || c < 1) return false;
+    for (int x = 0; x < n; ++x) {
+        volatile float a = (float)x + 0.5f;
+        volatile float b = a / (float)n;
+        volatile float t = b * (float)c;
+        volatile float tx = t - 0.5f;
+        const float fx = floorf(tx);
+        if ((int)fx != x / 2 - 1 + (x & 1)) return false;
+        volatile float wv = tx - fx;
+        w[x] = wv;
+    }
+    return true;
+}
+
+int rb_init_vector_paths(ss_sim* s, cudaStream_t st) {
+    s->rb_vec = (s->nx % 8) == 0 ? 1 : 0;
+    s->rb_prolong_vec = 0;
+    if (!s->rb_vec) return SS_OK;
+    const int nx = s->lv[0].n[0], ny = s->lv[0].n[1], nz = s->lv[0].n[2];
+    const int cx = s->lv[1].n[0], cy = s->lv[1].n[1], cz = s->lv[1].n[2];
+    std::vector<float> w((size_t)nx + ny + nz, 0.f);
+    bool ok = prolong_axis_table(nx, cx, w.data()) && prolong_axis_table(ny, cy, w.data() + nx);
+    if (s->dim == 3) ok = ok && prolong_axis_table(nz, cz, w.data() + nx + ny);
+    if (!ok) return SS_OK;
+    int rc = check_cuda(cudaMalloc((void**)&s->rb_pw, w.size() * sizeof(float)), "cudaMalloc");
+    if (rc) return rc;
+    rc = check_cuda(cudaMemcpyAsync(s->rb_pw, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, st), "weights upload");
+    if (rc) return rc;
+    rc = check_cuda(cudaStreamSynchronize(st), "weights upload");
+    if (!rc) s->rb_prolong_vec = 1;
+    return rc;
 }
 
 }  // namespace ss

@@ -78,6 +78,9 @@ struct ss_sim {
     float* rhs_s = nullptr;             // level-0 rho*h*div/dt of the current solve, colour-split (k_rb.cu)
     float* rhs_r = nullptr;             // level-0 rho*div/(dt*h) of the current solve, colour-split
     uint8_t* rb_mask = nullptr;         // colour-split copy of fmask
+    float* rb_pw = nullptr;             // level-0 prolongation weights per axis (x, then y, then z)
+    int rb_vec = 0;                     // level-0 kernels may work on 4 cells per thread (nx % 8 == 0)
+    int rb_prolong_vec = 0;             // ... and the prolongation too (even sizes, table pattern checked)
     ss::ReduceSlots red{};
 
     std::vector<ss_emitter> em;
@@ -143,6 +146,7 @@ int launch_rb_split_mask(ss_sim* s, cudaStream_t st);
 int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st);
 int launch_rb_residual_restrict(ss_sim* s, cudaStream_t st);
 int launch_rb_prolong(ss_sim* s, cudaStream_t st);
+int rb_init_vector_paths(ss_sim* s, cudaStream_t st);
 
 // ---- scene kernels (k_scene.cu) ----
 int launch_rasterize(ss_sim* s, cudaStream_t st);

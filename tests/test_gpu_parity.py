@@ -20,6 +20,10 @@ GRIDS = [
     ("2d_rgb_open", 2, (33, 40, 1), 3, 0),
     ("3d_odd", 3, (19, 17, 13), 1, 1),
     ("3d_rgb_open", 3, (16, 21, 18), 3, 0),
+    # nx % 8 == 0: the level-0 kernels take four cells per thread
+    ("2d_quad", 2, (64, 40, 1), 1, 1),
+    ("2d_quad_open_rgb", 2, (48, 34, 1), 3, 0),
+    ("3d_quad_odd_y", 3, (24, 19, 18), 1, 1),
 ]
 
 
