@@ -115,7 +115,8 @@ enum ss_stage_bits {
 
 enum ss_precision {
     SS_PREC_FP32 = 0,       /* FP32 V-cycles on the pressure itself */
-    SS_PREC_MIXED = 1       /* FP64 fine residual + refinement, FP32 smoothing, FP16 coarse corrections */
+    SS_PREC_MIXED = 1,      /* FP64 fine residual + refinement, FP32 smoothing, FP16 coarse corrections */
+    SS_PREC_MIXED_BF16 = 2  /* the same with BF16 coarse corrections */
 };
 
 /* Multigrid schedule.  Reference: 1 V-cycle per frame, 16 pre- and 16

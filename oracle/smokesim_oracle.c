@@ -63,10 +63,25 @@ typedef struct og_sim {
     ss_box* bx; int nb;
     int fp16_smoke, fp16_vort;  /* optional reference storage rounding (RGBA16F textures) */
     ss_stats st;
+    /* mixed-precision projection: FP64 level-0 pressure and the rounding
+     * (0 none, SS_PREC_MIXED FP16, SS_PREC_MIXED_BF16) of every coarse-level
+     * store of the correction V-cycle */
+    double* p64;
+    int p64_valid;
+    int cround;
 } og_sim;
 
 /* ---------------------------------------------------------------- helpers */
 static inline real f16(real x) { return (real)(_Float16)x; }
+/* float -> bfloat16 -> float, round to nearest even (finite values) */
+static inline real bf16(real x) {
+    float f = (float)x;
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+    memcpy(&f, &u, 4);
+    return (real)f;
+}
 static inline real lerp_(real a, real b, real t) { return a * ((real)1 - t) + b * t; }
 static inline real clampt(real t, real lo, real hi) { return fmin(fmax(t, lo), hi); }
 
@@ -222,6 +237,7 @@ void og_destroy(og_sim* s) {
         for (int c = 0; c < 4; ++c) free(s->solid[l][c]);
     }
     free(s->em); free(s->ob); free(s->bx);
+    free(s->p64);
     free(s);
 }
 
@@ -620,6 +636,10 @@ static void apply_vorticity_impl(og_sim* s, real dt, real eps_conf, real rho) {
 
 /* ------------------------------------------------------------- multigrid */
 static inline real hL(const og_sim* s, int L) { return s->h * (real)(1 << L); }
+/* value kept by a coarse-level store of the mixed-precision correction solve */
+static inline real cstore(const og_sim* s, real v) {
+    return s->cround == SS_PREC_MIXED ? f16(v) : s->cround == SS_PREC_MIXED_BF16 ? bf16(v) : v;
+}
 
 /* level-0 divergence with solid-velocity substitution; `oob_solid` selects the
  * residual kernel's out-of-grid rule (solid, vec4(0,0,0,1)) instead of the
@@ -701,7 +721,7 @@ void og_smooth_mode(og_sim* s, int L, int iterations, real dt, real rho, int qui
                     real p;
                     if (L == 0) p = (p_sum - rho * h * delta_v / dt) / f_sum;
                     else p = (p_sum - delta_v * (h * h)) / f_sum;
-                    P[ic] = p;
+                    P[ic] = L > 0 ? cstore(s, p) : p;
 #undef A_
 #undef P_
                 }
@@ -769,7 +789,7 @@ void og_compute_restrict(og_sim* s, int L) {
                 if (d3) {
                     real bottom = R[I3(X, Y, Z, fx, fy)] + R[I3(X, Y, Z + 1, fx, fy)] + R[I3(X + 1, Y, Z, fx, fy)] + R[I3(X + 1, Y, Z + 1, fx, fy)];
                     real top = R[I3(X, Y + 1, Z, fx, fy)] + R[I3(X, Y + 1, Z + 1, fx, fy)] + R[I3(X + 1, Y + 1, Z, fx, fy)] + R[I3(X + 1, Y + 1, Z + 1, fx, fy)];
-                    RC[o] = (bottom + top) / (real)8;
+                    RC[o] = cstore(s, (bottom + top) / (real)8);
                     for (int c = 0; c < 4; ++c) {
                         const real* S = s->solid[L][c];
                         real b = S[I3(X, Y, Z, fx, fy)] + S[I3(X, Y, Z + 1, fx, fy)] + S[I3(X + 1, Y, Z, fx, fy)] + S[I3(X + 1, Y, Z + 1, fx, fy)];
@@ -778,7 +798,7 @@ void og_compute_restrict(og_sim* s, int L) {
                     }
                 } else {
                     real sum = R[I3(X, Y, 0, fx, fy)] + R[I3(X + 1, Y, 0, fx, fy)] + R[I3(X, Y + 1, 0, fx, fy)] + R[I3(X + 1, Y + 1, 0, fx, fy)];
-                    RC[o] = sum / (real)4;
+                    RC[o] = cstore(s, sum / (real)4);
                     for (int c = 0; c < 4; ++c) {
                         const real* S = s->solid[L][c];
                         real sm = S[I3(X, Y, 0, fx, fy)] + S[I3(X + 1, Y, 0, fx, fy)] + S[I3(X, Y + 1, 0, fx, fy)] + S[I3(X + 1, Y + 1, 0, fx, fy)];
@@ -807,7 +827,8 @@ void og_prolong_and_add(og_sim* s, int L) {
                 real ty = (((real)y + hf) / (real)ay) * (real)cy - hf;
                 real tz = (((real)z + hf) / (real)az) * (real)cz - hf;
                 size_t i = I3(x, y, z, ax, ay);
-                P[i] = P[i] + sample_edge(PC, s->dim, cx, cy, cz, tx, ty, tz);
+                P[i] = L > 0 ? cstore(s, P[i] + sample_edge(PC, s->dim, cx, cy, cz, tx, ty, tz))
+                             : P[i] + sample_edge(PC, s->dim, cx, cy, cz, tx, ty, tz);
             }
 }
 
@@ -879,9 +900,208 @@ double og_projected_residual_norm(og_sim* s, real dt, real rho) {
     return sqrt(acc);
 }
 
+/* ------------------------------------------- mixed-precision projection
+ * Extension (no counterpart in the reference).  Iterative refinement of an
+ * FP64 level-0 pressure: the FP64 residual of the projection
+ *   rho_i = div_i - k (sum_{fluid nb} p_j - n_i p_i),  k = dt/(rho h),
+ * is the right-hand side of one correction V-cycle (level 0 in `real`,
+ * coarse levels rounded to FP16/BF16 on every store, the restricted residual
+ * scaled by a power of two first), and the correction is added in FP64.
+ * Level-0 operators use the corrected out-of-grid rule (solid if enclosed). */
+static inline int fluid0(const og_sim* s, int x, int y, int z) {
+    if (x < 0 || y < 0 || z < 0 || x >= NX || y >= NY || z >= NZ) return !s->enclosed;
+    return alpha0(s, x, y, z) < 1;
+}
+static inline int ingrid(const og_sim* s, int x, int y, int z) {
+    return !(x < 0 || y < 0 || z < 0 || x >= NX || y >= NY || z >= NZ);
+}
+static const int OFF6[6][3] = {{0, 1, 0}, {0, -1, 0}, {1, 0, 0}, {-1, 0, 0}, {0, 0, 1}, {0, 0, -1}};
+
+/* red-black sweeps on e with the level-0 right-hand side rhs_s */
+static void mx_smooth0(og_sim* s, real* e, const real* rhs_s, int iterations) {
+    const int nn = s->dim == 3 ? 6 : 4;
+    for (int it = 0; it < 2 * iterations; ++it) {
+        const int parity = it & 1;
+        OMP_FOR
+        for (int z = 0; z < NZ; ++z)
+            for (int y = 0; y < NY; ++y)
+                for (int x = 0; x < NX; ++x) {
+                    if (((x + y + z) & 1) != parity || !fluid0(s, x, y, z)) continue;
+                    real sum = 0;
+                    int fs = 0;
+                    for (int q = 0; q < nn; ++q) {
+                        int X = x + OFF6[q][0], Y = y + OFF6[q][1], Z = z + OFF6[q][2];
+                        if (!fluid0(s, X, Y, Z)) continue;
+                        ++fs;
+                        real v = ingrid(s, X, Y, Z) ? e[I3(X, Y, Z, NX, NY)] : (real)0;
+                        sum = q == 0 ? v : sum + v;
+                    }
+                    if (fs == 0) continue;
+                    e[I3(x, y, z, NX, NY)] = (sum - rhs_s[I3(x, y, z, NX, NY)]) / (real)fs;
+                }
+    }
+}
+
+/* residual of the correction equation at level 0, restricted into r[1]
+ * (scaled, rounded to the coarse storage) */
+static void mx_residual_restrict0(og_sim* s, const real* e, const real* rhs_r, real scale) {
+    const int nn = s->dim == 3 ? 6 : 4;
+    const real hh = hL(s, 0) * hL(s, 0);
+    const int cx = s->ls[1][0], cy = s->ls[1][1], cz = s->ls[1][2];
+    real* RC = s->r[1];
+    OMP_FOR
+    for (int Z = 0; Z < cz; ++Z)
+        for (int Y = 0; Y < cy; ++Y)
+            for (int X = 0; X < cx; ++X) {
+                real v[2][2][2];
+                for (int dz = 0; dz < (s->dim == 3 ? 2 : 1); ++dz)
+                    for (int dy = 0; dy < 2; ++dy)
+                        for (int dx = 0; dx < 2; ++dx) {
+                            int x = 2 * X + dx, y = 2 * Y + dy, z = s->dim == 3 ? 2 * Z + dz : 0;
+                            real res = 0;
+                            if (fluid0(s, x, y, z)) {
+                                real sum = 0;
+                                int fs = 0;
+                                for (int q = 0; q < nn; ++q) {
+                                    int XX = x + OFF6[q][0], YY = y + OFF6[q][1], ZZ = z + OFF6[q][2];
+                                    real w = 0;
+                                    if (fluid0(s, XX, YY, ZZ)) {
+                                        ++fs;
+                                        if (ingrid(s, XX, YY, ZZ)) w = e[I3(XX, YY, ZZ, NX, NY)];
+                                    }
+                                    sum = q == 0 ? w : sum + w;
+                                }
+                                const size_t c = I3(x, y, z, NX, NY);
+                                real lap = sum - (real)fs * e[c];
+                                res = rhs_r[c] - lap / hh;
+                            }
+                            v[dz][dy][dx] = res;
+                        }
+                real out;
+                if (s->dim == 3) {
+                    real bottom = v[0][0][0] + v[1][0][0] + v[0][0][1] + v[1][0][1];
+                    real top = v[0][1][0] + v[1][1][0] + v[0][1][1] + v[1][1][1];
+                    out = (bottom + top) / (real)8;
+                } else {
+                    out = (v[0][0][0] + v[0][0][1] + v[0][1][0] + v[0][1][1]) / (real)4;
+                }
+                RC[I3(X, Y, Z, cx, cy)] = cstore(s, out * scale);
+            }
+}
+
+/* e += (trilinear of p[1]) / scale on every level-0 cell */
+static void mx_prolong0(og_sim* s, real* e, real inv_scale) {
+    const int cx = s->ls[1][0], cy = s->ls[1][1], cz = s->ls[1][2];
+    const real* PC = s->p[1];
+    const real hf = (real)0.5;
+    OMP_FOR
+    for (int z = 0; z < NZ; ++z)
+        for (int y = 0; y < NY; ++y)
+            for (int x = 0; x < NX; ++x) {
+                real tx = (((real)x + hf) / (real)NX) * (real)cx - hf;
+                real ty = (((real)y + hf) / (real)NY) * (real)cy - hf;
+                real tz = (((real)z + hf) / (real)NZ) * (real)cz - hf;
+                size_t i = I3(x, y, z, NX, NY);
+                real sv = sample_edge(PC, s->dim, cx, cy, cz, tx, ty, tz) * inv_scale;
+                e[i] = e[i] + sv;
+            }
+}
+
+/* FP64 residual of the projection; right-hand sides of the correction
+ * equation; returns sum of squares and stores max|rho| */
+static double mx_ir_residual(og_sim* s, real dt, real rho, real* rhs_s, real* rhs_r, double* amax_out) {
+    const int nn = s->dim == 3 ? 6 : 4;
+    const double k = (double)dt / ((double)rho * (double)s->h);
+    const double inv_k = 1.0 / k;
+    const real hh = hL(s, 0) * hL(s, 0);
+    const double inv_khh = 1.0 / (k * (double)hh);
+    double acc = 0, amax = 0;
+#pragma omp parallel for collapse(2) reduction(+ : acc) reduction(max : amax) schedule(static)
+    for (int z = 0; z < NZ; ++z)
+        for (int y = 0; y < NY; ++y)
+            for (int x = 0; x < NX; ++x) {
+                const size_t c = I3(x, y, z, NX, NY);
+                rhs_s[c] = 0;
+                rhs_r[c] = 0;
+                if (!fluid0(s, x, y, z)) continue;
+                double sum = 0;
+                int cnt = 0;
+                for (int q = 0; q < nn; ++q) {
+                    int X = x + OFF6[q][0], Y = y + OFF6[q][1], Z = z + OFF6[q][2];
+                    double w = 0;
+                    if (fluid0(s, X, Y, Z)) {
+                        ++cnt;
+                        if (ingrid(s, X, Y, Z)) w = s->p64[I3(X, Y, Z, NX, NY)];
+                    }
+                    sum = q == 0 ? w : sum + w;
+                }
+                const double d = (double)delta_v0(s, x, y, z, 0);
+                const double r = d - k * (sum - (double)cnt * s->p64[c]);
+                acc += r * r;
+                if (fabs(r) > amax) amax = fabs(r);
+                rhs_s[c] = (real)(r * inv_k);
+                rhs_r[c] = (real)(r * inv_khh);
+            }
+    *amax_out = amax * inv_khh;
+    return acc;
+}
+
+static int og_mixed_pressure_solve(og_sim* s, const ss_mg_schedule* mg, real dt, real rho) {
+    if (s->levels < 2 || NX % 2 != 0 || mg->ref_quirks) return 0;
+    ss_mg_schedule m2 = *mg;
+    m2.ref_quirks = 0;
+    if (!s->p64) s->p64 = (double*)calloc(s->ncell, sizeof(double));
+    if (!s->p64_valid) {
+        for (size_t i = 0; i < s->ncell; ++i) s->p64[i] = (double)s->p[0][i];
+        s->p64_valid = 1;
+    }
+    real* e = (real*)malloc(sizeof(real) * s->ncell);
+    real* rhs_s = (real*)malloc(sizeof(real) * s->ncell);
+    real* rhs_r = (real*)malloc(sizeof(real) * s->ncell);
+    const double db = og_divergence_norm(s);
+    const int tol_mode = mg->tol > 0;
+    const int cap = mg->n_vcycles > 0 ? mg->n_vcycles : 1;
+    int done = 0, conv = 1;
+    double res = 0;
+    for (;;) {
+        double amax = 0;
+        res = sqrt(mx_ir_residual(s, dt, rho, rhs_s, rhs_r, &amax));
+        if (!tol_mode && done == cap) break;
+        if (tol_mode && res <= mg->tol * db) break;
+        if (done == cap) { conv = 0; break; }
+        int ex = 0;
+        frexp(amax, &ex);
+        ex = ex < -100 ? -100 : ex > 100 ? 100 : ex;
+        const real scale = (real)(float)ldexp(1.0, -ex), inv_scale = (real)(float)ldexp(1.0, ex);
+        memset(e, 0, sizeof(real) * s->ncell);
+        /* one V-cycle on e */
+        s->cround = mg->precision;
+        mx_smooth0(s, e, rhs_s, m2.n_pre);
+        og_compute_restrict(s, 0);          /* coarse solid pyramid (r[1] overwritten next) */
+        mx_residual_restrict0(s, e, rhs_r, scale);
+        memset(s->p[1], 0, sizeof(real) * (size_t)s->ls[1][0] * s->ls[1][1] * s->ls[1][2]);
+        og_v_cycle(s, 1, &m2, dt, rho);
+        mx_prolong0(s, e, inv_scale);
+        mx_smooth0(s, e, rhs_s, m2.n_post);
+        s->cround = 0;
+        for (size_t c = 0; c < s->ncell; ++c)
+            if (alpha0(s, (int)(c % NX), (int)((c / NX) % NY), (int)(c / ((size_t)NX * NY))) < 1) s->p64[c] += (double)e[c];
+        ++done;
+    }
+    for (size_t i = 0; i < s->ncell; ++i) s->p[0][i] = (real)s->p64[i];
+    free(e); free(rhs_s); free(rhs_r);
+    s->st.div_before = db;
+    s->st.residual = res;
+    s->st.vcycles = done;
+    s->st.converged = conv;
+    return conv;
+}
+
 /* multigrid_pressure_solve (common/physics/grid.c:173-175): n_vcycles V-cycles,
  * or (tol > 0) V-cycles until the projected residual <= tol * div_before. */
 int og_multigrid_pressure_solve(og_sim* s, const ss_mg_schedule* mg, real dt, real rho) {
+    if (mg->precision != SS_PREC_FP32) return og_mixed_pressure_solve(s, mg, dt, rho);
+    s->p64_valid = 0;
     double db = og_divergence_norm(s);
     s->st.div_before = db;
     int ncyc = mg->n_vcycles > 0 ? mg->n_vcycles : 1;
@@ -906,9 +1126,11 @@ int og_multigrid_pressure_solve(og_sim* s, const ss_mg_schedule* mg, real dt, re
 }
 
 /* update_vx/vy/vz (shaders3d/compute/update_vx.comp:45-62 and siblings; 2D :43-60). */
-static void update_velocities_impl(og_sim* s, real dt, real rho) {
+static void update_velocities_impl(og_sim* s, real dt, real rho, int use_p64) {
     const real k = -dt / (rho * s->h);
+    const double k64 = -(double)dt / ((double)rho * (double)s->h);
     const real* P = s->p[0];
+    const double* P64 = use_p64 ? s->p64 : NULL;
     for (int comp = 0; comp < s->dim; ++comp) {
         int ax = NX + (comp == 0), ay = NY + (comp == 1), az = NZ + (comp == 2);
         const real* src = comp == 0 ? CUR_VX : comp == 1 ? CUR_VY : CUR_VZ;
@@ -922,6 +1144,12 @@ static void update_velocities_impl(og_sim* s, real dt, real rho) {
                     if (solid_oob0(s, x, y, z) || solid_oob0(s, xm, ym, zm)) {
                         int oob = x >= NX || y >= NY || z >= NZ;
                         dst[i] = oob ? 0 : s->solid[0][comp][I3(x, y, z, NX, NY)];
+                        continue;
+                    }
+                    if (P64) {
+                        double q_hi = (x >= NX || y >= NY || z >= NZ) ? 0 : P64[I3(x, y, z, NX, NY)];
+                        double q_lo = (xm < 0 || ym < 0 || zm < 0) ? 0 : P64[I3(xm, ym, zm, NX, NY)];
+                        dst[i] = (real)((double)src[i] + k64 * (q_hi - q_lo));
                         continue;
                     }
                     real p_hi = (x >= NX || y >= NY || z >= NZ) ? 0 : P[I3(x, y, z, NX, NY)];
@@ -951,7 +1179,7 @@ void og_run_physics_step(og_sim* s, const ss_params* prm) {
     }
     if (m & SS_STAGE_RESOLVE_PRESSURE) og_multigrid_pressure_solve(s, &prm->mg, dt, rho);
     if (m & SS_STAGE_UPDATE_VELOCITIES) {
-        update_velocities_impl(s, dt, rho);
+        update_velocities_impl(s, dt, rho, prm->mg.precision != SS_PREC_FP32 && s->p64_valid);
         if (m & SS_STAGE_RESOLVE_PRESSURE) {
             s->st.div_after = og_divergence_norm(s);
             s->st.rel_div = s->st.div_before > 0 ? s->st.div_after / s->st.div_before : 0;
@@ -977,7 +1205,9 @@ void og_stage_apply_vorticity(og_sim* s, const ss_params* p) {
     calculate_vorticity_impl(s);
     apply_vorticity_impl(s, p->time_step, p->vorticity_confinement, p->density);
 }
-void og_stage_update_velocities(og_sim* s, const ss_params* p) { update_velocities_impl(s, p->time_step, p->density); }
+void og_stage_update_velocities(og_sim* s, const ss_params* p) {
+    update_velocities_impl(s, p->time_step, p->density, p->mg.precision != SS_PREC_FP32 && s->p64_valid);
+}
 void og_stage_advect_smoke(og_sim* s, const ss_params* p) { advect_smoke_impl(s, p->time_step, p->t_ambient); }
 void og_stage_handle_emitters(og_sim* s, const ss_params* p) {
     og_update_emitters_status(s, p->current_time);
@@ -1059,6 +1289,7 @@ int og_set_level(og_sim* s, int L, int what, const float* src, size_t count) {
     if (count != n) return SS_E_INVALID;
     real* d = what == 0 ? s->p[L] : s->r[L];
     for (size_t i = 0; i < n; ++i) d[i] = (real)src[i];
+    if (L == 0 && what == 0) s->p64_valid = 0;
     return 0;
 }
 /* Compute the coarse solid maps of every level (restrict_solid chain), as the

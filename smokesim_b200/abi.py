@@ -41,6 +41,7 @@ STAGE_ALL = 0xFF
 
 PREC_FP32 = 0
 PREC_MIXED = 1
+PREC_MIXED_BF16 = 2
 
 FIELD_VX = 0
 FIELD_VY = 1

@@ -86,6 +86,10 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->fmask);
     cudaFree(s->rb_mask);
     cudaFree(s->rb_pw);
+    cudaFree(s->p64);
+    cudaFree(s->d_scale);
+    cudaFree(s->red.partial_max);
+    for (int l = 0; l < SS_MAX_LEVELS; ++l) { cudaFree(s->cp[l]); cudaFree(s->cr[l]); }
     cudaFree(s->rhs_r);
     cudaFree(s->red.partial);
     cudaFree(s->red.out);
@@ -111,7 +115,7 @@ static int check_params(const ss_sim* s, const ss_params* p) {
     if (!(p->time_step > 0.f) || !(p->density > 0.f)) return set_error(SS_E_INVALID, "time_step and density must be > 0");
     if (p->mg.n_pre < 0 || p->mg.n_post < 0 || p->mg.n_coarse < 0 || p->mg.n_vcycles < 0 || p->mg.tol < 0)
         return set_error(SS_E_INVALID, "negative multigrid schedule entry");
-    if (p->mg.precision != SS_PREC_FP32 && p->mg.precision != SS_PREC_MIXED)
+    if (p->mg.precision != SS_PREC_FP32 && p->mg.precision != SS_PREC_MIXED && p->mg.precision != SS_PREC_MIXED_BF16)
         return set_error(SS_E_INVALID, "unknown precision mode");
     return SS_OK;
 }
@@ -523,6 +527,7 @@ int ss_clear_grid(ss_sim* s, float t_ambient, void* stream) {
         const size_t n = (size_t)s->lv[l].n[0] * s->lv[l].n[1] * s->lv[l].n[2];
         CU(cudaMemsetAsync(s->p[l], 0, n * 4, st), "memset");
     }
+    s->p64_valid = 0;
     CU(cudaStreamSynchronize(st), "clear sync");
     return SS_OK;
 }
@@ -562,6 +567,7 @@ int ss_set_level(ss_sim* s, int L, int what, const float* host, size_t count, vo
     float* d = what == SS_LEVEL_PRESSURE ? s->p[L] : what == SS_LEVEL_RESIDUAL ? s->r[L] : nullptr;
     if (!d) return set_error(SS_E_INVALID, "level array is read only");
     cudaStream_t st = as_stream(stream);
+    if (L == 0 && what == SS_LEVEL_PRESSURE) s->p64_valid = 0;
     CU(cudaMemcpyAsync(d, host, n * 4, cudaMemcpyHostToDevice, st), "set_level");
     CU(cudaStreamSynchronize(st), "sync");
     return SS_OK;
@@ -616,9 +622,110 @@ static int ensure_pyramid(ss_sim* s, cudaStream_t st) {
     return SS_OK;
 }
 
+// ------------------------------------------------------- mixed precision
+// Buffers of the mixed-precision solve, made on its first use: the FP64
+// level-0 pressure and 2-byte coarse levels.
+static int ensure_mixed(ss_sim* s, int prec, cudaStream_t st) {
+    if (!rb_supported(s, 0))
+        return set_error(SS_E_UNSUPPORTED, "the mixed-precision solve needs an even nx and at least two levels");
+    if (!s->p64) {
+        CU(cudaMalloc((void**)&s->p64, s->ncell * sizeof(double)), "cudaMalloc(p64)");
+        s->p64_valid = 0;
+    }
+    if (!s->red.partial_max)
+        CU(cudaMalloc((void**)&s->red.partial_max, (size_t)s->red.max_blocks * sizeof(double)), "cudaMalloc");
+    if (!s->d_scale) {
+        CU(cudaMalloc((void**)&s->d_scale, 2 * sizeof(float)), "cudaMalloc");
+        const float one[2] = {1.f, 1.f};
+        CU(cudaMemcpyAsync(s->d_scale, one, sizeof(one), cudaMemcpyHostToDevice, st), "scale init");
+        CU(cudaStreamSynchronize(st), "scale init");
+    }
+    for (int l = 1; l < s->levels; ++l) {
+        const size_t n = (size_t)s->lv[l].n[0] * s->lv[l].n[1] * s->lv[l].n[2];
+        if (!s->cp[l]) {
+            CU(cudaMalloc(&s->cp[l], n * 2), "cudaMalloc(coarse p)");
+            CU(cudaMemsetAsync(s->cp[l], 0, n * 2, st), "memset");
+        }
+        if (!s->cr[l]) {
+            CU(cudaMalloc(&s->cr[l], n * 2), "cudaMalloc(coarse r)");
+            CU(cudaMemsetAsync(s->cr[l], 0, n * 2, st), "memset");
+        }
+    }
+    s->cstore = prec;
+    return SS_OK;
+}
+
+// One V-cycle on the correction e (colour-split FP32 level 0 in p_alt[0],
+// coarse levels FP16/BF16), corrected operators (ref_quirks = 0).
+static int v_cycle_mixed(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int L, int prec, cudaStream_t st) {
+    if (L == 0) {
+        TRY(launch_rb_sweep(s, mg.n_pre, st));
+        TRY(launch_rb_residual_restrict_mixed(s, prec, st));
+        const size_t nc = (size_t)s->lv[1].n[0] * s->lv[1].n[1] * s->lv[1].n[2];
+        CU(cudaMemsetAsync(s->cp[1], 0, nc * 2, st), "clear coarse p");
+        TRY(v_cycle_mixed(s, c, mg, 1, prec, st));
+        TRY(launch_rb_prolong_mixed(s, prec, st));
+        return launch_rb_sweep(s, mg.n_post, st);
+    }
+    if (L >= s->bottom) return coarse_bottom(s, mg, L, prec, st);
+    if (L == s->levels - 1) return coarse_smooth(s, c, L, mg.n_coarse, prec, st);
+    TRY(coarse_smooth(s, c, L, mg.n_pre, prec, st));
+    TRY(coarse_residual_restrict(s, c, L, prec, st));
+    const size_t nc = (size_t)s->lv[L + 1].n[0] * s->lv[L + 1].n[1] * s->lv[L + 1].n[2];
+    CU(cudaMemsetAsync(s->cp[L + 1], 0, nc * 2, st), "clear coarse p");
+    TRY(v_cycle_mixed(s, c, mg, L + 1, prec, st));
+    TRY(coarse_prolong(s, L, prec, st));
+    return coarse_smooth(s, c, L, mg.n_post, prec, st);
+}
+
+// Mixed-precision projection: iterative refinement of the FP64 pressure with
+// FP32 V-cycles on the FP64 residual (k_mixed.cu).  Each refinement step
+// counts as one V-cycle in the statistics.
+static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts& c, cudaStream_t st) {
+    const ss_mg_schedule& mg = p->mg;
+    if (mg.ref_quirks) return set_error(SS_E_INVALID, "the mixed-precision solve runs the corrected operators (ref_quirks = 0)");
+    TRY(ensure_mixed(s, mg.precision, st));
+    TRY(ensure_pyramid(s, st));
+    const bool tol_mode = mg.tol > 0.0;
+    const bool stats = p->collect_stats || tol_mode;
+    TRY(launch_divergence(s, true, stats ? SLOT_DIV_BEFORE : -1, st));
+    if (!s->p64_valid) TRY(launch_p64_from_p0(s, st));
+    const int cap = mg.n_vcycles > 0 ? mg.n_vcycles : 1;
+    int done = 0;
+    double db = 0.0, res = 0.0;
+    bool conv = true;
+    for (;;) {
+        const bool last = !tol_mode && done == cap;
+        if (last && !stats) break;
+        TRY(launch_ir_residual(s, c, stats ? SLOT_RESIDUAL : -1, st));
+        if (tol_mode || last) {
+            TRY(read_slots(s, st));
+            db = sqrt(s->red.host[SLOT_DIV_BEFORE]);
+            res = sqrt(s->red.host[SLOT_RESIDUAL]);
+            if (last) break;
+            if (res <= mg.tol * db) break;
+            if (done == cap) { conv = false; break; }
+        }
+        CU(cudaMemsetAsync(s->p_alt[0], 0, s->ncell * sizeof(float), st), "clear correction");
+        TRY(v_cycle_mixed(s, c, mg, 0, mg.precision, st));
+        TRY(launch_ir_accumulate(s, st));
+        ++done;
+    }
+    TRY(launch_p0_from_p64(s, st));
+    if (stats) {
+        s->st.div_before = db;
+        s->st.residual = res;
+    }
+    s->st.vcycles = done;
+    s->st.converged = conv ? 1 : 0;
+    return SS_OK;
+}
+
 // multigrid_pressure_solve (common/physics/grid.c:173-175)
 static int pressure_solve(ss_sim* s, const ss_params* p, const StepConsts& c, cudaStream_t st) {
     const ss_mg_schedule& mg = p->mg;
+    if (mg.precision != SS_PREC_FP32) return pressure_solve_mixed(s, p, c, st);
+    s->p64_valid = 0;
     const bool tol_mode = mg.tol > 0.0;
     const bool stats = p->collect_stats || tol_mode;
     TRY(ensure_pyramid(s, st));
@@ -688,7 +795,8 @@ static int do_step(ss_sim* s, const ss_params* p, cudaStream_t st) {
     if (m & SS_STAGE_APPLY_VORTICITY) TRY(launch_vorticity(s, c, st));
     if (m & SS_STAGE_RESOLVE_PRESSURE) TRY(pressure_solve(s, p, c, st));
     if (m & SS_STAGE_UPDATE_VELOCITIES) {
-        TRY(launch_update_velocities(s, c, st));
+        if (p->mg.precision != SS_PREC_FP32 && s->p64_valid) TRY(launch_update_velocities_p64(s, c, st));
+        else TRY(launch_update_velocities(s, c, st));
         if ((m & SS_STAGE_RESOLVE_PRESSURE) && (p->collect_stats || p->mg.tol > 0.0)) {
             TRY(launch_divergence(s, false, SLOT_DIV_AFTER, st));
             TRY(read_slots(s, st));
@@ -769,6 +877,7 @@ int ss_multigrid_pressure_solve(ss_sim* s, const ss_params* p, void* stream) {
 
 int ss_v_cycle(ss_sim* s, const ss_params* p, int level, void* stream) {
     TRY(check_params(s, p));
+    if (level == 0) s->p64_valid = 0;
     if (level < 0 || level >= s->levels) return set_error(SS_E_INVALID, "level out of range");
     cudaStream_t st = as_stream(stream);
     TRY(ensure_pyramid(s, st));
@@ -787,6 +896,7 @@ int ss_v_cycle(ss_sim* s, const ss_params* p, int level, void* stream) {
 
 int ss_smooth(ss_sim* s, const ss_params* p, int level, int iterations, void* stream) {
     TRY(check_params(s, p));
+    if (level == 0) s->p64_valid = 0;
     if (level < 0 || level >= s->levels || iterations < 0) return set_error(SS_E_INVALID, "level/iterations out of range");
     cudaStream_t st = as_stream(stream);
     TRY(ensure_pyramid(s, st));
@@ -821,12 +931,15 @@ int ss_compute_restrict(ss_sim* s, const ss_params* p, int level, void* stream) 
 
 int ss_prolong_and_add(ss_sim* s, const ss_params* p, int level, void* stream) {
     TRY(check_params(s, p));
+    if (level == 0) s->p64_valid = 0;
     if (level < 0 || level >= s->levels) return set_error(SS_E_INVALID, "level out of range");
     return launch_prolong(s, level, as_stream(stream));
 }
 
 int ss_update_velocities(ss_sim* s, const ss_params* p, void* stream) {
     TRY(check_params(s, p));
+    if (p->mg.precision != SS_PREC_FP32 && s->p64_valid)
+        return launch_update_velocities_p64(s, make_consts(s, p), as_stream(stream));
     return launch_update_velocities(s, make_consts(s, p), as_stream(stream));
 }
 

@@ -11,6 +11,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
+#include <cuda_bf16.h>
 #include <stdint.h>
 
 #define SS_HD __host__ __device__ __forceinline__
@@ -222,6 +223,19 @@ SS_D float sample_taps_fast(const float* __restrict__ a, int ax, int ay, int az,
 }
 
 SS_D float round_half(float x) { return __half2float(__float2half_rn(x)); }
+
+// Storage types of the coarse multigrid levels: FP32, or FP16 / BF16 for the
+// corrections of the mixed-precision solve.  Arithmetic is FP32 throughout;
+// ld converts a stored value to float, st rounds to nearest even on store and
+// rnd<T> gives the float value that storing as T would keep.
+SS_D float ld(float v) { return v; }
+SS_D float ld(__half v) { return __half2float(v); }
+SS_D float ld(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <typename T> SS_D T st(float v);
+template <> SS_D float st<float>(float v) { return v; }
+template <> SS_D __half st<__half>(float v) { return __float2half_rn(v); }
+template <> SS_D __nv_bfloat16 st<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+template <typename T> SS_D float rnd(float v) { return ld(st<T>(v)); }
 
 // a / f for an integer count f in 1..6, value-identical to the IEEE quotient
 // (the same value; -0 may come back as +0): q0 = a*RN(1/f) followed by one

@@ -4,6 +4,8 @@
 // cited at the kernel.  Velocities are read from the current ping-pong buffer
 // and written to the other one (the reference's texture/image pairs,
 // 3d/grid3d.c:104-162), smoke likewise.
+#include <type_traits>
+
 #include "common.cuh"
 #include "ss_internal.h"
 
@@ -412,14 +414,16 @@ int launch_vorticity(ss_sim* s, const StepConsts& c, cudaStream_t st) {
 // update_vx/vy/vz (shaders3d/compute/update_vx.comp:45-62 and siblings; 2D
 // :43-60): faces touching solid (out of grid = fluid) take the solid map's
 // velocity of cell idx (0 outside the grid).
-template <int DIM>
-__global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const float* __restrict__ p) {
+// P = double: the mixed-precision solve's FP64 pressure; the face update is
+// then evaluated in FP64 (k64 = -dt/(rho h)) and rounded once to FP32.
+template <int DIM, typename P = float>
+__global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const P* __restrict__ p, double k64 = 0.0) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const bool in = x < nx && y < ny && z < nz;
-    const float pc = in ? __ldg(p + idx3(x, y, z, nx, ny)) : 0.f;
+    const P pc = in ? __ldg(p + idx3(x, y, z, nx, ny)) : P(0);
     const bool sc = in && (a.flags[idx3(x, y, z, nx, ny)] & F_SOLID);
 #pragma unroll
     for (int comp = 0; comp < DIM; ++comp) {
@@ -434,8 +438,9 @@ __global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const floa
             dst[i] = (in && sv) ? sv[idx3(x, y, z, nx, ny)] : 0.f;
             continue;
         }
-        const float plo = (xm < 0 || ym < 0 || zm < 0) ? 0.f : __ldg(p + idx3(xm, ym, zm, nx, ny));
-        dst[i] = __ldg(src + i) + a.c.k_upd * (pc - plo);
+        const P plo = (xm < 0 || ym < 0 || zm < 0) ? P(0) : __ldg(p + idx3(xm, ym, zm, nx, ny));
+        if constexpr (std::is_same<P, double>::value) dst[i] = (float)((double)__ldg(src + i) + k64 * (pc - plo));
+        else dst[i] = __ldg(src + i) + a.c.k_upd * (pc - plo);
     }
 }
 
@@ -448,6 +453,18 @@ int launch_update_velocities(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     for (int d = 0; d < s->dim; ++d) s->vi[d] ^= 1;
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_update_velocity");
+}
+
+int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st) {
+    FluidArgs a = fluid_args(s, c);
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, b);
+    const double k64 = -(double)c.dt / ((double)c.rho * (double)s->h);
+    if (s->dim == 3) k_update_velocity<3, double><<<g, b, 0, st>>>(a, s->p64, k64);
+    else k_update_velocity<2, double><<<g, b, 0, st>>>(a, s->p64, k64);
+    for (int d = 0; d < s->dim; ++d) s->vi[d] ^= 1;
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_update_velocity<p64>");
 }
 
 // ------------------------------------------------------------ smoke advection

@@ -12,9 +12,12 @@
 
 namespace ss {
 
-struct MGArgs {
-    float* __restrict__ p;
-    float* __restrict__ r;          // level right-hand side / residual (L >= 1)
+// T: storage type of p and r (float, or __half / __nv_bfloat16 on the coarse
+// levels of the mixed-precision solve)
+template <typename T>
+struct MGArgsT {
+    T* __restrict__ p;
+    T* __restrict__ r;              // level right-hand side / residual (L >= 1)
     const float* __restrict__ alpha;  // L >= 1
     const uint8_t* __restrict__ flags;  // L == 0
     const float* __restrict__ div0;   // L == 0, smoother rule
@@ -27,6 +30,7 @@ struct MGArgs {
     float rho;
     float dt_h;     // dt * h    (L == 0 residual)
 };
+using MGArgs = MGArgsT<float>;
 
 // Out-of-grid rule: ref_quirks keeps the reference's smoother (open, p = 0) /
 // residual (wall) mismatch; the corrected mode uses the physical rule of the
@@ -56,8 +60,10 @@ static MGArgs mg_args(ss_sim* s, const StepConsts& c, int L, float oobA) {
 // smooth.comp:79-136 (2D :74-123): red-black Gauss-Seidel in place; solid
 // cells and cells without fluid neighbours are skipped; out of grid = fluid
 // with p = 0.
-template <int DIM, bool L0>
-SS_D void smooth_cell(const MGArgs& a, int x, int y, int z) {
+// R: the type whose rounding every stored pressure gets (== T for global
+// arrays; the shared-memory bottom solve keeps float storage rounded as R).
+template <int DIM, bool L0, typename T = float, typename R = T>
+SS_D void smooth_cell(const MGArgsT<T>& a, int x, int y, int z) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int c = idx3(x, y, z, nx, ny);
     float f_top, f_bottom, f_right, f_left, f_front = 0.f, f_back = 0.f;
@@ -87,33 +93,33 @@ SS_D void smooth_cell(const MGArgs& a, int x, int y, int z) {
     float f_sum = f_top + f_bottom + f_right + f_left;
     if constexpr (DIM == 3) f_sum = f_sum + f_front + f_back;
     if (f_sum == 0.f) return;
-    const float* P = a.p;
-    const float p_top = y + 1 < ny ? P[c + nx] : 0.f;
-    const float p_bottom = y > 0 ? P[c - nx] : 0.f;
-    const float p_right = x + 1 < nx ? P[c + 1] : 0.f;
-    const float p_left = x > 0 ? P[c - 1] : 0.f;
+    const T* P = a.p;
+    const float p_top = y + 1 < ny ? ld(P[c + nx]) : 0.f;
+    const float p_bottom = y > 0 ? ld(P[c - nx]) : 0.f;
+    const float p_right = x + 1 < nx ? ld(P[c + 1]) : 0.f;
+    const float p_left = x > 0 ? ld(P[c - 1]) : 0.f;
     float p_sum = p_top * f_top + p_bottom * f_bottom;
     p_sum = p_sum + p_right * f_right;
     p_sum = p_sum + p_left * f_left;
     if constexpr (DIM == 3) {
-        const float p_front = z + 1 < nz ? P[c + nx * ny] : 0.f;
-        const float p_back = z > 0 ? P[c - nx * ny] : 0.f;
+        const float p_front = z + 1 < nz ? ld(P[c + nx * ny]) : 0.f;
+        const float p_back = z > 0 ? ld(P[c - nx * ny]) : 0.f;
         p_sum = p_sum + p_front * f_front;
         p_sum = p_sum + p_back * f_back;
     }
     float pn;
     if constexpr (L0) pn = (p_sum - a.rho_h * a.div0[c] / a.dt) / f_sum;
-    else pn = (p_sum - a.r[c] * a.hh) / f_sum;
-    a.p[c] = pn;
+    else pn = (p_sum - ld(a.r[c]) * a.hh) / f_sum;
+    a.p[c] = st<T>(rnd<R>(pn));
 }
 
-template <int DIM, bool L0>
-__global__ void __launch_bounds__(256) k_smooth(MGArgs a, int parity) {
+template <int DIM, bool L0, typename T = float>
+__global__ void __launch_bounds__(256) k_smooth(MGArgsT<T> a, int parity) {
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((y + z + parity) & 1);
     if (x >= a.nx || y >= a.ny || z >= a.nz) return;
-    smooth_cell<DIM, L0>(a, x, y, z);
+    smooth_cell<DIM, L0, T>(a, x, y, z);
 }
 
 static inline dim3 grid_for(int ax, int ay, int az, dim3 b) {
@@ -141,8 +147,8 @@ int launch_smooth(ss_sim* s, const StepConsts& c, int L, int iterations, int qui
 // ------------------------------------------------------------------ residual
 // compute_residual.comp:77-130 (2D :72-117): r = b - (sum_f p_nb - f_sum p)/h^2,
 // out of grid = solid; level 0 takes b = rho*div/(dt*h).
-template <int DIM, bool L0>
-SS_D float residual_cell(const MGArgs& a, int x, int y, int z) {
+template <int DIM, bool L0, typename T = float>
+SS_D float residual_cell(const MGArgsT<T>& a, int x, int y, int z) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int c = idx3(x, y, z, nx, ny);
     float f_top, f_bottom, f_right, f_left, f_front = 0.f, f_back = 0.f;
@@ -169,34 +175,34 @@ SS_D float residual_cell(const MGArgs& a, int x, int y, int z) {
             f_back = 1.f - (z > 0 ? a.alpha[c - nx * ny] : a.oobA);
         }
     }
-    const float* P = a.p;
-    const float p_top = y + 1 < ny ? P[c + nx] : 0.f;
-    const float p_bottom = y > 0 ? P[c - nx] : 0.f;
-    const float p_right = x + 1 < nx ? P[c + 1] : 0.f;
-    const float p_left = x > 0 ? P[c - 1] : 0.f;
+    const T* P = a.p;
+    const float p_top = y + 1 < ny ? ld(P[c + nx]) : 0.f;
+    const float p_bottom = y > 0 ? ld(P[c - nx]) : 0.f;
+    const float p_right = x + 1 < nx ? ld(P[c + 1]) : 0.f;
+    const float p_left = x > 0 ? ld(P[c - 1]) : 0.f;
     float p_sum = p_top * f_top + p_bottom * f_bottom;
     p_sum = p_sum + p_right * f_right;
     p_sum = p_sum + p_left * f_left;
     float f_sum = f_top + f_bottom + f_right + f_left;
     if constexpr (DIM == 3) {
-        const float p_front = z + 1 < nz ? P[c + nx * ny] : 0.f;
-        const float p_back = z > 0 ? P[c - nx * ny] : 0.f;
+        const float p_front = z + 1 < nz ? ld(P[c + nx * ny]) : 0.f;
+        const float p_back = z > 0 ? ld(P[c - nx * ny]) : 0.f;
         p_sum = p_sum + p_front * f_front;
         p_sum = p_sum + p_back * f_back;
         f_sum = f_sum + f_front + f_back;
     }
     float old;
     if constexpr (L0) old = a.rho * a.div0r[c] / a.dt_h;
-    else old = a.r[c];
-    return old - (p_sum - f_sum * P[c]) / a.hh;
+    else old = ld(a.r[c]);
+    return old - (p_sum - f_sum * ld(P[c])) / a.hh;
 }
 
 // One thread per coarse cell: residual of its 2^DIM children (written in place
 // when WRITE_FINE, the reference's in-place residual), then restrict_residual
 // (restrict_residual.comp:40-64, 2D :40-59) into the next level when
 // WRITE_COARSE.  The grid also covers the fine cells left over by odd sizes.
-template <int DIM, bool L0, bool WRITE_FINE, bool WRITE_COARSE>
-__global__ void __launch_bounds__(256) k_residual_restrict(MGArgs a, float* __restrict__ rc, int cx, int cy, int cz) {
+template <int DIM, bool L0, bool WRITE_FINE, bool WRITE_COARSE, typename T = float>
+__global__ void __launch_bounds__(256) k_residual_restrict(MGArgsT<T> a, T* __restrict__ rc, int cx, int cy, int cz) {
     const int X = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y * blockDim.y + threadIdx.y;
     const int Z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -213,8 +219,11 @@ __global__ void __launch_bounds__(256) k_residual_restrict(MGArgs a, float* __re
                 const int x = x0 + dx, y = y0 + dy, z = z0 + dz;
                 float res = 0.f;
                 if (x < nx && y < ny && z < nz) {
-                    res = residual_cell<DIM, L0>(a, x, y, z);
-                    if constexpr (WRITE_FINE) a.r[idx3(x, y, z, nx, ny)] = res;
+                    res = residual_cell<DIM, L0, T>(a, x, y, z);
+                    if constexpr (WRITE_FINE) {
+                        a.r[idx3(x, y, z, nx, ny)] = st<T>(res);
+                        res = rnd<T>(res);
+                    }
                 }
                 v[dz][dy][dx] = res;
             }
@@ -228,7 +237,7 @@ __global__ void __launch_bounds__(256) k_residual_restrict(MGArgs a, float* __re
             } else {
                 out = (v[0][0][0] + v[0][0][1] + v[0][1][0] + v[0][1][1]) / 4.f;
             }
-            rc[idx3(X, Y, Z, cx, cy)] = out;
+            rc[idx3(X, Y, Z, cx, cy)] = st<T>(out);
         }
     }
 }
@@ -300,9 +309,9 @@ int launch_restrict(ss_sim* s, int L, cudaStream_t st) {
 // --------------------------------------------------------------- prolongation
 // prolong_pressure.comp:39-51: p_L += GL_LINEAR, CLAMP_TO_EDGE sample of
 // p_{L+1} at the fine cell centre, on every cell.
-template <int DIM>
-__global__ void __launch_bounds__(256) k_prolong(float* __restrict__ p, int ax, int ay, int az,
-                                                 const float* __restrict__ pc, int cx, int cy, int cz) {
+template <int DIM, typename T = float>
+__global__ void __launch_bounds__(256) k_prolong(T* __restrict__ p, int ax, int ay, int az,
+                                                 const T* __restrict__ pc, int cx, int cy, int cz) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -316,22 +325,22 @@ __global__ void __launch_bounds__(256) k_prolong(float* __restrict__ p, int ax, 
     const int ya = min(max(y0, 0), cy - 1), yb = min(max(y0 + 1, 0), cy - 1);
     float s;
     if constexpr (DIM == 2) {
-        s = lerp_(lerp_(__ldg(pc + idx3(xa, ya, 0, cx, cy)), __ldg(pc + idx3(xb, ya, 0, cx, cy)), wx),
-                  lerp_(__ldg(pc + idx3(xa, yb, 0, cx, cy)), __ldg(pc + idx3(xb, yb, 0, cx, cy)), wx), wy);
+        s = lerp_(lerp_(ld(pc[idx3(xa, ya, 0, cx, cy)]), ld(pc[idx3(xb, ya, 0, cx, cy)]), wx),
+                  lerp_(ld(pc[idx3(xa, yb, 0, cx, cy)]), ld(pc[idx3(xb, yb, 0, cx, cy)]), wx), wy);
     } else {
         const float tz = (((float)z + 0.5f) / (float)az) * (float)cz - 0.5f;
         const float fz = floorf(tz);
         const int z0 = (int)fz;
         const float wz = tz - fz;
         const int za = min(max(z0, 0), cz - 1), zb = min(max(z0 + 1, 0), cz - 1);
-        const float c0 = lerp_(lerp_(__ldg(pc + idx3(xa, ya, za, cx, cy)), __ldg(pc + idx3(xb, ya, za, cx, cy)), wx),
-                               lerp_(__ldg(pc + idx3(xa, yb, za, cx, cy)), __ldg(pc + idx3(xb, yb, za, cx, cy)), wx), wy);
-        const float c1 = lerp_(lerp_(__ldg(pc + idx3(xa, ya, zb, cx, cy)), __ldg(pc + idx3(xb, ya, zb, cx, cy)), wx),
-                               lerp_(__ldg(pc + idx3(xa, yb, zb, cx, cy)), __ldg(pc + idx3(xb, yb, zb, cx, cy)), wx), wy);
+        const float c0 = lerp_(lerp_(ld(pc[idx3(xa, ya, za, cx, cy)]), ld(pc[idx3(xb, ya, za, cx, cy)]), wx),
+                               lerp_(ld(pc[idx3(xa, yb, za, cx, cy)]), ld(pc[idx3(xb, yb, za, cx, cy)]), wx), wy);
+        const float c1 = lerp_(lerp_(ld(pc[idx3(xa, ya, zb, cx, cy)]), ld(pc[idx3(xb, ya, zb, cx, cy)]), wx),
+                               lerp_(ld(pc[idx3(xa, yb, zb, cx, cy)]), ld(pc[idx3(xb, yb, zb, cx, cy)]), wx), wy);
         s = lerp_(c0, c1, wz);
     }
     const int i = idx3(x, y, z, ax, ay);
-    p[i] = p[i] + s;
+    p[i] = st<T>(ld(p[i]) + s);
 }
 
 int launch_prolong(ss_sim* s, int L, cudaStream_t st) {
@@ -475,18 +484,20 @@ struct BottomLevel {
     int off;        // offset of the level in the shared arrays
     float hh;
 };
-struct BottomArgs {
+template <typename T>
+struct BottomArgsT {
     int nlev;
     BottomLevel lv[SS_MAX_LEVELS];
-    float* p[SS_MAX_LEVELS];
-    float* r[SS_MAX_LEVELS];
+    T* p[SS_MAX_LEVELS];
+    T* r[SS_MAX_LEVELS];
     const float* alpha[SS_MAX_LEVELS];
     int total;
     int n_pre, n_post, n_coarse, quirks;
     float oob_smooth, oob_resid;
 };
 
-SS_D MGArgs bottom_level(const BottomArgs& b, float* sp, float* sr, float* sa, int l, float oobA) {
+template <typename T>
+SS_D MGArgs bottom_level(const BottomArgsT<T>& b, float* sp, float* sr, float* sa, int l, float oobA) {
     MGArgs a;
     a.p = sp + b.lv[l].off;
     a.r = sr + b.lv[l].off;
@@ -511,7 +522,7 @@ SS_D MGArgs bottom_level(const BottomArgs& b, float* sp, float* sr, float* sa, i
 // a level small enough for two cells per thread of fewer warps runs on those
 // warps only, synchronised by a named barrier.
 constexpr int kBottomCells = 4;
-template <int DIM>
+template <int DIM, typename R>
 SS_D void bottom_smooth(const MGArgs& a, int iterations) {
     const int n = a.nx * a.ny * a.nz;
     int nt = blockDim.x;
@@ -531,12 +542,12 @@ SS_D void bottom_smooth(const MGArgs& a, int iterations) {
             const int parity = it & 1;
             if (fits) {
                 for (int q = 0; q < k; ++q)
-                    if (col[q] == parity) smooth_cell<DIM, false>(a, cx[q], cy[q], cz[q]);
+                    if (col[q] == parity) smooth_cell<DIM, false, float, R>(a, cx[q], cy[q], cz[q]);
             } else {
                 for (int c = threadIdx.x; c < n; c += nt) {
                     const int x = c % a.nx, t = c / a.nx, y = t % a.ny, z = t / a.ny;
                     if (((x + y + z) & 1) != parity) continue;
-                    smooth_cell<DIM, false>(a, x, y, z);
+                    smooth_cell<DIM, false, float, R>(a, x, y, z);
                 }
             }
             if (nt == (int)blockDim.x) __syncthreads();
@@ -546,8 +557,10 @@ SS_D void bottom_smooth(const MGArgs& a, int iterations) {
     __syncthreads();
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(1024) k_bottom(BottomArgs b) {
+// T: storage type of the global level arrays; R: rounding of every value the
+// solve stores (T, or float for the FP32 solve).
+template <int DIM, typename T, typename R>
+__global__ void __launch_bounds__(1024) k_bottom(BottomArgsT<T> b) {
     extern __shared__ float sm[];
     float* sp = sm;
     float* sr = sm + b.total;
@@ -556,8 +569,8 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgs b) {
         const int n = b.lv[l].n[0] * b.lv[l].n[1] * b.lv[l].n[2];
         const int o = b.lv[l].off;
         for (int c = threadIdx.x; c < n; c += blockDim.x) {
-            sp[o + c] = b.p[l][c];
-            sr[o + c] = b.r[l][c];
+            sp[o + c] = ld(b.p[l][c]);
+            sr[o + c] = ld(b.r[l][c]);
             sa[o + c] = b.alpha[l][c];
         }
     }
@@ -565,7 +578,7 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgs b) {
     // down: pre-smoothing, residual (in place only with the reference's rule) + restriction, clear next p
     for (int l = 0; l + 1 < b.nlev; ++l) {
         const MGArgs a = bottom_level(b, sp, sr, sa, l, b.oob_smooth);
-        bottom_smooth<DIM>(a, b.n_pre);
+        bottom_smooth<DIM, R>(a, b.n_pre);
         const MGArgs ar = bottom_level(b, sp, sr, sa, l, b.oob_resid);
         const int cx = b.lv[l + 1].n[0], cy = b.lv[l + 1].n[1], cz = b.lv[l + 1].n[2];
         const int hx = (a.nx + 1) / 2, hy = (a.ny + 1) / 2, hz = DIM == 3 ? (a.nz + 1) / 2 : 1;
@@ -581,7 +594,10 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgs b) {
                         float res = 0.f;
                         if (x < a.nx && y < a.ny && z < a.nz) {
                             res = residual_cell<DIM, false>(ar, x, y, z);
-                            if (b.quirks) ar.r[idx3(x, y, z, a.nx, a.ny)] = res;
+                            if (b.quirks) {
+                                res = rnd<R>(res);
+                                ar.r[idx3(x, y, z, a.nx, a.ny)] = res;
+                            }
                         }
                         v[dz][dy][dx] = res;
                     }
@@ -594,7 +610,7 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgs b) {
                 } else {
                     out = (v[0][0][0] + v[0][0][1] + v[0][1][0] + v[0][1][1]) / 4.f;
                 }
-                rc[idx3(X, Y, Z, cx, cy)] = out;
+                rc[idx3(X, Y, Z, cx, cy)] = rnd<R>(out);
             }
         }
         float* pc = sp + b.lv[l + 1].off;
@@ -602,7 +618,7 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgs b) {
         __syncthreads();
     }
     // coarsest level
-    bottom_smooth<DIM>(bottom_level(b, sp, sr, sa, b.nlev - 1, b.oob_smooth), b.n_coarse);
+    bottom_smooth<DIM, R>(bottom_level(b, sp, sr, sa, b.nlev - 1, b.oob_smooth), b.n_coarse);
     // up: prolongation + post-smoothing
     for (int l = b.nlev - 2; l >= 0; --l) {
         const MGArgs a = bottom_level(b, sp, sr, sa, l, b.oob_smooth);
@@ -634,18 +650,18 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgs b) {
                                        lerp_(pc[idx3(xa, yb, zb, cx, cy)], pc[idx3(xb, yb, zb, cx, cy)], wx), wy);
                 sv = lerp_(c0, c1, wz);
             }
-            a.p[c] = a.p[c] + sv;
+            a.p[c] = rnd<R>(a.p[c] + sv);
         }
         __syncthreads();
-        bottom_smooth<DIM>(a, b.n_post);
+        bottom_smooth<DIM, R>(a, b.n_post);
     }
     // write back every level (pressure and, with the in-place rule, residual)
     for (int l = 0; l < b.nlev; ++l) {
         const int n = b.lv[l].n[0] * b.lv[l].n[1] * b.lv[l].n[2];
         const int o = b.lv[l].off;
         for (int c = threadIdx.x; c < n; c += blockDim.x) {
-            b.p[l][c] = sp[o + c];
-            b.r[l][c] = sr[o + c];
+            b.p[l][c] = st<T>(sp[o + c]);
+            b.r[l][c] = st<T>(sr[o + c]);
         }
     }
 }
@@ -663,8 +679,9 @@ int bottom_start(const ss_sim* s) {
     return start;
 }
 
-int launch_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, cudaStream_t st) {
-    BottomArgs b{};
+template <typename T, typename R>
+static int launch_bottom_t(ss_sim* s, const ss_mg_schedule& mg, int L, T* const* p, T* const* r, cudaStream_t st) {
+    BottomArgsT<T> b{};
     b.nlev = s->levels - L;
     int off = 0;
     for (int l = 0; l < b.nlev; ++l) {
@@ -672,8 +689,8 @@ int launch_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, cudaStream_t st) {
         b.lv[l].n[0] = lv.n[0]; b.lv[l].n[1] = lv.n[1]; b.lv[l].n[2] = lv.n[2];
         b.lv[l].off = off;
         b.lv[l].hh = lv.hh;
-        b.p[l] = s->p[L + l];
-        b.r[l] = s->r[L + l];
+        b.p[l] = p[L + l];
+        b.r[l] = r[L + l];
         b.alpha[l] = s->alpha[L + l];
         off += lv.n[0] * lv.n[1] * lv.n[2];
     }
@@ -684,19 +701,95 @@ int launch_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, cudaStream_t st) {
     b.oob_resid = resid_oob(s, mg.ref_quirks);
     const size_t smem = (size_t)3 * off * sizeof(float);
     if (smem > (size_t)kBottomSmemBytes) return set_error(SS_E_INVALID, "bottom levels exceed shared memory");
-    static bool attr_set[2] = {false, false};
-    const int di = s->dim == 3 ? 1 : 0;
-    if (!attr_set[di]) {
-        cudaError_t e = s->dim == 3
-            ? cudaFuncSetAttribute(k_bottom<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBytes)
-            : cudaFuncSetAttribute(k_bottom<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBytes);
-        if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute(k_bottom)");
-        attr_set[di] = true;
-    }
-    if (s->dim == 3) k_bottom<3><<<1, 1024, smem, st>>>(b);
-    else k_bottom<2><<<1, 1024, smem, st>>>(b);
+    // the attribute is per function; setting it on every launch is cheap
+    cudaError_t e = s->dim == 3
+        ? cudaFuncSetAttribute(k_bottom<3, T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBytes)
+        : cudaFuncSetAttribute(k_bottom<2, T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBytes);
+    if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute(k_bottom)");
+    if (s->dim == 3) k_bottom<3, T, R><<<1, 1024, smem, st>>>(b);
+    else k_bottom<2, T, R><<<1, 1024, smem, st>>>(b);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_bottom");
+}
+
+int launch_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, cudaStream_t st) {
+    return launch_bottom_t<float, float>(s, mg, L, s->p, s->r, st);
+}
+
+// ---------------------------------------------------- coarse-storage variants
+// The coarse levels of the mixed-precision correction solve: the same
+// operators as above (out-of-grid rule of the corrected mode) on FP16 or BF16
+// arrays; prec is SS_PREC_MIXED (FP16) or SS_PREC_MIXED_BF16.
+template <typename T>
+static MGArgsT<T> mg_args_t(ss_sim* s, const StepConsts& c, int L, float oobA, T* p, T* r) {
+    const MGArgs f = mg_args(s, c, L, oobA);
+    MGArgsT<T> a;
+    a.p = p; a.r = r;
+    a.alpha = f.alpha; a.flags = f.flags; a.div0 = f.div0; a.div0r = f.div0r;
+    a.nx = f.nx; a.ny = f.ny; a.nz = f.nz;
+    a.oobA = f.oobA; a.hh = f.hh; a.rho_h = f.rho_h; a.dt = f.dt; a.rho = f.rho; a.dt_h = f.dt_h;
+    return a;
+}
+
+template <typename T>
+static int coarse_smooth_t(ss_sim* s, const StepConsts& c, int L, int iterations, T* p, T* r, cudaStream_t st) {
+    MGArgsT<T> a = mg_args_t<T>(s, c, L, smooth_oob(s, 0), p, r);
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for((a.nx + 1) / 2, a.ny, a.nz, b);
+    for (int it = 0; it < 2 * iterations; ++it) {
+        if (s->dim == 3) k_smooth<3, false, T><<<g, b, 0, st>>>(a, it & 1);
+        else k_smooth<2, false, T><<<g, b, 0, st>>>(a, it & 1);
+    }
+    s->nlaunch += 2 * iterations;
+    return check_cuda(cudaGetLastError(), "k_smooth (coarse storage)");
+}
+
+template <typename T>
+static int coarse_residual_restrict_t(ss_sim* s, const StepConsts& c, int L, T* p, T* r, T* rc, cudaStream_t st) {
+    MGArgsT<T> a = mg_args_t<T>(s, c, L, resid_oob(s, 0), p, r);
+    const int cx = s->lv[L + 1].n[0], cy = s->lv[L + 1].n[1], cz = s->lv[L + 1].n[2];
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for((a.nx + 1) / 2, (a.ny + 1) / 2, s->dim == 3 ? (a.nz + 1) / 2 : 1, b);
+    if (s->dim == 3) k_residual_restrict<3, false, false, true, T><<<g, b, 0, st>>>(a, rc, cx, cy, cz);
+    else k_residual_restrict<2, false, false, true, T><<<g, b, 0, st>>>(a, rc, cx, cy, cz);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_residual_restrict (coarse storage)");
+}
+
+template <typename T>
+static int coarse_prolong_t(ss_sim* s, int L, T* p, const T* pc, cudaStream_t st) {
+    const int* f = s->lv[L].n;
+    const int* cc = s->lv[L + 1].n;
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for(f[0], f[1], f[2], b);
+    if (s->dim == 3) k_prolong<3, T><<<g, b, 0, st>>>(p, f[0], f[1], f[2], pc, cc[0], cc[1], cc[2]);
+    else k_prolong<2, T><<<g, b, 0, st>>>(p, f[0], f[1], f[2], pc, cc[0], cc[1], cc[2]);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_prolong (coarse storage)");
+}
+
+int coarse_smooth(ss_sim* s, const StepConsts& c, int L, int iterations, int prec, cudaStream_t st) {
+    if (prec == SS_PREC_MIXED) return coarse_smooth_t<__half>(s, c, L, iterations, (__half*)s->cp[L], (__half*)s->cr[L], st);
+    return coarse_smooth_t<__nv_bfloat16>(s, c, L, iterations, (__nv_bfloat16*)s->cp[L], (__nv_bfloat16*)s->cr[L], st);
+}
+
+int coarse_residual_restrict(ss_sim* s, const StepConsts& c, int L, int prec, cudaStream_t st) {
+    if (prec == SS_PREC_MIXED)
+        return coarse_residual_restrict_t<__half>(s, c, L, (__half*)s->cp[L], (__half*)s->cr[L], (__half*)s->cr[L + 1], st);
+    return coarse_residual_restrict_t<__nv_bfloat16>(s, c, L, (__nv_bfloat16*)s->cp[L], (__nv_bfloat16*)s->cr[L],
+                                                      (__nv_bfloat16*)s->cr[L + 1], st);
+}
+
+int coarse_prolong(ss_sim* s, int L, int prec, cudaStream_t st) {
+    if (prec == SS_PREC_MIXED) return coarse_prolong_t<__half>(s, L, (__half*)s->cp[L], (const __half*)s->cp[L + 1], st);
+    return coarse_prolong_t<__nv_bfloat16>(s, L, (__nv_bfloat16*)s->cp[L], (const __nv_bfloat16*)s->cp[L + 1], st);
+}
+
+int coarse_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, int prec, cudaStream_t st) {
+    if (prec == SS_PREC_MIXED)
+        return launch_bottom_t<__half, __half>(s, mg, L, (__half* const*)s->cp, (__half* const*)s->cr, st);
+    return launch_bottom_t<__nv_bfloat16, __nv_bfloat16>(s, mg, L, (__nv_bfloat16* const*)s->cp,
+                                                         (__nv_bfloat16* const*)s->cr, st);
 }
 
 }  // namespace ss

@@ -1,0 +1,193 @@
+// k_mixed.cu - FP64 parts of the mixed-precision pressure projection.
+//
+// The mixed solve keeps the level-0 pressure in FP64 (p64) and refines it:
+// each iteration evaluates the fine-level residual of the projection in FP64,
+//     rho_i = div_i - k * (sum_{fluid nb j} p64_j - n_i * p64_i),   k = dt/(rho h),
+// which is exactly the divergence the velocity update would leave, hands it
+// to one FP32 V-cycle as the right-hand side of the correction equation
+// (level 0 FP32, coarse levels FP16/BF16 storage), and adds the correction
+// back in FP64.  The residual norm (and its maximum, which sets the power-of-
+// two scale of the coarse storage) are FP64 reductions.  Extension of the
+// reference, whose multigrid_pressure_solve (common/physics/grid.c:173-209)
+// runs FP32 V-cycles on the pressure itself.
+#include "common.cuh"
+#include "ss_internal.h"
+
+namespace ss {
+
+static inline dim3 grid3(int ax, int ay, int az, dim3 b) {
+    return dim3((ax + b.x - 1) / b.x, (ay + b.y - 1) / b.y, (az + b.z - 1) / b.z);
+}
+
+SS_D int rb_pos(int x, int y, int z, int nx, int ny, int nz) {
+    const int half = nx >> 1;
+    return (((x + y + z) & 1) ? half * ny * nz : 0) + (z * ny + y) * half + (x >> 1);
+}
+
+SS_D void block_sum_max(double v, double m, double* sum_out, double* max_out) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v += __shfl_down_sync(0xffffffffu, v, o);
+        m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    }
+    __shared__ double ws[32], wm[32];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    if ((tid & 31) == 0) { ws[tid >> 5] = v; wm[tid >> 5] = m; }
+    __syncthreads();
+    if (tid < 32) {
+        double r = tid < (nthreads + 31) / 32 ? ws[tid] : 0.0;
+        double q = tid < (nthreads + 31) / 32 ? wm[tid] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            r += __shfl_down_sync(0xffffffffu, r, o);
+            q = fmax(q, __shfl_down_sync(0xffffffffu, q, o));
+        }
+        if (tid == 0) { *sum_out = r; *max_out = q; }
+    }
+}
+
+__global__ void k_p64_from_f32(const float* __restrict__ p, double* __restrict__ p64, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        p64[i] = (double)p[i];
+}
+
+__global__ void k_f32_from_p64(const double* __restrict__ p64, float* __restrict__ p, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = (float)p64[i];
+}
+
+// FP64 residual of the projection at every fluid cell; writes the FP32
+// right-hand sides of the correction equation colour-split (smoother form
+// rho/k, residual form rho/(k h^2)) and per-block sum of squares / max |rho|.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_ir_residual(const double* __restrict__ p64, const float* __restrict__ div0,
+                                                     const uint8_t* __restrict__ fmask, int nx, int ny, int nz,
+                                                     double k, double inv_k, double inv_khh,
+                                                     float* __restrict__ rhs_s, float* __restrict__ rhs_r,
+                                                     double* __restrict__ psum, double* __restrict__ pmax) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    double acc = 0.0, amax = 0.0;
+    if (x < nx && y < ny && z < nz) {
+        const int c = idx3(x, y, z, nx, ny);
+        const uint8_t m = fmask[c];
+        const int q = rb_pos(x, y, z, nx, ny, nz);
+        float s_out = 0.f, r_out = 0.f;
+        if (m & M_FLUID) {
+            const double t = (m & M_TOP) && y + 1 < ny ? p64[c + nx] : 0.0;
+            const double b = (m & M_BOTTOM) && y > 0 ? p64[c - nx] : 0.0;
+            const double r = (m & M_RIGHT) && x + 1 < nx ? p64[c + 1] : 0.0;
+            const double l = (m & M_LEFT) && x > 0 ? p64[c - 1] : 0.0;
+            double sum = t + b;
+            sum = sum + r;
+            sum = sum + l;
+            if constexpr (DIM == 3) {
+                const int pl = nx * ny;
+                const double f = (m & M_FRONT) && z + 1 < nz ? p64[c + pl] : 0.0;
+                const double k2 = (m & M_BACK) && z > 0 ? p64[c - pl] : 0.0;
+                sum = sum + f;
+                sum = sum + k2;
+            }
+            const double cnt = (double)__popc(m & 0x7Eu);
+            const double rho = (double)div0[c] - k * (sum - cnt * p64[c]);
+            acc = rho * rho;
+            amax = fabs(rho);
+            s_out = (float)(rho * inv_k);
+            r_out = (float)(rho * inv_khh);
+        }
+        rhs_s[q] = s_out;
+        rhs_r[q] = r_out;
+    }
+    block_sum_max(acc, amax, psum + blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
+                  pmax + blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
+}
+
+// Also derives the power-of-two scale of the coarse storage from max|rho|:
+// with max|rho| / (k h^2) = m * 2^e (m in [0.5, 1)), the restricted residual
+// is multiplied by 2^-e (largest magnitude below 1) on its way to the FP16 /
+// BF16 level and the prolonged correction by 2^e on its way back.
+__global__ void k_reduce_max_final(const double* __restrict__ partial, int n, double* __restrict__ out, int slot,
+                                   double inv_khh, float* __restrict__ scale) {
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, partial[i]);
+    __shared__ double sh[1024];
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[slot] = sh[0];
+        int e = 0;
+        frexp(sh[0] * inv_khh, &e);
+        e = max(-100, min(100, e));
+        scale[0] = (float)ldexp(1.0, -e);
+        scale[1] = (float)ldexp(1.0, e);
+    }
+}
+
+// p64 += e at every fluid cell (e: the correction, colour-split FP32)
+template <int DIM>
+__global__ void __launch_bounds__(256) k_ir_accumulate(double* __restrict__ p64, const float* __restrict__ e,
+                                                       const uint8_t* __restrict__ fmask, int nx, int ny, int nz) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (x >= nx || y >= ny || z >= nz) return;
+    const int c = idx3(x, y, z, nx, ny);
+    if (!(fmask[c] & M_FLUID)) return;
+    p64[c] = p64[c] + (double)e[rb_pos(x, y, z, nx, ny, nz)];
+}
+
+int launch_p64_from_p0(ss_sim* s, cudaStream_t st) {
+    k_p64_from_f32<<<4 * 148, 256, 0, st>>>(s->p[0], s->p64, s->ncell);
+    s->nlaunch += 1;
+    s->p64_valid = 1;
+    return check_cuda(cudaGetLastError(), "k_p64_from_f32");
+}
+
+int launch_p0_from_p64(ss_sim* s, cudaStream_t st) {
+    k_f32_from_p64<<<4 * 148, 256, 0, st>>>(s->p64, s->p[0], s->ncell);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_f32_from_p64");
+}
+
+int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, cudaStream_t st) {
+    dim3 b(32, 8, 1);
+    dim3 g = grid3(s->nx, s->ny, s->nz, b);
+    const int nblocks = (int)(g.x * g.y * g.z);
+    if (nblocks > s->red.max_blocks) return set_error(SS_E_INVALID, "reduction scratch too small");
+    const double k = (double)c.dt / ((double)c.rho * (double)s->h);
+    const double inv_k = 1.0 / k;
+    const double inv_khh = 1.0 / (k * (double)s->lv[0].hh);
+    if (s->dim == 3)
+        k_ir_residual<3><<<g, b, 0, st>>>(s->p64, s->div0, s->fmask, s->nx, s->ny, s->nz, k, inv_k, inv_khh,
+                                           s->rhs_s, s->rhs_r, s->red.partial, s->red.partial_max);
+    else
+        k_ir_residual<2><<<g, b, 0, st>>>(s->p64, s->div0, s->fmask, s->nx, s->ny, s->nz, k, inv_k, inv_khh,
+                                           s->rhs_s, s->rhs_r, s->red.partial, s->red.partial_max);
+    s->nlaunch += 1;
+    int rc = check_cuda(cudaGetLastError(), "k_ir_residual");
+    if (rc) return rc;
+    if (slot >= 0) {
+        rc = launch_reduce_final(s, nblocks, slot, st);
+        if (rc) return rc;
+    }
+    k_reduce_max_final<<<1, 1024, 0, st>>>(s->red.partial_max, nblocks, s->red.out, SLOT_AMAX, inv_khh, s->d_scale);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_reduce_max_final");
+}
+
+int launch_ir_accumulate(ss_sim* s, cudaStream_t st) {
+    dim3 b(32, 8, 1);
+    dim3 g = grid3(s->nx, s->ny, s->nz, b);
+    if (s->dim == 3) k_ir_accumulate<3><<<g, b, 0, st>>>(s->p64, s->p_alt[0], s->fmask, s->nx, s->ny, s->nz);
+    else k_ir_accumulate<2><<<g, b, 0, st>>>(s->p64, s->p_alt[0], s->fmask, s->nx, s->ny, s->nz);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_ir_accumulate");
+}
+
+}  // namespace ss

@@ -14,6 +14,7 @@
 // by the fluid-neighbour count through div_by_count, right-hand sides
 // precomputed with the reference's operations by k_divergence).
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -94,12 +95,15 @@ __global__ void __launch_bounds__(256) k_rb_smooth(float* __restrict__ pc, const
 
 // Residual of every fine cell, restricted into the coarse level (natural
 // layout): one thread per coarse cell and its 2^DIM children.
-template <int DIM, bool POW2>
+// T: storage of the coarse level; for the mixed-precision correction solve
+// (T = FP16 / BF16) the restricted value is multiplied by a power-of-two
+// scale before it is rounded, which keeps it in the normal range.
+template <int DIM, bool POW2, typename T = float>
 __global__ void __launch_bounds__(256) k_rb_residual_restrict(const float* __restrict__ p_red, const float* __restrict__ p_black,
                                                               const float* __restrict__ rr_red, const float* __restrict__ rr_black,
                                                               const uint8_t* __restrict__ m_red, const uint8_t* __restrict__ m_black,
-                                                              RBLevel g, float* __restrict__ rc, int cx, int cy, int cz,
-                                                              float hh, float inv_hh) {
+                                                              RBLevel g, T* __restrict__ rc, int cx, int cy, int cz,
+                                                              float hh, float inv_hh, const float* __restrict__ scale) {
     const int X = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y * blockDim.y + threadIdx.y;
     const int Z = blockIdx.z;
@@ -132,13 +136,15 @@ __global__ void __launch_bounds__(256) k_rb_residual_restrict(const float* __res
     } else {
         out = (v[0][0][0] + v[0][0][1] + v[0][1][0] + v[0][1][1]) / 4.f;
     }
-    rc[idx3(X, Y, Z, cx, cy)] = out;
+    if constexpr (!std::is_same<T, float>::value) out = out * scale[0];
+    rc[idx3(X, Y, Z, cx, cy)] = st<T>(out);
 }
 
 // prolong_pressure.comp:39-51 into the colour-split level 0
-template <int DIM>
+template <int DIM, typename T = float>
 __global__ void __launch_bounds__(256) k_rb_prolong(float* __restrict__ p_red, float* __restrict__ p_black, RBLevel g,
-                                                    const float* __restrict__ pc, int cx, int cy, int cz) {
+                                                    const T* __restrict__ pc, int cx, int cy, int cz,
+                                                    const float* __restrict__ scale) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
@@ -153,20 +159,21 @@ __global__ void __launch_bounds__(256) k_rb_prolong(float* __restrict__ p_red, f
     const int ya = min(max(y0, 0), cy - 1), yb = min(max(y0 + 1, 0), cy - 1);
     float s;
     if constexpr (DIM == 2) {
-        s = lerp_(lerp_(__ldg(pc + idx3(xa, ya, 0, cx, cy)), __ldg(pc + idx3(xb, ya, 0, cx, cy)), wx),
-                  lerp_(__ldg(pc + idx3(xa, yb, 0, cx, cy)), __ldg(pc + idx3(xb, yb, 0, cx, cy)), wx), wy);
+        s = lerp_(lerp_(ld(pc[idx3(xa, ya, 0, cx, cy)]), ld(pc[idx3(xb, ya, 0, cx, cy)]), wx),
+                  lerp_(ld(pc[idx3(xa, yb, 0, cx, cy)]), ld(pc[idx3(xb, yb, 0, cx, cy)]), wx), wy);
     } else {
         const float tz = (((float)z + 0.5f) / (float)az) * (float)cz - 0.5f;
         const float fz = floorf(tz);
         const int z0 = (int)fz;
         const float wz = tz - fz;
         const int za = min(max(z0, 0), cz - 1), zb = min(max(z0 + 1, 0), cz - 1);
-        const float c0 = lerp_(lerp_(__ldg(pc + idx3(xa, ya, za, cx, cy)), __ldg(pc + idx3(xb, ya, za, cx, cy)), wx),
-                               lerp_(__ldg(pc + idx3(xa, yb, za, cx, cy)), __ldg(pc + idx3(xb, yb, za, cx, cy)), wx), wy);
-        const float c1 = lerp_(lerp_(__ldg(pc + idx3(xa, ya, zb, cx, cy)), __ldg(pc + idx3(xb, ya, zb, cx, cy)), wx),
-                               lerp_(__ldg(pc + idx3(xa, yb, zb, cx, cy)), __ldg(pc + idx3(xb, yb, zb, cx, cy)), wx), wy);
+        const float c0 = lerp_(lerp_(ld(pc[idx3(xa, ya, za, cx, cy)]), ld(pc[idx3(xb, ya, za, cx, cy)]), wx),
+                               lerp_(ld(pc[idx3(xa, yb, za, cx, cy)]), ld(pc[idx3(xb, yb, za, cx, cy)]), wx), wy);
+        const float c1 = lerp_(lerp_(ld(pc[idx3(xa, ya, zb, cx, cy)]), ld(pc[idx3(xb, ya, zb, cx, cy)]), wx),
+                               lerp_(ld(pc[idx3(xa, yb, zb, cx, cy)]), ld(pc[idx3(xb, yb, zb, cx, cy)]), wx), wy);
         s = lerp_(c0, c1, wz);
     }
+    if constexpr (!std::is_same<T, float>::value) s = s * scale[1];
     float* dst = ((x + y + z) & 1) ? p_black : p_red;
     const int i = rb_index(x, y, z, g);
     dst[i] = dst[i] + s;
@@ -239,12 +246,12 @@ __global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, cons
 // Residual of the fine cells under four consecutive coarse cells of a row,
 // restricted: per fine row the even-x cells sit in one colour array and the
 // odd-x cells in the other, both at the coarse x index.
-template <int DIM, bool POW2>
+template <int DIM, bool POW2, typename T = float>
 __global__ void __launch_bounds__(256) k_rb_residual_restrict4(const float* __restrict__ p_red, const float* __restrict__ p_black,
                                                                const float* __restrict__ rr_red, const float* __restrict__ rr_black,
                                                                const uint8_t* __restrict__ m_red, const uint8_t* __restrict__ m_black,
-                                                               RBLevel g, float* __restrict__ rc, int cx, int cy,
-                                                               float hh, float inv_hh) {
+                                                               RBLevel g, T* __restrict__ rc, int cx, int cy,
+                                                               float hh, float inv_hh, const float* __restrict__ scale) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y * blockDim.y + threadIdx.y;
     const int Z = blockIdx.z;
@@ -324,7 +331,13 @@ __global__ void __launch_bounds__(256) k_rb_residual_restrict4(const float* __re
             out[k] = (v[0][0][0][k] + v[0][0][1][k] + v[0][1][0][k] + v[0][1][1][k]) / 4.f;
         }
     }
-    *reinterpret_cast<float4*>(rc + (Z * cy + Y) * cx + X0) = make_float4(out[0], out[1], out[2], out[3]);
+    T* dst = rc + (Z * cy + Y) * cx + X0;
+    if constexpr (std::is_same<T, float>::value) {
+        *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dst[k] = st<T>(out[k] * scale[0]);
+    }
 }
 
 // prolong_pressure.comp:39-51 for the fine cells under four consecutive
@@ -332,10 +345,10 @@ __global__ void __launch_bounds__(256) k_rb_residual_restrict4(const float* __re
 // computed with the same float expression as k_rb_prolong (whose lower
 // coarse index is x/2 - 1 + (x & 1), checked on the host when the tables are
 // made).
-template <int DIM>
+template <int DIM, typename T = float>
 __global__ void __launch_bounds__(256) k_rb_prolong4(float* __restrict__ p_red, float* __restrict__ p_black, RBLevel g,
-                                                     const float* __restrict__ pc, int cx, int cy, int cz,
-                                                     const float* __restrict__ pw) {
+                                                     const T* __restrict__ pc, int cx, int cy, int cz,
+                                                     const float* __restrict__ pw, const float* __restrict__ scale) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y * blockDim.y + threadIdx.y;
     const int Z = blockIdx.z;
@@ -360,10 +373,15 @@ __global__ void __launch_bounds__(256) k_rb_prolong4(float* __restrict__ p_red, 
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
                 const int base = ((DIM == 3 ? Zs[ez + pz] : 0) * cy + Ys[r]) * cx;
-                const float4 c = ldg4(pc + base + X0);
-                R[pz][r][0] = __ldg(pc + base + xl);
-                R[pz][r][1] = c.x; R[pz][r][2] = c.y; R[pz][r][3] = c.z; R[pz][r][4] = c.w;
-                R[pz][r][5] = __ldg(pc + base + xr);
+                if constexpr (std::is_same<T, float>::value) {
+                    const float4 c = ldg4(pc + base + X0);
+                    R[pz][r][1] = c.x; R[pz][r][2] = c.y; R[pz][r][3] = c.z; R[pz][r][4] = c.w;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) R[pz][r][1 + k] = ld(pc[base + X0 + k]);
+                }
+                R[pz][r][0] = ld(pc[base + xl]);
+                R[pz][r][5] = ld(pc[base + xr]);
             }
 #pragma unroll
         for (int ey = 0; ey < 2; ++ey) {
@@ -381,6 +399,7 @@ __global__ void __launch_bounds__(256) k_rb_prolong4(float* __restrict__ p_red, 
                         const float c1 = lerp_(lerp_(R[1][ey][lo], R[1][ey][hi], w), lerp_(R[1][ey + 1][lo], R[1][ey + 1][hi], w), wy);
                         sv = lerp_(sv, c1, wz);
                     }
+                    if constexpr (!std::is_same<T, float>::value) sv = sv * scale[1];
                     (e ? so : se)[k] = sv;
                 }
             const int c0 = (y + z) & 1;
@@ -466,59 +485,76 @@ static bool pow2f(float v) {
     return frexpf(v, &e) == 0.5f && v >= 1.1754944e-38f && v <= 1e30f;
 }
 
-int launch_rb_residual_restrict(ss_sim* s, cudaStream_t st) {
+template <typename T>
+static int rb_residual_restrict_t(ss_sim* s, T* rc, const float* scale, cudaStream_t st) {
     const RBLevel g = rb_level(s);
     const size_t h = s->ncell / 2;
     const int cx = s->lv[1].n[0], cy = s->lv[1].n[1], cz = s->lv[1].n[2];
     const float hh = s->lv[0].hh;
     const bool p2 = pow2f(hh);
+    const float ih = p2 ? 1.f / hh : 0.f;
     dim3 b, gr;
     const float* pr = s->p_alt[0];
     const float* pb = pr + h;
     const float* rr = s->rhs_r;
+    const uint8_t* mr = s->rb_mask;
+    const uint8_t* mb = s->rb_mask + h;
     if (s->rb_vec) {
         row_launch(cx / 4, cy, cz, b, gr);
-        const uint8_t* mr = s->rb_mask;
-        const uint8_t* mb = s->rb_mask + h;
         if (s->dim == 3) {
-            if (p2) k_rb_residual_restrict4<3, true><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, s->r[1], cx, cy, hh, 1.f / hh);
-            else k_rb_residual_restrict4<3, false><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, s->r[1], cx, cy, hh, 0.f);
+            if (p2) k_rb_residual_restrict4<3, true, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
+            else k_rb_residual_restrict4<3, false, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
         } else {
-            if (p2) k_rb_residual_restrict4<2, true><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, s->r[1], cx, cy, hh, 1.f / hh);
-            else k_rb_residual_restrict4<2, false><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, s->r[1], cx, cy, hh, 0.f);
+            if (p2) k_rb_residual_restrict4<2, true, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
+            else k_rb_residual_restrict4<2, false, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
         }
         s->nlaunch += 1;
         return check_cuda(cudaGetLastError(), "k_rb_residual_restrict4");
     }
     row_launch(cx, cy, cz, b, gr);
     if (s->dim == 3) {
-        if (p2) k_rb_residual_restrict<3, true><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, s->rb_mask, s->rb_mask + h, g, s->r[1], cx, cy, cz, hh, 1.f / hh);
-        else k_rb_residual_restrict<3, false><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, s->rb_mask, s->rb_mask + h, g, s->r[1], cx, cy, cz, hh, 0.f);
+        if (p2) k_rb_residual_restrict<3, true, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
+        else k_rb_residual_restrict<3, false, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
     } else {
-        if (p2) k_rb_residual_restrict<2, true><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, s->rb_mask, s->rb_mask + h, g, s->r[1], cx, cy, cz, hh, 1.f / hh);
-        else k_rb_residual_restrict<2, false><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, s->rb_mask, s->rb_mask + h, g, s->r[1], cx, cy, cz, hh, 0.f);
+        if (p2) k_rb_residual_restrict<2, true, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
+        else k_rb_residual_restrict<2, false, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
     }
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_rb_residual_restrict");
 }
 
-int launch_rb_prolong(ss_sim* s, cudaStream_t st) {
+template <typename T>
+static int rb_prolong_t(ss_sim* s, const T* pc, const float* scale, cudaStream_t st) {
     const RBLevel g = rb_level(s);
     const size_t h = s->ncell / 2;
     const int cx = s->lv[1].n[0], cy = s->lv[1].n[1], cz = s->lv[1].n[2];
     if (s->rb_prolong_vec) {
         dim3 b, gr;
         row_launch(cx / 4, cy, cz, b, gr);
-        if (s->dim == 3) k_rb_prolong4<3><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, s->p[1], cx, cy, cz, s->rb_pw);
-        else k_rb_prolong4<2><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, s->p[1], cx, cy, cz, s->rb_pw);
+        if (s->dim == 3) k_rb_prolong4<3, T><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw, scale);
+        else k_rb_prolong4<2, T><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw, scale);
         s->nlaunch += 1;
         return check_cuda(cudaGetLastError(), "k_rb_prolong4");
     }
     dim3 b(128), gr((g.nx + 127) / 128, g.ny, g.nz);
-    if (s->dim == 3) k_rb_prolong<3><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, s->p[1], cx, cy, cz);
-    else k_rb_prolong<2><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, s->p[1], cx, cy, cz);
+    if (s->dim == 3) k_rb_prolong<3, T><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, scale);
+    else k_rb_prolong<2, T><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, scale);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_rb_prolong");
+}
+
+int launch_rb_residual_restrict(ss_sim* s, cudaStream_t st) { return rb_residual_restrict_t<float>(s, s->r[1], nullptr, st); }
+
+int launch_rb_prolong(ss_sim* s, cudaStream_t st) { return rb_prolong_t<float>(s, s->p[1], nullptr, st); }
+
+int launch_rb_residual_restrict_mixed(ss_sim* s, int prec, cudaStream_t st) {
+    if (prec == SS_PREC_MIXED) return rb_residual_restrict_t<__half>(s, (__half*)s->cr[1], s->d_scale, st);
+    return rb_residual_restrict_t<__nv_bfloat16>(s, (__nv_bfloat16*)s->cr[1], s->d_scale, st);
+}
+
+int launch_rb_prolong_mixed(ss_sim* s, int prec, cudaStream_t st) {
+    if (prec == SS_PREC_MIXED) return rb_prolong_t<__half>(s, (const __half*)s->cp[1], s->d_scale, st);
+    return rb_prolong_t<__nv_bfloat16>(s, (const __nv_bfloat16*)s->cp[1], s->d_scale, st);
 }
 
 // Per-axis weight of the fine cell's coarse interpolation, the float

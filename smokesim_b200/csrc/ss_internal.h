@@ -31,11 +31,12 @@ struct StepConsts {
 
 struct ReduceSlots {
     double* partial;      // per-block partial sums (device scratch)
+    double* partial_max = nullptr;  // per-block maxima (mixed-precision solve)
     double* out;          // reduction results (device), SLOT_* below
     double* host;         // pinned mirror of out
     int max_blocks;
 };
-enum { SLOT_DIV_BEFORE = 0, SLOT_RESIDUAL = 1, SLOT_DIV_AFTER = 2, SLOT_COUNT = 8 };
+enum { SLOT_DIV_BEFORE = 0, SLOT_RESIDUAL = 1, SLOT_DIV_AFTER = 2, SLOT_AMAX = 3, SLOT_COUNT = 8 };
 
 struct TensorMapEntry {
     CUtensorMap map;
@@ -79,6 +80,13 @@ struct ss_sim {
     float* rhs_r = nullptr;             // level-0 rho*div/(dt*h) of the current solve, colour-split
     uint8_t* rb_mask = nullptr;         // colour-split copy of fmask
     float* rb_pw = nullptr;             // level-0 prolongation weights per axis (x, then y, then z)
+    // mixed-precision solve: FP64 level-0 pressure, FP16/BF16 coarse levels
+    double* p64 = nullptr;
+    int p64_valid = 0;                  // p64 holds the current pressure (else p[0] does)
+    int cstore = 0;                     // storage type of cp/cr (SS_PREC_MIXED or SS_PREC_MIXED_BF16)
+    void* cp[SS_MAX_LEVELS] = {};       // coarse pressure, 2 bytes per cell (L >= 1)
+    void* cr[SS_MAX_LEVELS] = {};       // coarse right-hand side / residual
+    float* d_scale = nullptr;           // [scale, 1/scale] of the coarse storage (device)
     int rb_vec = 0;                     // level-0 kernels may work on 4 cells per thread (nx % 8 == 0)
     int rb_prolong_vec = 0;             // ... and the prolongation too (even sizes, table pattern checked)
     ss::ReduceSlots red{};
@@ -147,6 +155,19 @@ int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st);
 int launch_rb_residual_restrict(ss_sim* s, cudaStream_t st);
 int launch_rb_prolong(ss_sim* s, cudaStream_t st);
 int rb_init_vector_paths(ss_sim* s, cudaStream_t st);
+
+// mixed-precision correction solve (k_mg.cu, k_rb.cu, k_mixed.cu)
+int coarse_smooth(ss_sim* s, const StepConsts& c, int L, int iterations, int prec, cudaStream_t st);
+int coarse_residual_restrict(ss_sim* s, const StepConsts& c, int L, int prec, cudaStream_t st);
+int coarse_prolong(ss_sim* s, int L, int prec, cudaStream_t st);
+int coarse_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, int prec, cudaStream_t st);
+int launch_rb_residual_restrict_mixed(ss_sim* s, int prec, cudaStream_t st);
+int launch_rb_prolong_mixed(ss_sim* s, int prec, cudaStream_t st);
+int launch_p64_from_p0(ss_sim* s, cudaStream_t st);
+int launch_p0_from_p64(ss_sim* s, cudaStream_t st);
+int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, cudaStream_t st);
+int launch_ir_accumulate(ss_sim* s, cudaStream_t st);
+int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st);
 
 // ---- scene kernels (k_scene.cu) ----
 int launch_rasterize(ss_sim* s, cudaStream_t st);

@@ -1,0 +1,106 @@
+"""Mixed-precision projection: FP64 fine-level residual and iterative
+refinement, FP32 level-0 smoothing, FP16 / BF16 coarse corrections.
+
+The oracle restates the same iteration (oracle/smokesim_oracle.c,
+og_mixed_pressure_solve), rounding every coarse-level store the way the CUDA
+path stores it, so a fixed number of refinement steps must agree bit for bit.
+"""
+import numpy as np
+import pytest
+
+from smokesim_b200 import abi, scene
+from test_gpu_parity import assert_same, make_pair
+
+# grids with an even nx (the mixed solve runs on the colour-split level 0)
+MIXED_GRIDS = [
+    ("3d_rgb_open", 3, (16, 21, 18), 3, 0, 4),
+    ("2d_quad", 2, (64, 40, 1), 1, 1, 4),
+    ("2d_quad_open_rgb", 2, (48, 34, 1), 3, 0, 4),
+    ("3d_quad_odd_y", 3, (24, 19, 18), 1, 1, 4),
+    ("3d_tma", 3, (32, 24, 20), 1, 1, 4),
+    ("3d_l1", 3, (64, 48, 48), 1, 1, 8),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,dim,n,nch,enc,mc", MIXED_GRIDS)
+@pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_MIXED_BF16])
+def test_mixed_solve_bitwise(name, dim, n, nch, enc, mc, prec):
+    g, o = make_pair(dim, n, nch, enc, seed=31, min_coarse=mc)
+    p = scene.workload_params(ref_quirks=0, precision=prec, n_vcycles=3, n_coarse=12)
+    for k in range(2):
+        g.step(p)
+        o.step(p)
+        assert_same(g, o, dim, f"mixed step {k}")
+    sg, so = g.stats(), o.stats()
+    assert sg.vcycles == so.vcycles == 3
+    assert abs(sg.residual - so.residual) <= 1e-9 * max(1e-30, so.residual)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_MIXED_BF16])
+def test_mixed_tolerance_matches_oracle(prec):
+    g, o = make_pair(3, (32, 24, 20), 1, 1, seed=3, min_coarse=4)
+    p = scene.workload_params(ref_quirks=0, precision=prec, n_vcycles=40, tol=1e-6)
+    for k in range(2):
+        g.step(p)
+        o.step(p)
+        sg, so = g.stats(), o.stats()
+        assert sg.converged == 1 and so.converged == 1
+        assert sg.vcycles == so.vcycles
+        assert sg.residual <= 1e-6 * sg.div_before
+        assert_same(g, o, 3, f"mixed tolerance step {k}")
+
+
+@pytest.mark.gpu
+def test_mixed_reaches_tolerance_where_fp32_stalls():
+    """GRF scene at 64^3: the FP32 V-cycle's FP32 residual floors above 1e-6
+    relative, while refinement on the FP64 residual reaches it."""
+    from smokesim_b200 import Sim, SmokeSimError
+    res = {}
+    for prec in (abi.PREC_FP32, abi.PREC_MIXED):
+        sc = scene.grf256(seed=0, n=64)
+        g = Sim(sc["desc"])
+        scene.apply(g, sc)
+        p = scene.workload_params(ref_quirks=0, precision=prec, n_vcycles=40, tol=1e-6)
+        try:
+            g.step(p)
+        except SmokeSimError as e:
+            assert e.code == abi.SS_E_NOT_CONVERGED
+        st = g.stats()
+        res[prec] = (st.converged, st.vcycles, st.residual / st.div_before)
+        g.close()
+    assert res[abi.PREC_MIXED][0] == 1 and res[abi.PREC_MIXED][1] <= 15, res
+    assert res[abi.PREC_FP32][0] == 0 or res[abi.PREC_FP32][1] > res[abi.PREC_MIXED][1], res
+
+
+@pytest.mark.gpu
+def test_mixed_unsupported_and_invalid():
+    from smokesim_b200 import SmokeSimError
+    g, _ = make_pair(3, (19, 17, 13), 1, 1, seed=2, min_coarse=3)
+    with pytest.raises(SmokeSimError) as e:
+        g.step(scene.workload_params(ref_quirks=0, precision=abi.PREC_MIXED))
+    assert e.value.code == abi.SS_E_UNSUPPORTED
+    g2, _ = make_pair(3, (16, 16, 16), 1, 1, seed=2)
+    with pytest.raises(SmokeSimError) as e:
+        g2.step(scene.workload_params(ref_quirks=1, precision=abi.PREC_MIXED))
+    assert e.value.code == abi.SS_E_INVALID
+
+
+@pytest.mark.gpu
+def test_mixed_then_fp32_warm_start():
+    """Switching precision mid-run: the FP32 solve continues from the rounded
+    FP64 pressure, the mixed solve from the FP32 pressure after a set_level."""
+    g, o = make_pair(3, (32, 24, 20), 1, 1, seed=8, min_coarse=4)
+    pm = scene.workload_params(ref_quirks=0, precision=abi.PREC_MIXED, n_vcycles=2)
+    pf = scene.workload_params(ref_quirks=0, precision=abi.PREC_FP32, n_vcycles=2)
+    for p in (pm, pf, pm):
+        g.step(p)
+        o.step(p)
+        assert_same(g, o, 3, "precision switch")
+    pr = np.linspace(-1, 1, 32 * 24 * 20).astype(np.float32)
+    g.set_level(0, abi.LEVEL_PRESSURE, pr)
+    o.set_level(0, abi.LEVEL_PRESSURE, pr)
+    g.step(pm)
+    o.step(pm)
+    assert_same(g, o, 3, "mixed after set_level")

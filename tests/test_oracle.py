@@ -214,3 +214,29 @@ def test_obstacle_falls_under_gravity(oracle_mod):
     vy = np.float32(0) + np.float32(-9.81) * np.float32(0.1) * np.float32(1.0)
     assert obs[0].velocity[1] == np.float32(vy * np.float32(0.999))
     assert obs[0].pos[1] == np.float32(np.float32(8.0) + vy * np.float32(0.1) * np.float32(1.0))
+
+
+def test_mixed_precision_refinement_reaches_tolerance(oracle_mod):
+    """GRF scene at 32^3: FP32 V-cycles floor above a 1e-6 relative projected
+    residual; refinement on the FP64 residual with FP16 / BF16 coarse
+    corrections reaches it within a few V-cycles and agrees with the FP64
+    oracle's pressure to the tolerance."""
+    out = {}
+    for prec in (abi.PREC_FP32, abi.PREC_MIXED, abi.PREC_MIXED_BF16):
+        sc = scene.grf256(seed=0, n=32)
+        o = oracle_mod.OracleSim(sc["desc"], "f32")
+        scene.apply(o, sc)
+        o.step(scene.workload_params(ref_quirks=0, tol=1e-6, n_vcycles=40, precision=prec))
+        st = o.stats()
+        out[prec] = (st.converged, st.vcycles, st.residual / st.div_before, o.get_field(abi.FIELD_PRESSURE, f64=True))
+    assert out[abi.PREC_FP32][0] == 0 and out[abi.PREC_FP32][2] > 1e-6
+    for prec in (abi.PREC_MIXED, abi.PREC_MIXED_BF16):
+        assert out[prec][0] == 1 and out[prec][1] <= 15 and out[prec][2] <= 1e-6
+    sc = scene.grf256(seed=0, n=32)
+    ref = oracle_mod.OracleSim(sc["desc"], "f64")
+    scene.apply(ref, sc)
+    ref.step(scene.workload_params(ref_quirks=0, tol=1e-10, n_vcycles=80))
+    p64 = ref.get_field(abi.FIELD_PRESSURE, f64=True)
+    fluid = ref.get_field(abi.FIELD_SOLID) == 0
+    err = rel_l2(out[abi.PREC_MIXED][3][fluid] - out[abi.PREC_MIXED][3][fluid].mean(), p64[fluid] - p64[fluid].mean())
+    assert err < 1e-4, err
