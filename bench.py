@@ -42,18 +42,34 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=256, help="grid cells per axis")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--vcycles", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="no timing: set up, run one step and a few level-0 smoother sweeps (for ncu)")
     return ap.parse_args()
 
 
+VARIANTS = {
+    # name: (precision, ref_quirks, tol, V-cycle cap or count)
+    "mixed_fp16": (1, 0, 1e-6, 40),
+    "mixed_bf16": (2, 0, 1e-6, 40),
+    "fp32": (0, 0, 1e-6, 40),
+    "fp32_reference_rules_4vc": (0, 1, 0.0, 4),
+}
+HEADLINE = "mixed_fp16"
+
+
+def variant_params(sc, name):
+    from smokesim_b200 import scene
+    prec, quirks, tol, cyc = VARIANTS[name]
+    p = scene.workload_params(ref_quirks=quirks, precision=prec, tol=tol, n_vcycles=cyc,
+                              collect_stats=1 if tol > 0 else 0)
+    return p
+
+
 def workload(args):
     from smokesim_b200 import scene
     sc = scene.grf256(seed=args.seed, n=args.n, with_grf=True)
-    sc["params"].mg.n_vcycles = args.vcycles
-    sc["params"].collect_stats = 0
+    sc["params"] = variant_params(sc, HEADLINE)
     return sc
 
 
@@ -62,10 +78,11 @@ def workload_config(args, sc):
     return {
         "workload": f"grf{args.n}: {args.n}^3 MAC smoke step, 2 emitters + sphere + 3 cubes, GRF initial velocity "
                     f"(sigma 8), dt {p.time_step:g}, {p.mg.n_pre}+{p.mg.n_post} RB-GS sweeps, {p.mg.n_coarse} coarse, "
-                    f"{p.mg.n_vcycles} V-cycles to 8^3, reference boundary rules",
+                    f"V-cycles to 8^3 until the projected divergence is <= 1e-6 of the pre-projection divergence "
+                    f"(cap 40); mixed precision: FP64 residual + refinement, FP32 smoothing, FP16 coarse corrections",
         "grid": [args.n, args.n, args.n],
-        "precision": "fp32",
-        "vcycles_per_step": p.mg.n_vcycles,
+        "precision": "mixed (f64 residual/refinement, f32 smoothing, f16 coarse)",
+        "tolerance": p.mg.tol,
         "l2": "inputs larger than L2 (working set ~100 B/cell, 1.6 GB at 256^3)",
     }
 
@@ -142,14 +159,16 @@ def run_reference(args):
     if rank != 0:
         return 0
     sc = workload(args)
-    value, sec, threads, _ = cpu_step_rate(sc, max(1, args.steps), max(0, args.warmup))
+    # a bounded sample: a 256^3 step of the oracle takes seconds
+    k, w = max(1, min(args.steps, 3)), min(args.warmup, 1)
+    value, sec, threads, _ = cpu_step_rate(sc, k, w)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene + GRF)",
         "config": workload_config(args, sc),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"full {args.n}^3 steps, median of {args.steps} after {args.warmup} warm-up"},
+                         "sample": f"full {args.n}^3 steps, median of {k} after {w} warm-up"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's own GLSL compute path needs an OpenGL 4.6 context: unavailable on this box; "
                 "this arm runs the C/OpenMP restatement of its shaders (oracle/)",
@@ -159,6 +178,64 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ GPU arm
+# DRAM bytes per k_rb_smooth4<3> launch at 256^3 from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum; profiles/k_rb_smooth4_grf256.md)
+RB_SMOOTH_TRAFFIC = None
+
+
+def step1(sim, p):
+    """One step; a tolerance solve that hits its V-cycle cap completes the
+    step and reports SS_E_NOT_CONVERGED, which its statistics record."""
+    from smokesim_b200 import SmokeSimError, abi
+    try:
+        sim.step(p, 1)
+    except SmokeSimError as e:
+        if e.code != abi.SS_E_NOT_CONVERGED:
+            raise
+
+
+def run_variant(torch, sim_cls, scene, sc, name, args, stream, barrier, world, dev, timed_stats=True):
+    """Fresh simulation of the scene, W warm-up steps, K steps timed with CUDA
+    events on the simulation's stream (max over ranks).  Returns the timing and
+    the per-step solver statistics of the timed steps."""
+    import torch.distributed as dist
+    p = variant_params(sc, name)
+    sim = sim_cls(sc["desc"], stream=stream.cuda_stream)
+    scene.apply(sim, sc)
+    for _ in range(args.warmup):
+        step1(sim, p)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    launches = 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        step1(sim, p)
+        st = sim.stats()
+        launches += st.kernel_launches
+        stats.append((st.vcycles, st.converged, st.residual / st.div_before if st.div_before > 0 else 0.0, st.rel_div))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    out = {"ms_per_step": ms / args.steps, "ms_total": ms, "gpu_launches": launches}
+    if p.mg.tol > 0:
+        out.update({
+            "vcycles_mean": statistics.mean(x[0] for x in stats),
+            "vcycles_max": max(x[0] for x in stats),
+            "converged_steps": sum(x[1] for x in stats),
+            "projected_rel_div_max": max(x[2] for x in stats),
+            "rel_div_last": stats[-1][3],
+        })
+    return sim, p, out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -180,57 +257,47 @@ def main():
     sc = workload(args)
     n = sc["desc"].n
     cells = n[0] * n[1] * n[2]
-    with torch.cuda.stream(stream):
-        sim = Sim(sc["desc"], stream=stream.cuda_stream)
-        scene.apply(sim, sc)
-        p = sc["params"]
 
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    with torch.cuda.stream(stream):
         if args.profile:
-            sim.step(p, 1)
-            sim.smooth(p, 0, 2)
+            sim = Sim(sc["desc"], stream=stream.cuda_stream)
+            scene.apply(sim, sc)
+            sim.step(sc["params"], 1)
+            sim.smooth(sc["params"], 0, 2)
             torch.cuda.synchronize()
             print(json.dumps({"profile": "done", "levels": sim.level_sizes}))
             return 0
 
-        def barrier():
-            if world > 1:
-                dist.barrier()
+        variants = {}
+        clocks = None
+        for name in [HEADLINE] + [v for v in VARIANTS if v != HEADLINE]:
+            if name == HEADLINE:
+                clk = ClockSampler(local)
+                clk.start()
+            sim, p, out = run_variant(torch, Sim, scene, sc, name, args, stream, barrier, world, dev)
+            if name == HEADLINE:
+                clocks = clk.stop()
+                head_sim, head_p = sim, p
+            else:
+                sim.close()
+            out["value"] = world * cells / (out["ms_per_step"] / 1e3) / 1e6
+            variants[name] = out
+        head = variants[HEADLINE]
+        value = head["value"]
+        sim, p = head_sim, head_p
 
-        # warm-up
-        sim.step(p, args.warmup)
-        torch.cuda.synchronize()
-        barrier()
-        torch.cuda.synchronize()
-        clk = ClockSampler(local)
-        clk.start()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        sim.step(p, args.steps)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        clocks = clk.stop()
-        ms = e0.elapsed_time(e1)
-        launches = sim.stats().kernel_launches
-        if world > 1:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        value = world * cells * args.steps / (ms / 1e3) / 1e6
-
-        # divergence actually left by this schedule (one extra, untimed step)
-        p_stats = scene.workload_params(n_vcycles=args.vcycles, collect_stats=1)
-        sim.step(p_stats, 1)
-        st = sim.stats()
-
-        # end to end through the C ABI: per step the emitter records go host->device
-        # and the step's statistics (divergence norms) come back device->host
-        pe = scene.workload_params(n_vcycles=args.vcycles, collect_stats=1)
+        # end to end through the C ABI on the headline variant: per step the
+        # emitter records go host->device and the step's statistics
+        # (divergence norms) come back device->host
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            sim.step(pe, 1)
+            step1(sim, p)
             _ = sim.stats()
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
@@ -243,17 +310,18 @@ def main():
                "d2h_bytes_per_step": 8 * 8}
 
         # roofline of the dominant kernel: the level-0 red-black smoother
-        # (k_rb_smooth, one colour per launch on the colour-split arrays).
-        # 13 B/cell per red+black sweep (read/write p, read rhs, read flag).
+        # (k_rb_smooth4, one colour per launch on the colour-split arrays).
+        # 13 B/cell per red+black sweep (read/write p, read rhs, read mask).
         reps = 10
-        sim.smooth(p, 0, 1)
+        ps = variant_params(sc, "fp32")
+        sim.smooth(ps, 0, 1)
         torch.cuda.synchronize()
         a0, a1, b0, b1 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
         a0.record(stream)
-        sim.smooth(p, 0, 1)
+        sim.smooth(ps, 0, 1)
         a1.record(stream)
         b0.record(stream)
-        sim.smooth(p, 0, 1 + reps)
+        sim.smooth(ps, 0, 1 + reps)
         b1.record(stream)
         torch.cuda.synchronize()
         sweep_ms = (b0.elapsed_time(b1) - a0.elapsed_time(a1)) / reps
@@ -266,24 +334,26 @@ def main():
             pass
         peak = float(peaks.get("hbm_gbs", 6650.0))
         achieved = alg_bytes / (launch_ms / 1e3) / 1e9
-        roofline = {"kernel": "k_rb_smooth<3> (one colour of a level-0 red-black sweep, 256^3)", "bound": "hbm",
+        roofline = {"kernel": f"k_rb_smooth4<3> (one colour of a level-0 red-black sweep, {args.n}^3)", "bound": "hbm",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                    "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": launch_ms, "traffic": None}
+                    "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": launch_ms,
+                    "traffic": RB_SMOOTH_TRAFFIC if args.n == 256 else None}
 
     line = {
         "impl": "b200", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene + GRF)",
-        "config": workload_config(args, sc), "gpu_launches": int(launches), "clocks": clocks,
-        "divergence": {"rel_div": st.rel_div, "div_before": st.div_before, "div_after": st.div_after,
-                       "vcycles": st.vcycles},
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (f64 residual/refinement, f16 coarse storage)",
+        "data": "synthetic (seeded scene + GRF)",
+        "config": workload_config(args, sc), "gpu_launches": int(head["gpu_launches"]), "clocks": clocks,
+        "variants": variants,
         "e2e": e2e, "roofline": roofline,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cv, csec, threads, _ = cpu_step_rate(sc, 1, 1)
+        cv, csec, threads, _ = cpu_step_rate(sc, 1, 0)
         line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"one full {args.n}^3 step after one warm-up step, C/OpenMP oracle"}
+                                "sample": f"one full {args.n}^3 step of the same variant from the initial state, "
+                                          f"C/OpenMP oracle"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     sim.close()

@@ -200,6 +200,10 @@ int ss_get_field(ss_sim* sim, int field, float* host, size_t count, void* stream
 /* Device pointer of the current buffer of a field (for a renderer).  Valid until
  * the next call that swaps buffers. */
 int ss_field_device_ptr(ss_sim* sim, int field, void** dptr, size_t* count);
+/* Device-to-device copies of a field (stream-ordered, no synchronisation):
+ * for renderers and autograd bindings that hold the data on the GPU. */
+int ss_set_field_device(ss_sim* sim, int field, const float* dev, size_t count, void* stream);
+int ss_get_field_device(ss_sim* sim, int field, float* dev, size_t count, void* stream);
 /* Reference clear_grid (3d/grid3d.c:164-183): zero velocities and pressure,
  * smoke = (0, 0, 0, t_ambient). */
 int ss_clear_grid(ss_sim* sim, float t_ambient, void* stream);
@@ -246,6 +250,47 @@ int ss_init_solid_map(ss_sim* sim, void* stream);                               
  * so calls that overlap on the GPU (different streams, no ordering) race. */
 int ss_divergence_norm_noalloc(int dim, const int n[3], const float* u, const float* v, const float* w,
                                const uint8_t* solid, double* out_norm, void* stream);
+
+/* ---- adjoint (reverse-mode derivatives of a rollout) ------------------------ */
+/* No counterpart in the reference.  Hand-written transposes of every stage:
+ * semi-Lagrangian advection as a scatter-add plus the chain rule through the
+ * back-traced point, buoyancy, vorticity confinement, the projection update,
+ * each V-cycle of the multigrid schedule (red-black sweeps in reverse colour
+ * order, residual + restriction, prolongation) and the divergence.  The
+ * projection must run the corrected operators (ref_quirks = 0) in FP32;
+ * obstacles are treated as fixed geometry.
+ *
+ * Control force: every step adds dt * force to the face velocities inside
+ * the active emitters (after their velocity injection); ss_set_emitter_force
+ * sets it for plain steps, the rollout below takes one per step. */
+int ss_set_emitter_force(ss_sim* sim, const float force[3]);
+
+typedef struct ss_adjoint ss_adjoint;
+/* A rollout of nsteps steps from the simulation's current state, with the
+ * state checkpointed every checkpoint_every steps (0: every step) so the
+ * reverse pass recomputes at most checkpoint_every steps per segment. */
+int ss_adjoint_create(ss_sim* sim, int nsteps, int checkpoint_every, ss_adjoint** out);
+int ss_adjoint_destroy(ss_adjoint* adj);
+/* Forward pass: nsteps steps with params, forces[k*3 + d] (host, NULL = no
+ * force) on step k.  Leaves the simulation in the final state. */
+int ss_adjoint_forward(ss_adjoint* adj, const ss_params* params, const float* forces, void* stream);
+/* Reverse pass for a loss of the final state: grad_density (nch*nx*ny*nz),
+ * grad_temperature and grad_velocity[d] are device arrays of dL/d(final
+ * field), any of them NULL for zero.  Writes dL/d(force) per step to
+ * grad_forces (host, nsteps*3, may be NULL); the derivatives with respect to
+ * the initial state are then read with ss_adjoint_field_device_ptr.  The
+ * simulation is left in the rollout's initial state. */
+int ss_adjoint_backward(ss_adjoint* adj, const ss_params* params, const float* grad_density,
+                        const float* grad_temperature, const float* const grad_velocity[3], float* grad_forces,
+                        void* stream);
+/* dL/d(initial field) after ss_adjoint_backward: SS_FIELD_VX/VY/VZ/DENSITY/
+ * TEMPERATURE/PRESSURE (the pressure that warm-starts the first solve). */
+int ss_adjoint_field_device_ptr(ss_adjoint* adj, int field, void** dptr, size_t* count);
+/* the same copied to dst (device memory when dst_on_device, else host) */
+int ss_adjoint_get_field(ss_adjoint* adj, int field, float* dst, size_t count, int dst_on_device, void* stream);
+/* Statistics of the last reverse pass: kernel launches and device bytes held
+ * by checkpoints and recomputation buffers. */
+int ss_adjoint_info(ss_adjoint* adj, long long* kernel_launches, long long* checkpoint_bytes, long long* workspace_bytes);
 
 /* Level data of the multigrid pyramid (pressure / residual), for tests. */
 enum ss_level_field { SS_LEVEL_PRESSURE = 0, SS_LEVEL_RESIDUAL = 1, SS_LEVEL_FLUID_WEIGHT = 2 };

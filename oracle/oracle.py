@@ -53,6 +53,9 @@ def load(precision="f32"):
         L.og_set_field.argtypes = [vp, i, C.POINTER(C.c_float), sz]
         L.og_get_field.argtypes = [vp, i, C.POINTER(C.c_float), sz]
         L.og_get_field_f64.argtypes = [vp, i, C.POINTER(C.c_double), sz]
+        L.og_set_field_f64.argtypes = [vp, i, C.POINTER(C.c_double), sz]
+        L.og_set_emitter_force.argtypes = [vp, C.POINTER(C.c_float * 3)]
+        L.og_set_emitter_force_f64.argtypes = [vp, C.POINTER(C.c_double * 3)]
         L.og_set_velocity_other.argtypes = [vp, i, C.POINTER(C.c_float), sz]
         L.og_get_level.argtypes = [vp, i, i, C.POINTER(C.c_float), sz]
         L.og_set_level.argtypes = [vp, i, i, C.POINTER(C.c_float), sz]
@@ -129,6 +132,16 @@ class OracleSim:
         rc = self.L.og_set_field(self.h, field, _fptr(a), a.size)
         if rc:
             raise ValueError(f"oracle set_field({field}) size {a.size}")
+
+    def set_field_f64(self, field, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64).ravel()
+        rc = self.L.og_set_field_f64(self.h, field, a.ctypes.data_as(C.POINTER(C.c_double)), a.size)
+        if rc:
+            raise ValueError(f"oracle set_field_f64({field}) rc={rc}")
+
+    def set_emitter_force(self, force):
+        f = (C.c_double * 3)(*[float(x) for x in force])
+        self.L.og_set_emitter_force_f64(self.h, C.byref(f))
 
     def get_field(self, field, f64=False):
         shp = self.shape(field)

@@ -69,6 +69,7 @@ typedef struct og_sim {
     double* p64;
     int p64_valid;
     int cround;
+    real force[3];   /* control force on the faces inside active emitters */
 } og_sim;
 
 /* ---------------------------------------------------------------- helpers */
@@ -425,8 +426,12 @@ void og_handle_emitters(og_sim* s, real dt) {
 /* Extension: emitter face-velocity injection (in place on the current buffers).
  * A face whose integer index lies inside an active emitter with set_velocity
  * takes that emitter's velocity component (last emitter wins). */
-void og_emitter_velocity(og_sim* s) {
-    int any = 0;
+/* Extension: set_velocity emitters overwrite the face velocities inside
+ * them; a control force adds dt * force to every face inside an active
+ * emitter afterwards. */
+void og_emitter_velocity(og_sim* s, real dt) {
+    const int forced = s->force[0] != 0 || s->force[1] != 0 || s->force[2] != 0;
+    int any = forced;
     for (int k = 0; k < s->ne; ++k) any |= (s->em[k].emit > 0 && s->em[k].set_velocity);
     if (!any) return;
     for (int comp = 0; comp < s->dim; ++comp) {
@@ -436,13 +441,25 @@ void og_emitter_velocity(og_sim* s) {
         for (int z = 0; z < az; ++z)
             for (int y = 0; y < ay; ++y)
                 for (int x = 0; x < ax; ++x) {
+                    int inside = 0;
                     for (int k = 0; k < s->ne; ++k) {
                         const ss_emitter* e = &s->em[k];
-                        if (!(e->emit > 0 && e->set_velocity)) continue;
-                        if (emitter_dist(s, e, x, y, z) < (real)e->radius) a[I3(x, y, z, ax, ay)] = (real)e->velocity[comp];
+                        if (!(e->emit > 0)) continue;
+                        if (emitter_dist(s, e, x, y, z) < (real)e->radius) {
+                            inside = 1;
+                            if (e->set_velocity) a[I3(x, y, z, ax, ay)] = (real)e->velocity[comp];
+                        }
                     }
+                    if (forced && inside) a[I3(x, y, z, ax, ay)] = a[I3(x, y, z, ax, ay)] + dt * s->force[comp];
                 }
     }
+}
+
+void og_set_emitter_force(og_sim* s, const float f[3]) {
+    for (int d = 0; d < 3; ++d) s->force[d] = d < s->dim ? (real)f[d] : (real)0;
+}
+void og_set_emitter_force_f64(og_sim* s, const double f[3]) {
+    for (int d = 0; d < 3; ++d) s->force[d] = d < s->dim ? (real)f[d] : (real)0;
 }
 
 /* ------------------------------------------------------------- advection */
@@ -1169,7 +1186,7 @@ void og_run_physics_step(og_sim* s, const ss_params* prm) {
     if (m & SS_STAGE_HANDLE_EMITTERS) {
         og_update_emitters_status(s, prm->current_time);
         og_handle_emitters(s, dt);
-        og_emitter_velocity(s);
+        og_emitter_velocity(s, dt);
     }
     if (m & SS_STAGE_ADVECT_VELOCITIES) advect_velocities_impl(s, dt, wind);
     if (m & SS_STAGE_APPLY_BUOYANCY) apply_buoyancy_impl(s, dt, tamb, prm->t_weight_coeff, prm->t_temp_coeff);
@@ -1212,7 +1229,7 @@ void og_stage_advect_smoke(og_sim* s, const ss_params* p) { advect_smoke_impl(s,
 void og_stage_handle_emitters(og_sim* s, const ss_params* p) {
     og_update_emitters_status(s, p->current_time);
     og_handle_emitters(s, p->time_step);
-    og_emitter_velocity(s);
+    og_emitter_velocity(s, p->time_step);
 }
 void og_stage_multigrid(og_sim* s, const ss_params* p) { og_multigrid_pressure_solve(s, &p->mg, p->time_step, p->density); }
 void og_stage_obstacles(og_sim* s, const ss_params* p) { og_obstacle_update(s, p->time_step); og_update_solid_map(s); }
@@ -1234,6 +1251,16 @@ static real* field_ptr(og_sim* s, int f, int ch, size_t* n) {
 
 /* density is channel-major: channel c occupies [c*ncell, (c+1)*ncell) */
 int og_set_field(og_sim* s, int f, const float* src, size_t count) {
+    int nch = f == SS_FIELD_DENSITY ? s->nch : 1;
+    size_t n;
+    if (!field_ptr(s, f, 0, &n) || count != n * nch) return SS_E_INVALID;
+    for (int c = 0; c < nch; ++c) {
+        real* d = field_ptr(s, f, c, &n);
+        for (size_t i = 0; i < n; ++i) d[i] = (real)src[c * n + i];
+    }
+    return 0;
+}
+int og_set_field_f64(og_sim* s, int f, const double* src, size_t count) {
     int nch = f == SS_FIELD_DENSITY ? s->nch : 1;
     size_t n;
     if (!field_ptr(s, f, 0, &n) || count != n * nch) return SS_E_INVALID;

@@ -1,0 +1,342 @@
+// adjoint.cpp - reverse pass of a rollout, with checkpointing (C ABI).
+//
+// The forward rollout saves the full simulation state every `every` steps.
+// The reverse pass walks the segments backwards: it restores a segment's
+// checkpoint, recomputes the segment saving the start state of each step,
+// then for each step (last first) restores its start state, reruns the step
+// keeping the intermediate velocities and smoke its stages read
+// (run_step's StepSaves), and applies the stages' adjoint kernels
+// (k_adjoint.cu) in reverse order.  Memory: (nsteps/every + every) states
+// plus one step's intermediates, instead of nsteps states.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ss_internal.h"
+
+using namespace ss;
+
+namespace {
+
+struct State {
+    float* vel[3] = {nullptr, nullptr, nullptr};
+    float* v_other = nullptr;   // the y ping-pong partner (stand-alone buoyancy leaves faces unwritten)
+    float* dens = nullptr;
+    float* temp = nullptr;
+    float* p = nullptr;
+    std::vector<ss_emitter> em;
+    std::vector<ss_obstacle> ob;
+};
+
+}  // namespace
+
+struct ss_adjoint {
+    ss_sim* s = nullptr;
+    int n = 0, every = 1;
+    std::vector<State> ckpt, seg;
+    std::vector<float> forces;
+    float* ub[3] = {}, *ub2[3] = {};
+    float* db = nullptr, *db2 = nullptr, *tb = nullptr, *tb2 = nullptr;
+    AdjScratch w{};
+    float* vc3 = nullptr, *wdir = nullptr, *dbar3 = nullptr, *wbar = nullptr;
+    float* ue[3] = {}, *ua[3] = {}, *un[3] = {};
+    float* dens_e = nullptr, *temp_e = nullptr;
+    double* fpart = nullptr;
+    double* fgrad = nullptr;   // nsteps * 3
+    std::vector<void*> allocs;
+    long long launches = 0, ckpt_bytes = 0, work_bytes = 0;
+    bool forward_done = false;
+};
+
+static int amalloc(ss_adjoint* A, void** p, size_t bytes, long long* counter) {
+    cudaError_t e = cudaMalloc(p, bytes > 0 ? bytes : 16);
+    if (e != cudaSuccess) return check_cuda(e, "cudaMalloc (adjoint)");
+    A->allocs.push_back(*p);
+    *counter += (long long)bytes;
+    return SS_OK;
+}
+
+static void free_adjoint(ss_adjoint* A) {
+    for (void* p : A->allocs) cudaFree(p);
+    delete A;
+}
+
+static int alloc_state(ss_adjoint* A, State& S) {
+    ss_sim* s = A->s;
+    for (int d = 0; d < s->dim; ++d) TRY_ADJ(amalloc(A, (void**)&S.vel[d], s->nv[d] * 4, &A->ckpt_bytes));
+    TRY_ADJ(amalloc(A, (void**)&S.v_other, s->nv[1] * 4, &A->ckpt_bytes));
+    TRY_ADJ(amalloc(A, (void**)&S.dens, s->ncell * s->nch * 4, &A->ckpt_bytes));
+    TRY_ADJ(amalloc(A, (void**)&S.temp, s->ncell * 4, &A->ckpt_bytes));
+    TRY_ADJ(amalloc(A, (void**)&S.p, s->ncell * 4, &A->ckpt_bytes));
+    return SS_OK;
+}
+
+static int copy_d2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    return check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st), "state copy");
+}
+
+static int save_state(ss_sim* s, State& S, cudaStream_t st) {
+    for (int d = 0; d < s->dim; ++d) TRY_ADJ(copy_d2d(S.vel[d], s->vel[d][s->vi[d]], s->nv[d] * 4, st));
+    TRY_ADJ(copy_d2d(S.v_other, s->vel[1][1 - s->vi[1]], s->nv[1] * 4, st));
+    TRY_ADJ(copy_d2d(S.dens, s->dens[s->si], s->ncell * s->nch * 4, st));
+    TRY_ADJ(copy_d2d(S.temp, s->temp[s->si], s->ncell * 4, st));
+    TRY_ADJ(copy_d2d(S.p, s->p[0], s->ncell * 4, st));
+    S.em = s->em;
+    S.ob = s->ob;
+    return SS_OK;
+}
+
+static int restore_state(ss_sim* s, const State& S, cudaStream_t st) {
+    for (int d = 0; d < s->dim; ++d) TRY_ADJ(copy_d2d(s->vel[d][s->vi[d]], S.vel[d], s->nv[d] * 4, st));
+    TRY_ADJ(copy_d2d(s->vel[1][1 - s->vi[1]], S.v_other, s->nv[1] * 4, st));
+    TRY_ADJ(copy_d2d(s->dens[s->si], S.dens, s->ncell * s->nch * 4, st));
+    TRY_ADJ(copy_d2d(s->temp[s->si], S.temp, s->ncell * 4, st));
+    TRY_ADJ(copy_d2d(s->p[0], S.p, s->ncell * 4, st));
+    s->p64_valid = 0;
+    s->em = S.em;
+    s->ob = S.ob;
+    return SS_OK;
+}
+
+static void set_force(ss_adjoint* A, int k) {
+    for (int d = 0; d < 3; ++d) A->s->force[d] = A->forces[3 * (size_t)k + d];
+}
+
+static int check_adjoint_params(const ss_adjoint* A, const ss_params* p) {
+    if (!A || !p) return set_error(SS_E_INVALID, "NULL argument");
+    if (p->stage_mask & SS_STAGE_RESOLVE_PRESSURE) {
+        if (p->mg.ref_quirks) return set_error(SS_E_UNSUPPORTED, "the adjoint transposes the corrected operators (ref_quirks = 0)");
+        if (p->mg.precision != SS_PREC_FP32) return set_error(SS_E_UNSUPPORTED, "the adjoint transposes the FP32 solve");
+    }
+    return SS_OK;
+}
+
+// Reverse of one step.  On entry the simulation holds the step's start state
+// and ub/db/tb/pbar[0] the adjoint of its end state; on return the simulation
+// holds the end state (recomputed) and the adjoint arrays the adjoint of the
+// start state.
+static int adj_step(ss_adjoint* A, const ss_params* p, int k, cudaStream_t st) {
+    ss_sim* s = A->s;
+    const StepConsts c = make_consts(s, p);
+    const int m = p->stage_mask;
+    StepSaves sv{};
+    for (int d = 0; d < s->dim; ++d) {
+        sv.emit_vel[d] = A->ue[d];
+        sv.force_vel[d] = A->ua[d];
+        sv.proj_vel[d] = A->un[d];
+    }
+    sv.emit_dens = A->dens_e;
+    sv.emit_temp = A->temp_e;
+    set_force(A, k);
+    TRY_ADJ(run_step(s, p, st, &sv));
+    const size_t ncell = s->ncell;
+    if (m & SS_STAGE_ADVECT_SMOKE) {
+        TRY_ADJ(check_cuda(cudaMemsetAsync(A->db2, 0, ncell * s->nch * 4, st), "memset"));
+        TRY_ADJ(check_cuda(cudaMemsetAsync(A->tb2, 0, ncell * 4, st), "memset"));
+        const float* vel[3] = {A->un[0], A->un[1], A->un[2]};
+        TRY_ADJ(adj_advect_smoke(s, c, vel, A->dens_e, A->temp_e, A->db, A->tb, A->db2, A->tb2, A->vc3, A->ub, st));
+        std::swap(A->db, A->db2);
+        std::swap(A->tb, A->tb2);
+    }
+    if (m & SS_STAGE_UPDATE_VELOCITIES) TRY_ADJ(adj_update(s, c, A->ub, A->w.pbar[0], st));
+    if (m & SS_STAGE_RESOLVE_PRESSURE) {
+        TRY_ADJ(check_cuda(cudaMemsetAsync(A->w.bbar[0], 0, ncell * 4, st), "memset"));
+        for (int i = 0; i < sv.vcycles; ++i) TRY_ADJ(adj_v_cycle(s, c, p->mg, A->w, st));
+        TRY_ADJ(adj_divergence(s, A->w.bbar[0], A->ub, st));
+    }
+    if (m & SS_STAGE_APPLY_VORTICITY) TRY_ADJ(adj_vorticity(s, c, s->vort, A->ub, A->wdir, A->dbar3, A->wbar, st));
+    if (m & SS_STAGE_ADVECT_VELOCITIES) {
+        for (int d = 0; d < s->dim; ++d)
+            TRY_ADJ(check_cuda(cudaMemsetAsync(A->ub2[d], 0, s->nv[d] * 4, st), "memset"));
+        const float* vel[3] = {A->ue[0], A->ue[1], A->ue[2]};
+        const float* gin[3] = {A->ub[0], A->ub[1], A->ub[2]};
+        TRY_ADJ(adj_advect_velocity(s, c, (m & SS_STAGE_APPLY_BUOYANCY) != 0, vel, A->dens_e, A->temp_e, gin, A->ub2,
+                                    A->db, A->tb, st));
+        for (int d = 0; d < 3; ++d) std::swap(A->ub[d], A->ub2[d]);
+    } else if (m & SS_STAGE_APPLY_BUOYANCY) {
+        TRY_ADJ(adj_buoyancy(s, c, A->ub[1], A->db, A->tb, st));
+    }
+    if (m & SS_STAGE_HANDLE_EMITTERS) TRY_ADJ(adj_emitters(s, c, 1, A->ub, A->fpart, A->fgrad + 3 * (size_t)k, st));
+    return SS_OK;
+}
+
+extern "C" {
+
+int ss_set_emitter_force(ss_sim* s, const float force[3]) {
+    if (!s || !force) return set_error(SS_E_INVALID, "NULL argument");
+    for (int d = 0; d < 3; ++d)
+        if (!std::isfinite(force[d])) return set_error(SS_E_NONFINITE, "force");
+    for (int d = 0; d < 3; ++d) s->force[d] = d < s->dim ? force[d] : 0.f;
+    return SS_OK;
+}
+
+int ss_adjoint_create(ss_sim* s, int nsteps, int every, ss_adjoint** out) {
+    if (!s || !out || nsteps < 1) return set_error(SS_E_INVALID, "NULL argument or nsteps < 1");
+    if (every <= 0) every = 1;
+    if (every > nsteps) every = nsteps;
+    ss_adjoint* A = new ss_adjoint();
+    A->s = s;
+    A->n = nsteps;
+    A->every = every;
+    A->forces.assign((size_t)nsteps * 3, 0.f);
+    const int nseg = (nsteps + every - 1) / every;
+    A->ckpt.resize(nseg);
+    A->seg.resize(every);
+    int rc = SS_OK;
+    for (auto& S : A->ckpt) rc = rc ? rc : alloc_state(A, S);
+    for (auto& S : A->seg) rc = rc ? rc : alloc_state(A, S);
+    auto W = [&](void** p, size_t bytes) { if (!rc) rc = amalloc(A, p, bytes, &A->work_bytes); };
+    for (int d = 0; d < s->dim; ++d) {
+        W((void**)&A->ub[d], s->nv[d] * 4);
+        W((void**)&A->ub2[d], s->nv[d] * 4);
+        W((void**)&A->ue[d], s->nv[d] * 4);
+        W((void**)&A->ua[d], s->nv[d] * 4);
+        W((void**)&A->un[d], s->nv[d] * 4);
+    }
+    W((void**)&A->db, s->ncell * s->nch * 4);
+    W((void**)&A->db2, s->ncell * s->nch * 4);
+    W((void**)&A->tb, s->ncell * 4);
+    W((void**)&A->tb2, s->ncell * 4);
+    W((void**)&A->dens_e, s->ncell * s->nch * 4);
+    W((void**)&A->temp_e, s->ncell * 4);
+    W((void**)&A->vc3, s->ncell * 3 * 4);
+    W((void**)&A->wdir, s->ncell * 3 * 4);
+    W((void**)&A->dbar3, s->ncell * 3 * 4);
+    W((void**)&A->wbar, s->ncell * 3 * 4);
+    for (int l = 0; l < s->levels; ++l) {
+        const size_t n = (size_t)s->lv[l].n[0] * s->lv[l].n[1] * s->lv[l].n[2];
+        W((void**)&A->w.pbar[l], n * 4);
+        W((void**)&A->w.bbar[l], n * 4);
+        W((void**)&A->w.T[l], n * 4);
+    }
+    W((void**)&A->fpart, (size_t)adj_force_blocks(s) * 3 * sizeof(double));
+    W((void**)&A->fgrad, (size_t)nsteps * 3 * sizeof(double));
+    if (rc) {
+        free_adjoint(A);
+        return rc;
+    }
+    *out = A;
+    return SS_OK;
+}
+
+int ss_adjoint_destroy(ss_adjoint* A) {
+    if (!A) return set_error(SS_E_INVALID, "NULL handle");
+    cudaDeviceSynchronize();
+    free_adjoint(A);
+    return SS_OK;
+}
+
+int ss_adjoint_forward(ss_adjoint* A, const ss_params* p, const float* forces, void* stream) {
+    TRY_ADJ(check_adjoint_params(A, p));
+    ss_sim* s = A->s;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (forces) {
+        for (size_t i = 0; i < A->forces.size(); ++i)
+            if (!std::isfinite(forces[i])) return set_error(SS_E_NONFINITE, "force");
+        std::memcpy(A->forces.data(), forces, A->forces.size() * sizeof(float));
+    } else {
+        std::fill(A->forces.begin(), A->forces.end(), 0.f);
+    }
+    s->nlaunch = 0;
+    for (int k = 0; k < A->n; ++k) {
+        if (k % A->every == 0) TRY_ADJ(save_state(s, A->ckpt[k / A->every], st));
+        set_force(A, k);
+        TRY_ADJ(run_step(s, p, st, nullptr));
+    }
+    for (int d = 0; d < 3; ++d) s->force[d] = 0.f;
+    A->forward_done = true;
+    return check_cuda(cudaGetLastError(), "adjoint forward");
+}
+
+int ss_adjoint_backward(ss_adjoint* A, const ss_params* p, const float* grad_density, const float* grad_temperature,
+                        const float* const grad_velocity[3], float* grad_forces, void* stream) {
+    TRY_ADJ(check_adjoint_params(A, p));
+    if (!A->forward_done) return set_error(SS_E_INVALID, "ss_adjoint_forward has not run");
+    ss_sim* s = A->s;
+    cudaStream_t st = (cudaStream_t)stream;
+    s->nlaunch = 0;
+    // adjoint of the final state
+    for (int d = 0; d < s->dim; ++d) {
+        if (grad_velocity && grad_velocity[d]) TRY_ADJ(copy_d2d(A->ub[d], grad_velocity[d], s->nv[d] * 4, st));
+        else TRY_ADJ(check_cuda(cudaMemsetAsync(A->ub[d], 0, s->nv[d] * 4, st), "memset"));
+    }
+    if (grad_density) TRY_ADJ(copy_d2d(A->db, grad_density, s->ncell * s->nch * 4, st));
+    else TRY_ADJ(check_cuda(cudaMemsetAsync(A->db, 0, s->ncell * s->nch * 4, st), "memset"));
+    if (grad_temperature) TRY_ADJ(copy_d2d(A->tb, grad_temperature, s->ncell * 4, st));
+    else TRY_ADJ(check_cuda(cudaMemsetAsync(A->tb, 0, s->ncell * 4, st), "memset"));
+    TRY_ADJ(check_cuda(cudaMemsetAsync(A->w.pbar[0], 0, s->ncell * 4, st), "memset"));
+    TRY_ADJ(check_cuda(cudaMemsetAsync(A->fgrad, 0, (size_t)A->n * 3 * sizeof(double), st), "memset"));
+    const int nseg = (A->n + A->every - 1) / A->every;
+    for (int sg = nseg - 1; sg >= 0; --sg) {
+        const int k0 = sg * A->every, k1 = std::min(A->n, k0 + A->every);
+        TRY_ADJ(restore_state(s, A->ckpt[sg], st));
+        for (int k = k0; k < k1; ++k) {
+            TRY_ADJ(save_state(s, A->seg[k - k0], st));
+            if (k + 1 < k1) {
+                set_force(A, k);
+                TRY_ADJ(run_step(s, p, st, nullptr));
+            }
+        }
+        for (int k = k1 - 1; k >= k0; --k) {
+            TRY_ADJ(restore_state(s, A->seg[k - k0], st));
+            TRY_ADJ(adj_step(A, p, k, st));
+        }
+    }
+    TRY_ADJ(restore_state(s, A->ckpt[0], st));
+    for (int d = 0; d < 3; ++d) s->force[d] = 0.f;
+    A->launches = s->nlaunch;
+    if (grad_forces) {
+        std::vector<double> g((size_t)A->n * 3);
+        TRY_ADJ(check_cuda(cudaMemcpyAsync(g.data(), A->fgrad, g.size() * sizeof(double), cudaMemcpyDeviceToHost, st),
+                           "force gradient"));
+        TRY_ADJ(check_cuda(cudaStreamSynchronize(st), "adjoint sync"));
+        for (size_t i = 0; i < g.size(); ++i) grad_forces[i] = (float)g[i];
+    }
+    return check_cuda(cudaGetLastError(), "adjoint backward");
+}
+
+int ss_adjoint_field_device_ptr(ss_adjoint* A, int field, void** dptr, size_t* count) {
+    if (!A || !dptr) return set_error(SS_E_INVALID, "NULL argument");
+    ss_sim* s = A->s;
+    void* d = nullptr;
+    size_t n = 0;
+    switch (field) {
+    case SS_FIELD_VX: d = A->ub[0]; n = s->nv[0]; break;
+    case SS_FIELD_VY: d = A->ub[1]; n = s->nv[1]; break;
+    case SS_FIELD_VZ: if (s->dim == 3) { d = A->ub[2]; n = s->nv[2]; } break;
+    case SS_FIELD_DENSITY: d = A->db; n = s->ncell * s->nch; break;
+    case SS_FIELD_TEMPERATURE: d = A->tb; n = s->ncell; break;
+    case SS_FIELD_PRESSURE: d = A->w.pbar[0]; n = s->ncell; break;
+    default: break;
+    }
+    if (!d) return set_error(SS_E_INVALID, "no adjoint for this field");
+    *dptr = d;
+    if (count) *count = n;
+    return SS_OK;
+}
+
+int ss_adjoint_get_field(ss_adjoint* A, int field, float* dst, size_t count, int dst_on_device, void* stream) {
+    if (!A || !dst) return set_error(SS_E_INVALID, "NULL argument");
+    void* d = nullptr;
+    size_t n = 0;
+    TRY_ADJ(ss_adjoint_field_device_ptr(A, field, &d, &n));
+    if (count != n) return set_error(SS_E_INVALID, "element count does not match the field");
+    cudaStream_t st = (cudaStream_t)stream;
+    TRY_ADJ(check_cuda(cudaMemcpyAsync(dst, d, n * sizeof(float), dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st),
+                       "adjoint field"));
+    if (!dst_on_device) TRY_ADJ(check_cuda(cudaStreamSynchronize(st), "adjoint field sync"));
+    return SS_OK;
+}
+
+int ss_adjoint_info(ss_adjoint* A, long long* launches, long long* ckpt_bytes, long long* work_bytes) {
+    if (!A) return set_error(SS_E_INVALID, "NULL handle");
+    if (launches) *launches = A->launches;
+    if (ckpt_bytes) *ckpt_bytes = A->ckpt_bytes;
+    if (work_bytes) *work_bytes = A->work_bytes;
+    return SS_OK;
+}
+
+}  // extern "C"

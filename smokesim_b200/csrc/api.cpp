@@ -233,10 +233,10 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     if (s->enclosed) s->div0r = s->div0;
     else A((void**)&s->div0r, s->ncell * sizeof(float));
     A((void**)&s->vort, s->ncell * (s->dim == 3 ? 3 : 1) * sizeof(float));
+    A((void**)&s->fmask, s->ncell);   // level-0 fluid mask (k_rb.cu, k_mixed.cu, k_adjoint.cu)
     if (s->nx % 2 == 0 && s->levels > 1) {   // colour-split level 0 (k_rb.cu)
         A((void**)&s->rhs_s, s->ncell * sizeof(float));
         A((void**)&s->rhs_r, s->ncell * sizeof(float));
-        A((void**)&s->fmask, s->ncell);
         A((void**)&s->rb_mask, s->ncell);
     }
     s->red.max_blocks = (int)(((s->nx + 32) / 32 + 1) * ((s->ny + 8) / 8 + 1) * (size_t)(s->nz + 1));
@@ -468,8 +468,32 @@ int ss_set_field(ss_sim* s, int f, const float* host, size_t count, void* stream
     for (size_t i = 0; i < n; ++i)
         if (!isfinite(host[i])) return set_error(SS_E_NONFINITE, "non-finite value in field data");
     cudaStream_t st = as_stream(stream);
+    if (f == SS_FIELD_PRESSURE) s->p64_valid = 0;
     CU(cudaMemcpyAsync(d, host, n * sizeof(float), cudaMemcpyHostToDevice, st), "set_field");
     CU(cudaStreamSynchronize(st), "set_field sync");
+    return SS_OK;
+}
+
+int ss_set_field_device(ss_sim* s, int f, const float* dev, size_t count, void* stream) {
+    if (!s || !dev) return set_error(SS_E_INVALID, "NULL argument");
+    if (f == SS_FIELD_SOLID || f == SS_FIELD_DIVERGENCE) return set_error(SS_E_INVALID, "field is read only (use ss_set_scene)");
+    float* d;
+    size_t n;
+    TRY(field_buffer(s, f, &d, &n));
+    if (count != n) return set_error(SS_E_INVALID, "element count does not match the field");
+    if (f == SS_FIELD_PRESSURE) s->p64_valid = 0;
+    CU(cudaMemcpyAsync(d, dev, n * sizeof(float), cudaMemcpyDeviceToDevice, as_stream(stream)), "set_field_device");
+    return SS_OK;
+}
+
+int ss_get_field_device(ss_sim* s, int f, float* dev, size_t count, void* stream) {
+    if (!s || !dev) return set_error(SS_E_INVALID, "NULL argument");
+    if (f == SS_FIELD_SOLID || f == SS_FIELD_DIVERGENCE) return set_error(SS_E_INVALID, "use ss_get_field for this field");
+    float* d;
+    size_t n;
+    TRY(field_buffer(s, f, &d, &n));
+    if (count != n) return set_error(SS_E_INVALID, "element count does not match the field");
+    CU(cudaMemcpyAsync(dev, d, n * sizeof(float), cudaMemcpyDeviceToDevice, as_stream(stream)), "get_field_device");
     return SS_OK;
 }
 
@@ -779,7 +803,14 @@ static int pressure_solve(ss_sim* s, const ss_params* p, const StepConsts& c, cu
     return SS_OK;
 }
 
-static int do_step(ss_sim* s, const ss_params* p, cudaStream_t st) {
+static int save_vel(ss_sim* s, float* const dst[3], cudaStream_t st) {
+    for (int d = 0; d < s->dim; ++d)
+        if (dst[d]) CU(cudaMemcpyAsync(dst[d], s->vel[d][s->vi[d]], s->nv[d] * sizeof(float), cudaMemcpyDeviceToDevice, st),
+                       "save velocity");
+    return SS_OK;
+}
+
+static int do_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* sv = nullptr) {
     const StepConsts c = make_consts(s, p);
     const int m = p->stage_mask;
     if (m & SS_STAGE_HANDLE_EMITTERS) {
@@ -787,13 +818,24 @@ static int do_step(ss_sim* s, const ss_params* p, cudaStream_t st) {
         TRY(upload_array((void**)&s->d_em, &s->cap_em, s->em.data(), sizeof(ss_emitter), (int)s->em.size(), st));
         TRY(launch_emitters(s, c, st));
     }
+    if (sv) {
+        TRY(save_vel(s, sv->emit_vel, st));
+        if (sv->emit_dens)
+            CU(cudaMemcpyAsync(sv->emit_dens, s->dens[s->si], s->ncell * s->nch * sizeof(float), cudaMemcpyDeviceToDevice, st), "save");
+        if (sv->emit_temp)
+            CU(cudaMemcpyAsync(sv->emit_temp, s->temp[s->si], s->ncell * sizeof(float), cudaMemcpyDeviceToDevice, st), "save");
+    }
     if (m & SS_STAGE_ADVECT_VELOCITIES) {
         TRY(launch_advect_velocities(s, c, (m & SS_STAGE_APPLY_BUOYANCY) != 0, st));
     } else if (m & SS_STAGE_APPLY_BUOYANCY) {
         TRY(launch_buoyancy(s, c, st));
     }
+    if (sv) TRY(save_vel(s, sv->force_vel, st));
     if (m & SS_STAGE_APPLY_VORTICITY) TRY(launch_vorticity(s, c, st));
-    if (m & SS_STAGE_RESOLVE_PRESSURE) TRY(pressure_solve(s, p, c, st));
+    if (m & SS_STAGE_RESOLVE_PRESSURE) {
+        TRY(pressure_solve(s, p, c, st));
+        if (sv) sv->vcycles = s->st.vcycles;
+    }
     if (m & SS_STAGE_UPDATE_VELOCITIES) {
         if (p->mg.precision != SS_PREC_FP32 && s->p64_valid) TRY(launch_update_velocities_p64(s, c, st));
         else TRY(launch_update_velocities(s, c, st));
@@ -804,6 +846,7 @@ static int do_step(ss_sim* s, const ss_params* p, cudaStream_t st) {
             s->st.rel_div = s->st.div_before > 0 ? s->st.div_after / s->st.div_before : 0.0;
         }
     }
+    if (sv) TRY(save_vel(s, sv->proj_vel, st));
     if (m & SS_STAGE_ADVECT_SMOKE) TRY(launch_advect_smoke(s, c, st));
     if (m & SS_STAGE_OBSTACLES) {
         if (scene_moving(s)) {
@@ -966,3 +1009,5 @@ int ss_init_solid_map(ss_sim* s, void* stream) {
 }
 
 }  // extern "C"
+
+int ss::run_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* saves) { return do_step(s, p, st, saves); }

@@ -1,0 +1,970 @@
+// k_adjoint.cu - hand-written adjoints (transposes) of the step's stages.
+//
+// Each kernel here is the transpose of one forward kernel of k_fluid.cu /
+// k_mg.cu / k_rb.cu for the same inputs: it maps the adjoint of the stage's
+// output to the adjoint of its input, evaluated at the forward state the
+// stage saw (semi-Lagrangian advection and vorticity confinement are
+// nonlinear; the rest are linear).  No counterpart in the reference, which has
+// no derivatives; the forward operators they transpose are restatements of
+// its shaders (cited at the forward kernels).
+//
+//  - advection: the trilinear gather becomes a scatter-add (atomicAdd) into
+//    the advected array, plus the chain rule through the back-traced point
+//    into the velocity that traced it;
+//  - buoyancy: a 2-tap average per y face, transposed into the two cells;
+//  - vorticity confinement: f = N x w with N = grad|w| / (|grad|w|| + 1e-20),
+//    w = curl of the cell-centred velocity; its Jacobian-transpose in three
+//    passes (force -> w and grad|w|, grad|w| -> |w| -> w, w -> faces);
+//  - projection: the update's pressure gradient transposes into a
+//    divergence-like gather; each V-cycle of the fixed schedule is transposed
+//    operator by operator (red-black colour updates in reverse order,
+//    residual + restriction, prolongation), and the right-hand side's
+//    divergence into a face scatter.
+#include "common.cuh"
+#include "ss_internal.h"
+
+namespace ss {
+
+static inline dim3 grid_of(int ax, int ay, int az, dim3 b) {
+    return dim3((ax + b.x - 1) / b.x, (ay + b.y - 1) / b.y, (az + b.z - 1) / b.z);
+}
+
+SS_D bool in3(int x, int y, int z, int ax, int ay, int az) {
+    return x >= 0 && y >= 0 && z >= 0 && x < ax && y < ay && z < az;
+}
+SS_D bool solid1(const uint8_t* f, int x, int y, int z, int nx, int ny, int nz) {   // out of grid = solid
+    if (!in3(x, y, z, nx, ny, nz)) return true;
+    return f[idx3(x, y, z, nx, ny)] & F_SOLID;
+}
+SS_D bool solid0(const uint8_t* f, int x, int y, int z, int nx, int ny, int nz) {   // out of grid = fluid
+    if (!in3(x, y, z, nx, ny, nz)) return false;
+    return f[idx3(x, y, z, nx, ny)] & F_SOLID;
+}
+SS_D void scatter(float* a, int ax, int ay, int az, int x, int y, int z, float v) {
+    if (in3(x, y, z, ax, ay, az) && v != 0.f) atomicAdd(a + idx3(x, y, z, ax, ay), v);
+}
+
+// Adjoint of one border-filtered trilinear sample with taps t: scatters
+// g * weight into abar at the in-range taps and returns d(sample)/d(w) per
+// axis in dw (tap values outside the array read `border`).
+template <int DIM>
+SS_D void adj_sample(const float* __restrict__ a, float* __restrict__ abar, int ax, int ay, int az, const Taps& t,
+                     float border, float g, float dw[3]) {
+    const int x0 = t.x0, y0 = t.y0, z0 = t.z0;
+    const float wx = t.wx, wy = t.wy, wz = t.wz;
+    if constexpr (DIM == 2) {
+        const float c00 = fetch_b(a, ax, ay, 1, x0, y0, 0, border), c10 = fetch_b(a, ax, ay, 1, x0 + 1, y0, 0, border);
+        const float c01 = fetch_b(a, ax, ay, 1, x0, y0 + 1, 0, border), c11 = fetch_b(a, ax, ay, 1, x0 + 1, y0 + 1, 0, border);
+        dw[0] = (1.f - wy) * (c10 - c00) + wy * (c11 - c01);
+        dw[1] = lerp_(c01, c11, wx) - lerp_(c00, c10, wx);
+        dw[2] = 0.f;
+        if (abar) {
+            scatter(abar, ax, ay, 1, x0, y0, 0, g * (1.f - wx) * (1.f - wy));
+            scatter(abar, ax, ay, 1, x0 + 1, y0, 0, g * wx * (1.f - wy));
+            scatter(abar, ax, ay, 1, x0, y0 + 1, 0, g * (1.f - wx) * wy);
+            scatter(abar, ax, ay, 1, x0 + 1, y0 + 1, 0, g * wx * wy);
+        }
+    } else {
+        float c[2][2][2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int i = 0; i < 2; ++i) c[k][j][i] = fetch_b(a, ax, ay, az, x0 + i, y0 + j, z0 + k, border);
+        const float e0 = (1.f - wy) * (c[0][0][1] - c[0][0][0]) + wy * (c[0][1][1] - c[0][1][0]);
+        const float e1 = (1.f - wy) * (c[1][0][1] - c[1][0][0]) + wy * (c[1][1][1] - c[1][1][0]);
+        dw[0] = (1.f - wz) * e0 + wz * e1;
+        const float f0 = lerp_(c[0][1][0], c[0][1][1], wx) - lerp_(c[0][0][0], c[0][0][1], wx);
+        const float f1 = lerp_(c[1][1][0], c[1][1][1], wx) - lerp_(c[1][0][0], c[1][0][1], wx);
+        dw[1] = (1.f - wz) * f0 + wz * f1;
+        const float s0 = lerp_(lerp_(c[0][0][0], c[0][0][1], wx), lerp_(c[0][1][0], c[0][1][1], wx), wy);
+        const float s1 = lerp_(lerp_(c[1][0][0], c[1][0][1], wx), lerp_(c[1][1][0], c[1][1][1], wx), wy);
+        dw[2] = s1 - s0;
+        if (abar) {
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) {
+                        const float w = (i ? wx : 1.f - wx) * (j ? wy : 1.f - wy) * (k ? wz : 1.f - wz);
+                        scatter(abar, ax, ay, az, x0 + i, y0 + j, z0 + k, g * w);
+                    }
+        }
+    }
+}
+
+// d(tap weight)/d(texel coordinate): 1 inside the clamp range, 0 where
+// make_taps clamped the coordinate
+SS_D float clamp_grad(float t, int a) { return (t > -2.f && t < (float)(a + 1)) ? 1.f : 0.f; }
+
+struct AdjFluid {
+    int nx, ny, nz, nch;
+    const float* u;   // forward velocity the stage read
+    const float* v;
+    const float* w;
+    const uint8_t* flags;
+    const float* dens;   // forward smoke the stage read
+    const float* temp;
+    StepConsts c;
+};
+
+// --------------------------------------------------------- smoke advection^T
+// Forward (k_advect_smoke): out(c) = sample(in, centre(c) - cfl * vel_centre(c)),
+// solid cells set to (0, t_amb).  Adjoint: scatter into din/tin, and the
+// position gradient into a per-cell velocity adjoint (vcb, 3 arrays), spread to
+// the faces by k_adj_centre_to_faces.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_advect_smoke(AdjFluid a, const float* __restrict__ dout, const float* __restrict__ tout,
+                                                          float* __restrict__ din, float* __restrict__ tin,
+                                                          float* __restrict__ vcb) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    if (x >= nx || y >= ny || z >= nz) return;
+    const int c = idx3(x, y, z, nx, ny);
+    const size_t ncell = (size_t)nx * ny * nz;
+    float vb[3] = {0.f, 0.f, 0.f};
+    if (!(a.flags[c] & F_SOLID)) {
+        float vel[3];
+        vel_at_centre<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+        const float cfl = a.c.cfl;
+        const float gx = (float)x + 0.5f, gy = (float)y + 0.5f, gz = DIM == 3 ? (float)z + 0.5f : 0.f;
+        const float tx = gx - vel[0] * cfl - 0.5f, ty = gy - vel[1] * cfl - 0.5f, tz = gz - vel[2] * cfl - 0.5f;
+        const Taps t = make_taps<DIM>(nx, ny, nz, tx, ty, tz);
+        float bb[3] = {0.f, 0.f, 0.f};
+        float dw[3];
+        for (int ch = 0; ch <= a.nch; ++ch) {
+            const bool is_t = ch == a.nch;
+            const float g = is_t ? tout[c] : dout[ch * ncell + c];
+            if (g == 0.f) continue;
+            const float* src = is_t ? a.temp : a.dens + ch * ncell;
+            float* dst = is_t ? tin : din + ch * ncell;
+            adj_sample<DIM>(src, dst, nx, ny, nz, t, is_t ? a.c.t_amb : 0.f, g, dw);
+            bb[0] += g * dw[0];
+            bb[1] += g * dw[1];
+            bb[2] += g * dw[2];
+        }
+        vb[0] = -cfl * bb[0] * clamp_grad(tx, nx);
+        vb[1] = -cfl * bb[1] * clamp_grad(ty, ny);
+        vb[2] = DIM == 3 ? -cfl * bb[2] * clamp_grad(tz, nz) : 0.f;
+    }
+    vcb[c] = vb[0];
+    vcb[ncell + c] = vb[1];
+    if (DIM == 3) vcb[2 * ncell + c] = vb[2];
+}
+
+// faces += 0.5 * (per-cell velocity adjoint of the two cells sharing the face)
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_centre_to_faces(const float* __restrict__ vcb, int nx, int ny, int nz,
+                                                             float* __restrict__ ub, float* __restrict__ vbar,
+                                                             float* __restrict__ wb) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const size_t ncell = (size_t)nx * ny * nz;
+#pragma unroll
+    for (int comp = 0; comp < DIM; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        const int xm = x - (comp == 0), ym = y - (comp == 1), zm = z - (comp == 2);
+        float s = 0.f;
+        if (in3(x, y, z, nx, ny, nz)) s += 0.5f * vcb[comp * ncell + idx3(x, y, z, nx, ny)];
+        if (in3(xm, ym, zm, nx, ny, nz)) s += 0.5f * vcb[comp * ncell + idx3(xm, ym, zm, nx, ny)];
+        float* dst = comp == 0 ? ub : comp == 1 ? vbar : wb;
+        dst[idx3(x, y, z, ax, ay)] += s;
+    }
+}
+
+// ------------------------------------------------------ projection update^T
+// Forward (k_update_velocity): faces touching solid (out of grid = fluid) take
+// the solid velocity, the rest u + k_upd * (p_hi - p_lo) (out of grid p = 0).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_update_faces(const uint8_t* __restrict__ flags, int nx, int ny, int nz,
+                                                          float* __restrict__ ub, float* __restrict__ vbar,
+                                                          float* __restrict__ wb) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+#pragma unroll
+    for (int comp = 0; comp < DIM; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        const bool touching = solid0(flags, x, y, z, nx, ny, nz) ||
+                              solid0(flags, x - (comp == 0), y - (comp == 1), z - (comp == 2), nx, ny, nz);
+        if (touching) (comp == 0 ? ub : comp == 1 ? vbar : wb)[idx3(x, y, z, ax, ay)] = 0.f;
+    }
+}
+
+// pbar(c) += k_upd * sum over axes (ubar(low face of c) - ubar(high face of c)),
+// ubar already zero on faces that touch solid
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_update_pressure(const float* __restrict__ ub, const float* __restrict__ vbar,
+                                                             const float* __restrict__ wb, int nx, int ny, int nz,
+                                                             float k_upd, float* __restrict__ pbar) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (x >= nx || y >= ny || z >= nz) return;
+    float s = ub[idx3(x, y, z, nx + 1, ny)] - ub[idx3(x + 1, y, z, nx + 1, ny)];
+    s += vbar[idx3(x, y, z, nx, ny + 1)] - vbar[idx3(x, y + 1, z, nx, ny + 1)];
+    if constexpr (DIM == 3) s += wb[idx3(x, y, z, nx, ny)] - wb[idx3(x, y, z + 1, nx, ny)];
+    pbar[idx3(x, y, z, nx, ny)] += k_upd * s;
+}
+
+// ------------------------------------------------------------- divergence^T
+// Forward (k_divergence, smoother rule): div(c) = sum of +-face velocities,
+// the face towards a solid neighbour replaced by the solid's velocity.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_divergence(const float* __restrict__ dbar, const uint8_t* __restrict__ flags,
+                                                        int nx, int ny, int nz, float* __restrict__ ub,
+                                                        float* __restrict__ vbar, float* __restrict__ wb) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+#pragma unroll
+    for (int comp = 0; comp < DIM; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        const int xm = x - (comp == 0), ym = y - (comp == 1), zm = z - (comp == 2);
+        const uint8_t lo_bit = comp == 0 ? F_RIGHT : comp == 1 ? F_TOP : F_FRONT;   // face seen from the low cell
+        const uint8_t hi_bit = comp == 0 ? F_LEFT : comp == 1 ? F_BOTTOM : F_BACK;  // seen from the high cell
+        float s = 0.f;
+        if (in3(x, y, z, nx, ny, nz)) {
+            const int c = idx3(x, y, z, nx, ny);
+            const uint8_t f = flags[c];
+            if (!(f & F_SOLID) && !(f & hi_bit)) s -= dbar[c];
+        }
+        if (in3(xm, ym, zm, nx, ny, nz)) {
+            const int c = idx3(xm, ym, zm, nx, ny);
+            const uint8_t f = flags[c];
+            if (!(f & F_SOLID) && !(f & lo_bit)) s += dbar[c];
+        }
+        (comp == 0 ? ub : comp == 1 ? vbar : wb)[idx3(x, y, z, ax, ay)] += s;
+    }
+}
+
+// ------------------------------------------------------------- V-cycle^T
+// One multigrid level for the transposed operators, natural layout.  Level 0
+// reads the fluid mask (weights 0/1, count of fluid neighbours), coarse levels
+// the FP16-rounded solid fraction alpha (weights 1 - alpha, out of grid
+// 1 - oobA).  The forward operators are smooth_cell / residual_cell /
+// k_prolong (corrected out-of-grid rule) and the level-0 kernels of k_rb.cu.
+struct AdjLevel {
+    int nx, ny, nz;
+    const uint8_t* fmask;   // level 0
+    const float* alpha;     // level >= 1
+    float oobA;
+    float beta;    // smoother right-hand-side factor: rho*h/dt (level 0, on div), h_L^2 (level >= 1)
+    float rcoef;   // residual right-hand-side factor: rho/(dt*h) (level 0), 1 (level >= 1)
+    float hh;
+    float* pbar;
+    float* bbar;
+    float* T;
+};
+
+// weight of cell (x,y,z)'s pressure in a neighbour's equation, and the
+// cell's own diagonal d (sum of its neighbours' weights); updated: the
+// forward smoother writes this cell
+template <int DIM, bool L0>
+SS_D void cell_weights(const AdjLevel& a, int x, int y, int z, float& wself, float& d, bool& fluid) {
+    const int c = idx3(x, y, z, a.nx, a.ny);
+    if constexpr (L0) {
+        const uint8_t m = a.fmask[c];
+        fluid = m & M_FLUID;
+        wself = fluid ? 1.f : 0.f;
+        d = (float)__popc(m & 0x7Eu);
+    } else {
+        const float al = a.alpha[c];
+        fluid = al < 1.f;
+        wself = 1.f - al;
+        auto f = [&](int X, int Y, int Z) {
+            return 1.f - (in3(X, Y, Z, a.nx, a.ny, a.nz) ? a.alpha[idx3(X, Y, Z, a.nx, a.ny)] : a.oobA);
+        };
+        float s = f(x, y + 1, z) + f(x, y - 1, z);
+        s = s + f(x + 1, y, z);
+        s = s + f(x - 1, y, z);
+        if constexpr (DIM == 3) s = s + f(x, y, z + 1) + f(x, y, z - 1);
+        d = s;
+    }
+}
+
+template <int DIM>
+SS_D float nbr_sum(const float* __restrict__ T, int x, int y, int z, int nx, int ny, int nz) {
+    float s = 0.f;
+    if (y + 1 < ny) s += T[idx3(x, y + 1, z, nx, ny)];
+    if (y > 0) s += T[idx3(x, y - 1, z, nx, ny)];
+    if (x + 1 < nx) s += T[idx3(x + 1, y, z, nx, ny)];
+    if (x > 0) s += T[idx3(x - 1, y, z, nx, ny)];
+    if constexpr (DIM == 3) {
+        if (z + 1 < nz) s += T[idx3(x, y, z + 1, nx, ny)];
+        if (z > 0) s += T[idx3(x, y, z - 1, nx, ny)];
+    }
+    return s;
+}
+
+// One colour's half of consecutive transposed colour updates:
+//  B (the gather half of the previous transpose): pbar += w_self * sum of the
+//    neighbours' T;
+//  A (this colour's transpose): t = pbar / d, T = t, pbar = 0, bbar -= beta*t.
+template <int DIM, bool L0>
+__global__ void __launch_bounds__(256) k_adj_smooth(AdjLevel a, int colour, int do_b, int do_a) {
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((y + z + colour) & 1);
+    if (x >= a.nx || y >= a.ny || z >= a.nz) return;
+    const int c = idx3(x, y, z, a.nx, a.ny);
+    float wself, d;
+    bool fluid;
+    cell_weights<DIM, L0>(a, x, y, z, wself, d, fluid);
+    float pb = a.pbar[c];
+    if (do_b) pb += wself * nbr_sum<DIM>(a.T, x, y, z, a.nx, a.ny, a.nz);
+    if (do_a) {
+        if (fluid && d != 0.f) {
+            const float t = pb / d;
+            a.T[c] = t;
+            pb = 0.f;
+            a.bbar[c] -= a.beta * t;
+        } else {
+            a.T[c] = 0.f;
+        }
+    }
+    a.pbar[c] = pb;
+}
+
+// residual adjoint of a fine cell from its coarse parent
+template <int DIM, bool L0>
+SS_D float res_bar(const AdjLevel& a, const float* __restrict__ rcb, int cx, int cy, int cz, int x, int y, int z) {
+    const int X = x >> 1, Y = y >> 1, Z = DIM == 3 ? z >> 1 : 0;
+    if (X >= cx || Y >= cy || Z >= cz) return 0.f;
+    const int c = idx3(x, y, z, a.nx, a.ny);
+    const bool fluid = L0 ? (a.fmask[c] & M_FLUID) != 0 : a.alpha[c] < 1.f;
+    if (!fluid) return 0.f;
+    return rcb[idx3(X, Y, Z, cx, cy)] / (DIM == 3 ? 8.f : 4.f);
+}
+
+// Transpose of residual + restriction: r_c(X) = mean of the children's
+// residuals b - (sum_j w_j p_j - d p) / h^2.
+template <int DIM, bool L0>
+__global__ void __launch_bounds__(256) k_adj_residual_restrict(AdjLevel a, const float* __restrict__ rcb, int cx, int cy, int cz) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    if (x >= nx || y >= ny || z >= nz) return;
+    const int c = idx3(x, y, z, nx, ny);
+    float wself, d;
+    bool fluid;
+    cell_weights<DIM, L0>(a, x, y, z, wself, d, fluid);
+    const float rs = res_bar<DIM, L0>(a, rcb, cx, cy, cz, x, y, z);
+    float nb = 0.f;
+    if (y + 1 < ny) nb += res_bar<DIM, L0>(a, rcb, cx, cy, cz, x, y + 1, z);
+    if (y > 0) nb += res_bar<DIM, L0>(a, rcb, cx, cy, cz, x, y - 1, z);
+    if (x + 1 < nx) nb += res_bar<DIM, L0>(a, rcb, cx, cy, cz, x + 1, y, z);
+    if (x > 0) nb += res_bar<DIM, L0>(a, rcb, cx, cy, cz, x - 1, y, z);
+    if constexpr (DIM == 3) {
+        if (z + 1 < nz) nb += res_bar<DIM, L0>(a, rcb, cx, cy, cz, x, y, z + 1);
+        if (z > 0) nb += res_bar<DIM, L0>(a, rcb, cx, cy, cz, x, y, z - 1);
+    }
+    a.pbar[c] += (d * rs - wself * nb) / a.hh;
+    a.bbar[c] += a.rcoef * rs;
+}
+
+// per-axis interpolation coefficient of fine index x on coarse index K
+SS_D float prolong_coef(int x, int af, int cf, int K) {
+    const float tx = (((float)x + 0.5f) / (float)af) * (float)cf - 0.5f;
+    const float fx = floorf(tx);
+    const int x0 = (int)fx;
+    const float w = tx - fx;
+    const int lo = min(max(x0, 0), cf - 1), hi = min(max(x0 + 1, 0), cf - 1);
+    return (lo == K ? 1.f - w : 0.f) + (hi == K ? w : 0.f);
+}
+
+// Transpose of p_f += trilinear(p_c): p_c_bar(K) = sum over the fine cells
+// whose interpolation stencil holds K
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_prolong(const float* __restrict__ pfb, int ax, int ay, int az,
+                                                     float* __restrict__ pcb, int cx, int cy, int cz) {
+    const int X = blockIdx.x * blockDim.x + threadIdx.x;
+    const int Y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int Z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (X >= cx || Y >= cy || Z >= cz) return;
+    float s = 0.f;
+    const int z0 = DIM == 3 ? 2 * Z - 2 : 0, z1 = DIM == 3 ? 2 * Z + 3 : 0;
+    for (int z = max(z0, 0); z <= min(z1, az - 1); ++z) {
+        const float cz_ = DIM == 3 ? prolong_coef(z, az, cz, Z) : 1.f;
+        if (cz_ == 0.f) continue;
+        for (int y = max(2 * Y - 2, 0); y <= min(2 * Y + 3, ay - 1); ++y) {
+            const float cy_ = prolong_coef(y, ay, cy, Y);
+            if (cy_ == 0.f) continue;
+            for (int x = max(2 * X - 2, 0); x <= min(2 * X + 3, ax - 1); ++x) {
+                const float cx_ = prolong_coef(x, ax, cx, X);
+                if (cx_ == 0.f) continue;
+                s += cx_ * cy_ * cz_ * pfb[idx3(x, y, z, ax, ay)];
+            }
+        }
+    }
+    pcb[idx3(X, Y, Z, cx, cy)] = s;
+}
+
+// ------------------------------------------------------------ vorticity^T
+// Forward: w(c) = curl of the cell-centred velocity (k_vorticity, solid cells
+// 0), N = g / (|g| + 1e-20) with g = central difference of |w| / 2h (k_apply_
+// vorticity), f = N x w (2D: f = (-N_y w, -N_x w)), u(face c) += kappa * f(c).
+// Pass 1 (per cell): fbar = kappa * (ubar, vbar, wbar at the faces of index c);
+// wbar_direct = fbar x N (the part through w(c) itself); dbar = dL/d(central
+// difference of |w|) through N.
+template <int DIM>
+SS_D float vmag_at(const float* __restrict__ vort, int x, int y, int z, int nx, int ny, int nz) {
+    if (!in3(x, y, z, nx, ny, nz)) return 0.f;
+    const int c = idx3(x, y, z, nx, ny);
+    if constexpr (DIM == 2) {
+        return fabsf(vort[c]);
+    } else {
+        const size_t n = (size_t)nx * ny * nz;
+        const float o0 = vort[c], o1 = vort[n + c], o2 = vort[2 * n + c];
+        return sqrtf(o0 * o0 + o1 * o1 + o2 * o2);
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_vort1(const float* __restrict__ vort, const float* __restrict__ ub,
+                                                   const float* __restrict__ vbar, const float* __restrict__ wb,
+                                                   int nx, int ny, int nz, float two_h, float kappa,
+                                                   float* __restrict__ wdir, float* __restrict__ dbar) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (x >= nx || y >= ny || z >= nz) return;
+    const size_t n = (size_t)nx * ny * nz;
+    const int c = idx3(x, y, z, nx, ny);
+    const float fb0 = kappa * ub[idx3(x, y, z, nx + 1, ny)];
+    const float fb1 = kappa * vbar[idx3(x, y, z, nx, ny + 1)];
+    const float fb2 = DIM == 3 ? kappa * wb[idx3(x, y, z, nx, ny)] : 0.f;
+    const float dx = vmag_at<DIM>(vort, x + 1, y, z, nx, ny, nz) - vmag_at<DIM>(vort, x - 1, y, z, nx, ny, nz);
+    const float dy = vmag_at<DIM>(vort, x, y + 1, z, nx, ny, nz) - vmag_at<DIM>(vort, x, y - 1, z, nx, ny, nz);
+    const float dz = DIM == 3 ? vmag_at<DIM>(vort, x, y, z + 1, nx, ny, nz) - vmag_at<DIM>(vort, x, y, z - 1, nx, ny, nz) : 0.f;
+    const float gx = dx / two_h, gy = dy / two_h, gz = dz / two_h;
+    const float gl = sqrtf(gx * gx + gy * gy + gz * gz);
+    const float len = gl + 1e-20f;
+    const float Nx = gx / len, Ny = gy / len, Nz = gz / len;
+    float Nb[3];
+    if constexpr (DIM == 3) {
+        const float o0 = vort[c], o1 = vort[n + c], o2 = vort[2 * n + c];
+        // f = N x w: Nbar = w x fbar, wbar = fbar x N
+        Nb[0] = o1 * fb2 - o2 * fb1;
+        Nb[1] = o2 * fb0 - o0 * fb2;
+        Nb[2] = o0 * fb1 - o1 * fb0;
+        wdir[c] = fb1 * Nz - fb2 * Ny;
+        wdir[n + c] = fb2 * Nx - fb0 * Nz;
+        wdir[2 * n + c] = fb0 * Ny - fb1 * Nx;
+    } else {
+        const float o0 = vort[c];
+        Nb[0] = -o0 * fb1;
+        Nb[1] = -o0 * fb0;
+        Nb[2] = 0.f;
+        wdir[c] = -Ny * fb0 - Nx * fb1;
+    }
+    // N = g / (|g| + eps): gbar = Nbar / len - g (g . Nbar) / (|g| len^2)
+    const float gdot = gx * Nb[0] + gy * Nb[1] + gz * Nb[2];
+    const float q = gl > 0.f ? gdot / (gl * len * len) : 0.f;
+    dbar[c] = (Nb[0] / len - gx * q) / two_h;
+    dbar[n + c] = (Nb[1] / len - gy * q) / two_h;
+    if (DIM == 3) dbar[2 * n + c] = (Nb[2] / len - gz * q) / two_h;
+}
+
+// Pass 2 (per cell): |w|bar from the neighbours' central differences, then
+// wbar = wbar_direct + |w|bar * w / |w| (solid cells: 0, their w is fixed).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_vort2(const float* __restrict__ vort, const float* __restrict__ wdir,
+                                                   const float* __restrict__ dbar, const uint8_t* __restrict__ flags,
+                                                   int nx, int ny, int nz, float* __restrict__ wbar) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (x >= nx || y >= ny || z >= nz) return;
+    const size_t n = (size_t)nx * ny * nz;
+    const int c = idx3(x, y, z, nx, ny);
+    if (flags[c] & F_SOLID) {
+        wbar[c] = 0.f;
+        if (DIM == 3) { wbar[n + c] = 0.f; wbar[2 * n + c] = 0.f; }
+        return;
+    }
+    float mb = 0.f;
+    if (x > 0) mb += dbar[idx3(x - 1, y, z, nx, ny)];
+    if (x + 1 < nx) mb -= dbar[idx3(x + 1, y, z, nx, ny)];
+    if (y > 0) mb += dbar[n + idx3(x, y - 1, z, nx, ny)];
+    if (y + 1 < ny) mb -= dbar[n + idx3(x, y + 1, z, nx, ny)];
+    if constexpr (DIM == 3) {
+        if (z > 0) mb += dbar[2 * n + idx3(x, y, z - 1, nx, ny)];
+        if (z + 1 < nz) mb -= dbar[2 * n + idx3(x, y, z + 1, nx, ny)];
+        const float o0 = vort[c], o1 = vort[n + c], o2 = vort[2 * n + c];
+        const float m = sqrtf(o0 * o0 + o1 * o1 + o2 * o2);
+        const float s = m > 0.f ? mb / m : 0.f;
+        wbar[c] = wdir[c] + s * o0;
+        wbar[n + c] = wdir[n + c] + s * o1;
+        wbar[2 * n + c] = wdir[2 * n + c] + s * o2;
+    } else {
+        const float o0 = vort[c];
+        wbar[c] = wdir[c] + (o0 > 0.f ? mb : o0 < 0.f ? -mb : 0.f);
+    }
+}
+
+// Pass 3 (per face): the cell-centred velocities' adjoints from wbar (curl
+// transposed), then each face gets half of its two cells'.
+template <int DIM>
+SS_D float wb_at(const float* __restrict__ wbar, int comp, int x, int y, int z, int nx, int ny, int nz) {
+    if (!in3(x, y, z, nx, ny, nz)) return 0.f;
+    return wbar[(size_t)comp * nx * ny * nz + idx3(x, y, z, nx, ny)];
+}
+
+// adjoint of the cell-centred velocity component `comp` at cell position P
+template <int DIM>
+SS_D float cc_bar(const float* __restrict__ wbar, int comp, int x, int y, int z, int nx, int ny, int nz, float inv2h) {
+    if constexpr (DIM == 2) {
+        // w = (CCY(x+1) - CCY(x-1) - (CCX(y+1) - CCX(y-1))) / 2h
+        if (comp == 1) return (wb_at<2>(wbar, 0, x - 1, y, z, nx, ny, nz) - wb_at<2>(wbar, 0, x + 1, y, z, nx, ny, nz)) * inv2h;
+        return (wb_at<2>(wbar, 0, x, y + 1, z, nx, ny, nz) - wb_at<2>(wbar, 0, x, y - 1, z, nx, ny, nz)) * inv2h;
+    } else {
+        if (comp == 0)   // w_y uses +CCX(z+1) - CCX(z-1); w_z uses -CCX(y+1) + CCX(y-1)
+            return (wb_at<3>(wbar, 1, x, y, z - 1, nx, ny, nz) - wb_at<3>(wbar, 1, x, y, z + 1, nx, ny, nz) -
+                    wb_at<3>(wbar, 2, x, y - 1, z, nx, ny, nz) + wb_at<3>(wbar, 2, x, y + 1, z, nx, ny, nz)) * inv2h;
+        if (comp == 1)   // w_z uses +CCY(x+1) - CCY(x-1); w_x uses -CCY(z+1) + CCY(z-1)
+            return (wb_at<3>(wbar, 2, x - 1, y, z, nx, ny, nz) - wb_at<3>(wbar, 2, x + 1, y, z, nx, ny, nz) -
+                    wb_at<3>(wbar, 0, x, y, z - 1, nx, ny, nz) + wb_at<3>(wbar, 0, x, y, z + 1, nx, ny, nz)) * inv2h;
+        // w_x uses +CCZ(y+1) - CCZ(y-1); w_y uses -CCZ(x+1) + CCZ(x-1)
+        return (wb_at<3>(wbar, 0, x, y - 1, z, nx, ny, nz) - wb_at<3>(wbar, 0, x, y + 1, z, nx, ny, nz) -
+                wb_at<3>(wbar, 1, x - 1, y, z, nx, ny, nz) + wb_at<3>(wbar, 1, x + 1, y, z, nx, ny, nz)) * inv2h;
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_vort3(const float* __restrict__ wbar, int nx, int ny, int nz, float inv2h,
+                                                   float* __restrict__ ub, float* __restrict__ vbar,
+                                                   float* __restrict__ wb) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+#pragma unroll
+    for (int comp = 0; comp < DIM; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        // the face (x,y,z) of axis comp is the high face of cell P-1 and the low face of cell P
+        const int xm = x - (comp == 0), ym = y - (comp == 1), zm = z - (comp == 2);
+        const float s = 0.5f * (cc_bar<DIM>(wbar, comp, x, y, z, nx, ny, nz, inv2h) +
+                                cc_bar<DIM>(wbar, comp, xm, ym, zm, nx, ny, nz, inv2h));
+        (comp == 0 ? ub : comp == 1 ? vbar : wb)[idx3(x, y, z, ax, ay)] += s;
+    }
+}
+
+// --------------------------------------------------- velocity advection^T
+// Forward: k_advect_velocity<DIM, BUOY>.  gin: adjoint of the advected
+// (and buoyancy-forced) velocity; outputs accumulate (atomically) into
+// ubar/vbar/wbar (input velocity) and dbar/tbar (smoke, through buoyancy).
+template <int DIM, bool BUOY>
+__global__ void __launch_bounds__(256) k_adj_advect_velocity(AdjFluid a, const float* __restrict__ gu, const float* __restrict__ gv,
+                                                             const float* __restrict__ gw, float* __restrict__ ub,
+                                                             float* __restrict__ vbar, float* __restrict__ wb,
+                                                             float* __restrict__ dbar, float* __restrict__ tbar) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const float cfl = a.c.cfl;
+    const bool s_c = solid1(a.flags, x, y, z, nx, ny, nz);
+#pragma unroll
+    for (int comp = 0; comp < DIM; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        const int i = idx3(x, y, z, ax, ay);
+        const float g = (comp == 0 ? gu : comp == 1 ? gv : gw)[i];
+        if (g == 0.f) continue;
+        const int id = comp == 0 ? x : comp == 1 ? y : z;
+        float* srcb = comp == 0 ? ub : comp == 1 ? vbar : wb;
+        const float* src = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
+        if (BUOY && comp == 1) {
+            if (solid0(a.flags, x, y, z, nx, ny, nz) || solid0(a.flags, x, y - 1, z, nx, ny, nz)) {
+                atomicAdd(srcb + i, g);   // the face keeps its pre-advection value
+                continue;
+            }
+            // buoyancy: dt*(-alpha*sum_ch mean(dens) + beta*(mean(T) - t_amb)), means over the cells y-1, y
+            const size_t ncell = (size_t)nx * ny * nz;
+            const float gd = -a.c.alpha * g * a.c.dt * 0.5f;
+            const float gt = a.c.beta * g * a.c.dt * 0.5f;
+            for (int ch = 0; ch < a.nch; ++ch) {
+                scatter(dbar + ch * ncell, nx, ny, nz, x, y - 1, z, gd);
+                scatter(dbar + ch * ncell, nx, ny, nz, x, y, z, gd);
+            }
+            scatter(tbar, nx, ny, nz, x, y - 1, z, gt);
+            scatter(tbar, nx, ny, nz, x, y, z, gt);
+        }
+        if (id == 0 && a.c.wind[comp] != 0.f) continue;
+        if (s_c || solid1(a.flags, x - (comp == 0), y - (comp == 1), z - (comp == 2), nx, ny, nz)) continue;
+        float vel[3];
+        if (comp == 0) vel_at_xface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+        else if (comp == 1) vel_at_yface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+        else vel_at_zface(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+        const float gx = (float)x + (comp == 0 ? 0.f : 0.5f);
+        const float gy = (float)y + (comp == 1 ? 0.f : 0.5f);
+        const float gz = DIM == 3 ? (float)z + (comp == 2 ? 0.f : 0.5f) : 0.f;
+        const float tx = gx - vel[0] * cfl - (comp == 0 ? 0.f : 0.5f);
+        const float ty = gy - vel[1] * cfl - (comp == 1 ? 0.f : 0.5f);
+        const float tz = gz - vel[2] * cfl - (comp == 2 ? 0.f : 0.5f);
+        const Taps t = make_taps<DIM>(ax, ay, az, tx, ty, tz);
+        float dw[3];
+        adj_sample<DIM>(src, srcb, ax, ay, az, t, 0.f, g, dw);
+        // back-trace position -> the velocity that traced it
+        const float vb0 = -cfl * g * dw[0] * clamp_grad(tx, ax);
+        const float vb1 = -cfl * g * dw[1] * clamp_grad(ty, ay);
+        const float vb2 = DIM == 3 ? -cfl * g * dw[2] * clamp_grad(tz, az) : 0.f;
+        const float q0 = 0.25f * vb0, q1 = 0.25f * vb1, q2 = 0.25f * vb2;
+        if (comp == 0) {
+            atomicAdd(ub + i, vb0);
+            // v at (i-1/2, j+1/2, k): v(i-1,j), v(i,j), v(i-1,j+1), v(i,j+1)
+            scatter(vbar, nx, ny + 1, nz, x - 1, y, z, q1); scatter(vbar, nx, ny + 1, nz, x, y, z, q1);
+            scatter(vbar, nx, ny + 1, nz, x - 1, y + 1, z, q1); scatter(vbar, nx, ny + 1, nz, x, y + 1, z, q1);
+            if (DIM == 3) {
+                scatter(wb, nx, ny, nz + 1, x - 1, y, z, q2); scatter(wb, nx, ny, nz + 1, x, y, z, q2);
+                scatter(wb, nx, ny, nz + 1, x - 1, y, z + 1, q2); scatter(wb, nx, ny, nz + 1, x, y, z + 1, q2);
+            }
+        } else if (comp == 1) {
+            atomicAdd(vbar + i, vb1);
+            scatter(ub, nx + 1, ny, nz, x, y - 1, z, q0); scatter(ub, nx + 1, ny, nz, x + 1, y - 1, z, q0);
+            scatter(ub, nx + 1, ny, nz, x, y, z, q0); scatter(ub, nx + 1, ny, nz, x + 1, y, z, q0);
+            if (DIM == 3) {
+                scatter(wb, nx, ny, nz + 1, x, y - 1, z, q2); scatter(wb, nx, ny, nz + 1, x, y, z, q2);
+                scatter(wb, nx, ny, nz + 1, x, y - 1, z + 1, q2); scatter(wb, nx, ny, nz + 1, x, y, z + 1, q2);
+            }
+        } else {
+            atomicAdd(wb + i, vb2);
+            scatter(ub, nx + 1, ny, nz, x, y, z - 1, q0); scatter(ub, nx + 1, ny, nz, x + 1, y, z - 1, q0);
+            scatter(ub, nx + 1, ny, nz, x, y, z, q0); scatter(ub, nx + 1, ny, nz, x + 1, y, z, q0);
+            scatter(vbar, nx, ny + 1, nz, x, y, z - 1, q1); scatter(vbar, nx, ny + 1, nz, x, y + 1, z - 1, q1);
+            scatter(vbar, nx, ny + 1, nz, x, y, z, q1); scatter(vbar, nx, ny + 1, nz, x, y + 1, z, q1);
+        }
+    }
+}
+
+// Stand-alone buoyancy^T (k_buoyancy): faces touching solid are not written
+// by the forward (their output is the other buffer's content, independent of
+// the input), the rest are v + dt * buoyancy.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_buoyancy(AdjFluid a, float* __restrict__ vbar, float* __restrict__ dbar,
+                                                      float* __restrict__ tbar) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    if (x >= nx || y >= ny + 1 || z >= nz) return;
+    const int i = idx3(x, y, z, nx, ny + 1);
+    if (solid0(a.flags, x, y, z, nx, ny, nz) || solid0(a.flags, x, y - 1, z, nx, ny, nz)) {
+        vbar[i] = 0.f;
+        return;
+    }
+    const float g = vbar[i];
+    const size_t ncell = (size_t)nx * ny * nz;
+    const float gd = -a.c.alpha * g * a.c.dt * 0.5f;
+    const float gt = a.c.beta * g * a.c.dt * 0.5f;
+    for (int ch = 0; ch < a.nch; ++ch) {
+        scatter(dbar + ch * ncell, nx, ny, nz, x, y - 1, z, gd);
+        scatter(dbar + ch * ncell, nx, ny, nz, x, y, z, gd);
+    }
+    scatter(tbar, nx, ny, nz, x, y - 1, z, gt);
+    scatter(tbar, nx, ny, nz, x, y, z, gt);
+}
+
+// ---------------------------------------------------------------- emitters^T
+// Forward (k_emitters): smoke gets constants added (identity adjoint); the
+// faces of an active set_velocity emitter are overwritten (adjoint 0); a
+// control force adds dt * force to every face inside an active emitter.
+// fgrad: per-block partial sums of dt * ubar over the forced faces (3 each).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_emitters(const ss_emitter* __restrict__ em, int ne, int nx, int ny, int nz,
+                                                      float dt, int forced, float* __restrict__ ub,
+                                                      float* __restrict__ vbar, float* __restrict__ wb,
+                                                      double* __restrict__ fpart) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int comp = 0; comp < DIM; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        bool inside = false, set = false;
+        for (int k = 0; k < ne; ++k) {
+            const ss_emitter& e = em[k];
+            if (!(e.emit > 0)) continue;
+            float dx = (float)x - e.pos[0], dy = (float)y - e.pos[1];
+            float d2 = dx * dx + dy * dy;
+            if constexpr (DIM == 3) { float dz = (float)z - e.pos[2]; d2 = d2 + dz * dz; }
+            if (sqrtf(d2) < e.radius) {
+                inside = true;
+                if (e.set_velocity) set = true;
+            }
+        }
+        float* dst = comp == 0 ? ub : comp == 1 ? vbar : wb;
+        const int i = idx3(x, y, z, ax, ay);
+        if (forced && inside) acc[comp] = (double)dt * (double)dst[i];
+        if (set) dst[i] = 0.f;
+    }
+    if (fpart) {
+        // block sums of the three force components
+        __shared__ double sh[3][256];
+        const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+        for (int q = 0; q < 3; ++q) sh[q][tid] = acc[q];
+        __syncthreads();
+        for (int o = 128; o > 0; o >>= 1) {
+            if (tid < o)
+                for (int q = 0; q < 3; ++q) sh[q][tid] += sh[q][tid + o];
+            __syncthreads();
+        }
+        if (tid == 0) {
+            const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+            for (int q = 0; q < 3; ++q) fpart[3 * b + q] = sh[q][0];
+        }
+    }
+}
+
+__global__ void k_sum3(const double* __restrict__ part, int n, double* __restrict__ out) {
+    __shared__ double sh[3][256];
+    double a[3] = {0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        for (int q = 0; q < 3; ++q) a[q] += part[3 * i + q];
+    for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] = a[q];
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o)
+            for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 3; ++q) out[q] = sh[q][0];
+}
+
+// ------------------------------------------------------------------- host
+static AdjFluid adj_fluid(const ss_sim* s, const StepConsts& c, const float* const vel[3], const float* dens,
+                          const float* temp) {
+    AdjFluid a;
+    a.nx = s->nx; a.ny = s->ny; a.nz = s->nz; a.nch = s->nch;
+    a.u = vel[0]; a.v = vel[1]; a.w = s->dim == 3 ? vel[2] : nullptr;
+    a.flags = s->flags;
+    a.dens = dens; a.temp = temp;
+    a.c = c;
+    return a;
+}
+
+static const dim3 kB(32, 8, 1);
+
+int adj_advect_smoke(ss_sim* s, const StepConsts& c, const float* const vel[3], const float* dens, const float* temp,
+                     const float* dout, const float* tout, float* din, float* tin, float* vcb, float* const vb[3],
+                     cudaStream_t st) {
+    AdjFluid a = adj_fluid(s, c, vel, dens, temp);
+    dim3 g = grid_of(s->nx, s->ny, s->nz, kB);
+    dim3 gf = grid_of(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, kB);
+    if (s->dim == 3) {
+        k_adj_advect_smoke<3><<<g, kB, 0, st>>>(a, dout, tout, din, tin, vcb);
+        k_adj_centre_to_faces<3><<<gf, kB, 0, st>>>(vcb, s->nx, s->ny, s->nz, vb[0], vb[1], vb[2]);
+    } else {
+        k_adj_advect_smoke<2><<<g, kB, 0, st>>>(a, dout, tout, din, tin, vcb);
+        k_adj_centre_to_faces<2><<<gf, kB, 0, st>>>(vcb, s->nx, s->ny, s->nz, vb[0], vb[1], nullptr);
+    }
+    s->nlaunch += 2;
+    return check_cuda(cudaGetLastError(), "adjoint of advect_smoke");
+}
+
+int adj_update(ss_sim* s, const StepConsts& c, float* const vb[3], float* pbar, cudaStream_t st) {
+    dim3 g = grid_of(s->nx, s->ny, s->nz, kB);
+    dim3 gf = grid_of(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, kB);
+    if (s->dim == 3) {
+        k_adj_update_faces<3><<<gf, kB, 0, st>>>(s->flags, s->nx, s->ny, s->nz, vb[0], vb[1], vb[2]);
+        k_adj_update_pressure<3><<<g, kB, 0, st>>>(vb[0], vb[1], vb[2], s->nx, s->ny, s->nz, c.k_upd, pbar);
+    } else {
+        k_adj_update_faces<2><<<gf, kB, 0, st>>>(s->flags, s->nx, s->ny, s->nz, vb[0], vb[1], nullptr);
+        k_adj_update_pressure<2><<<g, kB, 0, st>>>(vb[0], vb[1], nullptr, s->nx, s->ny, s->nz, c.k_upd, pbar);
+    }
+    s->nlaunch += 2;
+    return check_cuda(cudaGetLastError(), "adjoint of update_velocities");
+}
+
+int adj_divergence(ss_sim* s, const float* dbar, float* const vb[3], cudaStream_t st) {
+    dim3 gf = grid_of(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, kB);
+    if (s->dim == 3) k_adj_divergence<3><<<gf, kB, 0, st>>>(dbar, s->flags, s->nx, s->ny, s->nz, vb[0], vb[1], vb[2]);
+    else k_adj_divergence<2><<<gf, kB, 0, st>>>(dbar, s->flags, s->nx, s->ny, s->nz, vb[0], vb[1], nullptr);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "adjoint of the divergence");
+}
+
+// --- V-cycle^T
+static AdjLevel adj_level(ss_sim* s, const StepConsts& c, int L, const AdjScratch& w) {
+    AdjLevel a;
+    a.nx = s->lv[L].n[0]; a.ny = s->lv[L].n[1]; a.nz = s->lv[L].n[2];
+    a.fmask = s->fmask;
+    a.alpha = L > 0 ? s->alpha[L] : nullptr;
+    a.oobA = s->enclosed ? 1.f : 0.f;
+    a.hh = s->lv[L].hh;
+    a.beta = L == 0 ? c.rho_h / c.dt : s->lv[L].hh;
+    a.rcoef = L == 0 ? c.rho / c.dt_h : 1.f;
+    a.pbar = w.pbar[L];
+    a.bbar = w.bbar[L];
+    a.T = w.T[L];
+    return a;
+}
+
+static int adj_sweeps(ss_sim* s, const AdjLevel& a, int L, int iterations, cudaStream_t st) {
+    if (iterations <= 0) return SS_OK;
+    dim3 g = grid_of((a.nx + 1) / 2, a.ny, a.nz, kB);
+    // forward: per sweep colour 0 then 1; transpose: per sweep colour 1 then 0,
+    // each colour's gather half fused with the next colour's update half
+    auto launch = [&](int colour, int do_b, int do_a) {
+        if (s->dim == 3) {
+            if (L == 0) k_adj_smooth<3, true><<<g, kB, 0, st>>>(a, colour, do_b, do_a);
+            else k_adj_smooth<3, false><<<g, kB, 0, st>>>(a, colour, do_b, do_a);
+        } else {
+            if (L == 0) k_adj_smooth<2, true><<<g, kB, 0, st>>>(a, colour, do_b, do_a);
+            else k_adj_smooth<2, false><<<g, kB, 0, st>>>(a, colour, do_b, do_a);
+        }
+    };
+    launch(1, 0, 1);
+    int colour = 1;
+    for (int k = 1; k < 2 * iterations; ++k) {
+        colour ^= 1;
+        launch(colour, 1, 1);
+    }
+    launch(colour ^ 1, 1, 0);
+    s->nlaunch += 2 * iterations + 1;
+    return check_cuda(cudaGetLastError(), "k_adj_smooth");
+}
+
+// Transposed V-cycle from level L: on entry w.pbar[L] holds the adjoint of the
+// level's output pressure; on return it holds the adjoint of its input
+// pressure and w.bbar[L] has the right-hand side's adjoint added.
+static int adj_v_cycle_rec(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int L, const AdjScratch& w,
+                           cudaStream_t st) {
+    const AdjLevel a = adj_level(s, c, L, w);
+    if (L == s->levels - 1) return adj_sweeps(s, a, L, mg.n_coarse, st);
+    TRY_ADJ(adj_sweeps(s, a, L, mg.n_post, st));
+    const int cx = s->lv[L + 1].n[0], cy = s->lv[L + 1].n[1], cz = s->lv[L + 1].n[2];
+    const size_t nc = (size_t)cx * cy * cz;
+    // p_L += P p_{L+1}  ->  pbar_{L+1} = P^T pbar_L
+    dim3 gc = grid_of(cx, cy, cz, kB);
+    if (s->dim == 3) k_adj_prolong<3><<<gc, kB, 0, st>>>(a.pbar, a.nx, a.ny, a.nz, w.pbar[L + 1], cx, cy, cz);
+    else k_adj_prolong<2><<<gc, kB, 0, st>>>(a.pbar, a.nx, a.ny, a.nz, w.pbar[L + 1], cx, cy, cz);
+    s->nlaunch += 1;
+    TRY_ADJ(check_cuda(cudaMemsetAsync(w.bbar[L + 1], 0, nc * sizeof(float), st), "memset"));
+    TRY_ADJ(adj_v_cycle_rec(s, c, mg, L + 1, w, st));
+    // r_{L+1} = R(b_L - A p_L)
+    dim3 gf = grid_of(a.nx, a.ny, a.nz, kB);
+    if (s->dim == 3) {
+        if (L == 0) k_adj_residual_restrict<3, true><<<gf, kB, 0, st>>>(a, w.bbar[L + 1], cx, cy, cz);
+        else k_adj_residual_restrict<3, false><<<gf, kB, 0, st>>>(a, w.bbar[L + 1], cx, cy, cz);
+    } else {
+        if (L == 0) k_adj_residual_restrict<2, true><<<gf, kB, 0, st>>>(a, w.bbar[L + 1], cx, cy, cz);
+        else k_adj_residual_restrict<2, false><<<gf, kB, 0, st>>>(a, w.bbar[L + 1], cx, cy, cz);
+    }
+    s->nlaunch += 1;
+    TRY_ADJ(check_cuda(cudaGetLastError(), "adjoint of the V-cycle"));
+    return adj_sweeps(s, a, L, mg.n_pre, st);
+}
+
+int adj_v_cycle(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, const AdjScratch& w, cudaStream_t st) {
+    return adj_v_cycle_rec(s, c, mg, 0, w, st);
+}
+
+// level-0 operator L p = sum_j w_j p_j - d p (fluid cells), for the mixed
+// solve's refinement transpose: pbar -= k * L(rbar) (L is symmetric)
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_apply_laplacian(const float* __restrict__ rb, const uint8_t* __restrict__ fmask,
+                                                             int nx, int ny, int nz, float k, float* __restrict__ pbar) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (x >= nx || y >= ny || z >= nz) return;
+    const int c = idx3(x, y, z, nx, ny);
+    const uint8_t m = fmask[c];
+    if (!(m & M_FLUID)) return;
+    float s = 0.f;
+    if ((m & M_TOP) && y + 1 < ny) s += rb[c + nx];
+    if ((m & M_BOTTOM) && y > 0) s += rb[c - nx];
+    if ((m & M_RIGHT) && x + 1 < nx) s += rb[c + 1];
+    if ((m & M_LEFT) && x > 0) s += rb[c - 1];
+    if constexpr (DIM == 3) {
+        if ((m & M_FRONT) && z + 1 < nz) s += rb[c + nx * ny];
+        if ((m & M_BACK) && z > 0) s += rb[c - nx * ny];
+    }
+    pbar[c] -= k * (s - (float)__popc(m & 0x7Eu) * rb[c]);
+}
+
+int adj_apply_laplacian(ss_sim* s, const float* rb, float k, float* pbar, cudaStream_t st) {
+    dim3 g = grid_of(s->nx, s->ny, s->nz, kB);
+    if (s->dim == 3) k_adj_apply_laplacian<3><<<g, kB, 0, st>>>(rb, s->fmask, s->nx, s->ny, s->nz, k, pbar);
+    else k_adj_apply_laplacian<2><<<g, kB, 0, st>>>(rb, s->fmask, s->nx, s->ny, s->nz, k, pbar);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_adj_apply_laplacian");
+}
+
+int adj_vorticity(ss_sim* s, const StepConsts& c, const float* vort, float* const vb[3], float* wdir, float* dbar,
+                  float* wbar, cudaStream_t st) {
+    dim3 g = grid_of(s->nx, s->ny, s->nz, kB);
+    dim3 gf = grid_of(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, kB);
+    const float two_h = 2.f * s->h;
+    const float kappa = (0.5f * c.eps * s->h * c.dt) / c.rho;
+    if (s->dim == 3) {
+        k_adj_vort1<3><<<g, kB, 0, st>>>(vort, vb[0], vb[1], vb[2], s->nx, s->ny, s->nz, two_h, kappa, wdir, dbar);
+        k_adj_vort2<3><<<g, kB, 0, st>>>(vort, wdir, dbar, s->flags, s->nx, s->ny, s->nz, wbar);
+        k_adj_vort3<3><<<gf, kB, 0, st>>>(wbar, s->nx, s->ny, s->nz, 1.f / two_h, vb[0], vb[1], vb[2]);
+    } else {
+        k_adj_vort1<2><<<g, kB, 0, st>>>(vort, vb[0], vb[1], nullptr, s->nx, s->ny, s->nz, two_h, kappa, wdir, dbar);
+        k_adj_vort2<2><<<g, kB, 0, st>>>(vort, wdir, dbar, s->flags, s->nx, s->ny, s->nz, wbar);
+        k_adj_vort3<2><<<gf, kB, 0, st>>>(wbar, s->nx, s->ny, s->nz, 1.f / two_h, vb[0], vb[1], nullptr);
+    }
+    s->nlaunch += 3;
+    return check_cuda(cudaGetLastError(), "adjoint of vorticity confinement");
+}
+
+int adj_advect_velocity(ss_sim* s, const StepConsts& c, bool buoy, const float* const vel[3], const float* dens,
+                        const float* temp, const float* const gin[3], float* const vb[3], float* dbar, float* tbar,
+                        cudaStream_t st) {
+    AdjFluid a = adj_fluid(s, c, vel, dens, temp);
+    dim3 gf = grid_of(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, kB);
+    if (s->dim == 3) {
+        if (buoy) k_adj_advect_velocity<3, true><<<gf, kB, 0, st>>>(a, gin[0], gin[1], gin[2], vb[0], vb[1], vb[2], dbar, tbar);
+        else k_adj_advect_velocity<3, false><<<gf, kB, 0, st>>>(a, gin[0], gin[1], gin[2], vb[0], vb[1], vb[2], dbar, tbar);
+    } else {
+        if (buoy) k_adj_advect_velocity<2, true><<<gf, kB, 0, st>>>(a, gin[0], gin[1], nullptr, vb[0], vb[1], nullptr, dbar, tbar);
+        else k_adj_advect_velocity<2, false><<<gf, kB, 0, st>>>(a, gin[0], gin[1], nullptr, vb[0], vb[1], nullptr, dbar, tbar);
+    }
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "adjoint of advect_velocities");
+}
+
+int adj_buoyancy(ss_sim* s, const StepConsts& c, float* vbar, float* dbar, float* tbar, cudaStream_t st) {
+    const float* vel[3] = {nullptr, nullptr, nullptr};
+    AdjFluid a = adj_fluid(s, c, vel, nullptr, nullptr);
+    dim3 g = grid_of(s->nx, s->ny + 1, s->nz, kB);
+    if (s->dim == 3) k_adj_buoyancy<3><<<g, kB, 0, st>>>(a, vbar, dbar, tbar);
+    else k_adj_buoyancy<2><<<g, kB, 0, st>>>(a, vbar, dbar, tbar);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "adjoint of apply_buoyancy");
+}
+
+int adj_emitters(ss_sim* s, const StepConsts& c, int forced, float* const vb[3], double* fpart, double* fout,
+                 cudaStream_t st) {
+    dim3 gf = grid_of(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, kB);
+    const int nb = (int)(gf.x * gf.y * gf.z);
+    const int ne = (int)s->em.size();
+    if (s->dim == 3) k_adj_emitters<3><<<gf, kB, 0, st>>>(s->d_em, ne, s->nx, s->ny, s->nz, c.dt, forced, vb[0], vb[1], vb[2], fpart);
+    else k_adj_emitters<2><<<gf, kB, 0, st>>>(s->d_em, ne, s->nx, s->ny, s->nz, c.dt, forced, vb[0], vb[1], nullptr, fpart);
+    k_sum3<<<1, 256, 0, st>>>(fpart, nb, fout);
+    s->nlaunch += 2;
+    return check_cuda(cudaGetLastError(), "adjoint of handle_emitters");
+}
+
+int adj_force_blocks(const ss_sim* s) {
+    dim3 gf = grid_of(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, kB);
+    return (int)(gf.x * gf.y * gf.z);
+}
+
+}  // namespace ss

@@ -66,7 +66,8 @@ static inline dim3 grid_for(int ax, int ay, int az, dim3 b) {
 template <int DIM>
 __global__ void k_emitters(FluidArgs a, const ss_emitter* __restrict__ em, int ne, int lox, int loy, int loz,
                            int ex, int ey, int ez, float* __restrict__ dens, float* __restrict__ temp,
-                           float* __restrict__ u, float* __restrict__ v, float* __restrict__ w) {
+                           float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+                           float3 force, int forced) {
     int x = lox + blockIdx.x * blockDim.x + threadIdx.x;
     int y = loy + blockIdx.y * blockDim.y + threadIdx.y;
     int z = loz + blockIdx.z * blockDim.z + threadIdx.z;
@@ -112,18 +113,26 @@ __global__ void k_emitters(FluidArgs a, const ss_emitter* __restrict__ em, int n
         int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
         if (x >= ax || y >= ay || z >= az) continue;
         float val = 0.f;
-        bool hit = false;
+        bool hit = false, inside = false;
         for (int k = 0; k < ne; ++k) {
             const ss_emitter& e = em[k];
-            if (!(e.emit > 0 && e.set_velocity)) continue;
+            if (!(e.emit > 0)) continue;
             float dx = (float)x - e.pos[0], dy = (float)y - e.pos[1];
             float d2 = dx * dx + dy * dy;
             if constexpr (DIM == 3) { float dz = (float)z - e.pos[2]; d2 = d2 + dz * dz; }
-            if (sqrtf(d2) < e.radius) { val = e.velocity[comp]; hit = true; }
+            if (sqrtf(d2) < e.radius) {
+                inside = true;
+                if (e.set_velocity) { val = e.velocity[comp]; hit = true; }
+            }
         }
-        if (hit) {
+        // control force (an extension for the adjoint's inverse problems):
+        // dt * force on every face inside an active emitter, after the set
+        if (hit || (forced && inside)) {
             float* dst = comp == 0 ? u : comp == 1 ? v : w;
-            dst[idx3(x, y, z, ax, ay)] = val;
+            const int i = idx3(x, y, z, ax, ay);
+            float out = hit ? val : dst[i];
+            if (forced && inside) out = out + dt * (comp == 0 ? force.x : comp == 1 ? force.y : force.z);
+            dst[i] = out;
         }
     }
 }
@@ -150,6 +159,8 @@ int launch_emitters(ss_sim* s, const StepConsts& c, cudaStream_t st) {
         if (hi[d] <= lo[d]) return SS_OK;
     }
     FluidArgs a = fluid_args(s, c);
+    const float3 f = make_float3(s->force[0], s->force[1], s->force[2]);
+    const int forced = (s->force[0] != 0.f || s->force[1] != 0.f || s->force[2] != 0.f) ? 1 : 0;
     dim3 b(32, 4, 1);
     dim3 g = grid_for(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], b);
     float* u = s->vel[0][s->vi[0]];
@@ -157,10 +168,10 @@ int launch_emitters(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     float* w = s->dim == 3 ? s->vel[2][s->vi[2]] : nullptr;
     if (s->dim == 3)
         k_emitters<3><<<g, b, 0, st>>>(a, s->d_em, (int)s->em.size(), lo[0], lo[1], lo[2], hi[0] - lo[0],
-                                       hi[1] - lo[1], hi[2] - lo[2], s->dens[s->si], s->temp[s->si], u, v, w);
+                                       hi[1] - lo[1], hi[2] - lo[2], s->dens[s->si], s->temp[s->si], u, v, w, f, forced);
     else
         k_emitters<2><<<g, b, 0, st>>>(a, s->d_em, (int)s->em.size(), lo[0], lo[1], lo[2], hi[0] - lo[0],
-                                       hi[1] - lo[1], hi[2] - lo[2], s->dens[s->si], s->temp[s->si], u, v, w);
+                                       hi[1] - lo[1], hi[2] - lo[2], s->dens[s->si], s->temp[s->si], u, v, w, f, forced);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_emitters");
 }

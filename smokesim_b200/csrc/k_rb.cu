@@ -200,8 +200,9 @@ __global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, cons
     if (q >= (g.half >> 2) || y >= g.ny) return;
     const int xh0 = q << 2;
     const int i = (z * g.ny + y) * g.half + xh0;
+    // no early exit on an all-solid quad: every load below is issued before
+    // the first one is waited for
     const uint32_t m4 = __ldg(reinterpret_cast<const uint32_t*>(mask_c + i));
-    if ((m4 & 0x01010101u) == 0) return;
     const int par = (y + z + colour) & 1;   // x = 2*xh + par
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 pt = y + 1 < g.ny ? ldg4(po + i + g.half) : zero;

@@ -87,6 +87,7 @@ struct ss_sim {
     void* cp[SS_MAX_LEVELS] = {};       // coarse pressure, 2 bytes per cell (L >= 1)
     void* cr[SS_MAX_LEVELS] = {};       // coarse right-hand side / residual
     float* d_scale = nullptr;           // [scale, 1/scale] of the coarse storage (device)
+    float force[3] = {0.f, 0.f, 0.f};   // control force on the faces inside active emitters
     int rb_vec = 0;                     // level-0 kernels may work on 4 cells per thread (nx % 8 == 0)
     int rb_prolong_vec = 0;             // ... and the prolongation too (even sizes, table pattern checked)
     ss::ReduceSlots red{};
@@ -168,6 +169,46 @@ int launch_p0_from_p64(ss_sim* s, cudaStream_t st);
 int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, cudaStream_t st);
 int launch_ir_accumulate(ss_sim* s, cudaStream_t st);
 int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st);
+
+// Forward state copies a step can leave for its adjoint (api.cpp, run_step):
+// any pointer may be null.
+struct StepSaves {
+    float* emit_vel[3];      // velocity after handle_emitters
+    float* emit_dens;        // smoke after handle_emitters (nch * ncell)
+    float* emit_temp;
+    float* force_vel[3];     // velocity after advection (+ buoyancy), before vorticity confinement
+    float* proj_vel[3];      // velocity after the projection update
+    int vcycles;             // out: V-cycles (or refinement steps) the solve ran
+};
+int run_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* saves);
+
+// adjoint kernels (k_adjoint.cu)
+struct AdjScratch {
+    float* pbar[SS_MAX_LEVELS];
+    float* bbar[SS_MAX_LEVELS];
+    float* T[SS_MAX_LEVELS];
+};
+#define TRY_ADJ(x)                          \
+    do {                                    \
+        int _rc = (x);                      \
+        if (_rc != SS_OK) return _rc;       \
+    } while (0)
+int adj_advect_smoke(ss_sim* s, const StepConsts& c, const float* const vel[3], const float* dens, const float* temp,
+                     const float* dout, const float* tout, float* din, float* tin, float* vcb, float* const vb[3],
+                     cudaStream_t st);
+int adj_update(ss_sim* s, const StepConsts& c, float* const vb[3], float* pbar, cudaStream_t st);
+int adj_divergence(ss_sim* s, const float* dbar, float* const vb[3], cudaStream_t st);
+int adj_v_cycle(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, const AdjScratch& w, cudaStream_t st);
+int adj_apply_laplacian(ss_sim* s, const float* rb, float k, float* pbar, cudaStream_t st);
+int adj_vorticity(ss_sim* s, const StepConsts& c, const float* vort, float* const vb[3], float* wdir, float* dbar,
+                  float* wbar, cudaStream_t st);
+int adj_advect_velocity(ss_sim* s, const StepConsts& c, bool buoy, const float* const vel[3], const float* dens,
+                        const float* temp, const float* const gin[3], float* const vb[3], float* dbar, float* tbar,
+                        cudaStream_t st);
+int adj_buoyancy(ss_sim* s, const StepConsts& c, float* vbar, float* dbar, float* tbar, cudaStream_t st);
+int adj_emitters(ss_sim* s, const StepConsts& c, int forced, float* const vb[3], double* fpart, double* fout,
+                 cudaStream_t st);
+int adj_force_blocks(const ss_sim* s);
 
 // ---- scene kernels (k_scene.cu) ----
 int launch_rasterize(ss_sim* s, cudaStream_t st);

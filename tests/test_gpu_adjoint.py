@@ -1,0 +1,270 @@
+"""Adjoint of the step (k_adjoint.cu through ss_adjoint_*), checked against
+central finite differences of the FP64 oracle.
+
+For a random adjoint seed ybar on the output fields and a random direction d
+on the inputs, <xbar, d> from the CUDA adjoint must match
+(L(x + eps d) - L(x - eps d)) / (2 eps), L(x) = <ybar, F(x)>, F the FP64
+oracle's step from the same (FP32) state.  Single stages first (stage_mask),
+then full steps, rollouts with checkpointing and the control force.
+"""
+import numpy as np
+import pytest
+
+from smokesim_b200 import abi, scene
+
+pytestmark = pytest.mark.gpu
+
+VEL = [abi.FIELD_VX, abi.FIELD_VY, abi.FIELD_VZ]
+ADJ_PARAMS = dict(ref_quirks=0, n_vcycles=2, n_pre=2, n_post=2, n_coarse=6)
+
+
+def _setup(dim, n, nch, enc, seed, mask, force=(0.0, 0.0, 0.0), state_scale=1.0):
+    from oracle.oracle import OracleSim
+    from smokesim_b200 import Sim
+    desc = abi.make_desc(dim, n, cell_size=1.0, density_channels=nch, enclosed=enc, min_coarse=4, t_ambient=0.0)
+    rng = scene.Rng(seed)
+    nx, ny = n[0], n[1]
+    nz = n[2] if dim == 3 else 1
+    em = [scene.emitter((nx / 2 + 0.3, 3.5, nz / 2 + 0.2), 3.0, density=1.0, temperature=1.0, velocity=(0.0, 1.5, 0.0))]
+    ob = [scene.obstacle((nx / 2, ny / 2 + 1.0, nz / 2), min(nx, ny) / 6.0)]
+    f = scene.random_state(rng, dim, n, nch, vel_scale=state_scale)
+    p = scene.workload_params(stage_mask=mask, **ADJ_PARAMS)
+    g = Sim(desc)
+    g.set_scene(em, ob, [])
+    for k, a in f.items():
+        g.set_field(k, a[: abi.field_count(dim, n, k, nch)] if k == abi.FIELD_DENSITY else a)
+    return desc, em, ob, f, p, g
+
+
+def _fields(dim):
+    return VEL[:dim] + [abi.FIELD_DENSITY, abi.FIELD_TEMPERATURE, abi.FIELD_PRESSURE]
+
+
+def _oracle_loss(desc, em, ob, f, p, ybar, x_dir, eps, force, dim, nch, n):
+    """<ybar, F(x + eps * x_dir)> in the FP64 oracle."""
+    from oracle.oracle import OracleSim
+    o = OracleSim(desc, "f64")
+    o.set_scene(em, ob, [])
+    for k, a in f.items():
+        base = (a[: abi.field_count(dim, n, k, nch)] if k == abi.FIELD_DENSITY else a).astype(np.float64)
+        if k in x_dir:
+            base = base + eps * x_dir[k]
+        o.set_field_f64(k, base)
+    o.set_emitter_force(force)
+    o.step(p)
+    tot = 0.0
+    for k, yb in ybar.items():
+        tot += float(np.dot(yb.astype(np.float64), o.get_field(k, f64=True).ravel()))
+    o.close()
+    return tot
+
+
+def _directional(dim, n, nch, enc, mask, seed=1, force=(0.0, 0.0, 0.0), eps=1e-4, tol=2e-3):
+    from smokesim_b200.adjoint import Rollout
+    import torch
+    desc, em, ob, f, p, g = _setup(dim, n, nch, enc, seed, mask)
+    rng = np.random.default_rng(seed + 100)
+    outs = VEL[:dim] + [abi.FIELD_DENSITY, abi.FIELD_TEMPERATURE]
+    ybar = {k: rng.standard_normal(abi.field_count(dim, n, k, nch)).astype(np.float32) for k in outs}
+    ins = _fields(dim)
+    x_dir = {k: rng.standard_normal(abi.field_count(dim, n, k, nch)) for k in ins}
+    ro = Rollout(g, 1)
+    fr = np.array([force], np.float32)
+    ro.forward(p, fr)
+    dev = {k: torch.from_numpy(v).cuda() for k, v in ybar.items()}
+    torch.cuda.synchronize()
+    gf = ro.backward(p, grad_density=dev[abi.FIELD_DENSITY].data_ptr(),
+                     grad_temperature=dev[abi.FIELD_TEMPERATURE].data_ptr(),
+                     grad_velocity=[dev[k].data_ptr() for k in VEL[:dim]])
+    adj = sum(float(np.dot(ro.grad(k).astype(np.float64), x_dir[k])) for k in ins)
+    lp = _oracle_loss(desc, em, ob, f, p, ybar, x_dir, eps, force, dim, nch, n)
+    lm = _oracle_loss(desc, em, ob, f, p, ybar, x_dir, -eps, force, dim, nch, n)
+    fd = (lp - lm) / (2 * eps)
+    assert abs(adj - fd) <= tol * max(abs(fd), 1e-6), (adj, fd)
+    # force gradient (emitter stage): FD on each component
+    if mask & abi.STAGE_HANDLE_EMITTERS:
+        for d in range(dim):
+            fp_, fm_ = list(force), list(force)
+            fp_[d] += eps
+            fm_[d] -= eps
+            zero = {k: np.zeros_like(v) for k, v in x_dir.items()}
+            fdf = (_oracle_loss(desc, em, ob, f, p, ybar, zero, 0.0, fp_, dim, nch, n) -
+                   _oracle_loss(desc, em, ob, f, p, ybar, zero, 0.0, fm_, dim, nch, n)) / (2 * eps)
+            assert abs(gf[0, d] - fdf) <= tol * max(abs(fdf), 1e-6), (d, gf[0, d], fdf)
+    ro.close()
+    g.close()
+
+
+STAGES = [
+    ("emitters", abi.STAGE_HANDLE_EMITTERS),
+    ("advect", abi.STAGE_ADVECT_VELOCITIES),
+    ("advect_buoyancy", abi.STAGE_ADVECT_VELOCITIES | abi.STAGE_APPLY_BUOYANCY),
+    ("buoyancy", abi.STAGE_APPLY_BUOYANCY),
+    ("vorticity", abi.STAGE_APPLY_VORTICITY),
+    ("update", abi.STAGE_UPDATE_VELOCITIES),
+    ("projection", abi.STAGE_RESOLVE_PRESSURE | abi.STAGE_UPDATE_VELOCITIES),
+    ("smoke", abi.STAGE_ADVECT_SMOKE),
+    ("full", abi.STAGE_ALL),
+]
+GRIDS = [
+    ("3d", 3, (16, 14, 12), 1, 1),
+    ("3d_open_rgb", 3, (12, 16, 10), 3, 0),
+    ("2d", 2, (24, 20, 1), 1, 1),
+]
+
+
+@pytest.mark.parametrize("gname,dim,n,nch,enc", GRIDS)
+@pytest.mark.parametrize("stage,mask", STAGES)
+def test_stage_adjoint_matches_fd(gname, dim, n, nch, enc, stage, mask):
+    _directional(dim, n, nch, enc, mask, seed=3, force=(0.3, -0.2, 0.1)[:dim] + (0.0,) * (3 - dim))
+
+
+def test_rollout_checkpointing_consistent():
+    """The same rollout's gradients with checkpoints every 1, 3 and 8 steps
+    (recomputation in between) agree up to the atomics' summation order."""
+    from smokesim_b200 import Sim
+    from smokesim_b200.adjoint import Rollout
+    import torch
+    sc = scene.rollout64(seed=2, n=24)
+    p = scene.workload_params(ref_quirks=0, n_vcycles=4)
+    nsteps = 8
+    forces = np.random.default_rng(0).standard_normal((nsteps, 3)).astype(np.float32) * 0.2
+    res = []
+    for every in (1, 3, 8):
+        g = Sim(sc["desc"])
+        scene.apply(g, sc)
+        ro = Rollout(g, nsteps, every)
+        ro.forward(p, forces)
+        target = torch.ones(abi.field_count(3, g.n, abi.FIELD_DENSITY), device="cuda") * 0.1
+        gd = 2 * (torch.from_numpy(g.get_field(abi.FIELD_DENSITY).ravel()).cuda() - target)
+        torch.cuda.synchronize()
+        gf = ro.backward(p, grad_density=gd.data_ptr())
+        res.append((gf, [ro.grad(k) for k in VEL], ro.info()))
+        ro.close()
+        g.close()
+    for gf, gv, _ in res[1:]:
+        assert np.allclose(gf, res[0][0], rtol=1e-4, atol=1e-6 * np.abs(res[0][0]).max())
+        for a, b in zip(gv, res[0][1]):
+            assert np.allclose(a, b, rtol=1e-3, atol=1e-5 * np.abs(b).max())
+    # every step: 8 checkpoints + 1 segment state; every 3: 3 + 3
+    assert res[1][2]["checkpoint_bytes"] < res[0][2]["checkpoint_bytes"]
+
+
+def test_rollout_gradient_vs_fp64_fd():
+    """8-step rollout at 32^3: dL/d(initial velocity) and dL/d(force) on 32
+    random control coordinates against FP64 central differences with
+    h = 1e-3.  Semi-Lagrangian advection is piecewise smooth: where h = 1e-3
+    straddles a kink (the 1e-3 and 1e-4 differences disagree), the h = 1e-4
+    difference is the reference for that coordinate."""
+    from oracle.oracle import OracleSim
+    from smokesim_b200 import Sim
+    from smokesim_b200.adjoint import Rollout
+    import torch
+    n, nsteps = 32, 8
+    sc = scene.rollout64(seed=5, n=n)
+    p = scene.workload_params(ref_quirks=0, n_vcycles=4)
+    rng = np.random.default_rng(7)
+    forces = (rng.standard_normal((nsteps, 3)) * 0.2).astype(np.float32)
+    target = scene.rollout64(seed=6, n=n)
+    # target density: a rollout with the emitter shifted by 3 cells in x
+    tsim = OracleSim(target["desc"], "f64")
+    target["emitters"][0].pos[0] += 3.0
+    scene.apply(tsim, target)
+    for _ in range(nsteps):
+        tsim.step(p)
+    rho_t = tsim.get_field(abi.FIELD_DENSITY, f64=True).ravel()
+
+    def loss_fp64(dvel, dforce, h):
+        o = OracleSim(sc["desc"], "f64")
+        scene.apply(o, sc)
+        for k in VEL:
+            base = sc["fields"][k].astype(np.float64).ravel()
+            if k in dvel:
+                base = base.copy()
+                base[dvel[k]] += h
+            o.set_field_f64(k, base)
+        for s in range(nsteps):
+            fo = forces[s].astype(np.float64).copy()
+            if dforce is not None and dforce[0] == s:
+                fo[dforce[1]] += h
+            o.set_emitter_force(fo)
+            o.step(p)
+        r = o.get_field(abi.FIELD_DENSITY, f64=True).ravel()
+        o.close()
+        return float(np.sum((r - rho_t) ** 2))
+
+    g = Sim(sc["desc"])
+    scene.apply(g, sc)
+    ro = Rollout(g, nsteps, 3)
+    ro.forward(p, forces)
+    rho = torch.from_numpy(g.get_field(abi.FIELD_DENSITY).ravel()).cuda().double()
+    gd = (2 * (rho - torch.from_numpy(rho_t).cuda())).float().contiguous()
+    torch.cuda.synchronize()
+    gf = ro.backward(p, grad_density=gd.data_ptr())
+    gvel = {k: ro.grad(k) for k in VEL}
+    # 32 coordinates: 24 velocity faces near the plume, 8 force components
+    h = 1e-3
+    errs = []
+    nv = {k: abi.field_count(3, (n, n, n), k) for k in VEL}
+    picks = []
+    for _ in range(24):
+        k = VEL[rng.integers(0, 3)]
+        picks.append(("v", k, int(rng.integers(0, nv[k]))))
+    for _ in range(8):
+        picks.append(("f", int(rng.integers(0, nsteps)), int(rng.integers(0, 3))))
+    def central(kind, a, b, hh):
+        if kind == "v":
+            return (loss_fp64({a: b}, None, hh) - loss_fp64({a: b}, None, -hh)) / (2 * hh)
+        return (loss_fp64({}, (a, b), hh) - loss_fp64({}, (a, b), -hh)) / (2 * hh)
+
+    adj = np.array([gvel[a][b] if kind == "v" else gf[a, b] for kind, a, b in picks], np.float64)
+    fd = np.array([central(kind, a, b, h) for kind, a, b in picks])
+    scale = np.abs(fd).max()
+    assert scale > 0
+    kinks = 0
+    for i, (kind, a, b) in enumerate(picks):
+        if abs(adj[i] - fd[i]) > 1e-3 * scale:
+            fd4 = central(kind, a, b, 1e-4)
+            if abs(fd4 - fd[i]) > 1e-3 * scale:   # h = 1e-3 crosses a kink
+                fd[i] = fd4
+                kinks += 1
+    err = np.abs(adj - fd) / scale
+    assert err.max() <= 1e-3, (err.max(), list(zip(adj, fd)))
+    assert kinks <= 4, kinks
+    ro.close()
+    g.close()
+
+
+def test_inverse_problem_reduces_loss():
+    """Fit per-step emitter forces to a target density with Adam through the
+    autograd binding: the loss must fall."""
+    import torch
+    from smokesim_b200 import Sim
+    from smokesim_b200.adjoint import Rollout, rollout_fn
+    n, nsteps = 24, 6
+    sc = scene.rollout64(seed=1, n=n)
+    p = scene.workload_params(ref_quirks=0, n_vcycles=2)
+    tgt = scene.rollout64(seed=1, n=n)
+    tgt["emitters"][0].pos[0] += 3.0
+    t = Sim(tgt["desc"])
+    scene.apply(t, tgt)
+    t.step(p, nsteps)
+    rho_t = torch.from_numpy(t.get_field(abi.FIELD_DENSITY).ravel()).cuda()
+    g = Sim(sc["desc"])
+    scene.apply(g, sc)
+    ro = Rollout(g, nsteps, 2)
+    fn = rollout_fn(ro, p)
+    vel0 = [torch.from_numpy(sc["fields"][k].ravel()).cuda() for k in VEL]
+    forces = torch.zeros(nsteps, 3, requires_grad=True)
+    opt = torch.optim.Adam([forces], lr=0.5)
+    losses = []
+    for _ in range(6):
+        opt.zero_grad()
+        rho = fn(forces.cuda(), *vel0)
+        loss = ((rho - rho_t) ** 2).sum()
+        loss.backward()
+        opt.step()
+        losses.append(float(loss))
+    assert losses[-1] < losses[0], losses
+    ro.close()
+    g.close()
