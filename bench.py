@@ -27,6 +27,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
@@ -43,6 +45,9 @@ def parse():
     ap.add_argument("--n", type=int, default=256, help="grid cells per axis")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint rollout timing")
+    ap.add_argument("--profile-adjoint", action="store_true",
+                    help="no timing: a 4-step forward+reverse rollout of the plume scene at --n (for ncu)")
     ap.add_argument("--profile", action="store_true",
                     help="no timing: set up, run one step and a few level-0 smoother sweeps (for ncu)")
     return ap.parse_args()
@@ -236,6 +241,72 @@ def run_variant(torch, sim_cls, scene, sc, name, args, stream, barrier, world, d
     return sim, p, out
 
 
+ADJOINT_CASES = [
+    # name, scene, steps, checkpoint interval
+    ("rollout64", dict(kind="rollout64", n=64), 64, 8),
+    ("plume128", dict(kind="plume3d", n=128), 200, 14),
+]
+
+
+def adjoint_bench(torch, stream):
+    """Forward rollout with checkpoints + reverse pass (ss_adjoint_*) against
+    the plain forward steps of the same scene: FP32 projection with the
+    corrected operators, 4 V-cycles per step, L2 loss on the final density."""
+    from smokesim_b200 import Sim, abi, scene
+    from smokesim_b200.adjoint import Rollout
+    out = {}
+    for name, sa, nsteps, every in ADJOINT_CASES:
+        sc = scene.rollout64(seed=0, n=sa["n"]) if sa["kind"] == "rollout64" else scene.plume3d(seed=0, n=sa["n"])
+        sc.pop("rng", None)
+        p = scene.workload_params(ref_quirks=0, n_vcycles=4, collect_stats=0)
+        cells = sa["n"] ** 3
+        forces = np.zeros((nsteps, 3), np.float32)
+        forces[:, 1] = 0.5
+        e0, e_mid, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        # plain forward steps
+        sim = Sim(sc["desc"], stream=stream.cuda_stream)
+        scene.apply(sim, sc)
+        sim.set_emitter_force((0.0, 0.5, 0.0))
+        sim.step(p, 3)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sim.step(p, nsteps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fwd_ms = e0.elapsed_time(e1) / nsteps
+        sim.close()
+        # rollout with checkpoints + reverse pass (the first repetition warms up;
+        # the reverse pass leaves the simulation in the rollout's initial state)
+        sim = Sim(sc["desc"], stream=stream.cuda_stream)
+        scene.apply(sim, sc)
+        ro = Rollout(sim, nsteps, every)
+        rho = torch.empty(abi.field_count(3, sim.n, abi.FIELD_DENSITY), device="cuda")
+        for _ in range(2):
+            torch.cuda.synchronize()
+            e0.record(stream)
+            ro.forward(p, forces, stream=stream.cuda_stream)
+            e_mid.record(stream)
+            sim.L.ss_get_field_device(sim.h, abi.FIELD_DENSITY, C.c_void_p(rho.data_ptr()), rho.numel(),
+                                      C.c_void_p(stream.cuda_stream))
+            with torch.cuda.stream(stream):
+                gd = (2.0 * (rho - 0.1)).contiguous()
+            ro.backward(p, grad_density=gd.data_ptr(), stream=stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        f_ms = e0.elapsed_time(e_mid) / nsteps
+        fb_ms = e0.elapsed_time(e1) / nsteps
+        info = ro.info()
+        ro.close()
+        sim.close()
+        out[name] = {"grid": [sa["n"]] * 3, "steps": nsteps, "checkpoint_every": every,
+                     "forward_ms_per_step": fwd_ms, "forward_with_checkpoints_ms_per_step": f_ms,
+                     "fwd_adjoint_ms_per_step": fb_ms, "fwd_adjoint_over_forward": fb_ms / fwd_ms,
+                     "fwd_adjoint_mcell_steps_per_s": cells / (fb_ms / 1e3) / 1e6,
+                     "reverse_kernel_launches": info["kernel_launches"],
+                     "checkpoint_bytes": info["checkpoint_bytes"], "workspace_bytes": info["workspace_bytes"]}
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -261,6 +332,24 @@ def main():
     def barrier():
         if world > 1:
             dist.barrier()
+
+    if args.profile_adjoint:
+        from smokesim_b200.adjoint import Rollout
+        sc = scene.plume3d(seed=0, n=args.n)
+        sc.pop("rng", None)
+        p = scene.workload_params(ref_quirks=0, n_vcycles=4, collect_stats=0)
+        sim = Sim(sc["desc"], stream=stream.cuda_stream)
+        scene.apply(sim, sc)
+        ro = Rollout(sim, 4, 2)
+        forces = np.zeros((4, 3), np.float32)
+        forces[:, 1] = 0.5
+        ro.forward(p, forces, stream=stream.cuda_stream)
+        rho = torch.ones(abi.field_count(3, sim.n, abi.FIELD_DENSITY), device="cuda")
+        torch.cuda.synchronize()
+        ro.backward(p, grad_density=rho.data_ptr(), stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_adjoint": "done", "reverse": ro.info()}))
+        return 0
 
     with torch.cuda.stream(stream):
         if args.profile:
@@ -340,6 +429,10 @@ def main():
                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": launch_ms,
                     "traffic": RB_SMOOTH_TRAFFIC if args.n == 256 else None}
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_bench(torch, stream)
+
     line = {
         "impl": "b200", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -347,6 +440,7 @@ def main():
         "data": "synthetic (seeded scene + GRF)",
         "config": workload_config(args, sc), "gpu_launches": int(head["gpu_launches"]), "clocks": clocks,
         "variants": variants,
+        "adjoint": adjoint,
         "e2e": e2e, "roofline": roofline,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

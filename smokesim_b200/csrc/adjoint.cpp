@@ -2,12 +2,13 @@
 //
 // The forward rollout saves the full simulation state every `every` steps.
 // The reverse pass walks the segments backwards: it restores a segment's
-// checkpoint, recomputes the segment saving the start state of each step,
-// then for each step (last first) restores its start state, reruns the step
-// keeping the intermediate velocities and smoke its stages read
-// (run_step's StepSaves), and applies the stages' adjoint kernels
-// (k_adjoint.cu) in reverse order.  Memory: (nsteps/every + every) states
-// plus one step's intermediates, instead of nsteps states.
+// checkpoint and recomputes the segment once, keeping for each step the
+// intermediate velocities, smoke and vorticity its stages read (run_step's
+// StepSaves); then, last step first, it applies the stages' adjoint kernels
+// (k_adjoint.cu) in reverse stage order.  Every step is thus run twice
+// (forward pass, segment recomputation) plus its adjoint; memory is
+// nsteps/every states plus `every` steps of intermediates instead of
+// nsteps steps of intermediates.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,19 +32,30 @@ struct State {
     std::vector<ss_obstacle> ob;
 };
 
+// what one step's adjoint reads of its forward pass
+struct Record {
+    float* ue[3] = {nullptr, nullptr, nullptr};   // velocity after handle_emitters
+    float* ua[3] = {nullptr, nullptr, nullptr};   // after advection (+ buoyancy)
+    float* un[3] = {nullptr, nullptr, nullptr};   // after the projection update
+    float* dens_e = nullptr;                      // smoke after handle_emitters
+    float* temp_e = nullptr;
+    float* vort = nullptr;                        // vorticity of ua
+    int vcycles = 0;
+    std::vector<ss_emitter> em;                   // emitter records the step used
+};
+
 }  // namespace
 
 struct ss_adjoint {
     ss_sim* s = nullptr;
     int n = 0, every = 1;
-    std::vector<State> ckpt, seg;
+    std::vector<State> ckpt;
+    std::vector<Record> rec;
     std::vector<float> forces;
     float* ub[3] = {}, *ub2[3] = {};
     float* db = nullptr, *db2 = nullptr, *tb = nullptr, *tb2 = nullptr;
     AdjScratch w{};
     float* vc3 = nullptr, *wdir = nullptr, *dbar3 = nullptr, *wbar = nullptr;
-    float* ue[3] = {}, *ua[3] = {}, *un[3] = {};
-    float* dens_e = nullptr, *temp_e = nullptr;
     double* fpart = nullptr;
     double* fgrad = nullptr;   // nsteps * 3
     std::vector<void*> allocs;
@@ -71,6 +83,19 @@ static int alloc_state(ss_adjoint* A, State& S) {
     TRY_ADJ(amalloc(A, (void**)&S.dens, s->ncell * s->nch * 4, &A->ckpt_bytes));
     TRY_ADJ(amalloc(A, (void**)&S.temp, s->ncell * 4, &A->ckpt_bytes));
     TRY_ADJ(amalloc(A, (void**)&S.p, s->ncell * 4, &A->ckpt_bytes));
+    return SS_OK;
+}
+
+static int alloc_record(ss_adjoint* A, Record& R) {
+    ss_sim* s = A->s;
+    for (int d = 0; d < s->dim; ++d) {
+        TRY_ADJ(amalloc(A, (void**)&R.ue[d], s->nv[d] * 4, &A->ckpt_bytes));
+        TRY_ADJ(amalloc(A, (void**)&R.ua[d], s->nv[d] * 4, &A->ckpt_bytes));
+        TRY_ADJ(amalloc(A, (void**)&R.un[d], s->nv[d] * 4, &A->ckpt_bytes));
+    }
+    TRY_ADJ(amalloc(A, (void**)&R.dens_e, s->ncell * s->nch * 4, &A->ckpt_bytes));
+    TRY_ADJ(amalloc(A, (void**)&R.temp_e, s->ncell * 4, &A->ckpt_bytes));
+    TRY_ADJ(amalloc(A, (void**)&R.vort, s->ncell * (s->dim == 3 ? 3 : 1) * 4, &A->ckpt_bytes));
     return SS_OK;
 }
 
@@ -114,52 +139,66 @@ static int check_adjoint_params(const ss_adjoint* A, const ss_params* p) {
     return SS_OK;
 }
 
-// Reverse of one step.  On entry the simulation holds the step's start state
-// and ub/db/tb/pbar[0] the adjoint of its end state; on return the simulation
-// holds the end state (recomputed) and the adjoint arrays the adjoint of the
-// start state.
-static int adj_step(ss_adjoint* A, const ss_params* p, int k, cudaStream_t st) {
+// Forward step k keeping what its adjoint reads.
+static int record_step(ss_adjoint* A, const ss_params* p, int k, Record& R, cudaStream_t st) {
+    ss_sim* s = A->s;
+    StepSaves sv{};
+    for (int d = 0; d < s->dim; ++d) {
+        sv.emit_vel[d] = R.ue[d];
+        sv.force_vel[d] = R.ua[d];
+        sv.proj_vel[d] = R.un[d];
+    }
+    sv.emit_dens = R.dens_e;
+    sv.emit_temp = R.temp_e;
+    set_force(A, k);
+    TRY_ADJ(run_step(s, p, st, &sv));
+    R.vcycles = sv.vcycles;
+    R.em = s->em;
+    if (p->stage_mask & SS_STAGE_APPLY_VORTICITY)
+        TRY_ADJ(copy_d2d(R.vort, s->vort, s->ncell * (s->dim == 3 ? 3 : 1) * 4, st));
+    return SS_OK;
+}
+
+// Reverse of one step from its record: on entry ub/db/tb/pbar[0] hold the
+// adjoint of the step's end state, on return that of its start state.
+static int adj_step(ss_adjoint* A, const ss_params* p, int k, const Record& R, cudaStream_t st) {
     ss_sim* s = A->s;
     const StepConsts c = make_consts(s, p);
     const int m = p->stage_mask;
-    StepSaves sv{};
-    for (int d = 0; d < s->dim; ++d) {
-        sv.emit_vel[d] = A->ue[d];
-        sv.force_vel[d] = A->ua[d];
-        sv.proj_vel[d] = A->un[d];
-    }
-    sv.emit_dens = A->dens_e;
-    sv.emit_temp = A->temp_e;
-    set_force(A, k);
-    TRY_ADJ(run_step(s, p, st, &sv));
     const size_t ncell = s->ncell;
     if (m & SS_STAGE_ADVECT_SMOKE) {
         TRY_ADJ(check_cuda(cudaMemsetAsync(A->db2, 0, ncell * s->nch * 4, st), "memset"));
         TRY_ADJ(check_cuda(cudaMemsetAsync(A->tb2, 0, ncell * 4, st), "memset"));
-        const float* vel[3] = {A->un[0], A->un[1], A->un[2]};
-        TRY_ADJ(adj_advect_smoke(s, c, vel, A->dens_e, A->temp_e, A->db, A->tb, A->db2, A->tb2, A->vc3, A->ub, st));
+        const float* vel[3] = {R.un[0], R.un[1], R.un[2]};
+        TRY_ADJ(adj_advect_smoke(s, c, vel, R.dens_e, R.temp_e, A->db, A->tb, A->db2, A->tb2, A->vc3, A->ub, st));
         std::swap(A->db, A->db2);
         std::swap(A->tb, A->tb2);
     }
     if (m & SS_STAGE_UPDATE_VELOCITIES) TRY_ADJ(adj_update(s, c, A->ub, A->w.pbar[0], st));
     if (m & SS_STAGE_RESOLVE_PRESSURE) {
         TRY_ADJ(check_cuda(cudaMemsetAsync(A->w.bbar[0], 0, ncell * 4, st), "memset"));
-        for (int i = 0; i < sv.vcycles; ++i) TRY_ADJ(adj_v_cycle(s, c, p->mg, A->w, st));
+        for (int i = 0; i < R.vcycles; ++i) TRY_ADJ(adj_v_cycle(s, c, p->mg, A->w, st));
         TRY_ADJ(adj_divergence(s, A->w.bbar[0], A->ub, st));
     }
-    if (m & SS_STAGE_APPLY_VORTICITY) TRY_ADJ(adj_vorticity(s, c, s->vort, A->ub, A->wdir, A->dbar3, A->wbar, st));
+    if (m & SS_STAGE_APPLY_VORTICITY) TRY_ADJ(adj_vorticity(s, c, R.vort, A->ub, A->wdir, A->dbar3, A->wbar, st));
     if (m & SS_STAGE_ADVECT_VELOCITIES) {
         for (int d = 0; d < s->dim; ++d)
             TRY_ADJ(check_cuda(cudaMemsetAsync(A->ub2[d], 0, s->nv[d] * 4, st), "memset"));
-        const float* vel[3] = {A->ue[0], A->ue[1], A->ue[2]};
+        const float* vel[3] = {R.ue[0], R.ue[1], R.ue[2]};
         const float* gin[3] = {A->ub[0], A->ub[1], A->ub[2]};
-        TRY_ADJ(adj_advect_velocity(s, c, (m & SS_STAGE_APPLY_BUOYANCY) != 0, vel, A->dens_e, A->temp_e, gin, A->ub2,
+        TRY_ADJ(adj_advect_velocity(s, c, (m & SS_STAGE_APPLY_BUOYANCY) != 0, vel, R.dens_e, R.temp_e, gin, A->ub2,
                                     A->db, A->tb, st));
         for (int d = 0; d < 3; ++d) std::swap(A->ub[d], A->ub2[d]);
     } else if (m & SS_STAGE_APPLY_BUOYANCY) {
         TRY_ADJ(adj_buoyancy(s, c, A->ub[1], A->db, A->tb, st));
     }
-    if (m & SS_STAGE_HANDLE_EMITTERS) TRY_ADJ(adj_emitters(s, c, 1, A->ub, A->fpart, A->fgrad + 3 * (size_t)k, st));
+    if (m & SS_STAGE_HANDLE_EMITTERS) {
+        // the emitter records of this step (their status changes over time)
+        if (!R.em.empty())
+            TRY_ADJ(check_cuda(cudaMemcpyAsync(s->d_em, R.em.data(), R.em.size() * sizeof(ss_emitter),
+                                               cudaMemcpyHostToDevice, st), "emitter records"));
+        TRY_ADJ(adj_emitters(s, c, 1, A->ub, A->fpart, A->fgrad + 3 * (size_t)k, st));
+    }
     return SS_OK;
 }
 
@@ -184,24 +223,19 @@ int ss_adjoint_create(ss_sim* s, int nsteps, int every, ss_adjoint** out) {
     A->forces.assign((size_t)nsteps * 3, 0.f);
     const int nseg = (nsteps + every - 1) / every;
     A->ckpt.resize(nseg);
-    A->seg.resize(every);
+    A->rec.resize(every);
     int rc = SS_OK;
     for (auto& S : A->ckpt) rc = rc ? rc : alloc_state(A, S);
-    for (auto& S : A->seg) rc = rc ? rc : alloc_state(A, S);
+    for (auto& R : A->rec) rc = rc ? rc : alloc_record(A, R);
     auto W = [&](void** p, size_t bytes) { if (!rc) rc = amalloc(A, p, bytes, &A->work_bytes); };
     for (int d = 0; d < s->dim; ++d) {
         W((void**)&A->ub[d], s->nv[d] * 4);
         W((void**)&A->ub2[d], s->nv[d] * 4);
-        W((void**)&A->ue[d], s->nv[d] * 4);
-        W((void**)&A->ua[d], s->nv[d] * 4);
-        W((void**)&A->un[d], s->nv[d] * 4);
     }
     W((void**)&A->db, s->ncell * s->nch * 4);
     W((void**)&A->db2, s->ncell * s->nch * 4);
     W((void**)&A->tb, s->ncell * 4);
     W((void**)&A->tb2, s->ncell * 4);
-    W((void**)&A->dens_e, s->ncell * s->nch * 4);
-    W((void**)&A->temp_e, s->ncell * 4);
     W((void**)&A->vc3, s->ncell * 3 * 4);
     W((void**)&A->wdir, s->ncell * 3 * 4);
     W((void**)&A->dbar3, s->ncell * 3 * 4);
@@ -273,17 +307,8 @@ int ss_adjoint_backward(ss_adjoint* A, const ss_params* p, const float* grad_den
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int k0 = sg * A->every, k1 = std::min(A->n, k0 + A->every);
         TRY_ADJ(restore_state(s, A->ckpt[sg], st));
-        for (int k = k0; k < k1; ++k) {
-            TRY_ADJ(save_state(s, A->seg[k - k0], st));
-            if (k + 1 < k1) {
-                set_force(A, k);
-                TRY_ADJ(run_step(s, p, st, nullptr));
-            }
-        }
-        for (int k = k1 - 1; k >= k0; --k) {
-            TRY_ADJ(restore_state(s, A->seg[k - k0], st));
-            TRY_ADJ(adj_step(A, p, k, st));
-        }
+        for (int k = k0; k < k1; ++k) TRY_ADJ(record_step(A, p, k, A->rec[k - k0], st));
+        for (int k = k1 - 1; k >= k0; --k) TRY_ADJ(adj_step(A, p, k, A->rec[k - k0], st));
     }
     TRY_ADJ(restore_state(s, A->ckpt[0], st));
     for (int d = 0; d < 3; ++d) s->force[d] = 0.f;

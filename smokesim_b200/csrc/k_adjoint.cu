@@ -838,12 +838,189 @@ static int adj_sweeps(ss_sim* s, const AdjLevel& a, int L, int iterations, cudaS
     return check_cuda(cudaGetLastError(), "k_adj_smooth");
 }
 
+// ------------------------------------------------ single-block lower V-cycle^T
+// The transpose of k_bottom: levels Lb..coarsest in one thread block with the
+// adjoint arrays (pbar, bbar, T of every level) in shared memory - the
+// 2*n_coarse + 1 launches of the coarsest level's transposed sweeps alone
+// would otherwise dominate.  Same per-cell operations as the level kernels
+// above, one __syncthreads per half-step.
+struct AdjBottomArgs {
+    int nlev;
+    int n[SS_MAX_LEVELS][3];
+    int off[SS_MAX_LEVELS];
+    float hh[SS_MAX_LEVELS];
+    const float* alpha[SS_MAX_LEVELS];
+    float* pbar0;   // global adjoint pressure of level Lb (in/out)
+    float* bbar0;   // global right-hand-side adjoint of level Lb (accumulated)
+    int total;
+    int n_pre, n_post, n_coarse;
+    float oobA;
+};
+
+SS_D AdjLevel bottom_adj_level(const AdjBottomArgs& b, int l, float* sp, float* sb, float* sT) {
+    AdjLevel a;
+    a.nx = b.n[l][0]; a.ny = b.n[l][1]; a.nz = b.n[l][2];
+    a.fmask = nullptr;
+    a.alpha = b.alpha[l];
+    a.oobA = b.oobA;
+    a.hh = b.hh[l];
+    a.beta = b.hh[l];
+    a.rcoef = 1.f;
+    a.pbar = sp + b.off[l];
+    a.bbar = sb + b.off[l];
+    a.T = sT + b.off[l];
+    return a;
+}
+
+template <int DIM>
+SS_D void bottom_adj_half(const AdjLevel& a, int colour, bool do_b, bool do_a) {
+    const int n = a.nx * a.ny * a.nz;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const int x = q % a.nx, t = q / a.nx, y = t % a.ny, z = t / a.ny;
+        if (((x + y + z) & 1) != colour) continue;
+        float wself, d;
+        bool fluid;
+        cell_weights<DIM, false>(a, x, y, z, wself, d, fluid);
+        float pb = a.pbar[q];
+        if (do_b) pb += wself * nbr_sum<DIM>(a.T, x, y, z, a.nx, a.ny, a.nz);
+        if (do_a) {
+            if (fluid && d != 0.f) {
+                const float tt = pb / d;
+                a.T[q] = tt;
+                pb = 0.f;
+                a.bbar[q] -= a.beta * tt;
+            } else {
+                a.T[q] = 0.f;
+            }
+        }
+        a.pbar[q] = pb;
+    }
+    __syncthreads();
+}
+
+template <int DIM>
+SS_D void bottom_adj_sweeps(const AdjLevel& a, int iterations) {
+    if (iterations <= 0) return;
+    bottom_adj_half<DIM>(a, 1, false, true);
+    int colour = 1;
+    for (int k = 1; k < 2 * iterations; ++k) {
+        colour ^= 1;
+        bottom_adj_half<DIM>(a, colour, true, true);
+    }
+    bottom_adj_half<DIM>(a, colour ^ 1, true, false);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(1024) k_adj_bottom(AdjBottomArgs b) {
+    extern __shared__ float sm[];
+    float* sp = sm;
+    float* sb = sm + b.total;
+    float* sT = sm + 2 * b.total;
+    const int n0 = b.n[0][0] * b.n[0][1] * b.n[0][2];
+    for (int c = threadIdx.x; c < b.total; c += blockDim.x) {
+        sp[c] = c < n0 ? b.pbar0[c] : 0.f;
+        sb[c] = 0.f;
+        sT[c] = 0.f;
+    }
+    __syncthreads();
+    const int last = b.nlev - 1;
+    // down: post-smoothing^T, then prolongation^T into the (fresh) coarse pbar
+    for (int l = 0; l < last; ++l) {
+        const AdjLevel a = bottom_adj_level(b, l, sp, sb, sT);
+        bottom_adj_sweeps<DIM>(a, b.n_post);
+        const int cx = b.n[l + 1][0], cy = b.n[l + 1][1], cz = b.n[l + 1][2];
+        float* pc = sp + b.off[l + 1];
+        for (int q = threadIdx.x; q < cx * cy * cz; q += blockDim.x) {
+            const int X = q % cx, t = q / cx, Y = t % cy, Z = t / cy;
+            float s = 0.f;
+            const int z0 = DIM == 3 ? 2 * Z - 2 : 0, z1 = DIM == 3 ? 2 * Z + 3 : 0;
+            for (int z = max(z0, 0); z <= min(z1, a.nz - 1); ++z) {
+                const float wz = DIM == 3 ? prolong_coef(z, a.nz, cz, Z) : 1.f;
+                if (wz == 0.f) continue;
+                for (int y = max(2 * Y - 2, 0); y <= min(2 * Y + 3, a.ny - 1); ++y) {
+                    const float wy = prolong_coef(y, a.ny, cy, Y);
+                    if (wy == 0.f) continue;
+                    for (int x = max(2 * X - 2, 0); x <= min(2 * X + 3, a.nx - 1); ++x) {
+                        const float wx = prolong_coef(x, a.nx, cx, X);
+                        if (wx == 0.f) continue;
+                        s += wx * wy * wz * a.pbar[idx3(x, y, z, a.nx, a.ny)];
+                    }
+                }
+            }
+            pc[q] = s;
+        }
+        __syncthreads();
+    }
+    bottom_adj_sweeps<DIM>(bottom_adj_level(b, last, sp, sb, sT), b.n_coarse);
+    // up: residual + restriction^T, then pre-smoothing^T
+    for (int l = last - 1; l >= 0; --l) {
+        const AdjLevel a = bottom_adj_level(b, l, sp, sb, sT);
+        const int cx = b.n[l + 1][0], cy = b.n[l + 1][1], cz = b.n[l + 1][2];
+        const float* rcb = sb + b.off[l + 1];
+        const int n = a.nx * a.ny * a.nz;
+        for (int q = threadIdx.x; q < n; q += blockDim.x) {
+            const int x = q % a.nx, t = q / a.nx, y = t % a.ny, z = t / a.ny;
+            float wself, d;
+            bool fluid;
+            cell_weights<DIM, false>(a, x, y, z, wself, d, fluid);
+            const float rs = res_bar<DIM, false>(a, rcb, cx, cy, cz, x, y, z);
+            float nb = 0.f;
+            if (y + 1 < a.ny) nb += res_bar<DIM, false>(a, rcb, cx, cy, cz, x, y + 1, z);
+            if (y > 0) nb += res_bar<DIM, false>(a, rcb, cx, cy, cz, x, y - 1, z);
+            if (x + 1 < a.nx) nb += res_bar<DIM, false>(a, rcb, cx, cy, cz, x + 1, y, z);
+            if (x > 0) nb += res_bar<DIM, false>(a, rcb, cx, cy, cz, x - 1, y, z);
+            if constexpr (DIM == 3) {
+                if (z + 1 < a.nz) nb += res_bar<DIM, false>(a, rcb, cx, cy, cz, x, y, z + 1);
+                if (z > 0) nb += res_bar<DIM, false>(a, rcb, cx, cy, cz, x, y, z - 1);
+            }
+            a.pbar[q] += (d * rs - wself * nb) / a.hh;
+            a.bbar[q] += rs;
+        }
+        __syncthreads();
+        bottom_adj_sweeps<DIM>(a, b.n_pre);
+    }
+    for (int c = threadIdx.x; c < n0; c += blockDim.x) {
+        b.pbar0[c] = sp[c];
+        b.bbar0[c] += sb[c];
+    }
+}
+
+static int adj_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, const AdjScratch& w, cudaStream_t st) {
+    AdjBottomArgs b{};
+    b.nlev = s->levels - L;
+    int off = 0;
+    for (int l = 0; l < b.nlev; ++l) {
+        const ss::Level& lv = s->lv[L + l];
+        b.n[l][0] = lv.n[0]; b.n[l][1] = lv.n[1]; b.n[l][2] = lv.n[2];
+        b.off[l] = off;
+        b.hh[l] = lv.hh;
+        b.alpha[l] = s->alpha[L + l];
+        off += lv.n[0] * lv.n[1] * lv.n[2];
+    }
+    b.total = off;
+    b.pbar0 = w.pbar[L];
+    b.bbar0 = w.bbar[L];
+    b.n_pre = mg.n_pre; b.n_post = mg.n_post; b.n_coarse = mg.n_coarse;
+    b.oobA = s->enclosed ? 1.f : 0.f;
+    const size_t smem = (size_t)3 * off * sizeof(float);
+    if (smem > (size_t)kBottomSmemBytes) return set_error(SS_E_INVALID, "adjoint bottom levels exceed shared memory");
+    cudaError_t e = s->dim == 3
+        ? cudaFuncSetAttribute(k_adj_bottom<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBytes)
+        : cudaFuncSetAttribute(k_adj_bottom<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBytes);
+    if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute(k_adj_bottom)");
+    if (s->dim == 3) k_adj_bottom<3><<<1, 1024, smem, st>>>(b);
+    else k_adj_bottom<2><<<1, 1024, smem, st>>>(b);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_adj_bottom");
+}
+
 // Transposed V-cycle from level L: on entry w.pbar[L] holds the adjoint of the
 // level's output pressure; on return it holds the adjoint of its input
 // pressure and w.bbar[L] has the right-hand side's adjoint added.
 static int adj_v_cycle_rec(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int L, const AdjScratch& w,
                            cudaStream_t st) {
     const AdjLevel a = adj_level(s, c, L, w);
+    if (L >= 1 && L >= s->bottom) return adj_bottom(s, mg, L, w, st);
     if (L == s->levels - 1) return adj_sweeps(s, a, L, mg.n_coarse, st);
     TRY_ADJ(adj_sweeps(s, a, L, mg.n_post, st));
     const int cx = s->lv[L + 1].n[0], cy = s->lv[L + 1].n[1], cz = s->lv[L + 1].n[2];

@@ -112,6 +112,10 @@ class Sim:
         a = np.ascontiguousarray(arr, dtype=np.float32).reshape(-1)
         _check(self.L.ss_set_level(self.h, level, what, _fptr(a), a.size, self.stream), "ss_set_level")
 
+    def set_emitter_force(self, force):
+        f = (C.c_float * 3)(*[float(x) for x in force])
+        _check(self.L.ss_set_emitter_force(self.h, C.byref(f)), "ss_set_emitter_force")
+
     def clear_grid(self, t_ambient):
         _check(self.L.ss_clear_grid(self.h, C.c_float(t_ambient), self.stream), "ss_clear_grid")
 

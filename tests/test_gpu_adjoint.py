@@ -146,7 +146,7 @@ def test_rollout_checkpointing_consistent():
         assert np.allclose(gf, res[0][0], rtol=1e-4, atol=1e-6 * np.abs(res[0][0]).max())
         for a, b in zip(gv, res[0][1]):
             assert np.allclose(a, b, rtol=1e-3, atol=1e-5 * np.abs(b).max())
-    # every step: 8 checkpoints + 1 segment state; every 3: 3 + 3
+    # every step: 8 checkpoints + 1 step record; every 3: 3 checkpoints + 3 records
     assert res[1][2]["checkpoint_bytes"] < res[0][2]["checkpoint_bytes"]
 
 
