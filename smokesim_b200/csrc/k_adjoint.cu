@@ -391,19 +391,29 @@ __global__ void __launch_bounds__(256) k_adj_prolong(const float* __restrict__ p
     const int Y = blockIdx.y * blockDim.y + threadIdx.y;
     const int Z = blockIdx.z * blockDim.z + threadIdx.z;
     if (X >= cx || Y >= cy || Z >= cz) return;
+    // per-axis coefficients of the fine window [2K-2, 2K+3] (0 outside the grid)
+    float wx[6], wy[6], wz[6];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        const int x = 2 * X - 2 + j, y = 2 * Y - 2 + j, z = 2 * Z - 2 + j;
+        wx[j] = (x >= 0 && x < ax) ? prolong_coef(x, ax, cx, X) : 0.f;
+        wy[j] = (y >= 0 && y < ay) ? prolong_coef(y, ay, cy, Y) : 0.f;
+        wz[j] = DIM == 3 ? ((z >= 0 && z < az) ? prolong_coef(z, az, cz, Z) : 0.f) : (j == 2 ? 1.f : 0.f);
+    }
     float s = 0.f;
-    const int z0 = DIM == 3 ? 2 * Z - 2 : 0, z1 = DIM == 3 ? 2 * Z + 3 : 0;
-    for (int z = max(z0, 0); z <= min(z1, az - 1); ++z) {
-        const float cz_ = DIM == 3 ? prolong_coef(z, az, cz, Z) : 1.f;
-        if (cz_ == 0.f) continue;
-        for (int y = max(2 * Y - 2, 0); y <= min(2 * Y + 3, ay - 1); ++y) {
-            const float cy_ = prolong_coef(y, ay, cy, Y);
-            if (cy_ == 0.f) continue;
-            for (int x = max(2 * X - 2, 0); x <= min(2 * X + 3, ax - 1); ++x) {
-                const float cx_ = prolong_coef(x, ax, cx, X);
-                if (cx_ == 0.f) continue;
-                s += cx_ * cy_ * cz_ * pfb[idx3(x, y, z, ax, ay)];
-            }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        if (wz[k] == 0.f) continue;
+        const int z = DIM == 3 ? 2 * Z - 2 + k : 0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            if (wy[j] == 0.f) continue;
+            const int y = 2 * Y - 2 + j;
+            float row = 0.f;
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+                if (wx[i] != 0.f) row += wx[i] * pfb[idx3(2 * X - 2 + i, y, z, ax, ay)];
+            s += wz[k] * wy[j] * row;
         }
     }
     pcb[idx3(X, Y, Z, cx, cy)] = s;
@@ -898,9 +908,80 @@ SS_D void bottom_adj_half(const AdjLevel& a, int colour, bool do_b, bool do_a) {
     __syncthreads();
 }
 
+// A level of at most two cells per active thread (the coarsest one): the
+// cells' weights and neighbour masks stay in registers for all the sweeps.
+template <int DIM>
+SS_D void bottom_adj_sweeps_cached(const AdjLevel& a, int iterations, int nt) {
+    const int n = a.nx * a.ny * a.nz;
+    const int nx = a.nx, ny = a.ny, pl = nx * ny;
+    int ci[2], col[2], inr[2];
+    bool act[2], upd[2];
+    float ws[2], dd[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int c = threadIdx.x + k * nt;
+        act[k] = c < n;
+        ci[k] = c; col[k] = 0; inr[k] = 0; upd[k] = false; ws[k] = 0.f; dd[k] = 1.f;
+        if (!act[k]) continue;
+        const int x = c % nx, t = c / nx, y = t % ny, z = t / ny;
+        col[k] = (x + y + z) & 1;
+        inr[k] = (y + 1 < ny ? 1 : 0) | (y > 0 ? 2 : 0) | (x + 1 < nx ? 4 : 0) | (x > 0 ? 8 : 0) |
+                 (z + 1 < a.nz ? 16 : 0) | (z > 0 ? 32 : 0);
+        bool fluid;
+        cell_weights<DIM, false>(a, x, y, z, ws[k], dd[k], fluid);
+        upd[k] = fluid && dd[k] != 0.f;
+    }
+    auto half = [&](int colour, bool do_b, bool do_a) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (!act[k] || col[k] != colour) continue;
+            const int c = ci[k], m = inr[k];
+            float pb = a.pbar[c];
+            if (do_b) {
+                float sum = 0.f;
+                if (m & 1) sum += a.T[c + nx];
+                if (m & 2) sum += a.T[c - nx];
+                if (m & 4) sum += a.T[c + 1];
+                if (m & 8) sum += a.T[c - 1];
+                if (DIM == 3 && (m & 16)) sum += a.T[c + pl];
+                if (DIM == 3 && (m & 32)) sum += a.T[c - pl];
+                pb += ws[k] * sum;
+            }
+            if (do_a) {
+                if (upd[k]) {
+                    const float tt = pb / dd[k];
+                    a.T[c] = tt;
+                    pb = 0.f;
+                    a.bbar[c] -= a.beta * tt;
+                } else {
+                    a.T[c] = 0.f;
+                }
+            }
+            a.pbar[c] = pb;
+        }
+        if (nt == (int)blockDim.x) __syncthreads();
+        else asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
+    };
+    half(1, false, true);
+    int colour = 1;
+    for (int k = 1; k < 2 * iterations; ++k) {
+        colour ^= 1;
+        half(colour, true, true);
+    }
+    half(colour ^ 1, true, false);
+}
+
 template <int DIM>
 SS_D void bottom_adj_sweeps(const AdjLevel& a, int iterations) {
     if (iterations <= 0) return;
+    const int n = a.nx * a.ny * a.nz;
+    int nt = blockDim.x;
+    while (nt > 128 && (n + nt / 2 - 1) / (nt / 2) <= 2) nt /= 2;
+    if ((n + nt - 1) / nt <= 2) {
+        if ((int)threadIdx.x < nt) bottom_adj_sweeps_cached<DIM>(a, iterations, nt);
+        __syncthreads();
+        return;
+    }
     bottom_adj_half<DIM>(a, 1, false, true);
     int colour = 1;
     for (int k = 1; k < 2 * iterations; ++k) {

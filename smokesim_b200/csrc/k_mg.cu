@@ -522,11 +522,86 @@ SS_D MGArgs bottom_level(const BottomArgsT<T>& b, float* sp, float* sr, float* s
 // a level small enough for two cells per thread of fewer warps runs on those
 // warps only, synchronised by a named barrier.
 constexpr int kBottomCells = 4;
+
+// A level of at most two cells per active thread (the coarsest level, which
+// takes n_coarse sweeps): each thread keeps its cells' neighbour weights,
+// diagonal and r*h^2 term in registers for all the sweeps - the arithmetic
+// of smooth_cell, minus its per-sweep solid-fraction loads.
+template <int DIM, typename R>
+SS_D void bottom_smooth_cached(const MGArgs& a, int iterations, int nt) {
+    const int n = a.nx * a.ny * a.nz;
+    const int nx = a.nx, ny = a.ny, nz = a.nz, pl = nx * ny;
+    int ci[2], col[2], inr[2];
+    bool act[2];
+    float f[2][6], rhh[2], fs[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int c = threadIdx.x + k * nt;
+        act[k] = c < n;
+        ci[k] = c;
+        col[k] = 0;
+        inr[k] = 0;
+        rhh[k] = 0.f;
+        fs[k] = 1.f;
+#pragma unroll
+        for (int d = 0; d < 6; ++d) f[k][d] = 0.f;
+        if (!act[k]) continue;
+        const int x = c % nx, t = c / nx, y = t % ny, z = t / ny;
+        col[k] = (x + y + z) & 1;
+        if (a.alpha[c] >= 1.f) { act[k] = false; continue; }
+        inr[k] = (y + 1 < ny ? 1 : 0) | (y > 0 ? 2 : 0) | (x + 1 < nx ? 4 : 0) | (x > 0 ? 8 : 0) |
+                 (z + 1 < nz ? 16 : 0) | (z > 0 ? 32 : 0);
+        f[k][0] = 1.f - (y + 1 < ny ? a.alpha[c + nx] : a.oobA);
+        f[k][1] = 1.f - (y > 0 ? a.alpha[c - nx] : a.oobA);
+        f[k][2] = 1.f - (x + 1 < nx ? a.alpha[c + 1] : a.oobA);
+        f[k][3] = 1.f - (x > 0 ? a.alpha[c - 1] : a.oobA);
+        if constexpr (DIM == 3) {
+            f[k][4] = 1.f - (z + 1 < nz ? a.alpha[c + pl] : a.oobA);
+            f[k][5] = 1.f - (z > 0 ? a.alpha[c - pl] : a.oobA);
+        }
+        float f_sum = f[k][0] + f[k][1] + f[k][2] + f[k][3];
+        if constexpr (DIM == 3) f_sum = f_sum + f[k][4] + f[k][5];
+        if (f_sum == 0.f) { act[k] = false; continue; }
+        fs[k] = f_sum;
+        rhh[k] = ld(a.r[c]) * a.hh;
+    }
+    const float* P = a.p;
+    for (int it = 0; it < 2 * iterations; ++it) {
+        const int parity = it & 1;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (!act[k] || col[k] != parity) continue;
+            const int c = ci[k], m = inr[k];
+            const float p_top = (m & 1) ? P[c + nx] : 0.f;
+            const float p_bottom = (m & 2) ? P[c - nx] : 0.f;
+            const float p_right = (m & 4) ? P[c + 1] : 0.f;
+            const float p_left = (m & 8) ? P[c - 1] : 0.f;
+            float p_sum = p_top * f[k][0] + p_bottom * f[k][1];
+            p_sum = p_sum + p_right * f[k][2];
+            p_sum = p_sum + p_left * f[k][3];
+            if constexpr (DIM == 3) {
+                const float p_front = (m & 16) ? P[c + pl] : 0.f;
+                const float p_back = (m & 32) ? P[c - pl] : 0.f;
+                p_sum = p_sum + p_front * f[k][4];
+                p_sum = p_sum + p_back * f[k][5];
+            }
+            a.p[c] = rnd<R>((p_sum - rhh[k]) / fs[k]);
+        }
+        if (nt == (int)blockDim.x) __syncthreads();
+        else asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
+    }
+}
+
 template <int DIM, typename R>
 SS_D void bottom_smooth(const MGArgs& a, int iterations) {
     const int n = a.nx * a.ny * a.nz;
     int nt = blockDim.x;
     while (nt > 128 && (n + nt / 2 - 1) / (nt / 2) <= 2) nt /= 2;
+    if ((n + nt - 1) / nt <= 2) {
+        if ((int)threadIdx.x < nt) bottom_smooth_cached<DIM, R>(a, iterations, nt);
+        __syncthreads();
+        return;
+    }
     if ((int)threadIdx.x < nt) {
         int cx[kBottomCells], cy[kBottomCells], cz[kBottomCells], col[kBottomCells];
         int k = 0;
