@@ -92,6 +92,25 @@ def workload_config(args, sc):
     }
 
 
+# ------------------------------------------------------------------ ranks
+def max_over_ranks(value, world, device):
+    """The largest of the ranks' values (every rank gets it): timings of a
+    multi-rank run are the slowest rank's."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, cells, steps, ms):
+    """Whole-job Mcell-steps/s: every rank advances its own replica of
+    `cells` cells by `steps` steps in `ms` milliseconds (slowest rank)."""
+    return world * cells * steps / (ms / 1e3) / 1e6
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -183,9 +202,10 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ GPU arm
-# DRAM bytes per k_rb_smooth4<3> launch at 256^3 from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum; profiles/k_rb_smooth4_grf256.md)
-RB_SMOOTH_TRAFFIC = None
+# DRAM bytes per k_rb_smooth4<3> launch at 256^3 from one ncu capture of
+# that launch (dram__bytes_read.sum + dram__bytes_write.sum: 76,061,440 +
+# 10,889,472); the figure is for the 256^3 workload only.
+RB_SMOOTH_TRAFFIC = 86950912
 
 
 def step1(sim, p):
@@ -224,11 +244,7 @@ def run_variant(torch, sim_cls, scene, sc, name, args, stream, barrier, world, d
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
     out = {"ms_per_step": ms / args.steps, "ms_total": ms, "gpu_launches": launches}
     if p.mg.tol > 0:
         out.update({
@@ -373,7 +389,7 @@ def main():
                 head_sim, head_p = sim, p
             else:
                 sim.close()
-            out["value"] = world * cells / (out["ms_per_step"] / 1e3) / 1e6
+            out["value"] = job_rate(world, cells, 1, out["ms_per_step"])
             variants[name] = out
         head = variants[HEADLINE]
         value = head["value"]
@@ -389,12 +405,8 @@ def main():
             step1(sim, p)
             _ = sim.stats()
         torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e = {"value": world * cells * args.steps / e2e_s / 1e6, "unit": UNIT,
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
+        e2e = {"value": job_rate(world, cells, args.steps, e2e_s * 1e3), "unit": UNIT,
                "h2d_bytes_per_step": C.sizeof(abi.Emitter) * len(sc["emitters"]),
                "d2h_bytes_per_step": 8 * 8}
 

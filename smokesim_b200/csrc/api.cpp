@@ -87,11 +87,13 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->rb_mask);
     cudaFree(s->rb_pw);
     cudaFree(s->p64);
+    cudaFree(s->p64b);
     cudaFree(s->d_scale);
     cudaFree(s->red.partial_max);
     for (int l = 0; l < SS_MAX_LEVELS; ++l) { cudaFree(s->cp[l]); cudaFree(s->cr[l]); }
     cudaFree(s->rhs_r);
     cudaFree(s->red.partial);
+    cudaFree(s->red.partial2);
     cudaFree(s->red.out);
     if (s->red.host) cudaFreeHost(s->red.host);
     cudaFree(s->d_em);
@@ -241,6 +243,8 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     }
     s->red.max_blocks = (int)(((s->nx + 32) / 32 + 1) * ((s->ny + 8) / 8 + 1) * (size_t)(s->nz + 1));
     A((void**)&s->red.partial, (size_t)s->red.max_blocks * sizeof(double));
+    s->red.stage2 = s->red.max_blocks / 1024 + 2;
+    A((void**)&s->red.partial2, (size_t)2 * s->red.stage2 * sizeof(double));
     A((void**)&s->red.out, SLOT_COUNT * sizeof(double));
     A((void**)&s->d_err, sizeof(int));
     if (rc == SS_OK) {
@@ -654,6 +658,7 @@ static int ensure_mixed(ss_sim* s, int prec, cudaStream_t st) {
         return set_error(SS_E_UNSUPPORTED, "the mixed-precision solve needs an even nx and at least two levels");
     if (!s->p64) {
         CU(cudaMalloc((void**)&s->p64, s->ncell * sizeof(double)), "cudaMalloc(p64)");
+        CU(cudaMalloc((void**)&s->p64b, s->ncell * sizeof(double)), "cudaMalloc(p64)");
         s->p64_valid = 0;
     }
     if (!s->red.partial_max)
@@ -718,10 +723,13 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
     int done = 0;
     double db = 0.0, res = 0.0;
     bool conv = true;
+    bool pending = false;   // the last V-cycle's correction is not in p64 yet
     for (;;) {
         const bool last = !tol_mode && done == cap;
         if (last && !stats) break;
-        TRY(launch_ir_residual(s, c, stats ? SLOT_RESIDUAL : -1, st));
+        // adds the pending correction and evaluates the residual in one pass
+        TRY(launch_ir_residual(s, c, stats ? SLOT_RESIDUAL : -1, pending, st));
+        pending = false;
         if (tol_mode || last) {
             TRY(read_slots(s, st));
             db = sqrt(s->red.host[SLOT_DIV_BEFORE]);
@@ -732,9 +740,10 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
         }
         CU(cudaMemsetAsync(s->p_alt[0], 0, s->ncell * sizeof(float), st), "clear correction");
         TRY(v_cycle_mixed(s, c, mg, 0, mg.precision, st));
-        TRY(launch_ir_accumulate(s, st));
+        pending = true;
         ++done;
     }
+    if (pending) TRY(launch_ir_accumulate(s, st));
     TRY(launch_p0_from_p64(s, st));
     if (stats) {
         s->st.div_before = db;

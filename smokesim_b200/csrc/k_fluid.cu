@@ -652,8 +652,51 @@ __global__ void k_reduce_final(const double* __restrict__ partial, int n, double
     if (threadIdx.x == 0) out[slot] = sh[0];
 }
 
+// Sum (or maximum) of each group of 1024 consecutive partials, in a fixed
+// order: the single block that finishes a reduction then reads one value per
+// group instead of walking every partial in a long dependent chain.
+template <bool MAX>
+__global__ void __launch_bounds__(256) k_reduce_stage(const double* __restrict__ in, int n, double* __restrict__ out) {
+    __shared__ double sh[256];
+    const int base = blockIdx.x * 1024;
+    double a = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int i = base + threadIdx.x + 256 * j;
+        if (i < n) a = MAX ? fmax(a, in[i]) : a + in[i];
+    }
+    sh[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) sh[threadIdx.x] = MAX ? fmax(sh[threadIdx.x], sh[threadIdx.x + o]) : sh[threadIdx.x] + sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+
+int reduce_stage1(ss_sim* s, const double* in, int n, bool is_max, const double** res, int* nres, cudaStream_t st) {
+    if (n <= 1024) {
+        *res = in;
+        *nres = n;
+        return SS_OK;
+    }
+    const int nb = (n + 1023) / 1024;
+    if (nb > s->red.stage2) return set_error(SS_E_INVALID, "reduction scratch too small");
+    double* out = s->red.partial2 + (is_max ? s->red.stage2 : 0);
+    if (is_max) k_reduce_stage<true><<<nb, 256, 0, st>>>(in, n, out);
+    else k_reduce_stage<false><<<nb, 256, 0, st>>>(in, n, out);
+    s->nlaunch += 1;
+    *res = out;
+    *nres = nb;
+    return check_cuda(cudaGetLastError(), "k_reduce_stage");
+}
+
 int launch_reduce_final(ss_sim* s, int nblocks, int slot, cudaStream_t st) {
-    k_reduce_final<<<1, 1024, 0, st>>>(s->red.partial, nblocks, s->red.out, slot);
+    const double* in;
+    int n;
+    int rc = reduce_stage1(s, s->red.partial, nblocks, false, &in, &n, st);
+    if (rc) return rc;
+    k_reduce_final<<<1, 1024, 0, st>>>(in, n, s->red.out, slot);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_reduce_final");
 }

@@ -10,6 +10,8 @@
 // two scale of the coarse storage) are FP64 reductions.  Extension of the
 // reference, whose multigrid_pressure_solve (common/physics/grid.c:173-209)
 // runs FP32 V-cycles on the pressure itself.
+#include <utility>
+
 #include "common.cuh"
 #include "ss_internal.h"
 
@@ -60,42 +62,60 @@ __global__ void k_f32_from_p64(const double* __restrict__ p64, float* __restrict
 // FP64 residual of the projection at every fluid cell; writes the FP32
 // right-hand sides of the correction equation colour-split (smoother form
 // rho/k, residual form rho/(k h^2)) and per-block sum of squares / max |rho|.
-template <int DIM>
-__global__ void __launch_bounds__(256) k_ir_residual(const double* __restrict__ p64, const float* __restrict__ div0,
+// With ACC the pending correction e (colour-split FP32) is first added to the
+// fluid cells' pressure: p_out = p_in + e, and the residual is that of p_out
+// (p_in and p_out are different buffers - neighbours read p_in + e).  Each
+// thread takes kIrPlanes z planes, so a block reduces 256 * kIrPlanes cells.
+constexpr int kIrPlanes = 4;
+
+template <int DIM, bool ACC>
+__global__ void __launch_bounds__(256) k_ir_residual(const double* __restrict__ p_in, const float* __restrict__ e,
+                                                     double* __restrict__ p_out, const float* __restrict__ div0,
                                                      const uint8_t* __restrict__ fmask, int nx, int ny, int nz,
                                                      double k, double inv_k, double inv_khh,
                                                      float* __restrict__ rhs_s, float* __restrict__ rhs_r,
                                                      double* __restrict__ psum, double* __restrict__ pmax) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z * blockDim.z + threadIdx.z;
     double acc = 0.0, amax = 0.0;
-    if (x < nx && y < ny && z < nz) {
+    const int pl = nx * ny;
+    // pressure of cell c after the pending correction (fluid cells only)
+    auto P = [&](int c, int xx, int yy, int zz) -> double {
+        double v = p_in[c];
+        if (ACC) v = v + (double)e[rb_pos(xx, yy, zz, nx, ny, nz)];
+        return v;
+    };
+    for (int j = 0; j < kIrPlanes; ++j) {
+        const int z = blockIdx.z * kIrPlanes + j;
+        if (x >= nx || y >= ny || z >= nz) break;
         const int c = idx3(x, y, z, nx, ny);
         const uint8_t m = fmask[c];
         const int q = rb_pos(x, y, z, nx, ny, nz);
         float s_out = 0.f, r_out = 0.f;
         if (m & M_FLUID) {
-            const double t = (m & M_TOP) && y + 1 < ny ? p64[c + nx] : 0.0;
-            const double b = (m & M_BOTTOM) && y > 0 ? p64[c - nx] : 0.0;
-            const double r = (m & M_RIGHT) && x + 1 < nx ? p64[c + 1] : 0.0;
-            const double l = (m & M_LEFT) && x > 0 ? p64[c - 1] : 0.0;
+            const double t = (m & M_TOP) && y + 1 < ny ? P(c + nx, x, y + 1, z) : 0.0;
+            const double b = (m & M_BOTTOM) && y > 0 ? P(c - nx, x, y - 1, z) : 0.0;
+            const double r = (m & M_RIGHT) && x + 1 < nx ? P(c + 1, x + 1, y, z) : 0.0;
+            const double l = (m & M_LEFT) && x > 0 ? P(c - 1, x - 1, y, z) : 0.0;
             double sum = t + b;
             sum = sum + r;
             sum = sum + l;
             if constexpr (DIM == 3) {
-                const int pl = nx * ny;
-                const double f = (m & M_FRONT) && z + 1 < nz ? p64[c + pl] : 0.0;
-                const double k2 = (m & M_BACK) && z > 0 ? p64[c - pl] : 0.0;
+                const double f = (m & M_FRONT) && z + 1 < nz ? P(c + pl, x, y, z + 1) : 0.0;
+                const double k2 = (m & M_BACK) && z > 0 ? P(c - pl, x, y, z - 1) : 0.0;
                 sum = sum + f;
                 sum = sum + k2;
             }
+            const double pc = P(c, x, y, z);
+            if (ACC) p_out[c] = pc;
             const double cnt = (double)__popc(m & 0x7Eu);
-            const double rho = (double)div0[c] - k * (sum - cnt * p64[c]);
-            acc = rho * rho;
-            amax = fabs(rho);
+            const double rho = (double)div0[c] - k * (sum - cnt * pc);
+            acc += rho * rho;
+            amax = fmax(amax, fabs(rho));
             s_out = (float)(rho * inv_k);
             r_out = (float)(rho * inv_khh);
+        } else if (ACC) {
+            p_out[c] = p_in[c];
         }
         rhs_s[q] = s_out;
         rhs_r[q] = r_out;
@@ -155,28 +175,37 @@ int launch_p0_from_p64(ss_sim* s, cudaStream_t st) {
     return check_cuda(cudaGetLastError(), "k_f32_from_p64");
 }
 
-int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, cudaStream_t st) {
+int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate, cudaStream_t st) {
     dim3 b(32, 8, 1);
-    dim3 g = grid3(s->nx, s->ny, s->nz, b);
+    dim3 g((s->nx + 31) / 32, (s->ny + 7) / 8, (s->nz + kIrPlanes - 1) / kIrPlanes);
     const int nblocks = (int)(g.x * g.y * g.z);
     if (nblocks > s->red.max_blocks) return set_error(SS_E_INVALID, "reduction scratch too small");
     const double k = (double)c.dt / ((double)c.rho * (double)s->h);
     const double inv_k = 1.0 / k;
     const double inv_khh = 1.0 / (k * (double)s->lv[0].hh);
-    if (s->dim == 3)
-        k_ir_residual<3><<<g, b, 0, st>>>(s->p64, s->div0, s->fmask, s->nx, s->ny, s->nz, k, inv_k, inv_khh,
-                                           s->rhs_s, s->rhs_r, s->red.partial, s->red.partial_max);
-    else
-        k_ir_residual<2><<<g, b, 0, st>>>(s->p64, s->div0, s->fmask, s->nx, s->ny, s->nz, k, inv_k, inv_khh,
-                                           s->rhs_s, s->rhs_r, s->red.partial, s->red.partial_max);
+#define IR_ARGS(ACC) s->p64, s->p_alt[0], s->p64b, s->div0, s->fmask, s->nx, s->ny, s->nz, k, inv_k, inv_khh, \
+                     s->rhs_s, s->rhs_r, s->red.partial, s->red.partial_max
+    if (s->dim == 3) {
+        if (accumulate) k_ir_residual<3, true><<<g, b, 0, st>>>(IR_ARGS(true));
+        else k_ir_residual<3, false><<<g, b, 0, st>>>(IR_ARGS(false));
+    } else {
+        if (accumulate) k_ir_residual<2, true><<<g, b, 0, st>>>(IR_ARGS(true));
+        else k_ir_residual<2, false><<<g, b, 0, st>>>(IR_ARGS(false));
+    }
+#undef IR_ARGS
     s->nlaunch += 1;
     int rc = check_cuda(cudaGetLastError(), "k_ir_residual");
     if (rc) return rc;
+    if (accumulate) std::swap(s->p64, s->p64b);
     if (slot >= 0) {
         rc = launch_reduce_final(s, nblocks, slot, st);
         if (rc) return rc;
     }
-    k_reduce_max_final<<<1, 1024, 0, st>>>(s->red.partial_max, nblocks, s->red.out, SLOT_AMAX, inv_khh, s->d_scale);
+    const double* in;
+    int n;
+    rc = reduce_stage1(s, s->red.partial_max, nblocks, true, &in, &n, st);
+    if (rc) return rc;
+    k_reduce_max_final<<<1, 1024, 0, st>>>(in, n, s->red.out, SLOT_AMAX, inv_khh, s->d_scale);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_reduce_max_final");
 }

@@ -32,6 +32,8 @@ struct StepConsts {
 struct ReduceSlots {
     double* partial;      // per-block partial sums (device scratch)
     double* partial_max = nullptr;  // per-block maxima (mixed-precision solve)
+    double* partial2 = nullptr;     // second-stage partials: sums, then maxima (2 * stage2 entries)
+    int stage2 = 0;
     double* out;          // reduction results (device), SLOT_* below
     double* host;         // pinned mirror of out
     int max_blocks;
@@ -82,6 +84,7 @@ struct ss_sim {
     float* rb_pw = nullptr;             // level-0 prolongation weights per axis (x, then y, then z)
     // mixed-precision solve: FP64 level-0 pressure, FP16/BF16 coarse levels
     double* p64 = nullptr;
+    double* p64b = nullptr;             // ping-pong partner of p64 (update + residual in one pass)
     int p64_valid = 0;                  // p64 holds the current pressure (else p[0] does)
     int cstore = 0;                     // storage type of cp/cr (SS_PREC_MIXED or SS_PREC_MIXED_BF16)
     void* cp[SS_MAX_LEVELS] = {};       // coarse pressure, 2 bytes per cell (L >= 1)
@@ -166,9 +169,13 @@ int launch_rb_residual_restrict_mixed(ss_sim* s, int prec, cudaStream_t st);
 int launch_rb_prolong_mixed(ss_sim* s, int prec, cudaStream_t st);
 int launch_p64_from_p0(ss_sim* s, cudaStream_t st);
 int launch_p0_from_p64(ss_sim* s, cudaStream_t st);
-int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, cudaStream_t st);
+int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate, cudaStream_t st);
 int launch_ir_accumulate(ss_sim* s, cudaStream_t st);
 int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st);
+// first stage of a deterministic reduction over n per-block partials: sums
+// (or maxima) of consecutive groups of 1024; *res / *nres describe what is
+// left for a single final block (the input itself when n <= 1024)
+int reduce_stage1(ss_sim* s, const double* in, int n, bool is_max, const double** res, int* nres, cudaStream_t st);
 
 // Forward state copies a step can leave for its adjoint (api.cpp, run_step):
 // any pointer may be null.
