@@ -88,6 +88,8 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->rb_pw);
     cudaFree(s->p64);
     cudaFree(s->p64b);
+    for (auto& g : s->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     cudaFree(s->d_scale);
     cudaFree(s->red.partial_max);
     for (int l = 0; l < SS_MAX_LEVELS; ++l) { cudaFree(s->cp[l]); cudaFree(s->cr[l]); }
@@ -234,7 +236,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     A((void**)&s->div0, s->ncell * sizeof(float));
     if (s->enclosed) s->div0r = s->div0;
     else A((void**)&s->div0r, s->ncell * sizeof(float));
-    A((void**)&s->vort, s->ncell * (s->dim == 3 ? 3 : 1) * sizeof(float));
+    A((void**)&s->vort, s->ncell * (s->dim == 3 ? 4 : 1) * sizeof(float));   // 3D: w and |w|
     A((void**)&s->fmask, s->ncell);   // level-0 fluid mask (k_rb.cu, k_mixed.cu, k_adjoint.cu)
     if (s->nx % 2 == 0 && s->levels > 1) {   // colour-split level 0 (k_rb.cu)
         A((void**)&s->rhs_s, s->ncell * sizeof(float));
@@ -650,6 +652,73 @@ static int ensure_pyramid(ss_sim* s, cudaStream_t st) {
     return SS_OK;
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------- solve graphs
+// The multigrid part of a solve is the same sequence of launches every step
+// (same pointers, schedule and constants): it is recorded once as a CUDA
+// graph and replayed, which removes the per-launch CPU and GPU gaps of its
+// many small coarse-level kernels.  The key holds everything the recorded
+// launches bake in besides the simulation's own (stable) buffers.  Runs the
+// body directly on the legacy stream or when the caller is capturing.
+struct GraphKey {
+    int kind, parity, slot, rb, bottom;
+    ss_mg_schedule mg;
+    float dt, rho;
+};
+
+template <typename F>
+static int run_graph(ss_sim* s, int which, const GraphKey& key, cudaStream_t st, F body) {
+    if (!s->use_graphs || st == nullptr) return body();
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CU(cudaStreamIsCapturing(st, &cs), "cudaStreamIsCapturing");
+    if (cs != cudaStreamCaptureStatusNone) return body();
+    static_assert(sizeof(GraphKey) <= sizeof(s->graphs[0].key), "graph key size");
+    unsigned char kb[sizeof(s->graphs[0].key)] = {};
+    memcpy(kb, &key, sizeof(GraphKey));
+    ss_sim::SolveGraph& g = s->graphs[which];
+    if (g.exec && memcmp(g.key, kb, sizeof kb) == 0) {
+        CU(cudaGraphLaunch(g.exec, st), "cudaGraphLaunch");
+        s->nlaunch += g.launches;
+        return SS_OK;
+    }
+    if (g.exec) {
+        cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+    const long long before = s->nlaunch;
+    CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+    const int rc = body();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (rc != SS_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    CU(e, "cudaStreamEndCapture");
+    const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+        g.exec = nullptr;
+        return check_cuda(ei, "cudaGraphInstantiate");
+    }
+    memcpy(g.key, kb, sizeof kb);
+    g.launches = s->nlaunch - before;
+    CU(cudaGraphLaunch(g.exec, st), "cudaGraphLaunch");
+    return SS_OK;
+}
+
+static GraphKey graph_key(const ss_sim* s, int kind, int parity, int slot, int rb, const ss_params* p) {
+    GraphKey k;
+    memset(&k, 0, sizeof k);
+    k.kind = kind; k.parity = parity; k.slot = slot; k.rb = rb; k.bottom = s->bottom;
+    k.mg = p->mg;
+    k.dt = p->time_step; k.rho = p->density;
+    return k;
+}
+
+extern "C" {
+
 // ------------------------------------------------------- mixed precision
 // Buffers of the mixed-precision solve, made on its first use: the FP64
 // level-0 pressure and 2-byte coarse levels.
@@ -727,8 +796,20 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
     for (;;) {
         const bool last = !tol_mode && done == cap;
         if (last && !stats) break;
-        // adds the pending correction and evaluates the residual in one pass
-        TRY(launch_ir_residual(s, c, stats ? SLOT_RESIDUAL : -1, pending, st));
+        if (pending) {
+            // the last V-cycle + adding its correction and evaluating the
+            // residual in one pass, recorded as one graph per buffer parity
+            const int slot = stats ? SLOT_RESIDUAL : -1;
+            TRY(run_graph(s, 2 + s->p64_parity, graph_key(s, 2, s->p64_parity, slot, 1, p), st, [&]() -> int {
+                CU(cudaMemsetAsync(s->p_alt[0], 0, s->ncell * sizeof(float), st), "clear correction");
+                TRY(v_cycle_mixed(s, c, mg, 0, mg.precision, st));
+                return launch_ir_residual(s, c, slot, true, st);
+            }));
+            std::swap(s->p64, s->p64b);
+            s->p64_parity ^= 1;
+        } else {
+            TRY(launch_ir_residual(s, c, stats ? SLOT_RESIDUAL : -1, false, st));
+        }
         pending = false;
         if (tol_mode || last) {
             TRY(read_slots(s, st));
@@ -738,12 +819,16 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
             if (res <= mg.tol * db) break;
             if (done == cap) { conv = false; break; }
         }
-        CU(cudaMemsetAsync(s->p_alt[0], 0, s->ncell * sizeof(float), st), "clear correction");
-        TRY(v_cycle_mixed(s, c, mg, 0, mg.precision, st));
-        pending = true;
+        pending = true;   // the V-cycle runs at the top of the next pass
         ++done;
+        if (!tol_mode && done == cap && !stats) {
+            CU(cudaMemsetAsync(s->p_alt[0], 0, s->ncell * sizeof(float), st), "clear correction");
+            TRY(v_cycle_mixed(s, c, mg, 0, mg.precision, st));
+            TRY(launch_ir_accumulate(s, st));
+            pending = false;
+            break;
+        }
     }
-    if (pending) TRY(launch_ir_accumulate(s, st));
     TRY(launch_p0_from_p64(s, st));
     if (stats) {
         s->st.div_before = db;
@@ -777,15 +862,19 @@ static int pressure_solve(ss_sim* s, const ss_params* p, const StepConsts& c, cu
         return SS_OK;
     };
     if (!tol_mode) {
-        if (rb) TRY(launch_rb_convert(s, true, st));
-        s->rb_active = rb ? 1 : 0;
-        for (; done < cap; ++done) {
-            int rc = v_cycle_rec(s, c, mg, 0, st);
-            if (rc) { s->rb_active = 0; return rc; }
-        }
-        s->rb_active = 0;
-        if (rb) TRY(launch_rb_convert(s, false, st));
-        if (stats) TRY(launch_projected_residual_norm(s, c, SLOT_RESIDUAL, st));
+        TRY(run_graph(s, 0, graph_key(s, 0, 0, stats ? SLOT_RESIDUAL : -1, rb, p), st, [&]() -> int {
+            if (rb) TRY(launch_rb_convert(s, true, st));
+            s->rb_active = rb ? 1 : 0;
+            for (int i = 0; i < cap; ++i) {
+                int rc = v_cycle_rec(s, c, mg, 0, st);
+                if (rc) { s->rb_active = 0; return rc; }
+            }
+            s->rb_active = 0;
+            if (rb) TRY(launch_rb_convert(s, false, st));
+            if (stats) TRY(launch_projected_residual_norm(s, c, SLOT_RESIDUAL, st));
+            return SS_OK;
+        }));
+        done = cap;
         if (stats) {
             TRY(read_slots(s, st));
             s->st.div_before = sqrt(s->red.host[SLOT_DIV_BEFORE]);
@@ -797,9 +886,11 @@ static int pressure_solve(ss_sim* s, const ss_params* p, const StepConsts& c, cu
         const double db = sqrt(s->red.host[SLOT_DIV_BEFORE]);
         double res = sqrt(s->red.host[SLOT_RESIDUAL]);
         while (done < cap && !(res <= mg.tol * db)) {
-            TRY(cycle());
+            TRY(run_graph(s, 1, graph_key(s, 1, 0, SLOT_RESIDUAL, rb, p), st, [&]() -> int {
+                TRY(cycle());
+                return launch_projected_residual_norm(s, c, SLOT_RESIDUAL, st);
+            }));
             ++done;
-            TRY(launch_projected_residual_norm(s, c, SLOT_RESIDUAL, st));
             TRY(read_slots(s, st));
             res = sqrt(s->red.host[SLOT_RESIDUAL]);
         }

@@ -191,6 +191,45 @@ SS_D void vel_at_zface(const float* __restrict__ u, const float* __restrict__ v,
     out[2] = __ldg(w + idx3(i, j, k, nx, ny));
 }
 
+// The same three face velocities for a face whose every tap is inside the
+// arrays (1 <= i, j, k and i < nx, j < ny, k < nz): direct loads, no border
+// checks - the values (and lerp order) of vel_at_*face.
+template <int DIM>
+SS_D void vel_at_face_interior(const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+                               int nx, int ny, int nz, int comp, int i, int j, int k, float out[3]) {
+    const int ux = nx + 1, vy = ny + 1;
+    if (comp == 0) {
+        out[0] = __ldg(u + idx3(i, j, k, ux, ny));
+        const float* pv = v + idx3(i - 1, j, k, nx, vy);
+        out[1] = lerp_(lerp_(__ldg(pv), __ldg(pv + 1), 0.5f), lerp_(__ldg(pv + nx), __ldg(pv + nx + 1), 0.5f), 0.5f);
+        if constexpr (DIM == 3) {
+            const float* pw = w + idx3(i - 1, j, k, nx, ny);
+            const int pl = nx * ny;
+            out[2] = lerp_(lerp_(__ldg(pw), __ldg(pw + 1), 0.5f), lerp_(__ldg(pw + pl), __ldg(pw + pl + 1), 0.5f), 0.5f);
+        } else {
+            out[2] = 0.f;
+        }
+    } else if (comp == 1) {
+        const float* pu = u + idx3(i, j - 1, k, ux, ny);
+        out[0] = lerp_(lerp_(__ldg(pu), __ldg(pu + 1), 0.5f), lerp_(__ldg(pu + ux), __ldg(pu + ux + 1), 0.5f), 0.5f);
+        out[1] = __ldg(v + idx3(i, j, k, nx, vy));
+        if constexpr (DIM == 3) {
+            const float* pw = w + idx3(i, j - 1, k, nx, ny);
+            const int pl = nx * ny;
+            out[2] = lerp_(lerp_(__ldg(pw), __ldg(pw + nx), 0.5f), lerp_(__ldg(pw + pl), __ldg(pw + pl + nx), 0.5f), 0.5f);
+        } else {
+            out[2] = 0.f;
+        }
+    } else {
+        const int plu = ux * ny, plv = nx * vy;
+        const float* pu = u + idx3(i, j, k - 1, ux, ny);
+        out[0] = lerp_(lerp_(__ldg(pu), __ldg(pu + 1), 0.5f), lerp_(__ldg(pu + plu), __ldg(pu + plu + 1), 0.5f), 0.5f);
+        const float* pv = v + idx3(i, j, k - 1, nx, vy);
+        out[1] = lerp_(lerp_(__ldg(pv), __ldg(pv + nx), 0.5f), lerp_(__ldg(pv + plv), __ldg(pv + plv + nx), 0.5f), 0.5f);
+        out[2] = __ldg(w + idx3(i, j, k, nx, ny));
+    }
+}
+
 // Velocity at the cell centre (i+1/2, j+1/2, k+1/2): each component is the
 // mean of the cell's two faces on its axis.
 template <int DIM>

@@ -199,6 +199,8 @@ __global__ void __launch_bounds__(256) k_advect_velocity(FluidArgs a) {
     const float cfl = a.c.cfl;
     // solid flags of this cell and of its -x, -y, -z neighbours (out of grid = solid)
     const bool s_c = solid_oob1(a.flags, x, y, z, nx, ny, nz);
+    // every tap of the face velocities below lies inside the arrays
+    const bool interior = x >= 1 && y >= 1 && (DIM == 2 || z >= 1) && x < nx && y < ny && z < nz;
 #pragma unroll
     for (int comp = 0; comp < DIM; ++comp) {
         const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
@@ -214,7 +216,8 @@ __global__ void __launch_bounds__(256) k_advect_velocity(FluidArgs a) {
             out = 0.f;
         } else {
             float vel[3];
-            if (comp == 0) vel_at_xface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+            if (interior) vel_at_face_interior<DIM>(a.u, a.v, a.w, nx, ny, nz, comp, x, y, z, vel);
+            else if (comp == 0) vel_at_xface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
             else if (comp == 1) vel_at_yface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
             else vel_at_zface(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
             const float gx = (float)x + (comp == 0 ? 0.f : 0.5f);
@@ -311,7 +314,7 @@ __global__ void k_vorticity(FluidArgs a, float* __restrict__ vort) {
     const float two_h = 2.f * a.c.vort_k;
     if (a.flags[c] & F_SOLID) {
         vort[c] = 0.f;
-        if constexpr (DIM == 3) { vort[ncell + c] = 0.f; vort[2 * ncell + c] = 0.f; }
+        if constexpr (DIM == 3) { vort[ncell + c] = 0.f; vort[2 * ncell + c] = 0.f; vort[3 * ncell + c] = 0.f; }
         return;
     }
     const float* u = a.u;
@@ -331,9 +334,12 @@ __global__ void k_vorticity(FluidArgs a, float* __restrict__ vort) {
         const float y2 = CCZ(x + 1, y, z) - CCZ(x - 1, y, z);
         const float z1 = CCY(x + 1, y, z) - CCY(x - 1, y, z);
         const float z2 = CCX(x, y + 1, z) - CCX(x, y - 1, z);
-        vort[c] = (x1 - x2) / two_h;
-        vort[ncell + c] = (y1 - y2) / two_h;
-        vort[2 * ncell + c] = (z1 - z2) / two_h;
+        const float o0 = (x1 - x2) / two_h, o1 = (y1 - y2) / two_h, o2 = (z1 - z2) / two_h;
+        vort[c] = o0;
+        vort[ncell + c] = o1;
+        vort[2 * ncell + c] = o2;
+        // |w|, read six times by the neighbours' confinement force
+        vort[3 * ncell + c] = sqrtf(o0 * o0 + o1 * o1 + o2 * o2);
     }
 #undef CCX
 #undef CCY
@@ -347,9 +353,8 @@ SS_D float vmag(const float* __restrict__ vort, int x, int y, int z, int nx, int
     if constexpr (DIM == 2) {
         return fabsf(__ldg(vort + c));
     } else {
-        const size_t n = (size_t)nx * ny * nz;
-        const float o0 = __ldg(vort + c), o1 = __ldg(vort + n + c), o2 = __ldg(vort + 2 * n + c);
-        return sqrtf(o0 * o0 + o1 * o1 + o2 * o2);
+        // |w| stored by k_vorticity with the same expression
+        return __ldg(vort + 3 * (size_t)nx * ny * nz + c);
     }
 }
 
@@ -489,14 +494,15 @@ __global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a) {
     if (x >= nx || y >= ny || z >= nz) return;
     const int c = idx3(x, y, z, nx, ny);
     const size_t ncell = (size_t)nx * ny * nz;
+    // the cell's faces always exist: loaded before the solid test
+    float vel[3];
+    vel_at_centre<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
     if (a.flags[c] & F_SOLID) {
         for (int ch = 0; ch < a.nch; ++ch) a.dens_o[ch * ncell + c] = 0.f;
         a.temp_o[c] = a.c.t_amb;
         return;
     }
     const float gx = (float)x + 0.5f, gy = (float)y + 0.5f, gz = DIM == 3 ? (float)z + 0.5f : 0.f;
-    float vel[3];
-    vel_at_centre<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
     const float cfl = a.c.cfl;
     const float bx = gx - vel[0] * cfl, by = gy - vel[1] * cfl, bz = gz - vel[2] * cfl;
     const Taps t = make_taps<DIM>(nx, ny, nz, bx - 0.5f, by - 0.5f, bz - 0.5f);
@@ -567,19 +573,30 @@ __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restri
     double acc = 0.0;
     if (x < nx && y < ny && z < nz) {
         const int c = idx3(x, y, z, nx, ny);
+        // the cell's six faces always exist: load them before the flag test
+        // so the loads do not wait for it
+        const float f_top = __ldg(a.v + idx3(x, y + 1, z, nx, ny + 1));
+        const float f_bottom = __ldg(a.v + idx3(x, y, z, nx, ny + 1));
+        const float f_right = __ldg(a.u + idx3(x + 1, y, z, nx + 1, ny));
+        const float f_left = __ldg(a.u + idx3(x, y, z, nx + 1, ny));
+        float f_front = 0.f, f_back = 0.f;
+        if constexpr (DIM == 3) {
+            f_front = __ldg(a.w + idx3(x, y, z + 1, nx, ny));
+            f_back = __ldg(a.w + idx3(x, y, z, nx, ny));
+        }
         const uint8_t fl = a.flags[c];
         if (!(fl & F_SOLID)) {
             const bool sv = a.sv0 != nullptr;
-            const float v_top = (fl & F_TOP) ? (sv ? a.sv1[c + nx] : 0.f) : __ldg(a.v + idx3(x, y + 1, z, nx, ny + 1));
-            const float v_bottom = (fl & F_BOTTOM) ? (sv ? a.sv1[c - nx] : 0.f) : __ldg(a.v + idx3(x, y, z, nx, ny + 1));
-            const float v_right = (fl & F_RIGHT) ? (sv ? a.sv0[c + 1] : 0.f) : __ldg(a.u + idx3(x + 1, y, z, nx + 1, ny));
-            const float v_left = (fl & F_LEFT) ? (sv ? a.sv0[c - 1] : 0.f) : __ldg(a.u + idx3(x, y, z, nx + 1, ny));
+            const float v_top = (fl & F_TOP) ? (sv ? a.sv1[c + nx] : 0.f) : f_top;
+            const float v_bottom = (fl & F_BOTTOM) ? (sv ? a.sv1[c - nx] : 0.f) : f_bottom;
+            const float v_right = (fl & F_RIGHT) ? (sv ? a.sv0[c + 1] : 0.f) : f_right;
+            const float v_left = (fl & F_LEFT) ? (sv ? a.sv0[c - 1] : 0.f) : f_left;
             float d = v_right - v_left + v_top - v_bottom;
             float v_front = 0.f, v_back = 0.f;
             if constexpr (DIM == 3) {
                 const int pl = nx * ny;
-                v_front = (fl & F_FRONT) ? (sv ? a.sv2[c + pl] : 0.f) : __ldg(a.w + idx3(x, y, z + 1, nx, ny));
-                v_back = (fl & F_BACK) ? (sv ? a.sv2[c - pl] : 0.f) : __ldg(a.w + idx3(x, y, z, nx, ny));
+                v_front = (fl & F_FRONT) ? (sv ? a.sv2[c + pl] : 0.f) : f_front;
+                v_back = (fl & F_BACK) ? (sv ? a.sv2[c - pl] : 0.f) : f_back;
                 d = d + v_front - v_back;
             }
             if (div0) div0[c] = d;

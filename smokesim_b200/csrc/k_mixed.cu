@@ -196,7 +196,8 @@ int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate
     s->nlaunch += 1;
     int rc = check_cuda(cudaGetLastError(), "k_ir_residual");
     if (rc) return rc;
-    if (accumulate) std::swap(s->p64, s->p64b);
+    // with accumulate the caller swaps s->p64 / s->p64b afterwards (the launch
+    // may be recorded into a graph and replayed, the swap is host state)
     if (slot >= 0) {
         rc = launch_reduce_final(s, nblocks, slot, st);
         if (rc) return rc;

@@ -85,6 +85,7 @@ struct ss_sim {
     // mixed-precision solve: FP64 level-0 pressure, FP16/BF16 coarse levels
     double* p64 = nullptr;
     double* p64b = nullptr;             // ping-pong partner of p64 (update + residual in one pass)
+    int p64_parity = 0;                 // which of the two allocations p64 currently is
     int p64_valid = 0;                  // p64 holds the current pressure (else p[0] does)
     int cstore = 0;                     // storage type of cp/cr (SS_PREC_MIXED or SS_PREC_MIXED_BF16)
     void* cp[SS_MAX_LEVELS] = {};       // coarse pressure, 2 bytes per cell (L >= 1)
@@ -108,6 +109,16 @@ struct ss_sim {
     long long nlaunch = 0;     // kernels launched since the counter was reset
     int* d_err = nullptr;      // device error word: bit 0 = a bounded barrier wait gave up
     int use_tma = 1;           // TMA tile loads in the coarse-level sweeps where the layout allows
+    // The multigrid part of a solve recorded once as a CUDA graph and replayed
+    // (api.cpp, run_graph): slot 0 fixed-count FP32 V-cycles, 1 one FP32
+    // tolerance cycle, 2/3 one mixed refinement step per FP64 buffer parity.
+    struct SolveGraph {
+        cudaGraphExec_t exec = nullptr;
+        unsigned char key[96] = {};
+        long long launches = 0;
+    };
+    SolveGraph graphs[4];
+    int use_graphs = 1;
     int rb_active = 0;         // level-0 pressure currently lives colour-split in p_alt[0]
     std::vector<ss::TensorMapEntry> tmaps;
     cudaStream_t stream0 = nullptr;
