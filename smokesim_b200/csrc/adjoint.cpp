@@ -61,6 +61,10 @@ struct ss_adjoint {
     std::vector<void*> allocs;
     long long launches = 0, ckpt_bytes = 0, work_bytes = 0;
     bool forward_done = false;
+    // the transposed V-cycles of one step, recorded once as a CUDA graph
+    cudaGraphExec_t vgraph = nullptr;
+    unsigned char vkey[64] = {};
+    long long vlaunches = 0;
 };
 
 static int amalloc(ss_adjoint* A, void** p, size_t bytes, long long* counter) {
@@ -72,6 +76,7 @@ static int amalloc(ss_adjoint* A, void** p, size_t bytes, long long* counter) {
 }
 
 static void free_adjoint(ss_adjoint* A) {
+    if (A->vgraph) cudaGraphExecDestroy(A->vgraph);
     for (void* p : A->allocs) cudaFree(p);
     delete A;
 }
@@ -139,6 +144,57 @@ static int check_adjoint_params(const ss_adjoint* A, const ss_params* p) {
     return SS_OK;
 }
 
+// The transposed V-cycles of one step (adjoint of the right-hand side in
+// w.bbar[0], of the warm-start pressure in w.pbar[0]).  Every step runs the
+// same launches on the same buffers, so they are recorded once as a CUDA
+// graph and replayed (directly on the legacy stream or inside a caller's
+// capture).
+static int adj_solve(ss_adjoint* A, const ss_params* p, const StepConsts& c, int vcycles, cudaStream_t st) {
+    ss_sim* s = A->s;
+    auto body = [&]() -> int {
+        TRY_ADJ(check_cuda(cudaMemsetAsync(A->w.bbar[0], 0, s->ncell * 4, st), "memset"));
+        for (int i = 0; i < vcycles; ++i) TRY_ADJ(adj_v_cycle(s, c, p->mg, A->w, st));
+        return SS_OK;
+    };
+    if (st == nullptr) return body();
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    TRY_ADJ(check_cuda(cudaStreamIsCapturing(st, &cs), "cudaStreamIsCapturing"));
+    if (cs != cudaStreamCaptureStatusNone) return body();
+    struct Key { int vcycles; ss_mg_schedule mg; float dt, rho; } key;
+    std::memset(&key, 0, sizeof key);
+    key.vcycles = vcycles; key.mg = p->mg; key.dt = p->time_step; key.rho = p->density;
+    static_assert(sizeof(Key) <= sizeof(A->vkey), "graph key size");
+    unsigned char kb[sizeof(A->vkey)] = {};
+    std::memcpy(kb, &key, sizeof key);
+    if (A->vgraph && std::memcmp(kb, A->vkey, sizeof kb) == 0) {
+        s->nlaunch += A->vlaunches;
+        return check_cuda(cudaGraphLaunch(A->vgraph, st), "cudaGraphLaunch");
+    }
+    if (A->vgraph) {
+        cudaGraphExecDestroy(A->vgraph);
+        A->vgraph = nullptr;
+    }
+    const long long before = s->nlaunch;
+    TRY_ADJ(check_cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture"));
+    const int rc = body();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (rc != SS_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    TRY_ADJ(check_cuda(e, "cudaStreamEndCapture"));
+    const cudaError_t ei = cudaGraphInstantiate(&A->vgraph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+        A->vgraph = nullptr;
+        return check_cuda(ei, "cudaGraphInstantiate");
+    }
+    std::memcpy(A->vkey, kb, sizeof kb);
+    A->vlaunches = s->nlaunch - before;
+    return check_cuda(cudaGraphLaunch(A->vgraph, st), "cudaGraphLaunch");
+}
+
 // Forward step k keeping what its adjoint reads.
 static int record_step(ss_adjoint* A, const ss_params* p, int k, Record& R, cudaStream_t st) {
     ss_sim* s = A->s;
@@ -176,8 +232,7 @@ static int adj_step(ss_adjoint* A, const ss_params* p, int k, const Record& R, c
     }
     if (m & SS_STAGE_UPDATE_VELOCITIES) TRY_ADJ(adj_update(s, c, A->ub, A->w.pbar[0], st));
     if (m & SS_STAGE_RESOLVE_PRESSURE) {
-        TRY_ADJ(check_cuda(cudaMemsetAsync(A->w.bbar[0], 0, ncell * 4, st), "memset"));
-        for (int i = 0; i < R.vcycles; ++i) TRY_ADJ(adj_v_cycle(s, c, p->mg, A->w, st));
+        TRY_ADJ(adj_solve(A, p, c, R.vcycles, st));
         TRY_ADJ(adj_divergence(s, A->w.bbar[0], A->ub, st));
     }
     if (m & SS_STAGE_APPLY_VORTICITY) TRY_ADJ(adj_vorticity(s, c, R.vort, A->ub, A->wdir, A->dbar3, A->wbar, st));
@@ -197,7 +252,7 @@ static int adj_step(ss_adjoint* A, const ss_params* p, int k, const Record& R, c
         if (!R.em.empty())
             TRY_ADJ(check_cuda(cudaMemcpyAsync(s->d_em, R.em.data(), R.em.size() * sizeof(ss_emitter),
                                                cudaMemcpyHostToDevice, st), "emitter records"));
-        TRY_ADJ(adj_emitters(s, c, 1, A->ub, A->fpart, A->fgrad + 3 * (size_t)k, st));
+        TRY_ADJ(adj_emitters(s, c, 1, A->ub, A->fpart, A->fgrad + 3 * (size_t)k, R.em.data(), (int)R.em.size(), st));
     }
     return SS_OK;
 }

@@ -694,10 +694,13 @@ template <int DIM>
 __global__ void __launch_bounds__(256) k_adj_emitters(const ss_emitter* __restrict__ em, int ne, int nx, int ny, int nz,
                                                       float dt, int forced, float* __restrict__ ub,
                                                       float* __restrict__ vbar, float* __restrict__ wb,
-                                                      double* __restrict__ fpart) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+                                                      double* __restrict__ fpart, int3 lo, int3 ext) {
+    // launched over the active emitters' bounding box of faces
+    const int tx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ty = blockIdx.y * blockDim.y + threadIdx.y;
+    const int tz = blockIdx.z * blockDim.z + threadIdx.z;
+    const bool in_box = tx < ext.x && ty < ext.y && tz < ext.z;
+    const int x = in_box ? lo.x + tx : 1 << 30, y = lo.y + ty, z = lo.z + tz;
     double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int comp = 0; comp < DIM; ++comp) {
@@ -1209,12 +1212,34 @@ int adj_buoyancy(ss_sim* s, const StepConsts& c, float* vbar, float* dbar, float
 }
 
 int adj_emitters(ss_sim* s, const StepConsts& c, int forced, float* const vb[3], double* fpart, double* fout,
-                 cudaStream_t st) {
-    dim3 gf = grid_of(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, kB);
+                 const ss_emitter* em, int ne, cudaStream_t st) {
+    // bounding box (faces) of the active emitters, as the forward launch takes it
+    int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-1, -1, -1};
+    int active = 0;
+    for (int k = 0; k < ne; ++k) {
+        if (!(em[k].emit > 0)) continue;
+        ++active;
+        for (int d = 0; d < s->dim; ++d) {
+            const int a = (int)floorf(em[k].pos[d] - em[k].radius) - 1, b = (int)ceilf(em[k].pos[d] + em[k].radius) + 2;
+            lo[d] = lo[d] < a ? lo[d] : a;
+            hi[d] = hi[d] > b ? hi[d] : b;
+        }
+    }
+    if (s->dim == 2) { lo[2] = 0; hi[2] = 1; }
+    const int ext_all[3] = {s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1};
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = lo[d] < 0 ? 0 : lo[d];
+        hi[d] = hi[d] > ext_all[d] ? ext_all[d] : hi[d];
+        if (hi[d] < lo[d]) hi[d] = lo[d];
+    }
+    if (!active) { lo[0] = lo[1] = lo[2] = 0; hi[0] = hi[1] = hi[2] = 0; }
+    const int3 l = make_int3(lo[0], lo[1], lo[2]);
+    const int3 e = make_int3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]);
+    dim3 gf = grid_of(e.x > 0 ? e.x : 1, e.y > 0 ? e.y : 1, e.z > 0 ? e.z : 1, kB);
     const int nb = (int)(gf.x * gf.y * gf.z);
-    const int ne = (int)s->em.size();
-    if (s->dim == 3) k_adj_emitters<3><<<gf, kB, 0, st>>>(s->d_em, ne, s->nx, s->ny, s->nz, c.dt, forced, vb[0], vb[1], vb[2], fpart);
-    else k_adj_emitters<2><<<gf, kB, 0, st>>>(s->d_em, ne, s->nx, s->ny, s->nz, c.dt, forced, vb[0], vb[1], nullptr, fpart);
+    if (nb > adj_force_blocks(s)) return set_error(SS_E_INVALID, "force scratch too small");
+    if (s->dim == 3) k_adj_emitters<3><<<gf, kB, 0, st>>>(s->d_em, ne, s->nx, s->ny, s->nz, c.dt, forced, vb[0], vb[1], vb[2], fpart, l, e);
+    else k_adj_emitters<2><<<gf, kB, 0, st>>>(s->d_em, ne, s->nx, s->ny, s->nz, c.dt, forced, vb[0], vb[1], nullptr, fpart, l, e);
     k_sum3<<<1, 256, 0, st>>>(fpart, nb, fout);
     s->nlaunch += 2;
     return check_cuda(cudaGetLastError(), "adjoint of handle_emitters");

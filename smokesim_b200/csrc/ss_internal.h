@@ -225,7 +225,7 @@ int adj_advect_velocity(ss_sim* s, const StepConsts& c, bool buoy, const float* 
                         cudaStream_t st);
 int adj_buoyancy(ss_sim* s, const StepConsts& c, float* vbar, float* dbar, float* tbar, cudaStream_t st);
 int adj_emitters(ss_sim* s, const StepConsts& c, int forced, float* const vb[3], double* fpart, double* fout,
-                 cudaStream_t st);
+                 const ss_emitter* em, int ne, cudaStream_t st);
 int adj_force_blocks(const ss_sim* s);
 
 // ---- scene kernels (k_scene.cu) ----
