@@ -441,6 +441,22 @@ def main():
                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": launch_ms,
                     "traffic": RB_SMOOTH_TRAFFIC if args.n == 256 else None}
 
+    # headless ray-marched frame of the final 256^3 smoke (k_raymarch), 1024x1024
+    render = None
+    with torch.cuda.stream(stream):
+        d = sim.render_desc(1024, 1024)
+        img = torch.empty(1024 * 1024 * 4, dtype=torch.uint8, device=dev)
+        for _ in range(2):
+            sim.L.ss_render(sim.h, C.byref(d), C.c_void_p(img.data_ptr()), 1, C.c_void_p(stream.cuda_stream))
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r0.record(stream)
+        for _ in range(5):
+            sim.L.ss_render(sim.h, C.byref(d), C.c_void_p(img.data_ptr()), 1, C.c_void_p(stream.cuda_stream))
+        r1.record(stream)
+        torch.cuda.synchronize()
+        render = {"image": [1024, 1024], "ms_per_frame": r0.elapsed_time(r1) / 5,
+                  "step_size": d.step_size, "shadow_steps": d.shadow_steps}
+
     adjoint = None
     if not args.no_adjoint:
         adjoint = adjoint_bench(torch, stream)
@@ -453,6 +469,7 @@ def main():
         "config": workload_config(args, sc), "gpu_launches": int(head["gpu_launches"]), "clocks": clocks,
         "variants": variants,
         "adjoint": adjoint,
+        "render": render,
         "e2e": e2e, "roofline": roofline,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

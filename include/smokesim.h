@@ -292,6 +292,37 @@ int ss_adjoint_get_field(ss_adjoint* adj, int field, float* dst, size_t count, i
  * by checkpoints and recomputation buffers. */
 int ss_adjoint_info(ss_adjoint* adj, long long* kernel_launches, long long* checkpoint_bytes, long long* workspace_bytes);
 
+/* ---- headless renderer -------------------------------------------------- */
+/* Replaces the reference's GL fragment shaders with CUDA kernels writing an
+ * RGBA8 image: 3D ray_march_smoke.frag:114-175 (front-to-back compositing
+ * with alpha = 1 - exp(-density * k * step), a shadow march towards the light,
+ * a Henyey-Greenstein phase of g = 0.5 scaled by 3, a per-pixel hash
+ * jitter of the first sample), 2D draw_smoke.frag:43-58 (ambient / smoke
+ * colour mix).  The box spans [0, n_d / min(n)] per axis; there is no scene
+ * depth buffer headless, so every ray runs to the box exit.  Single-channel
+ * density renders as grey smoke (r = g = b = density). */
+typedef struct ss_render_desc {
+    int width, height;              /* image size; rows are written top row first */
+    float camera_pos[3];            /* box space (3D) */
+    float camera_target[3];
+    float camera_up[3];
+    float fov_y;                    /* vertical field of view, radians */
+    float light_direction[3];       /* towards the light (normalised by the renderer) */
+    float light_color[3];
+    float ambient_color[3];
+    float smoke_density_factor;
+    float shadow_density_factor;
+    float step_size;                /* box units */
+    float shadow_step_factor;
+    int shadow_steps;
+    float phase_g;
+} ss_render_desc;
+/* defaults of the reference's graphics_settings (common/graphics/graphics.c:9-25)
+ * and a camera outside the +z face looking at the box centre */
+int ss_render_default(const ss_sim* sim, int width, int height, ss_render_desc* out);
+/* rgba: width*height*4 bytes, device memory when on_device, else host */
+int ss_render(ss_sim* sim, const ss_render_desc* desc, uint8_t* rgba, int on_device, void* stream);
+
 /* Level data of the multigrid pyramid (pressure / residual), for tests. */
 enum ss_level_field { SS_LEVEL_PRESSURE = 0, SS_LEVEL_RESIDUAL = 1, SS_LEVEL_FLUID_WEIGHT = 2 };
 int ss_get_level(ss_sim* sim, int level, int what, float* host, size_t count, void* stream);

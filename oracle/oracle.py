@@ -56,6 +56,8 @@ def load(precision="f32"):
         L.og_set_field_f64.argtypes = [vp, i, C.POINTER(C.c_double), sz]
         L.og_set_emitter_force.argtypes = [vp, C.POINTER(C.c_float * 3)]
         L.og_set_emitter_force_f64.argtypes = [vp, C.POINTER(C.c_double * 3)]
+        L.og_render.argtypes = [vp, C.POINTER(abi.RenderDesc), C.c_void_p]
+        L.og_render.restype = None
         L.og_set_velocity_other.argtypes = [vp, i, C.POINTER(C.c_float), sz]
         L.og_get_level.argtypes = [vp, i, i, C.POINTER(C.c_float), sz]
         L.og_set_level.argtypes = [vp, i, i, C.POINTER(C.c_float), sz]
@@ -138,6 +140,11 @@ class OracleSim:
         rc = self.L.og_set_field_f64(self.h, field, a.ctypes.data_as(C.POINTER(C.c_double)), a.size)
         if rc:
             raise ValueError(f"oracle set_field_f64({field}) rc={rc}")
+
+    def render(self, desc):
+        out = np.empty((desc.height, desc.width, 4), np.uint8)
+        self.L.og_render(self.h, C.byref(desc), out.ctypes.data)
+        return out
 
     def set_emitter_force(self, force):
         f = (C.c_double * 3)(*[float(x) for x in force])

@@ -1177,6 +1177,149 @@ static void update_velocities_impl(og_sim* s, real dt, real rho, int use_p64) {
     s->vxi ^= 1; s->vyi ^= 1; if (s->dim == 3) s->vzi ^= 1;
 }
 
+/* -------------------------------------------------------------- renderer
+ * Restatement of the reference's smoke fragment shaders for the headless
+ * image the CUDA renderer writes: shaders3d/graphics/ray_march_smoke.frag:
+ * 80-175 (AABB entry/exit, per-pixel sine-hash jitter, front-to-back
+ * compositing, shadow march, Henyey-Greenstein phase with the shader's
+ * PI = 3.14 and factor 3) and shaders2d/graphics/draw_smoke.frag:43-58.
+ * Pinhole camera in box space [0, n/min(n)]; no scene depth buffer;
+ * single-channel density is grey (r = g = b). */
+static void rn_normalize(float v[3]) {
+    float l = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    for (int k = 0; k < 3; ++k) v[k] = v[k] / l;
+}
+static void rn_cross(const float a[3], const float b[3], float o[3]) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+static unsigned char rn_unorm8(float v) {
+    v = fminf(fmaxf(v, 0.f), 1.f);
+    return (unsigned char)(v * 255.f + 0.5f);
+}
+static void rn_rgb(const og_sim* s, const float box[3], float px, float py, float pz, float rgb[3]) {
+    const real* const* sm = (const real* const*)s->smoke[s->si];
+    float tx = (px / box[0]) * (float)NX - 0.5f;
+    float ty = (py / box[1]) * (float)NY - 0.5f;
+    float tz = (pz / box[2]) * (float)NZ - 0.5f;
+    rgb[0] = (float)sample_border(sm[0], 3, NX, NY, NZ, tx, ty, tz, 0);
+    if (s->nch == 3) {
+        rgb[1] = (float)sample_border(sm[1], 3, NX, NY, NZ, tx, ty, tz, 0);
+        rgb[2] = (float)sample_border(sm[2], 3, NX, NY, NZ, tx, ty, tz, 0);
+    } else {
+        rgb[1] = rgb[0];
+        rgb[2] = rgb[0];
+    }
+}
+
+void og_render(const og_sim* s, const ss_render_desc* d, unsigned char* rgba) {
+    const int W = d->width, H = d->height;
+    int mn = NX < NY ? NX : NY;
+    if (s->dim == 3 && NZ < mn) mn = NZ;
+    const float m = (float)mn;
+    const float box[3] = {(float)NX / m, (float)NY / m, s->dim == 3 ? (float)NZ / m : 1.f};
+    float fwd[3], right[3], up[3], light[3];
+    for (int k = 0; k < 3; ++k) { fwd[k] = d->camera_target[k] - d->camera_pos[k]; light[k] = d->light_direction[k]; }
+    rn_normalize(fwd);
+    rn_cross(fwd, d->camera_up, right);
+    rn_normalize(right);
+    rn_cross(right, fwd, up);
+    rn_normalize(light);
+    const float tan_half = tanf(0.5f * d->fov_y), aspect = (float)W / (float)H;
+    const float step = d->step_size, shadow_step = d->step_size * d->shadow_step_factor;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int row = 0; row < H; ++row)
+        for (int px = 0; px < W; ++px) {
+            unsigned char* out = rgba + 4 * ((size_t)row * W + px);
+            const int py = H - 1 - row;
+            const float u = ((float)px + 0.5f) / (float)W, v = ((float)py + 0.5f) / (float)H;
+            if (s->dim == 2) {
+                const real* const* sm = (const real* const*)s->smoke[s->si];
+                float tx = u * (float)NX - 0.5f, ty = v * (float)NY - 0.5f;
+                float rgb[3];
+                rgb[0] = (float)sample_border(sm[0], 2, NX, NY, 1, tx, ty, 0, 0);
+                if (s->nch == 3) {
+                    rgb[1] = (float)sample_border(sm[1], 2, NX, NY, 1, tx, ty, 0, 0);
+                    rgb[2] = (float)sample_border(sm[2], 2, NX, NY, 1, tx, ty, 0, 0);
+                } else {
+                    rgb[1] = rgb[0];
+                    rgb[2] = rgb[0];
+                }
+                const float raw = fmaxf(rgb[0], fmaxf(rgb[1], rgb[2]));
+                const float alpha = 1.f - expf(-raw * d->smoke_density_factor);
+                for (int k = 0; k < 3; ++k) {
+                    const float sc = raw > 0.001f ? rgb[k] / raw : 0.f;
+                    out[k] = rn_unorm8(d->ambient_color[k] * (1.f - alpha) + sc * alpha);
+                }
+                out[3] = 255;
+                continue;
+            }
+            const float ndx = 2.f * u - 1.f, ndy = 2.f * v - 1.f;
+            const float sx = ndx * tan_half * aspect, sy = ndy * tan_half;
+            float dv[3], dir[3];
+            for (int k = 0; k < 3; ++k) dv[k] = fwd[k] + right[k] * sx + up[k] * sy;
+            const float dl = sqrtf(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+            for (int k = 0; k < 3; ++k) dir[k] = dv[k] / dl;
+            float enter = -INFINITY, exit_ = INFINITY;
+            for (int k = 0; k < 3; ++k) {
+                const float inv = 1.f / dir[k];
+                const float t0 = (0.f - d->camera_pos[k]) * inv, t1 = (box[k] - d->camera_pos[k]) * inv;
+                enter = fmaxf(enter, fminf(t0, t1));
+                exit_ = fminf(exit_, fmaxf(t0, t1));
+            }
+            if (exit_ < fmaxf(enter, 0.f)) {
+                out[0] = out[1] = out[2] = out[3] = 0;
+                continue;
+            }
+            const int steps = (int)((exit_ - enter) / step) + 1;
+            const float sn = sinf(u * 12.9898f + v * 78.233f) * 43758.5453f;
+            const float noise = sn - floorf(sn);
+            float t = enter + noise * step;
+            const float cos_t = (-dir[0]) * light[0] + (-dir[1]) * light[1] + (-dir[2]) * light[2];
+            const float g = d->phase_g;
+            float phase;
+            if (g == 0.f) {
+                phase = 1.f / 3.14f;
+            } else {
+                const float den = 1.f + g * g - 2.f * g * cos_t;
+                phase = 1.f / (4.f * 3.14f) * (1.f - g * g) / (den * sqrtf(den));
+            }
+            phase = phase * 3.f;
+            float T = 1.f, col[3] = {0.f, 0.f, 0.f};
+            for (int i = 0; i < steps; ++i) {
+                if (t > exit_) break;
+                const float pos[3] = {d->camera_pos[0] + dir[0] * t, d->camera_pos[1] + dir[1] * t, d->camera_pos[2] + dir[2] * t};
+                float rgb[3];
+                rn_rgb(s, box, pos[0], pos[1], pos[2], rgb);
+                const float total = rgb[0] + rgb[1] + rgb[2];
+                if (total > 0.001f) {
+                    float ld = 0.f, lp[3] = {pos[0], pos[1], pos[2]};
+                    for (int j = 0; j < d->shadow_steps; ++j) {
+                        for (int k = 0; k < 3; ++k) lp[k] = lp[k] + light[k] * shadow_step;
+                        float sh[3];
+                        rn_rgb(s, box, lp[0], lp[1], lp[2], sh);
+                        ld = ld + (sh[0] + sh[1] + sh[2]);
+                    }
+                    const float atten = expf(-ld * d->shadow_density_factor * shadow_step);
+                    const float alpha = 1.f - expf(-total * d->smoke_density_factor * step);
+                    const float ta = T * alpha;
+                    for (int k = 0; k < 3; ++k) {
+                        const float lc = d->ambient_color[k] + (d->light_color[k] * atten) * phase;
+                        col[k] = col[k] + ta * ((rgb[k] / total) * lc);
+                    }
+                    T = T * (1.f - alpha);
+                    if (T < 0.001f) break;
+                }
+                t = t + step;
+            }
+            out[0] = rn_unorm8(col[0]);
+            out[1] = rn_unorm8(col[1]);
+            out[2] = rn_unorm8(col[2]);
+            out[3] = rn_unorm8(1.f - T);
+        }
+}
+
 /* ------------------------------------------------------------- the step */
 /* run_physics_step (common/physics/physics.c:72-101). */
 void og_run_physics_step(og_sim* s, const ss_params* prm) {

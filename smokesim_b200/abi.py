@@ -144,6 +144,26 @@ class Stats(C.Structure):
     ]
 
 
+class RenderDesc(C.Structure):
+    _fields_ = [
+        ("width", C.c_int),
+        ("height", C.c_int),
+        ("camera_pos", C.c_float * 3),
+        ("camera_target", C.c_float * 3),
+        ("camera_up", C.c_float * 3),
+        ("fov_y", C.c_float),
+        ("light_direction", C.c_float * 3),
+        ("light_color", C.c_float * 3),
+        ("ambient_color", C.c_float * 3),
+        ("smoke_density_factor", C.c_float),
+        ("shadow_density_factor", C.c_float),
+        ("step_size", C.c_float),
+        ("shadow_step_factor", C.c_float),
+        ("shadow_steps", C.c_int),
+        ("phase_g", C.c_float),
+    ]
+
+
 def make_desc(dim, n, cell_size=1.0, density_channels=1, enclosed=1, min_coarse=4, t_ambient=0.0):
     d = Desc()
     d.dim = dim
@@ -274,7 +294,7 @@ EXPORTED = [
     "ss_get_level", "ss_set_level", "ss_divergence_norm_noalloc",
     "ss_set_emitter_force", "ss_adjoint_create", "ss_adjoint_destroy", "ss_adjoint_forward",
     "ss_adjoint_backward", "ss_adjoint_field_device_ptr", "ss_adjoint_get_field", "ss_adjoint_info",
-    "ss_set_field_device", "ss_get_field_device",
+    "ss_set_field_device", "ss_get_field_device", "ss_render_default", "ss_render",
 ]
 
 
@@ -322,4 +342,6 @@ def _declare(L):
     L.ss_adjoint_info.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     L.ss_adjoint_get_field.argtypes = [vp, i, vp, sz, i, vp]
     L.ss_set_field_device.argtypes = [vp, i, vp, sz, vp]
+    L.ss_render_default.argtypes = [vp, i, i, C.POINTER(RenderDesc)]
+    L.ss_render.argtypes = [vp, C.POINTER(RenderDesc), vp, i, vp]
     L.ss_get_field_device.argtypes = [vp, i, vp, sz, vp]

@@ -88,6 +88,7 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->rb_pw);
     cudaFree(s->p64);
     cudaFree(s->p64b);
+    cudaFree(s->render_buf);
     for (auto& g : s->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     cudaFree(s->d_scale);

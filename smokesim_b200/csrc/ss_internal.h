@@ -92,6 +92,8 @@ struct ss_sim {
     void* cr[SS_MAX_LEVELS] = {};       // coarse right-hand side / residual
     float* d_scale = nullptr;           // [scale, 1/scale] of the coarse storage (device)
     float force[3] = {0.f, 0.f, 0.f};   // control force on the faces inside active emitters
+    void* render_buf = nullptr;         // device image of ss_render with a host destination
+    size_t render_bytes = 0;
     int rb_vec = 0;                     // level-0 kernels may work on 4 cells per thread (nx % 8 == 0)
     int rb_prolong_vec = 0;             // ... and the prolongation too (even sizes, table pattern checked)
     ss::ReduceSlots red{};

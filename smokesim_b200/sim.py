@@ -112,6 +112,19 @@ class Sim:
         a = np.ascontiguousarray(arr, dtype=np.float32).reshape(-1)
         _check(self.L.ss_set_level(self.h, level, what, _fptr(a), a.size, self.stream), "ss_set_level")
 
+    def render_desc(self, width=256, height=256):
+        """The reference's default render settings for this grid (ss_render_default)."""
+        d = abi.RenderDesc()
+        _check(self.L.ss_render_default(self.h, width, height, C.byref(d)), "ss_render_default")
+        return d
+
+    def render(self, desc=None, width=256, height=256):
+        """Headless image of the current smoke, (height, width, 4) uint8, top row first."""
+        d = desc if desc is not None else self.render_desc(width, height)
+        out = np.empty((d.height, d.width, 4), np.uint8)
+        _check(self.L.ss_render(self.h, C.byref(d), out.ctypes.data, 0, self.stream), "ss_render")
+        return out
+
     def set_emitter_force(self, force):
         f = (C.c_float * 3)(*[float(x) for x in force])
         _check(self.L.ss_set_emitter_force(self.h, C.byref(f)), "ss_set_emitter_force")
@@ -178,3 +191,16 @@ class Sim:
 
     def update_solid_map(self):
         _check(self.L.ss_update_solid_map(self.h, self.stream), "ss_update_solid_map")
+
+
+def write_ppm(path, rgba, background=(0, 0, 0)):
+    """Binary PPM (P6) of an RGBA8 image, composited over `background`
+    (premultiplied colour + (1 - alpha) * background)."""
+    img = np.asarray(rgba, dtype=np.float32)
+    a = img[..., 3:4] / 255.0
+    rgb = img[..., :3] + (1.0 - a) * np.asarray(background, np.float32)
+    rgb = np.clip(rgb + 0.5, 0, 255).astype(np.uint8)
+    h, w = rgb.shape[:2]
+    with open(path, "wb") as f:
+        f.write(b"P6\n%d %d\n255\n" % (w, h))
+        f.write(rgb.tobytes())

@@ -43,7 +43,8 @@ def test_struct_layouts_match_header(tmp_path):
     """Compile the header with the system C compiler and compare sizeof/offsetof
     of every ABI struct with the ctypes mirror."""
     structs = {"ss_desc": abi.Desc, "ss_emitter": abi.Emitter, "ss_obstacle": abi.Obstacle, "ss_box": abi.Box,
-               "ss_mg_schedule": abi.MGSchedule, "ss_params": abi.Params, "ss_stats": abi.Stats}
+               "ss_mg_schedule": abi.MGSchedule, "ss_params": abi.Params, "ss_stats": abi.Stats,
+               "ss_render_desc": abi.RenderDesc}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

@@ -240,3 +240,33 @@ def test_mixed_precision_refinement_reaches_tolerance(oracle_mod):
     fluid = ref.get_field(abi.FIELD_SOLID) == 0
     err = rel_l2(out[abi.PREC_MIXED][3][fluid] - out[abi.PREC_MIXED][3][fluid].mean(), p64[fluid] - p64[fluid].mean())
     assert err < 1e-4, err
+
+
+def test_render_known_answers(oracle_mod):
+    """The render restatement: an empty 3D grid leaves every pixel transparent
+    (the ray marches through zero density); an empty 2D grid shows the ambient
+    colour; a dense block in front of the camera is opaque in the middle."""
+    d = abi.RenderDesc()
+    d.width, d.height = 48, 32
+    o = oracle_mod.OracleSim(abi.make_desc(3, (16, 16, 16), enclosed=1))
+    d.camera_pos[:] = [0.5, 0.5, 2.3]
+    d.camera_target[:] = [0.5, 0.5, 0.5]
+    d.camera_up[:] = [0.0, 1.0, 0.0]
+    d.fov_y = 0.785398
+    d.light_direction[:] = [1.0, 1.0, 1.0]
+    d.light_color[:] = [1.5, 1.35, 1.2]
+    d.ambient_color[:] = [0.678, 0.847, 0.902]
+    d.smoke_density_factor, d.shadow_density_factor = 50.0, 50.0
+    d.step_size, d.shadow_step_factor, d.shadow_steps, d.phase_g = 0.01, 3.0, 6, 0.5
+    img = o.render(d)
+    assert img.shape == (32, 48, 4) and not img.any()
+    rho = np.zeros((16, 16, 16), np.float32)
+    rho[4:12, 4:12, 4:12] = 5.0
+    o.set_field(abi.FIELD_DENSITY, rho)
+    img = o.render(d)
+    assert img[16, 24, 3] == 255 and img[0, 0, 3] == 0
+    o2 = oracle_mod.OracleSim(abi.make_desc(2, (20, 20, 1), enclosed=1))
+    d.width, d.height = 10, 10
+    img2 = o2.render(d)
+    amb = np.round(np.array([0.678, 0.847, 0.902]) * 255).astype(np.uint8)
+    assert (img2[..., :3] == amb).all() and (img2[..., 3] == 255).all()
