@@ -323,6 +323,17 @@ int ss_render_default(const ss_sim* sim, int width, int height, ss_render_desc* 
 /* rgba: width*height*4 bytes, device memory when on_device, else host */
 int ss_render(ss_sim* sim, const ss_render_desc* desc, uint8_t* rgba, int on_device, void* stream);
 
+/* ---- snapshots ---------------------------------------------------------- */
+/* No counterpart in the reference (its state lives in GL textures).  One line
+ * of JSON (format "smokesim-state", grid, and for every section its name,
+ * dtype, shape, byte offset and length; padded to 64 bytes) followed by raw
+ * little-endian sections: vx, vy[, vz], density, temperature, pressure
+ * (FP32, x fastest) and the emitter / obstacle / box records.  Loading needs
+ * a simulation with the same grid description; it restores the scene, then
+ * the fields. */
+int ss_save_state(ss_sim* sim, const char* path, void* stream);
+int ss_load_state(ss_sim* sim, const char* path, void* stream);
+
 /* Level data of the multigrid pyramid (pressure / residual), for tests. */
 enum ss_level_field { SS_LEVEL_PRESSURE = 0, SS_LEVEL_RESIDUAL = 1, SS_LEVEL_FLUID_WEIGHT = 2 };
 int ss_get_level(ss_sim* sim, int level, int what, float* host, size_t count, void* stream);

@@ -295,6 +295,7 @@ EXPORTED = [
     "ss_set_emitter_force", "ss_adjoint_create", "ss_adjoint_destroy", "ss_adjoint_forward",
     "ss_adjoint_backward", "ss_adjoint_field_device_ptr", "ss_adjoint_get_field", "ss_adjoint_info",
     "ss_set_field_device", "ss_get_field_device", "ss_render_default", "ss_render",
+    "ss_save_state", "ss_load_state",
 ]
 
 
@@ -344,4 +345,6 @@ def _declare(L):
     L.ss_set_field_device.argtypes = [vp, i, vp, sz, vp]
     L.ss_render_default.argtypes = [vp, i, i, C.POINTER(RenderDesc)]
     L.ss_render.argtypes = [vp, C.POINTER(RenderDesc), vp, i, vp]
+    L.ss_save_state.argtypes = [vp, C.c_char_p, vp]
+    L.ss_load_state.argtypes = [vp, C.c_char_p, vp]
     L.ss_get_field_device.argtypes = [vp, i, vp, sz, vp]

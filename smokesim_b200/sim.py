@@ -125,6 +125,12 @@ class Sim:
         _check(self.L.ss_render(self.h, C.byref(d), out.ctypes.data, 0, self.stream), "ss_render")
         return out
 
+    def save_state(self, path):
+        _check(self.L.ss_save_state(self.h, str(path).encode(), self.stream), "ss_save_state")
+
+    def load_state(self, path):
+        _check(self.L.ss_load_state(self.h, str(path).encode(), self.stream), "ss_load_state")
+
     def set_emitter_force(self, force):
         f = (C.c_float * 3)(*[float(x) for x in force])
         _check(self.L.ss_set_emitter_force(self.h, C.byref(f)), "ss_set_emitter_force")
@@ -204,3 +210,18 @@ def write_ppm(path, rgba, background=(0, 0, 0)):
     with open(path, "wb") as f:
         f.write(b"P6\n%d %d\n255\n" % (w, h))
         f.write(rgb.tobytes())
+
+
+def read_state(path):
+    """A snapshot written by ss_save_state as (header dict, {section: array});
+    FP32 sections are numpy arrays in their stated shape, record sections
+    raw bytes."""
+    import json
+    with open(path, "rb") as f:
+        header = json.loads(f.readline().decode())
+        out = {}
+        for sec in header["sections"]:
+            f.seek(sec["offset"])
+            raw = f.read(sec["bytes"])
+            out[sec["name"]] = (np.frombuffer(raw, "<f4").reshape(sec["shape"]) if sec["dtype"] == "<f4" else raw)
+    return header, out
