@@ -105,7 +105,7 @@ int ss_save_state(ss_sim* s, const char* path, void* stream) {
         size_t off = data_start;
         for (size_t i = 0; i < secs.size(); ++i) {
             char num[64];
-            snprintf(num, sizeof num, "%020zu", off);
+            snprintf(num, sizeof num, "%20zu", off);   // fixed width (JSON allows the spaces)
             h += (i ? ", " : "") + std::string("{\"name\": \"") + secs[i].name + "\", \"dtype\": \"" + secs[i].dtype +
                  "\", \"shape\": " + json_shape(secs[i].shape) + ", \"offset\": " + num +
                  ", \"bytes\": " + std::to_string(secs[i].bytes) + "}";
