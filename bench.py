@@ -258,8 +258,9 @@ def run_variant(torch, sim_cls, scene, sc, name, args, stream, barrier, world, d
 
 
 ADJOINT_CASES = [
-    # name, scene, steps, checkpoint interval
+    # name, scene, steps, checkpoint interval (= steps: every intermediate kept, no recomputation)
     ("rollout64", dict(kind="rollout64", n=64), 64, 8),
+    ("rollout64_no_recompute", dict(kind="rollout64", n=64), 64, 64),
     ("plume128", dict(kind="plume3d", n=128), 200, 14),
 ]
 

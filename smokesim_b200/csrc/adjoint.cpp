@@ -5,10 +5,11 @@
 // checkpoint and recomputes the segment once, keeping for each step the
 // intermediate velocities, smoke and vorticity its stages read (run_step's
 // StepSaves); then, last step first, it applies the stages' adjoint kernels
-// (k_adjoint.cu) in reverse stage order.  Every step is thus run twice
-// (forward pass, segment recomputation) plus its adjoint; memory is
-// nsteps/every states plus `every` steps of intermediates instead of
-// nsteps steps of intermediates.
+// (k_adjoint.cu) in reverse stage order.  The forward pass keeps the last
+// segment's intermediates itself, so every step but those is run twice
+// (forward pass, segment recomputation) plus its adjoint - and with one
+// segment (checkpoint_every >= nsteps) nothing is recomputed.  Memory is
+// nsteps/every states plus `every` steps of intermediates.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -61,6 +62,7 @@ struct ss_adjoint {
     std::vector<void*> allocs;
     long long launches = 0, ckpt_bytes = 0, work_bytes = 0;
     bool forward_done = false;
+    bool last_recorded = false;   // rec holds the last segment, written by the forward pass
     // the transposed V-cycles of one step, recorded once as a CUDA graph
     cudaGraphExec_t vgraph = nullptr;
     unsigned char vkey[64] = {};
@@ -330,13 +332,21 @@ int ss_adjoint_forward(ss_adjoint* A, const ss_params* p, const float* forces, v
         std::fill(A->forces.begin(), A->forces.end(), 0.f);
     }
     s->nlaunch = 0;
+    A->last_recorded = false;
+    const int last0 = ((A->n - 1) / A->every) * A->every;   // first step of the last segment
     for (int k = 0; k < A->n; ++k) {
         if (k % A->every == 0) TRY_ADJ(save_state(s, A->ckpt[k / A->every], st));
-        set_force(A, k);
-        TRY_ADJ(run_step(s, p, st, nullptr));
+        // the last segment keeps its intermediates now: the reverse pass
+        // starts there without recomputing it
+        if (k >= last0) TRY_ADJ(record_step(A, p, k, A->rec[k - last0], st));
+        else {
+            set_force(A, k);
+            TRY_ADJ(run_step(s, p, st, nullptr));
+        }
     }
     for (int d = 0; d < 3; ++d) s->force[d] = 0.f;
     A->forward_done = true;
+    A->last_recorded = true;
     return check_cuda(cudaGetLastError(), "adjoint forward");
 }
 
@@ -361,8 +371,11 @@ int ss_adjoint_backward(ss_adjoint* A, const ss_params* p, const float* grad_den
     const int nseg = (A->n + A->every - 1) / A->every;
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int k0 = sg * A->every, k1 = std::min(A->n, k0 + A->every);
-        TRY_ADJ(restore_state(s, A->ckpt[sg], st));
-        for (int k = k0; k < k1; ++k) TRY_ADJ(record_step(A, p, k, A->rec[k - k0], st));
+        if (!(sg == nseg - 1 && A->last_recorded)) {
+            TRY_ADJ(restore_state(s, A->ckpt[sg], st));
+            for (int k = k0; k < k1; ++k) TRY_ADJ(record_step(A, p, k, A->rec[k - k0], st));
+        }
+        A->last_recorded = false;   // rec now holds this segment
         for (int k = k1 - 1; k >= k0; --k) TRY_ADJ(adj_step(A, p, k, A->rec[k - k0], st));
     }
     TRY_ADJ(restore_state(s, A->ckpt[0], st));

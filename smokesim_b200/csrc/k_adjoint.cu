@@ -913,32 +913,32 @@ SS_D void bottom_adj_half(const AdjLevel& a, int colour, bool do_b, bool do_a) {
 
 // A level of at most two cells per active thread (the coarsest one): the
 // cells' weights and neighbour masks stay in registers for all the sweeps.
-template <int DIM>
+template <int DIM, int CELLS>
 SS_D void bottom_adj_sweeps_cached(const AdjLevel& a, int iterations, int nt) {
     const int n = a.nx * a.ny * a.nz;
     const int nx = a.nx, ny = a.ny, pl = nx * ny;
-    int ci[2], col[2], inr[2];
-    bool act[2], upd[2];
-    float ws[2], dd[2];
+    // per cell: bits 0-5 neighbour in grid (+y,-y,+x,-x,+z,-z), 6 colour,
+    // 7 present, 8 updated by the forward smoother
+    int fl[CELLS];
+    float ws[CELLS], dd[CELLS];
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < CELLS; ++k) {
         const int c = threadIdx.x + k * nt;
-        act[k] = c < n;
-        ci[k] = c; col[k] = 0; inr[k] = 0; upd[k] = false; ws[k] = 0.f; dd[k] = 1.f;
-        if (!act[k]) continue;
+        fl[k] = 0; ws[k] = 0.f; dd[k] = 1.f;
+        if (c >= n) continue;
         const int x = c % nx, t = c / nx, y = t % ny, z = t / ny;
-        col[k] = (x + y + z) & 1;
-        inr[k] = (y + 1 < ny ? 1 : 0) | (y > 0 ? 2 : 0) | (x + 1 < nx ? 4 : 0) | (x > 0 ? 8 : 0) |
-                 (z + 1 < a.nz ? 16 : 0) | (z > 0 ? 32 : 0);
         bool fluid;
         cell_weights<DIM, false>(a, x, y, z, ws[k], dd[k], fluid);
-        upd[k] = fluid && dd[k] != 0.f;
+        fl[k] = (y + 1 < ny ? 1 : 0) | (y > 0 ? 2 : 0) | (x + 1 < nx ? 4 : 0) | (x > 0 ? 8 : 0) |
+                (z + 1 < a.nz ? 16 : 0) | (z > 0 ? 32 : 0) | (((x + y + z) & 1) << 6) | 128 |
+                ((fluid && dd[k] != 0.f) ? 256 : 0);
     }
     auto half = [&](int colour, bool do_b, bool do_a) {
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            if (!act[k] || col[k] != colour) continue;
-            const int c = ci[k], m = inr[k];
+        for (int k = 0; k < CELLS; ++k) {
+            const int m = fl[k];
+            if (!(m & 128) || ((m >> 6) & 1) != colour) continue;
+            const int c = threadIdx.x + k * nt;
             float pb = a.pbar[c];
             if (do_b) {
                 float sum = 0.f;
@@ -951,7 +951,7 @@ SS_D void bottom_adj_sweeps_cached(const AdjLevel& a, int iterations, int nt) {
                 pb += ws[k] * sum;
             }
             if (do_a) {
-                if (upd[k]) {
+                if (m & 256) {
                     const float tt = pb / dd[k];
                     a.T[c] = tt;
                     pb = 0.f;
@@ -965,13 +965,9 @@ SS_D void bottom_adj_sweeps_cached(const AdjLevel& a, int iterations, int nt) {
         if (nt == (int)blockDim.x) __syncthreads();
         else asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
     };
-    half(1, false, true);
-    int colour = 1;
-    for (int k = 1; k < 2 * iterations; ++k) {
-        colour ^= 1;
-        half(colour, true, true);
-    }
-    half(colour ^ 1, true, false);
+    // half-steps h = 0..2*iterations: colour 1, 0, 1, ..., the first without
+    // the gather, the last without the update (one call site keeps the code small)
+    for (int h = 0; h <= 2 * iterations; ++h) half((h & 1) ? 0 : 1, h > 0, h < 2 * iterations);
 }
 
 template <int DIM>
@@ -981,7 +977,12 @@ SS_D void bottom_adj_sweeps(const AdjLevel& a, int iterations) {
     int nt = blockDim.x;
     while (nt > 128 && (n + nt / 2 - 1) / (nt / 2) <= 2) nt /= 2;
     if ((n + nt - 1) / nt <= 2) {
-        if ((int)threadIdx.x < nt) bottom_adj_sweeps_cached<DIM>(a, iterations, nt);
+        if ((int)threadIdx.x < nt) bottom_adj_sweeps_cached<DIM, 2>(a, iterations, nt);
+        __syncthreads();
+        return;
+    }
+    if ((n + (int)blockDim.x - 1) / (int)blockDim.x <= 4) {
+        bottom_adj_sweeps_cached<DIM, 4>(a, iterations, blockDim.x);
         __syncthreads();
         return;
     }
