@@ -19,6 +19,7 @@ MIXED_GRIDS = [
     ("3d_quad_odd_y", 3, (24, 19, 18), 1, 1, 4),
     ("3d_tma", 3, (32, 24, 20), 1, 1, 4),
     ("3d_l1", 3, (64, 48, 48), 1, 1, 8),
+    ("3d_even_not_quad", 3, (20, 18, 14), 1, 0, 4),   # nx % 8 != 0: one cell per thread
 ]
 
 
