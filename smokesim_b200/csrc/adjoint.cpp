@@ -102,7 +102,7 @@ static int alloc_record(ss_adjoint* A, Record& R) {
     }
     TRY_ADJ(amalloc(A, (void**)&R.dens_e, s->ncell * s->nch * 4, &A->ckpt_bytes));
     TRY_ADJ(amalloc(A, (void**)&R.temp_e, s->ncell * 4, &A->ckpt_bytes));
-    TRY_ADJ(amalloc(A, (void**)&R.vort, s->ncell * (s->dim == 3 ? 3 : 1) * 4, &A->ckpt_bytes));
+    TRY_ADJ(amalloc(A, (void**)&R.vort, s->ncell * (s->dim == 3 ? 4 : 1) * 4, &A->ckpt_bytes));
     return SS_OK;
 }
 
@@ -212,8 +212,10 @@ static int record_step(ss_adjoint* A, const ss_params* p, int k, Record& R, cuda
     TRY_ADJ(run_step(s, p, st, &sv));
     R.vcycles = sv.vcycles;
     R.em = s->em;
-    if (p->stage_mask & SS_STAGE_APPLY_VORTICITY)
-        TRY_ADJ(copy_d2d(R.vort, s->vort, s->ncell * (s->dim == 3 ? 3 : 1) * 4, st));
+    if (p->stage_mask & SS_STAGE_APPLY_VORTICITY) {
+        const float* ua[3] = {R.ua[0], R.ua[1], R.ua[2]};
+        TRY_ADJ(launch_vorticity_field(s, make_consts(s, p), ua, R.vort, st));
+    }
     return SS_OK;
 }
 

@@ -237,7 +237,8 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     A((void**)&s->div0, s->ncell * sizeof(float));
     if (s->enclosed) s->div0r = s->div0;
     else A((void**)&s->div0r, s->ncell * sizeof(float));
-    A((void**)&s->vort, s->ncell * (s->dim == 3 ? 4 : 1) * sizeof(float));   // 3D: w and |w|
+    // 2D: w between its two kernels (3D computes w in shared memory)
+    if (s->dim == 2) A((void**)&s->vort, s->ncell * sizeof(float));
     A((void**)&s->fmask, s->ncell);   // level-0 fluid mask (k_rb.cu, k_mixed.cu, k_adjoint.cu)
     if (s->nx % 2 == 0 && s->levels > 1) {   // colour-split level 0 (k_rb.cu)
         A((void**)&s->rhs_s, s->ncell * sizeof(float));

@@ -408,6 +408,159 @@ __global__ void __launch_bounds__(256) k_apply_vorticity(FluidArgs a, const floa
     }
 }
 
+// ------------------------------------------------- fused vorticity (3D)
+// k_vorticity + k_apply_vorticity in one pass.  A block owns a 32x8 column of
+// cells and marches up a chunk of z: each z-plane of u, v, w faces (with a
+// two-cell x/y halo) is loaded once into a 4-plane ring in shared memory, w
+// and |w| of plane z+1 are computed from the rings, and the confinement force
+// of plane z updates its faces.  The per-cell expressions and their order are
+// those of the two kernels above; w never goes through global memory.
+constexpr int kMX = 32, kMY = 8, kMZ = 32;   // tile and z chunk
+constexpr int kUW = kMX + 3, kUH = kMY + 4;  // u faces x0-1 .. x0+kMX+1, rows y0-2 .. y0+kMY+1
+constexpr int kVW = kMX + 4, kVH = kMY + 3;  // v faces: cols x0-2 .. x0+kMX+1, face rows y0-1 .. y0+kMY+1
+constexpr int kWW = kMX + 4, kWH = kMY + 4;  // w faces: cols x0-2 .. x0+kMX+1, rows y0-2 .. y0+kMY+1
+constexpr int kHW = kMX + 2, kHH = kMY + 2;  // |w|: cells x0-1 .. x0+kMX, y0-1 .. y0+kMY
+constexpr int kMT = kMX * kMY;               // threads
+constexpr int kUL = (kUW * kUH + kMT - 1) / kMT, kVL = (kVW * kVH + kMT - 1) / kMT, kWL = (kWW * kWH + kMT - 1) / kMT;
+
+struct VortSmem {
+    float u[4][kUH][kUW];
+    float v[4][kVH][kVW];
+    float w[4][kWH][kWW];
+    float m[4][kHH][kHW];
+    float o[2][3][kMY][kMX];
+};
+
+__global__ void __launch_bounds__(kMT) k_vorticity_march(FluidArgs a) {
+    __shared__ VortSmem S;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY;
+    const int zb = blockIdx.z * kMZ, ze = min(zb + kMZ, nz);
+    const int tid = threadIdx.x;
+    // in-plane offsets of this thread's loads (-1: outside the face array)
+    int ou[kUL], ov[kVL], ow[kWL];
+#pragma unroll
+    for (int j = 0; j < kUL; ++j) {
+        const int i = tid + j * kMT, X = x0 - 1 + i % kUW, Y = y0 - 2 + i / kUW;
+        ou[j] = (i < kUW * kUH && X >= 0 && X <= nx && Y >= 0 && Y < ny) ? Y * (nx + 1) + X : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < kVL; ++j) {
+        const int i = tid + j * kMT, X = x0 - 2 + i % kVW, Y = y0 - 1 + i / kVW;
+        ov[j] = (i < kVW * kVH && X >= 0 && X < nx && Y >= 0 && Y <= ny) ? Y * nx + X : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < kWL; ++j) {
+        const int i = tid + j * kMT, X = x0 - 2 + i % kWW, Y = y0 - 2 + i / kWW;
+        ow[j] = (i < kWW * kWH && X >= 0 && X < nx && Y >= 0 && Y < ny) ? Y * nx + X : -1;
+    }
+    const size_t pu = (size_t)(nx + 1) * ny, pv = (size_t)nx * (ny + 1), pw = (size_t)nx * ny;
+    float ru[kUL], rv[kVL], rw[kWL];
+    // plane z of the three face arrays into registers (0 outside, as fetch_b)
+    auto fetch_plane = [&](int z) {
+        const bool zu = z >= 0 && z < nz, zw = z >= 0 && z <= nz;
+#pragma unroll
+        for (int j = 0; j < kUL; ++j) ru[j] = (zu && ou[j] >= 0) ? __ldg(a.u + z * pu + ou[j]) : 0.f;
+#pragma unroll
+        for (int j = 0; j < kVL; ++j) rv[j] = (zu && ov[j] >= 0) ? __ldg(a.v + z * pv + ov[j]) : 0.f;
+#pragma unroll
+        for (int j = 0; j < kWL; ++j) rw[j] = (zw && ow[j] >= 0) ? __ldg(a.w + z * pw + ow[j]) : 0.f;
+    };
+    auto store_plane = [&](int z) {
+        const int sl = (z + 4) & 3;
+#pragma unroll
+        for (int j = 0; j < kUL; ++j) {
+            const int i = tid + j * kMT;
+            if (i < kUW * kUH) (&S.u[sl][0][0])[i] = ru[j];
+        }
+#pragma unroll
+        for (int j = 0; j < kVL; ++j) {
+            const int i = tid + j * kMT;
+            if (i < kVW * kVH) (&S.v[sl][0][0])[i] = rv[j];
+        }
+#pragma unroll
+        for (int j = 0; j < kWL; ++j) {
+            const int i = tid + j * kMT;
+            if (i < kWW * kWH) (&S.w[sl][0][0])[i] = rw[j];
+        }
+    };
+    const float two_h = 2.f * a.c.vort_k;
+    // w and |w| of plane k from the rings (planes k-1 .. k+1 resident)
+    auto vorticity_plane = [&](int k) {
+        const int sm = (k + 3) & 3, s0 = (k + 4) & 3, sp = (k + 5) & 3;
+        for (int i = tid; i < kHW * kHH; i += kMT) {
+            const int hx = i % kHW, hy = i / kHW;
+            const int x = x0 - 1 + hx, y = y0 - 1 + hy;
+            float o0 = 0.f, o1 = 0.f, o2 = 0.f, m = 0.f;
+            if (x >= 0 && y >= 0 && k >= 0 && x < nx && y < ny && k < nz &&
+                !(a.flags[idx3(x, y, k, nx, ny)] & F_SOLID)) {
+#define CCX(SL, R, C) ((S.u[SL][R][C] + S.u[SL][R][(C) + 1]) * 0.5f)
+#define CCY(SL, R, C) ((S.v[SL][R][C] + S.v[SL][(R) + 1][C]) * 0.5f)
+#define CCZ(R, C) ((S.w[s0][R][C] + S.w[sp][R][C]) * 0.5f)
+                const float x1 = CCZ(hy + 2, hx + 1) - CCZ(hy, hx + 1);
+                const float x2 = CCY(sp, hy, hx + 1) - CCY(sm, hy, hx + 1);
+                const float y1 = CCX(sp, hy + 1, hx) - CCX(sm, hy + 1, hx);
+                const float y2 = CCZ(hy + 1, hx + 2) - CCZ(hy + 1, hx);
+                const float z1 = CCY(s0, hy, hx + 2) - CCY(s0, hy, hx);
+                const float z2 = CCX(s0, hy + 2, hx) - CCX(s0, hy, hx);
+#undef CCX
+#undef CCY
+#undef CCZ
+                o0 = (x1 - x2) / two_h;
+                o1 = (y1 - y2) / two_h;
+                o2 = (z1 - z2) / two_h;
+                m = sqrtf(o0 * o0 + o1 * o1 + o2 * o2);
+            }
+            S.m[s0][hy][hx] = m;
+            if (hx >= 1 && hy >= 1 && hx <= kMX && hy <= kMY) {
+                S.o[k & 1][0][hy - 1][hx - 1] = o0;
+                S.o[k & 1][1][hy - 1][hx - 1] = o1;
+                S.o[k & 1][2][hy - 1][hx - 1] = o2;
+            }
+        }
+    };
+    // prologue: planes zb-2 .. zb+1 of the faces, |w| of zb-1 and zb
+    for (int z = zb - 2; z <= zb + 1; ++z) {
+        fetch_plane(z);
+        store_plane(z);
+    }
+    fetch_plane(zb + 2);
+    __syncthreads();
+    vorticity_plane(zb - 1);
+    vorticity_plane(zb);
+    __syncthreads();   // plane zb-2's slot is refilled next
+    const int tx = tid % kMX, ty = tid / kMX;
+    const int x = x0 + tx, y = y0 + ty;
+    const float eps = 1e-20f;
+    for (int z = zb; z < ze; ++z) {
+        store_plane(z + 2);
+        if (z + 1 < ze) fetch_plane(z + 3);
+        __syncthreads();
+        vorticity_plane(z + 1);
+        __syncthreads();
+        if (x < nx && y < ny) {
+            const int sm = (z + 3) & 3, s0 = (z + 4) & 3, sp = (z + 5) & 3;
+            const float dx = S.m[s0][ty + 1][tx + 2] - S.m[s0][ty + 1][tx];
+            const float dy = S.m[s0][ty + 2][tx + 1] - S.m[s0][ty][tx + 1];
+            const float dz = S.m[sp][ty + 1][tx + 1] - S.m[sm][ty + 1][tx + 1];
+            const float gx = dx / two_h, gy = dy / two_h, gz = dz / two_h;
+            const float len = sqrtf(gx * gx + gy * gy + gz * gz) + eps;
+            const float nxv = gx / len, nyv = gy / len, nzv = gz / len;
+            const float o0 = S.o[z & 1][0][ty][tx], o1 = S.o[z & 1][1][ty][tx], o2 = S.o[z & 1][2][ty][tx];
+            const float f0 = nyv * o2 - o1 * nzv, f1 = nzv * o0 - o2 * nxv, f2 = nxv * o1 - o0 * nyv;
+            const float k = a.c.eps, vk = a.c.vort_k, dt = a.c.dt, rho = a.c.rho;
+            a.uo[idx3(x, y, z, nx + 1, ny)] = S.u[s0][ty + 2][tx + 1] + (f0 * 0.5f * k * vk * dt) / rho;
+            a.vo[idx3(x, y, z, nx, ny + 1)] = S.v[s0][ty + 1][tx + 2] + (f1 * 0.5f * k * vk * dt) / rho;
+            a.wo[idx3(x, y, z, nx, ny)] = S.w[s0][ty + 2][tx + 2] + (f2 * 0.5f * k * vk * dt) / rho;
+            // faces past the last cell: the force there is +0 (w = 0 outside the grid)
+            const float zero_term = (0.f * 0.5f * k * vk * dt) / rho;
+            if (x == nx - 1) a.uo[idx3(nx, y, z, nx + 1, ny)] = S.u[s0][ty + 2][tx + 2] + zero_term;
+            if (y == ny - 1) a.vo[idx3(x, ny, z, nx, ny + 1)] = S.v[s0][ty + 2][tx + 2] + zero_term;
+            if (z == nz - 1) a.wo[idx3(x, y, nz, nx, ny)] = S.w[sp][ty + 2][tx + 2] + zero_term;
+        }
+    }
+}
+
 int launch_vorticity(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     FluidArgs a = fluid_args(s, c);
     a.c.vort_k = s->h;
@@ -415,14 +568,29 @@ int launch_vorticity(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     dim3 gc = grid_for(s->nx, s->ny, s->nz, b);
     dim3 gf = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, b);
     if (s->dim == 3) {
-        k_vorticity<3><<<gc, b, 0, st>>>(a, s->vort);
-        k_apply_vorticity<3><<<gf, b, 0, st>>>(a, s->vort);
+        dim3 gt((s->nx + kMX - 1) / kMX, (s->ny + kMY - 1) / kMY, (s->nz + kMZ - 1) / kMZ);
+        k_vorticity_march<<<gt, kMT, 0, st>>>(a);
+        s->nlaunch += 1;
     } else {
         k_vorticity<2><<<gc, b, 0, st>>>(a, s->vort);
         k_apply_vorticity<2><<<gf, b, 0, st>>>(a, s->vort);
+        s->nlaunch += 2;
     }
     for (int d = 0; d < s->dim; ++d) s->vi[d] ^= 1;
-    s->nlaunch += 2;
+    return check_cuda(cudaGetLastError(), "vorticity confinement");
+}
+
+// the vorticity of the given velocities into out (3 planes in 3D, plus |w|):
+// what the adjoint of vorticity confinement reads
+int launch_vorticity_field(ss_sim* s, const StepConsts& c, const float* const vel[3], float* out, cudaStream_t st) {
+    FluidArgs a = fluid_args(s, c);
+    a.u = vel[0]; a.v = vel[1]; a.w = s->dim == 3 ? vel[2] : nullptr;
+    a.c.vort_k = s->h;
+    dim3 b(32, 8, 1);
+    dim3 gc = grid_for(s->nx, s->ny, s->nz, b);
+    if (s->dim == 3) k_vorticity<3><<<gc, b, 0, st>>>(a, out);
+    else k_vorticity<2><<<gc, b, 0, st>>>(a, out);
+    s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_vorticity");
 }
 

@@ -201,6 +201,7 @@ struct StepSaves {
     int vcycles;             // out: V-cycles (or refinement steps) the solve ran
 };
 int run_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* saves);
+int launch_vorticity_field(ss_sim* s, const StepConsts& c, const float* const vel[3], float* out, cudaStream_t st);
 
 // adjoint kernels (k_adjoint.cu)
 struct AdjScratch {

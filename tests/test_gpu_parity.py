@@ -24,6 +24,9 @@ GRIDS = [
     ("2d_quad", 2, (64, 40, 1), 1, 1),
     ("2d_quad_open_rgb", 2, (48, 34, 1), 3, 0),
     ("3d_quad_odd_y", 3, (24, 19, 18), 1, 1),
+    # taller than two z chunks and wider than one x tile of the fused
+    # vorticity kernel (32 x 8 cells, 32 planes per block)
+    ("3d_tall_open", 3, (35, 10, 70), 1, 0),
 ]
 
 
