@@ -17,8 +17,8 @@ CSRC = os.path.join(PKG_DIR, "csrc")
 OUT = os.path.join(PKG_DIR, "libsmokesim.so")
 BUILD_DIR = os.path.join(PKG_DIR, "_build")
 
-SOURCES = ["api.cpp", "k_fluid.cu", "k_mg.cu", "k_rbgs.cu", "k_rbgs_tma.cu", "k_rb.cu", "k_scene.cu", "k_mixed.cu", "k_adjoint.cu", "adjoint.cpp", "k_render.cu", "state_io.cpp", "k_noalloc.cu"]
-HEADERS = ["common.cuh", "ss_internal.h"]
+SOURCES = ["api.cpp", "k_fluid.cu", "k_mg.cu", "k_rbgs.cu", "k_rbgs_tma.cu", "k_rb.cu", "k_rb_tma.cu", "k_scene.cu", "k_mixed.cu", "k_adjoint.cu", "adjoint.cpp", "k_render.cu", "state_io.cpp", "k_noalloc.cu"]
+HEADERS = ["common.cuh", "ss_internal.h", "tma.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

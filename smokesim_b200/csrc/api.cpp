@@ -7,6 +7,7 @@
 // (both tiny, run on the host), and device memory ownership.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -190,6 +191,10 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     s->h = d->cell_size;
     s->t_amb0 = d->t_ambient;
     s->ncell = (size_t)s->nx * s->ny * s->nz;
+    // SMOKESIM_TMA: 0 keeps every sweep on per-thread loads, 1 (default) feeds
+    // the coarse-level tiled sweeps with TMA, 2 also the level-0 colour sweeps
+    // (the warp-specialised pipeline of k_rb_tma.cu); the results are the same
+    if (const char* e = getenv("SMOKESIM_TMA")) s->use_tma = atoi(e);
     s->nv[0] = (size_t)(s->nx + 1) * s->ny * s->nz;
     s->nv[1] = (size_t)s->nx * (s->ny + 1) * s->nz;
     s->nv[2] = s->dim == 3 ? (size_t)s->nx * s->ny * (s->nz + 1) : 0;

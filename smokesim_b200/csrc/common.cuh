@@ -276,6 +276,10 @@ template <> SS_D __half st<__half>(float v) { return __float2half_rn(v); }
 template <> SS_D __nv_bfloat16 st<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 template <typename T> SS_D float rnd(float v) { return ld(st<T>(v)); }
 
+// a float4 through the read-only path, and lane k of a float4
+SS_D float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+SS_D float f4(const float4& v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+
 // a / f for an integer count f in 1..6, value-identical to the IEEE quotient
 // (the same value; -0 may come back as +0): q0 = a*RN(1/f) followed by one
 // residual correction with fused multiply-adds, verified exhaustively against
@@ -284,9 +288,13 @@ template <typename T> SS_D float rnd(float v) { return ld(st<T>(v)); }
 // takes the IEEE path.
 SS_D float div_by_count(float a, int f) {
     if (f == 6) {
+        // the f = 3 steps below on a/2, written out so the interior cells'
+        // path carries no selection of the reciprocal
         if (fabsf(a) < 7.52316385e-37f) return a / 6.f;
-        a = a * 0.5f;
-        f = 3;
+        const float h = a * 0.5f;
+        const float q0 = __fmul_rn(h, 1.0f / 3.0f);
+        const float r = __fmaf_rn(-3.0f, q0, h);
+        return __fmaf_rn(r, 1.0f / 3.0f, q0);
     }
     const float y = f == 1 ? 1.f : f == 2 ? 0.5f : f == 3 ? (1.0f / 3.0f) : f == 4 ? 0.25f : (1.0f / 5.0f);
     const float q0 = __fmul_rn(a, y);

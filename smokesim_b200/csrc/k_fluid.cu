@@ -600,38 +600,56 @@ int launch_vorticity_field(ss_sim* s, const StepConsts& c, const float* const ve
 // velocity of cell idx (0 outside the grid).
 // P = double: the mixed-precision solve's FP64 pressure; the face update is
 // then evaluated in FP64 (k64 = -dt/(rho h)) and rounded once to FP32.
+// Each thread takes kUpdPlanes face positions up z; the pressure and solid
+// flag of the cell below (z-1) carry over from the previous plane.
+constexpr int kUpdPlanes = 8;
+
 template <int DIM, typename P = float>
 __global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const P* __restrict__ p, double k64 = 0.0) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z * blockDim.z + threadIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const bool in = x < nx && y < ny && z < nz;
-    const P pc = in ? __ldg(p + idx3(x, y, z, nx, ny)) : P(0);
-    const bool sc = in && (a.flags[idx3(x, y, z, nx, ny)] & F_SOLID);
+    const int zb = blockIdx.z * kUpdPlanes;
+    const int zend = min(zb + kUpdPlanes, DIM == 3 ? nz + 1 : 1);
+    const bool inxy = x < nx && y < ny;
+    P p_back = P(0);
+    bool s_back = false;
+    if (DIM == 3 && inxy && zb > 0) {
+        p_back = __ldg(p + idx3(x, y, zb - 1, nx, ny));
+        s_back = a.flags[idx3(x, y, zb - 1, nx, ny)] & F_SOLID;
+    }
+    for (int z = zb; z < zend; ++z) {
+        const bool in = inxy && z < nz;
+        const P pc = in ? __ldg(p + idx3(x, y, z, nx, ny)) : P(0);
+        const bool sc = in && (a.flags[idx3(x, y, z, nx, ny)] & F_SOLID);
 #pragma unroll
-    for (int comp = 0; comp < DIM; ++comp) {
-        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
-        if (x >= ax || y >= ay || z >= az) continue;
-        const int xm = x - (comp == 0), ym = y - (comp == 1), zm = z - (comp == 2);
-        const float* __restrict__ src = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
-        float* __restrict__ dst = comp == 0 ? a.uo : comp == 1 ? a.vo : a.wo;
-        const int i = idx3(x, y, z, ax, ay);
-        if (sc || solid_oob0(a.flags, xm, ym, zm, nx, ny, nz)) {
-            const float* sv = comp == 0 ? a.sv0 : comp == 1 ? a.sv1 : a.sv2;
-            dst[i] = (in && sv) ? sv[idx3(x, y, z, nx, ny)] : 0.f;
-            continue;
+        for (int comp = 0; comp < DIM; ++comp) {
+            const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+            if (x >= ax || y >= ay || z >= az) continue;
+            const int xm = x - (comp == 0), ym = y - (comp == 1), zm = z - (comp == 2);
+            const float* __restrict__ src = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
+            float* __restrict__ dst = comp == 0 ? a.uo : comp == 1 ? a.vo : a.wo;
+            const int i = idx3(x, y, z, ax, ay);
+            const bool s_lo = comp == 2 ? s_back : solid_oob0(a.flags, xm, ym, zm, nx, ny, nz);
+            if (sc || s_lo) {
+                const float* sv = comp == 0 ? a.sv0 : comp == 1 ? a.sv1 : a.sv2;
+                dst[i] = (in && sv) ? sv[idx3(x, y, z, nx, ny)] : 0.f;
+                continue;
+            }
+            const P plo = comp == 2 ? p_back
+                                    : ((xm < 0 || ym < 0) ? P(0) : __ldg(p + idx3(xm, ym, zm, nx, ny)));
+            if constexpr (std::is_same<P, double>::value) dst[i] = (float)((double)__ldg(src + i) + k64 * (pc - plo));
+            else dst[i] = __ldg(src + i) + a.c.k_upd * (pc - plo);
         }
-        const P plo = (xm < 0 || ym < 0 || zm < 0) ? P(0) : __ldg(p + idx3(xm, ym, zm, nx, ny));
-        if constexpr (std::is_same<P, double>::value) dst[i] = (float)((double)__ldg(src + i) + k64 * (pc - plo));
-        else dst[i] = __ldg(src + i) + a.c.k_upd * (pc - plo);
+        p_back = pc;
+        s_back = sc;
     }
 }
 
 int launch_update_velocities(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     FluidArgs a = fluid_args(s, c);
     dim3 b(32, 8, 1);
-    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, b);
+    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? (s->nz + kUpdPlanes) / kUpdPlanes : 1, b);
     if (s->dim == 3) k_update_velocity<3><<<g, b, 0, st>>>(a, s->p[0]);
     else k_update_velocity<2><<<g, b, 0, st>>>(a, s->p[0]);
     for (int d = 0; d < s->dim; ++d) s->vi[d] ^= 1;
@@ -642,7 +660,7 @@ int launch_update_velocities(ss_sim* s, const StepConsts& c, cudaStream_t st) {
 int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     FluidArgs a = fluid_args(s, c);
     dim3 b(32, 8, 1);
-    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, b);
+    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? (s->nz + kUpdPlanes) / kUpdPlanes : 1, b);
     const double k64 = -(double)c.dt / ((double)c.rho * (double)s->h);
     if (s->dim == 3) k_update_velocity<3, double><<<g, b, 0, st>>>(a, s->p64, k64);
     else k_update_velocity<2, double><<<g, b, 0, st>>>(a, s->p64, k64);
@@ -731,64 +749,71 @@ struct RhsOut {
     int s_solid, r_solid;   // out-of-grid neighbours count as solid in the smoother / residual
 };
 
+// Each thread takes kDivPlanes cells up z (the face between two of them is
+// loaded once), so a block reduces up to 256 * kDivPlanes cells.
+constexpr int kDivPlanes = 8;
+
 template <int DIM>
 __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restrict__ div0, float* __restrict__ div0r,
                                                     double* __restrict__ partial, RhsOut ro) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int zb = blockIdx.z * kDivPlanes;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     double acc = 0.0;
-    if (x < nx && y < ny && z < nz) {
-        const int c = idx3(x, y, z, nx, ny);
-        // the cell's six faces always exist: load them before the flag test
-        // so the loads do not wait for it
-        const float f_top = __ldg(a.v + idx3(x, y + 1, z, nx, ny + 1));
-        const float f_bottom = __ldg(a.v + idx3(x, y, z, nx, ny + 1));
-        const float f_right = __ldg(a.u + idx3(x + 1, y, z, nx + 1, ny));
-        const float f_left = __ldg(a.u + idx3(x, y, z, nx + 1, ny));
-        float f_front = 0.f, f_back = 0.f;
-        if constexpr (DIM == 3) {
-            f_front = __ldg(a.w + idx3(x, y, z + 1, nx, ny));
-            f_back = __ldg(a.w + idx3(x, y, z, nx, ny));
-        }
-        const uint8_t fl = a.flags[c];
-        if (!(fl & F_SOLID)) {
-            const bool sv = a.sv0 != nullptr;
-            const float v_top = (fl & F_TOP) ? (sv ? a.sv1[c + nx] : 0.f) : f_top;
-            const float v_bottom = (fl & F_BOTTOM) ? (sv ? a.sv1[c - nx] : 0.f) : f_bottom;
-            const float v_right = (fl & F_RIGHT) ? (sv ? a.sv0[c + 1] : 0.f) : f_right;
-            const float v_left = (fl & F_LEFT) ? (sv ? a.sv0[c - 1] : 0.f) : f_left;
-            float d = v_right - v_left + v_top - v_bottom;
-            float v_front = 0.f, v_back = 0.f;
-            if constexpr (DIM == 3) {
-                const int pl = nx * ny;
-                v_front = (fl & F_FRONT) ? (sv ? a.sv2[c + pl] : 0.f) : f_front;
-                v_back = (fl & F_BACK) ? (sv ? a.sv2[c - pl] : 0.f) : f_back;
-                d = d + v_front - v_back;
-            }
-            if (div0) div0[c] = d;
-            if (div0r || ro.rhs_s) {
-                // residual rule: out-of-grid neighbours are solid with velocity 0
-                const float rt = y + 1 >= ny ? 0.f : v_top, rb = y == 0 ? 0.f : v_bottom;
-                const float rr = x + 1 >= nx ? 0.f : v_right, rl = x == 0 ? 0.f : v_left;
-                float dr = rr - rl + rt - rb;
+    if (x < nx && y < ny) {
+        const int ze = min(zb + kDivPlanes, nz);
+        float f_back = 0.f;
+        if constexpr (DIM == 3) f_back = __ldg(a.w + idx3(x, y, zb, nx, ny));
+        for (int z = zb; z < ze; ++z) {
+            const int c = idx3(x, y, z, nx, ny);
+            // the cell's six faces always exist: load them before the flag test
+            // so the loads do not wait for it
+            const float f_top = __ldg(a.v + idx3(x, y + 1, z, nx, ny + 1));
+            const float f_bottom = __ldg(a.v + idx3(x, y, z, nx, ny + 1));
+            const float f_right = __ldg(a.u + idx3(x + 1, y, z, nx + 1, ny));
+            const float f_left = __ldg(a.u + idx3(x, y, z, nx + 1, ny));
+            float f_front = 0.f;
+            if constexpr (DIM == 3) f_front = __ldg(a.w + idx3(x, y, z + 1, nx, ny));
+            const uint8_t fl = __ldg(a.flags + c);
+            if (!(fl & F_SOLID)) {
+                const bool sv = a.sv0 != nullptr;
+                const float v_top = (fl & F_TOP) ? (sv ? a.sv1[c + nx] : 0.f) : f_top;
+                const float v_bottom = (fl & F_BOTTOM) ? (sv ? a.sv1[c - nx] : 0.f) : f_bottom;
+                const float v_right = (fl & F_RIGHT) ? (sv ? a.sv0[c + 1] : 0.f) : f_right;
+                const float v_left = (fl & F_LEFT) ? (sv ? a.sv0[c - 1] : 0.f) : f_left;
+                float d = v_right - v_left + v_top - v_bottom;
+                float v_front = 0.f, v_back = 0.f;
                 if constexpr (DIM == 3) {
-                    const float rf = z + 1 >= nz ? 0.f : v_front, rk = z == 0 ? 0.f : v_back;
-                    dr = dr + rf - rk;
+                    const int pl = nx * ny;
+                    v_front = (fl & F_FRONT) ? (sv ? a.sv2[c + pl] : 0.f) : f_front;
+                    v_back = (fl & F_BACK) ? (sv ? a.sv2[c - pl] : 0.f) : f_back;
+                    d = d + v_front - v_back;
                 }
-                if (div0r) div0r[c] = dr;
-                if (ro.rhs_s) {
-                    const int q = rb_slot(x, y, z, nx, ny, nz);
-                    ro.rhs_s[q] = ro.rho_h * (ro.s_solid ? dr : d) / ro.dt;
-                    ro.rhs_r[q] = ro.rho * (ro.r_solid ? dr : d) / ro.dt_h;
+                if (div0) div0[c] = d;
+                if (div0r || ro.rhs_s) {
+                    // residual rule: out-of-grid neighbours are solid with velocity 0
+                    const float rt = y + 1 >= ny ? 0.f : v_top, rb = y == 0 ? 0.f : v_bottom;
+                    const float rr = x + 1 >= nx ? 0.f : v_right, rl = x == 0 ? 0.f : v_left;
+                    float dr = rr - rl + rt - rb;
+                    if constexpr (DIM == 3) {
+                        const float rf = z + 1 >= nz ? 0.f : v_front, rk = z == 0 ? 0.f : v_back;
+                        dr = dr + rf - rk;
+                    }
+                    if (div0r) div0r[c] = dr;
+                    if (ro.rhs_s) {
+                        const int q = rb_slot(x, y, z, nx, ny, nz);
+                        ro.rhs_s[q] = ro.rho_h * (ro.s_solid ? dr : d) / ro.dt;
+                        ro.rhs_r[q] = ro.rho * (ro.r_solid ? dr : d) / ro.dt_h;
+                    }
                 }
+                acc += (double)d * (double)d;
+            } else if (ro.rhs_s) {
+                const int q = rb_slot(x, y, z, nx, ny, nz);
+                ro.rhs_s[q] = 0.f;
+                ro.rhs_r[q] = 0.f;
             }
-            acc = (double)d * (double)d;
-        } else if (ro.rhs_s) {
-            const int q = rb_slot(x, y, z, nx, ny, nz);
-            ro.rhs_s[q] = 0.f;
-            ro.rhs_r[q] = 0.f;
+            f_back = f_front;
         }
     }
     if (partial) {
@@ -810,7 +835,7 @@ int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st, const St
         ro.r_solid = quirks ? 1 : s->enclosed;
     }
     dim3 b(32, 8, 1);
-    dim3 g = grid_for(s->nx, s->ny, s->nz, b);
+    dim3 g = grid_for(s->nx, s->ny, (s->nz + kDivPlanes - 1) / kDivPlanes, b);
     const int nblocks = (int)(g.x * g.y * g.z);
     float* d0 = write ? s->div0 : nullptr;
     float* d0r = (write && s->div0r != s->div0) ? s->div0r : nullptr;

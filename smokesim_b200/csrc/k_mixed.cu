@@ -65,60 +65,106 @@ __global__ void k_f32_from_p64(const double* __restrict__ p64, float* __restrict
 // With ACC the pending correction e (colour-split FP32) is first added to the
 // fluid cells' pressure: p_out = p_in + e, and the residual is that of p_out
 // (p_in and p_out are different buffers - neighbours read p_in + e).  Each
-// thread takes kIrPlanes z planes, so a block reduces 256 * kIrPlanes cells.
-constexpr int kIrPlanes = 4;
+// block takes kIrChunk z planes of a 32x8 column, so a block reduces up to
+// 256 * kIrChunk cells.
+// A block owns a 32x8 column of cells and marches up kIrChunk z planes.  The
+// pressure after the pending correction, P = p_in + e, is evaluated once per
+// cell: the column's own values roll through registers (the z neighbours),
+// each plane's tile plus its one-cell x/y rim goes through shared memory (the
+// x and y neighbours), double-buffered so a plane costs one barrier.
+constexpr int kIrTX = 32, kIrTY = 8, kIrChunk = 16;
+constexpr int kIrRim = 2 * kIrTX + 2 * kIrTY;   // rim cells of a tile (no corners: 5/7-point stencil)
 
 template <int DIM, bool ACC>
-__global__ void __launch_bounds__(256) k_ir_residual(const double* __restrict__ p_in, const float* __restrict__ e,
-                                                     double* __restrict__ p_out, const float* __restrict__ div0,
-                                                     const uint8_t* __restrict__ fmask, int nx, int ny, int nz,
-                                                     double k, double inv_k, double inv_khh,
-                                                     float* __restrict__ rhs_s, float* __restrict__ rhs_r,
-                                                     double* __restrict__ psum, double* __restrict__ pmax) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    double acc = 0.0, amax = 0.0;
-    const int pl = nx * ny;
-    // pressure of cell c after the pending correction (fluid cells only)
-    auto P = [&](int c, int xx, int yy, int zz) -> double {
-        double v = p_in[c];
+__global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
+    const double* __restrict__ p_in, const float* __restrict__ e, double* __restrict__ p_out,
+    const float* __restrict__ div0, const uint8_t* __restrict__ fmask, int nx, int ny, int nz, double k,
+    double inv_k, double inv_khh, float* __restrict__ rhs_s, float* __restrict__ rhs_r, double* __restrict__ psum,
+    double* __restrict__ pmax) {
+    __shared__ double sP[2][kIrTY + 2][kIrTX + 2];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kIrTX * ty;
+    const int x0 = blockIdx.x * kIrTX, y0 = blockIdx.y * kIrTY;
+    const int x = x0 + tx, y = y0 + ty;
+    const int zb = blockIdx.z * kIrChunk, ze = min(zb + kIrChunk, nz);
+    const bool in = x < nx && y < ny;
+    // this thread's rim cell (tid < kIrRim), in tile coordinates
+    int hx = 0, hy = 0;
+    if (tid < kIrTX) { hx = tid + 1; hy = 0; }
+    else if (tid < 2 * kIrTX) { hx = tid - kIrTX + 1; hy = kIrTY + 1; }
+    else if (tid < 2 * kIrTX + kIrTY) { hx = 0; hy = tid - 2 * kIrTX + 1; }
+    else if (tid < kIrRim) { hx = kIrTX + 1; hy = tid - 2 * kIrTX - kIrTY + 1; }
+    const int gx = x0 - 1 + hx, gy = y0 - 1 + hy;
+    const bool hin = tid < kIrRim && gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+    auto P = [&](int xx, int yy, int zz) -> double {
+        double v = p_in[idx3(xx, yy, zz, nx, ny)];
         if (ACC) v = v + (double)e[rb_pos(xx, yy, zz, nx, ny, nz)];
         return v;
     };
-    for (int j = 0; j < kIrPlanes; ++j) {
-        const int z = blockIdx.z * kIrPlanes + j;
-        if (x >= nx || y >= ny || z >= nz) break;
-        const int c = idx3(x, y, z, nx, ny);
-        const uint8_t m = fmask[c];
-        const int q = rb_pos(x, y, z, nx, ny, nz);
-        float s_out = 0.f, r_out = 0.f;
-        if (m & M_FLUID) {
-            const double t = (m & M_TOP) && y + 1 < ny ? P(c + nx, x, y + 1, z) : 0.0;
-            const double b = (m & M_BOTTOM) && y > 0 ? P(c - nx, x, y - 1, z) : 0.0;
-            const double r = (m & M_RIGHT) && x + 1 < nx ? P(c + 1, x + 1, y, z) : 0.0;
-            const double l = (m & M_LEFT) && x > 0 ? P(c - 1, x - 1, y, z) : 0.0;
-            double sum = t + b;
-            sum = sum + r;
-            sum = sum + l;
-            if constexpr (DIM == 3) {
-                const double f = (m & M_FRONT) && z + 1 < nz ? P(c + pl, x, y, z + 1) : 0.0;
-                const double k2 = (m & M_BACK) && z > 0 ? P(c - pl, x, y, z - 1) : 0.0;
-                sum = sum + f;
-                sum = sum + k2;
-            }
-            const double pc = P(c, x, y, z);
-            if (ACC) p_out[c] = pc;
-            const double cnt = (double)__popc(m & 0x7Eu);
-            const double rho = (double)div0[c] - k * (sum - cnt * pc);
-            acc += rho * rho;
-            amax = fmax(amax, fabs(rho));
-            s_out = (float)(rho * inv_k);
-            r_out = (float)(rho * inv_khh);
-        } else if (ACC) {
-            p_out[c] = p_in[c];
+    double pm = 0.0, p0 = 0.0, pp = 0.0, h0 = 0.0;
+    if (in) {
+        if (zb > 0) pm = P(x, y, zb - 1);
+        p0 = P(x, y, zb);
+        if (zb + 1 < nz) pp = P(x, y, zb + 1);
+    }
+    if (hin) h0 = P(gx, gy, zb);
+    uint8_t m = in ? fmask[idx3(x, y, zb, nx, ny)] : 0;
+    float dv = in ? div0[idx3(x, y, zb, nx, ny)] : 0.f;
+    double acc = 0.0, amax = 0.0;
+    for (int z = zb; z < ze; ++z) {
+        const int sl = z & 1;
+        sP[sl][ty + 1][tx + 1] = p0;
+        if (tid < kIrRim) sP[sl][hy][hx] = h0;
+        // the next planes' values, in flight across the barrier and this plane's work
+        double pn = 0.0, hn = 0.0;
+        uint8_t mn = 0;
+        float dvn = 0.f;
+        if (in && z + 1 < ze) {
+            if (z + 2 < nz) pn = P(x, y, z + 2);
+            mn = fmask[idx3(x, y, z + 1, nx, ny)];
+            dvn = div0[idx3(x, y, z + 1, nx, ny)];
         }
-        rhs_s[q] = s_out;
-        rhs_r[q] = r_out;
+        if (hin && z + 1 < ze) hn = P(gx, gy, z + 1);
+        const int c = idx3(x, y, z, nx, ny);
+        __syncthreads();
+        if (in) {
+            const int q = rb_pos(x, y, z, nx, ny, nz);
+            float s_out = 0.f, r_out = 0.f;
+            if (m & M_FLUID) {
+                // out-of-grid neighbours (a set bit on an open grid) hold +0 in the
+                // tile, the rim and the z registers: no bounds tests needed
+                const double t = (m & M_TOP) ? sP[sl][ty + 2][tx + 1] : 0.0;
+                const double b = (m & M_BOTTOM) ? sP[sl][ty][tx + 1] : 0.0;
+                const double r = (m & M_RIGHT) ? sP[sl][ty + 1][tx + 2] : 0.0;
+                const double l = (m & M_LEFT) ? sP[sl][ty + 1][tx] : 0.0;
+                double sum = t + b;
+                sum = sum + r;
+                sum = sum + l;
+                if constexpr (DIM == 3) {
+                    const double f = (m & M_FRONT) ? pp : 0.0;
+                    const double k2 = (m & M_BACK) ? pm : 0.0;
+                    sum = sum + f;
+                    sum = sum + k2;
+                }
+                if (ACC) p_out[c] = p0;
+                const double cnt = (double)__popc(m & 0x7Eu);
+                const double rho = (double)dv - k * (sum - cnt * p0);
+                acc += rho * rho;
+                const double ar = fabs(rho);
+                amax = ar > amax ? ar : amax;
+                s_out = (float)(rho * inv_k);
+                r_out = (float)(rho * inv_khh);
+            } else if (ACC) {
+                p_out[c] = p_in[c];
+            }
+            rhs_s[q] = s_out;
+            rhs_r[q] = r_out;
+        }
+        pm = p0;
+        p0 = pp;
+        pp = pn;
+        h0 = hn;
+        m = mn;
+        dv = dvn;
     }
     block_sum_max(acc, amax, psum + blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
                   pmax + blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
@@ -176,8 +222,8 @@ int launch_p0_from_p64(ss_sim* s, cudaStream_t st) {
 }
 
 int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate, cudaStream_t st) {
-    dim3 b(32, 8, 1);
-    dim3 g((s->nx + 31) / 32, (s->ny + 7) / 8, (s->nz + kIrPlanes - 1) / kIrPlanes);
+    dim3 b(kIrTX, kIrTY, 1);
+    dim3 g((s->nx + kIrTX - 1) / kIrTX, (s->ny + kIrTY - 1) / kIrTY, (s->nz + kIrChunk - 1) / kIrChunk);
     const int nblocks = (int)(g.x * g.y * g.z);
     if (nblocks > s->red.max_blocks) return set_error(SS_E_INVALID, "reduction scratch too small");
     const double k = (double)c.dt / ((double)c.rho * (double)s->h);

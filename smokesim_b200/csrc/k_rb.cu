@@ -13,6 +13,7 @@
 // 77-130 (value-identical; fluid mask with select instead of p*f, the division
 // by the fluid-neighbour count through div_by_count, right-hand sides
 // precomputed with the reference's operations by k_divergence).
+#include <algorithm>
 #include <cmath>
 #include <type_traits>
 #include <vector>
@@ -187,60 +188,80 @@ __global__ void __launch_bounds__(256) k_rb_prolong(float* __restrict__ p_red, f
 // mask bytes in one word.  Same values as the one-cell kernels above: the
 // neighbour sum keeps the order +y, -y, +x, -x, +z, -z and selects 0 for a
 // non-fluid or out-of-grid neighbour.
-SS_D float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
-SS_D float f4(const float4& v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+
+// A thread marches up `planes` z planes of its row: the other colour's row in
+// its own plane is the previous plane's front row and the back row is the
+// previous plane's own row (both kept in registers), and the loads of plane
+// z+1 are issued before plane z is computed.
+struct RbPlane {
+    uint32_t m4;
+    float4 rhs, pt, pb, pf;
+    float extra;
+};
 
 template <int DIM>
 __global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, const float* __restrict__ po,
                                                     const float* __restrict__ rhs_c, const uint8_t* __restrict__ mask_c,
-                                                    RBLevel g, int colour) {
+                                                    RBLevel g, int colour, int planes) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
     if (q >= (g.half >> 2) || y >= g.ny) return;
+    const int zb = blockIdx.z * planes, ze = min(zb + planes, g.nz);
     const int xh0 = q << 2;
-    const int i = (z * g.ny + y) * g.half + xh0;
-    // no early exit on an all-solid quad: every load below is issued before
-    // the first one is waited for
-    const uint32_t m4 = __ldg(reinterpret_cast<const uint32_t*>(mask_c + i));
-    const int par = (y + z + colour) & 1;   // x = 2*xh + par
+    const int pl = g.ny * g.half;
+    const bool up = y + 1 < g.ny, dn = y > 0;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 pt = y + 1 < g.ny ? ldg4(po + i + g.half) : zero;
-    const float4 pb = y > 0 ? ldg4(po + i - g.half) : zero;
-    const float4 pm = ldg4(po + i);
-    float4 pf = zero, pk = zero;
-    if constexpr (DIM == 3) {
-        const int pl = g.ny * g.half;
-        if (z + 1 < g.nz) pf = ldg4(po + i + pl);
-        if (z > 0) pk = ldg4(po + i - pl);
-    }
-    // row-end neighbour: left of the first cell (par 0) or right of the last (par 1)
-    const float extra = par == 0 ? (xh0 > 0 ? __ldg(po + i - 1) : 0.f) : (xh0 + 4 < g.half ? __ldg(po + i + 4) : 0.f);
-    const float4 rhs = ldg4(rhs_c + i);
-    float out[4];
-    bool wr[4];
+    // every load of a plane is issued before the first one is waited for (no
+    // early exit on an all-solid quad)
+    auto load = [&](int z, RbPlane& P) {
+        const int i = (z * g.ny + y) * g.half + xh0;
+        const int par = (y + z + colour) & 1;   // x = 2*xh + par
+        P.m4 = __ldg(reinterpret_cast<const uint32_t*>(mask_c + i));
+        P.pt = up ? ldg4(po + i + g.half) : zero;
+        P.pb = dn ? ldg4(po + i - g.half) : zero;
+        P.pf = (DIM == 3 && z + 1 < g.nz) ? ldg4(po + i + pl) : zero;
+        // row-end neighbour: left of the first cell (par 0) or right of the last (par 1)
+        P.extra = par == 0 ? (xh0 > 0 ? __ldg(po + i - 1) : 0.f) : (xh0 + 4 < g.half ? __ldg(po + i + 4) : 0.f);
+        P.rhs = ldg4(rhs_c + i);
+    };
+    const int i0 = (zb * g.ny + y) * g.half + xh0;
+    float4 pm = ldg4(po + i0);
+    float4 pk = (DIM == 3 && zb > 0) ? ldg4(po + i0 - pl) : zero;
+    RbPlane cur, nxt;
+    load(zb, cur);
+    nxt = cur;
+    for (int z = zb; z < ze; ++z) {
+        if (z + 1 < ze) load(z + 1, nxt);
+        const int i = (z * g.ny + y) * g.half + xh0;
+        const int par = (y + z + colour) & 1;
+        float out[4];
+        bool wr[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint32_t m = (m4 >> (8 * k)) & 0xFFu;
-        const int fs = __popc(m & 0x7Eu);
-        wr[k] = (m & M_FLUID) && fs != 0;
-        const float left = par ? f4(pm, k) : (k ? f4(pm, k - 1) : extra);
-        const float right = par ? (k < 3 ? f4(pm, k + 1) : extra) : f4(pm, k);
-        float sum = ((m & M_TOP) ? f4(pt, k) : 0.f) + ((m & M_BOTTOM) ? f4(pb, k) : 0.f);
-        sum = sum + ((m & M_RIGHT) ? right : 0.f);
-        sum = sum + ((m & M_LEFT) ? left : 0.f);
-        if constexpr (DIM == 3) {
-            sum = sum + ((m & M_FRONT) ? f4(pf, k) : 0.f);
-            sum = sum + ((m & M_BACK) ? f4(pk, k) : 0.f);
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t m = (cur.m4 >> (8 * k)) & 0xFFu;
+            const int fs = __popc(m & 0x7Eu);
+            wr[k] = (m & M_FLUID) && fs != 0;
+            const float left = par ? f4(pm, k) : (k ? f4(pm, k - 1) : cur.extra);
+            const float right = par ? (k < 3 ? f4(pm, k + 1) : cur.extra) : f4(pm, k);
+            float sum = ((m & M_TOP) ? f4(cur.pt, k) : 0.f) + ((m & M_BOTTOM) ? f4(cur.pb, k) : 0.f);
+            sum = sum + ((m & M_RIGHT) ? right : 0.f);
+            sum = sum + ((m & M_LEFT) ? left : 0.f);
+            if constexpr (DIM == 3) {
+                sum = sum + ((m & M_FRONT) ? f4(cur.pf, k) : 0.f);
+                sum = sum + ((m & M_BACK) ? f4(pk, k) : 0.f);
+            }
+            out[k] = wr[k] ? div_by_count(sum - f4(cur.rhs, k), fs) : 0.f;
         }
-        out[k] = wr[k] ? div_by_count(sum - f4(rhs, k), fs) : 0.f;
-    }
-    if (wr[0] && wr[1] && wr[2] && wr[3]) {
-        *reinterpret_cast<float4*>(pc + i) = make_float4(out[0], out[1], out[2], out[3]);
-    } else {
+        if (wr[0] && wr[1] && wr[2] && wr[3]) {
+            *reinterpret_cast<float4*>(pc + i) = make_float4(out[0], out[1], out[2], out[3]);
+        } else {
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if (wr[k]) pc[i + k] = out[k];
+            for (int k = 0; k < 4; ++k)
+                if (wr[k]) pc[i + k] = out[k];
+        }
+        pk = pm;
+        pm = cur.pf;
+        cur = nxt;
     }
 }
 
@@ -248,7 +269,7 @@ __global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, cons
 // restricted: per fine row the even-x cells sit in one colour array and the
 // odd-x cells in the other, both at the coarse x index.
 template <int DIM, bool POW2, typename T = float>
-__global__ void __launch_bounds__(256) k_rb_residual_restrict4(const float* __restrict__ p_red, const float* __restrict__ p_black,
+__global__ void __launch_bounds__(256, 3) k_rb_residual_restrict4(const float* __restrict__ p_red, const float* __restrict__ p_black,
                                                                const float* __restrict__ rr_red, const float* __restrict__ rr_black,
                                                                const uint8_t* __restrict__ m_red, const uint8_t* __restrict__ m_black,
                                                                RBLevel g, T* __restrict__ rc, int cx, int cy,
@@ -466,11 +487,23 @@ int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st) {
     const uint8_t* mask[2] = {s->rb_mask, s->rb_mask + h};
     dim3 b, gr;
     row_launch(s->rb_vec ? g.half / 4 : g.half, g.ny, g.nz, b, gr);
+    // z planes per thread of the four-cell kernel: about three waves of
+    // four 256-thread blocks per SM
+    int planes = 1;
+    if (s->rb_vec && s->dim == 3) {
+        const long long per_plane = (long long)gr.x * gr.y;
+        planes = (int)std::max(1LL, std::min(16LL, per_plane * g.nz / (148LL * 4 * 3)));
+    }
+    dim3 gr4(gr.x, gr.y, (g.nz + planes - 1) / planes);
+    const bool tma = rb_tma_supported(s);
     for (int it = 0; it < iterations; ++it)
         for (int c = 0; c < 2; ++c) {
-            if (s->rb_vec) {
-                if (s->dim == 3) k_rb_smooth4<3><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
-                else k_rb_smooth4<2><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
+            if (tma) {
+                const int rc = launch_rb_smooth_tma(s, p[c], p[1 - c], rhs[c], mask[c], c, st);
+                if (rc) return rc;
+            } else if (s->rb_vec) {
+                if (s->dim == 3) k_rb_smooth4<3><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
+                else k_rb_smooth4<2><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
             } else {
                 if (s->dim == 3) k_rb_smooth<3><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
                 else k_rb_smooth<2><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);

@@ -20,54 +20,9 @@
 
 #include "common.cuh"
 #include "ss_internal.h"
+#include "tma.cuh"
 
 namespace ss {
-
-SS_D uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-SS_D void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-SS_D void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-SS_D void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-SS_D bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(phase)
-        : "memory");
-    return ok != 0;
-}
-SS_D void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
-            smem_u32(dst)),
-        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// Bounded wait on an mbarrier phase: polls with back-off for at most about a
-// second and reports whether the phase completed.
-SS_D bool wait_bounded(uint64_t* bar, uint32_t phase) {
-    for (int k = 0; k < (1 << 22); ++k) {
-        if (mbar_try_wait(bar, phase)) return true;
-        if (k > 64) __nanosleep(32);
-    }
-    return false;
-}
-
-// Block-uniform wait for a tile: every thread waits (bounded), then the block
-// agrees; on failure the error word is set and every thread sees false, so no
-// thread is left behind at a later barrier.
-SS_D bool wait_tile(uint64_t* bar, uint32_t phase, int* err) {
-    const bool ok = wait_bounded(bar, phase);
-    const bool all = __syncthreads_and(ok) != 0;
-    if (!all && threadIdx.x == 0) atomicOr(err, 1);
-    return all;
-}
 
 struct TmaArgs {
     float* __restrict__ p_out;
@@ -267,7 +222,7 @@ __global__ void __launch_bounds__(256) k_rbgs_tma(const __grid_constant__ CUtens
 }
 
 // ------------------------------------------------------------------ host
-static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+PFN_cuTensorMapEncodeTiled_v12000 tma_encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     if (!fn) {
         cudaDriverEntryPointQueryResult q;
@@ -280,7 +235,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // 3D tiled tensor map of an x-fastest array; cached per (address, box).
-static int tensor_map(ss_sim* s, const void* ptr, bool bytes, const int dims[3], const int box[3], CUtensorMap* out) {
+int tma_tensor_map(ss_sim* s, const void* ptr, bool bytes, const int dims[3], const int box[3], CUtensorMap* out) {
     for (const auto& e : s->tmaps) {
         if (e.ptr == ptr && e.bytes == bytes && e.box[0] == box[0] && e.box[1] == box[1] && e.box[2] == box[2] &&
             e.dims[0] == dims[0] && e.dims[1] == dims[1] && e.dims[2] == dims[2]) {
@@ -288,7 +243,7 @@ static int tensor_map(ss_sim* s, const void* ptr, bool bytes, const int dims[3],
             return SS_OK;
         }
     }
-    auto fn = encode_fn();
+    auto fn = tma_encode_fn();
     if (!fn) return set_error(SS_E_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
     const int es = bytes ? 1 : 4;
     cuuint64_t gdim[3] = {(cuuint64_t)dims[0], (cuuint64_t)dims[1], (cuuint64_t)dims[2]};
@@ -310,7 +265,7 @@ static int tensor_map(ss_sim* s, const void* ptr, bool bytes, const int dims[3],
 
 bool tma_sweep_supported(const ss_sim* s, int L) {
     // 16-byte row pitch for the flag bytes and whole 16^3 tiles' alignment rules
-    return s->dim == 3 && s->use_tma && (s->lv[L].n[0] % 16) == 0 && encode_fn() != nullptr;
+    return s->dim == 3 && s->use_tma && (s->lv[L].n[0] % 16) == 0 && tma_encode_fn() != nullptr;
 }
 
 template <bool L0, bool RESID, bool POW2>
@@ -368,9 +323,9 @@ int launch_rbgs_sweep_tma(ss_sim* s, const StepConsts& c, int L, int quirks, boo
     const bool write_fine = resid && quirks && L > 0;
     a.r_out = write_fine ? s->r_alt[L] : nullptr;
     CUtensorMap tp, tr, tf;
-    int rc = tensor_map(s, s->p[L], false, dims, pbox, &tp);
-    if (!rc) rc = tensor_map(s, rhs, false, dims, rbox, &tr);
-    if (!rc) rc = L == 0 ? tensor_map(s, s->flags, true, dims, fbox, &tf) : tensor_map(s, s->alpha[L], false, dims, pbox, &tf);
+    int rc = tma_tensor_map(s, s->p[L], false, dims, pbox, &tp);
+    if (!rc) rc = tma_tensor_map(s, rhs, false, dims, rbox, &tr);
+    if (!rc) rc = L == 0 ? tma_tensor_map(s, s->flags, true, dims, fbox, &tf) : tma_tensor_map(s, s->alpha[L], false, dims, pbox, &tf);
     if (rc) return rc;
     if (L == 0) rc = resid ? launch_tma_p<true, true>(s, pow2, tp, tr, tf, a, st) : launch_tma_p<true, false>(s, pow2, tp, tr, tf, a, st);
     else rc = resid ? launch_tma_p<false, true>(s, pow2, tp, tr, tf, a, st) : launch_tma_p<false, false>(s, pow2, tp, tr, tf, a, st);

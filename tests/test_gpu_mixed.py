@@ -20,6 +20,7 @@ MIXED_GRIDS = [
     ("3d_tma", 3, (32, 24, 20), 1, 1, 4),
     ("3d_l1", 3, (64, 48, 48), 1, 1, 8),
     ("3d_even_not_quad", 3, (20, 18, 14), 1, 0, 4),   # nx % 8 != 0: one cell per thread
+    ("3d_two_segments", 3, (512, 12, 10), 1, 1, 4),    # TMA-fed level-0 sweep, two row segments
 ]
 
 

@@ -27,6 +27,9 @@ GRIDS = [
     # taller than two z chunks and wider than one x tile of the fused
     # vorticity kernel (32 x 8 cells, 32 planes per block)
     ("3d_tall_open", 3, (35, 10, 70), 1, 0),
+    # colour rows of 256 cells: the TMA-fed level-0 sweep runs two 128-wide
+    # segments per row and a row block (8 rows) that straddles the grid edge
+    ("3d_two_segments", 3, (512, 12, 10), 1, 1),
 ]
 
 
@@ -280,3 +283,27 @@ def test_full_step_bitwise_tma(name, dim, n, nch, enc, mc):
         g.step(p)
         o.step(p)
         assert_same(g, o, dim, f"tma full step {k}")
+
+
+# Level-0 colour sweeps on every path: per-thread loads (SMOKESIM_TMA=0 and
+# the default) and the warp-specialised TMA pipeline (SMOKESIM_TMA=2), which
+# runs where the colour rows are whole 16-byte units of mask bytes.
+L0_TMA_GRIDS = [
+    ("3d_tma", 3, (32, 24, 20), 1, 1, 4),
+    ("3d_tma_l1", 3, (64, 48, 48), 1, 1, 8),
+    ("3d_two_segments", 3, (512, 12, 10), 1, 1, 4),
+    ("3d_two_segments_open", 3, (512, 20, 9), 1, 0, 4),
+]
+
+
+@pytest.mark.parametrize("name,dim,n,nch,enc,mc", L0_TMA_GRIDS)
+@pytest.mark.parametrize("tma", ["0", "2"])
+@pytest.mark.parametrize("prec", [abi.PREC_FP32, abi.PREC_MIXED])
+def test_full_step_bitwise_level0_paths(monkeypatch, name, dim, n, nch, enc, mc, tma, prec):
+    monkeypatch.setenv("SMOKESIM_TMA", tma)
+    g, o = make_pair(dim, n, nch, enc, seed=23, min_coarse=mc, t_amb=0.1)
+    p = scene.workload_params(t_ambient=0.1, n_coarse=12, ref_quirks=0, precision=prec, n_vcycles=2)
+    for k in range(2):
+        g.step(p)
+        o.step(p)
+        assert_same(g, o, dim, f"level-0 path {tma} step {k}")
