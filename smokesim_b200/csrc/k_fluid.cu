@@ -6,6 +6,8 @@
 // 3d/grid3d.c:104-162), smoke likewise.
 #include <type_traits>
 
+#include <cmath>
+
 #include "common.cuh"
 #include "ss_internal.h"
 
@@ -415,6 +417,13 @@ __global__ void __launch_bounds__(256) k_apply_vorticity(FluidArgs a, const floa
 // and |w| of plane z+1 are computed from the rings, and the confinement force
 // of plane z updates its faces.  The per-cell expressions and their order are
 // those of the two kernels above; w never goes through global memory.
+// v is a power of two whose reciprocal is a normal float too
+static bool pow2_normal(float v) {
+    if (!(v > 0.f) || !std::isfinite(v)) return false;
+    int e;
+    return std::frexp(v, &e) == 0.5f && v >= 1.1754944e-38f && v <= 8.5070592e37f;
+}
+
 constexpr int kMX = 32, kMY = 8, kMZ = 32;   // tile and z chunk
 constexpr int kUW = kMX + 3, kUH = kMY + 4;  // u faces x0-1 .. x0+kMX+1, rows y0-2 .. y0+kMY+1
 constexpr int kVW = kMX + 4, kVH = kMY + 3;  // v faces: cols x0-2 .. x0+kMX+1, face rows y0-1 .. y0+kMY+1
@@ -431,7 +440,10 @@ struct VortSmem {
     float o[2][3][kMY][kMX];
 };
 
-__global__ void __launch_bounds__(kMT) k_vorticity_march(FluidArgs a) {
+// POW2: 2h and rho are powers of two, so dividing by them is multiplying by
+// their exact reciprocals (inv_2h, inv_rho) - the same correctly rounded value.
+template <bool POW2>
+__global__ void __launch_bounds__(kMT) k_vorticity_march(FluidArgs a, float inv_2h, float inv_rho) {
     __shared__ VortSmem S;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY;
@@ -506,9 +518,9 @@ __global__ void __launch_bounds__(kMT) k_vorticity_march(FluidArgs a) {
 #undef CCX
 #undef CCY
 #undef CCZ
-                o0 = (x1 - x2) / two_h;
-                o1 = (y1 - y2) / two_h;
-                o2 = (z1 - z2) / two_h;
+                o0 = POW2 ? (x1 - x2) * inv_2h : (x1 - x2) / two_h;
+                o1 = POW2 ? (y1 - y2) * inv_2h : (y1 - y2) / two_h;
+                o2 = POW2 ? (z1 - z2) * inv_2h : (z1 - z2) / two_h;
                 m = sqrtf(o0 * o0 + o1 * o1 + o2 * o2);
             }
             S.m[s0][hy][hx] = m;
@@ -543,17 +555,23 @@ __global__ void __launch_bounds__(kMT) k_vorticity_march(FluidArgs a) {
             const float dx = S.m[s0][ty + 1][tx + 2] - S.m[s0][ty + 1][tx];
             const float dy = S.m[s0][ty + 2][tx + 1] - S.m[s0][ty][tx + 1];
             const float dz = S.m[sp][ty + 1][tx + 1] - S.m[sm][ty + 1][tx + 1];
-            const float gx = dx / two_h, gy = dy / two_h, gz = dz / two_h;
+            const float gx = POW2 ? dx * inv_2h : dx / two_h;
+            const float gy = POW2 ? dy * inv_2h : dy / two_h;
+            const float gz = POW2 ? dz * inv_2h : dz / two_h;
             const float len = sqrtf(gx * gx + gy * gy + gz * gz) + eps;
             const float nxv = gx / len, nyv = gy / len, nzv = gz / len;
             const float o0 = S.o[z & 1][0][ty][tx], o1 = S.o[z & 1][1][ty][tx], o2 = S.o[z & 1][2][ty][tx];
             const float f0 = nyv * o2 - o1 * nzv, f1 = nzv * o0 - o2 * nxv, f2 = nxv * o1 - o0 * nyv;
             const float k = a.c.eps, vk = a.c.vort_k, dt = a.c.dt, rho = a.c.rho;
-            a.uo[idx3(x, y, z, nx + 1, ny)] = S.u[s0][ty + 2][tx + 1] + (f0 * 0.5f * k * vk * dt) / rho;
-            a.vo[idx3(x, y, z, nx, ny + 1)] = S.v[s0][ty + 1][tx + 2] + (f1 * 0.5f * k * vk * dt) / rho;
-            a.wo[idx3(x, y, z, nx, ny)] = S.w[s0][ty + 2][tx + 2] + (f2 * 0.5f * k * vk * dt) / rho;
+            auto term = [&](float f) {
+                const float t = f * 0.5f * k * vk * dt;
+                return POW2 ? t * inv_rho : t / rho;
+            };
+            a.uo[idx3(x, y, z, nx + 1, ny)] = S.u[s0][ty + 2][tx + 1] + term(f0);
+            a.vo[idx3(x, y, z, nx, ny + 1)] = S.v[s0][ty + 1][tx + 2] + term(f1);
+            a.wo[idx3(x, y, z, nx, ny)] = S.w[s0][ty + 2][tx + 2] + term(f2);
             // faces past the last cell: the force there is +0 (w = 0 outside the grid)
-            const float zero_term = (0.f * 0.5f * k * vk * dt) / rho;
+            const float zero_term = term(0.f);
             if (x == nx - 1) a.uo[idx3(nx, y, z, nx + 1, ny)] = S.u[s0][ty + 2][tx + 2] + zero_term;
             if (y == ny - 1) a.vo[idx3(x, ny, z, nx, ny + 1)] = S.v[s0][ty + 2][tx + 2] + zero_term;
             if (z == nz - 1) a.wo[idx3(x, y, nz, nx, ny)] = S.w[sp][ty + 2][tx + 2] + zero_term;
@@ -569,7 +587,11 @@ int launch_vorticity(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     dim3 gf = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, b);
     if (s->dim == 3) {
         dim3 gt((s->nx + kMX - 1) / kMX, (s->ny + kMY - 1) / kMY, (s->nz + kMZ - 1) / kMZ);
-        k_vorticity_march<<<gt, kMT, 0, st>>>(a);
+        const float two_h = 2.f * s->h;
+        if (pow2_normal(two_h) && pow2_normal(c.rho))
+            k_vorticity_march<true><<<gt, kMT, 0, st>>>(a, 1.f / two_h, 1.f / c.rho);
+        else
+            k_vorticity_march<false><<<gt, kMT, 0, st>>>(a, 0.f, 0.f);
         s->nlaunch += 1;
     } else {
         k_vorticity<2><<<gc, b, 0, st>>>(a, s->vort);

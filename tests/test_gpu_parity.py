@@ -307,3 +307,26 @@ def test_full_step_bitwise_level0_paths(monkeypatch, name, dim, n, nch, enc, mc,
         g.step(p)
         o.step(p)
         assert_same(g, o, dim, f"level-0 path {tma} step {k}")
+
+
+@pytest.mark.parametrize("h,rho", [(1.0, 2.0), (0.5, 0.75), (0.3, 0.5)])
+def test_vorticity_divisor_paths(h, rho):
+    """Fused vorticity confinement with 2h and rho powers of two (divisions
+    taken as multiplications by the exact reciprocals) and not."""
+    from oracle.oracle import OracleSim
+    from smokesim_b200 import Sim
+    n = (35, 10, 40)
+    desc = abi.make_desc(3, n, cell_size=h, density_channels=1, enclosed=0, min_coarse=3)
+    g, o = Sim(desc), OracleSim(desc)
+    rng = scene.Rng(29)
+    em, ob, bx = _scene_for(3, n, rng)
+    for s in (g, o):
+        s.set_scene(em, ob, bx)
+    for k, a in scene.random_state(rng, 3, n, 1).items():
+        g.set_field(k, a)
+        o.set_field(k, a)
+    p = scene.workload_params(stage_mask=abi.STAGE_APPLY_VORTICITY, rho=rho, eps=0.7)
+    for _ in range(2):
+        g.step(p)
+        o.step(p)
+    assert_same(g, o, 3, f"vorticity h={h} rho={rho}")
