@@ -49,7 +49,9 @@ def parse():
     ap.add_argument("--profile-adjoint", action="store_true",
                     help="no timing: a 4-step forward+reverse rollout of the plume scene at --n (for ncu)")
     ap.add_argument("--profile", action="store_true",
-                    help="no timing: set up, run one step and a few level-0 smoother sweeps (for ncu)")
+                    help="no timing: set up, run --profile-steps steps and a few level-0 smoother sweeps (for ncu)")
+    ap.add_argument("--profile-steps", type=int, default=1,
+                    help="steps of the --profile run (the first one starts from the GRF state)")
     return ap.parse_args()
 
 
@@ -372,7 +374,7 @@ def main():
         if args.profile:
             sim = Sim(sc["desc"], stream=stream.cuda_stream)
             scene.apply(sim, sc)
-            sim.step(sc["params"], 1)
+            sim.step(sc["params"], args.profile_steps)
             sim.smooth(sc["params"], 0, 2)
             torch.cuda.synchronize()
             print(json.dumps({"profile": "done", "levels": sim.level_sizes}))

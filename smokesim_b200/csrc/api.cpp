@@ -104,6 +104,7 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->d_ob);
     cudaFree(s->d_bx);
     cudaFree(s->d_err);
+    cudaFree(s->coop_bar);
     delete s;
 }
 
@@ -195,6 +196,9 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     // the coarse-level tiled sweeps with TMA, 2 also the level-0 colour sweeps
     // (the warp-specialised pipeline of k_rb_tma.cu); the results are the same
     if (const char* e = getenv("SMOKESIM_TMA")) s->use_tma = atoi(e);
+    // SMOKESIM_COOP_CELLS: coarse levels of at most this many cells run as two
+    // cooperative launches per V-cycle (default 0: one launch per operator)
+    if (const char* e = getenv("SMOKESIM_COOP_CELLS")) s->coop_cells = atoll(e);
     s->nv[0] = (size_t)(s->nx + 1) * s->ny * s->nz;
     s->nv[1] = (size_t)s->nx * (s->ny + 1) * s->nz;
     s->nv[2] = s->dim == 3 ? (size_t)s->nx * s->ny * (s->nz + 1) : 0;
@@ -256,6 +260,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     A((void**)&s->red.partial2, (size_t)2 * s->red.stage2 * sizeof(double));
     A((void**)&s->red.out, SLOT_COUNT * sizeof(double));
     A((void**)&s->d_err, sizeof(int));
+    A((void**)&s->coop_bar, 2 * sizeof(unsigned int));
     if (rc == SS_OK) {
         cudaError_t e = cudaMallocHost((void**)&s->red.host, SLOT_COUNT * sizeof(double));
         if (e != cudaSuccess) rc = check_cuda(e, "cudaMallocHost");
@@ -277,6 +282,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
         if (!rc) rc = check_cuda(cudaMemsetAsync(s->r[l], 0, n * 4, st), "memset");
     }
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->d_err, 0, sizeof(int), st), "memset");
+    if (!rc) rc = check_cuda(cudaMemsetAsync(s->coop_bar, 0, 2 * sizeof(unsigned int), st), "memset");
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->div0, 0, s->ncell * 4, st), "memset");
     if (!rc && s->div0r != s->div0) rc = check_cuda(cudaMemsetAsync(s->div0r, 0, s->ncell * 4, st), "memset");
     if (!rc && s->rb_mask) rc = rb_init_vector_paths(s, st);
@@ -774,6 +780,12 @@ static int v_cycle_mixed(ss_sim* s, const StepConsts& c, const ss_mg_schedule& m
     }
     if (L >= s->bottom) return coarse_bottom(s, mg, L, prec, st);
     if (L == s->levels - 1) return coarse_smooth(s, c, L, mg.n_coarse, prec, st);
+    if (L == coarse_coop_first(s)) {
+        // levels L .. bottom-1 in one cooperative launch per leg
+        TRY(launch_coarse_coop(s, c, mg, prec, true, st));
+        TRY(coarse_bottom(s, mg, s->bottom, prec, st));
+        return launch_coarse_coop(s, c, mg, prec, false, st);
+    }
     TRY(coarse_smooth(s, c, L, mg.n_pre, prec, st));
     TRY(coarse_residual_restrict(s, c, L, prec, st));
     const size_t nc = (size_t)s->lv[L + 1].n[0] * s->lv[L + 1].n[1] * s->lv[L + 1].n[2];
@@ -795,6 +807,7 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
     const bool stats = p->collect_stats || tol_mode;
     TRY(launch_divergence(s, true, stats ? SLOT_DIV_BEFORE : -1, st));
     if (!s->p64_valid) TRY(launch_p64_from_p0(s, st));
+    CU(cudaMemsetAsync(s->coop_bar, 0, 2 * sizeof(unsigned int), st), "clear grid barrier");
     const int cap = mg.n_vcycles > 0 ? mg.n_vcycles : 1;
     int done = 0;
     double db = 0.0, res = 0.0;

@@ -7,10 +7,19 @@
 // reference recomputes it from the velocities in every sweep); coarse levels
 // read the FP16-rounded solid fraction alpha (the reference stores the solid
 // pyramid as RGBA16F images).
+#include <algorithm>
+
 #include "common.cuh"
 #include "ss_internal.h"
 
 namespace ss {
+
+#define TRY_CUDA_MG(x, what)                              \
+    do {                                                  \
+        const int _rc = check_cuda((x), what);            \
+        if (_rc != SS_OK) return _rc;                     \
+    } while (0)
+
 
 // T: storage type of p and r (float, or __half / __nv_bfloat16 on the coarse
 // levels of the mixed-precision solve)
@@ -57,16 +66,26 @@ static MGArgs mg_args(ss_sim* s, const StepConsts& c, int L, float oobA) {
 }
 
 // ------------------------------------------------------------------ smoother
+// A level value as float; CG reads through L2 only (ld.global.cg), for
+// arrays other blocks of the same cooperative launch wrote since this SM last
+// cached them (L1 is not coherent across SMs).
+template <bool CG, typename T>
+SS_D float ldv(const T* p) {
+    if constexpr (CG) return ld(__ldcg(p));
+    else return ld(*p);
+}
+
 // smooth.comp:79-136 (2D :74-123): red-black Gauss-Seidel in place; solid
 // cells and cells without fluid neighbours are skipped; out of grid = fluid
 // with p = 0.
 // R: the type whose rounding every stored pressure gets (== T for global
 // arrays; the shared-memory bottom solve keeps float storage rounded as R).
-template <int DIM, bool L0, typename T = float, typename R = T>
+template <int DIM, bool L0, typename T = float, typename R = T, bool CG = false>
 SS_D void smooth_cell(const MGArgsT<T>& a, int x, int y, int z) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int c = idx3(x, y, z, nx, ny);
     float f_top, f_bottom, f_right, f_left, f_front = 0.f, f_back = 0.f;
+    float r_c = 0.f;
     if constexpr (L0) {
         const uint8_t fl = a.flags[c];
         if (fl & F_SOLID) return;
@@ -80,36 +99,52 @@ SS_D void smooth_cell(const MGArgsT<T>& a, int x, int y, int z) {
             f_back = (fl & F_BACK) ? 0.f : (z > 0 ? 1.f : fo);
         }
     } else {
-        if (a.alpha[c] >= 1.f) return;
-        f_top = 1.f - (y + 1 < ny ? a.alpha[c + nx] : a.oobA);
-        f_bottom = 1.f - (y > 0 ? a.alpha[c - nx] : a.oobA);
-        f_right = 1.f - (x + 1 < nx ? a.alpha[c + 1] : a.oobA);
-        f_left = 1.f - (x > 0 ? a.alpha[c - 1] : a.oobA);
+        // every load of the cell is issued before the solid test, so one
+        // memory latency covers the fraction, pressure and residual reads
+        const float a_c = a.alpha[c];
+        const float a_t = y + 1 < ny ? a.alpha[c + nx] : a.oobA;
+        const float a_b = y > 0 ? a.alpha[c - nx] : a.oobA;
+        const float a_r = x + 1 < nx ? a.alpha[c + 1] : a.oobA;
+        const float a_l = x > 0 ? a.alpha[c - 1] : a.oobA;
+        float a_f = 0.f, a_k = 0.f;
         if constexpr (DIM == 3) {
-            f_front = 1.f - (z + 1 < nz ? a.alpha[c + nx * ny] : a.oobA);
-            f_back = 1.f - (z > 0 ? a.alpha[c - nx * ny] : a.oobA);
+            a_f = z + 1 < nz ? a.alpha[c + nx * ny] : a.oobA;
+            a_k = z > 0 ? a.alpha[c - nx * ny] : a.oobA;
         }
+        r_c = ldv<CG>(a.r + c);
+        if (a_c >= 1.f) return;
+        f_top = 1.f - a_t;
+        f_bottom = 1.f - a_b;
+        f_right = 1.f - a_r;
+        f_left = 1.f - a_l;
+        if constexpr (DIM == 3) {
+            f_front = 1.f - a_f;
+            f_back = 1.f - a_k;
+        }
+    }
+    const T* P = a.p;
+    const float p_top = y + 1 < ny ? ldv<CG>(P + c + nx) : 0.f;
+    const float p_bottom = y > 0 ? ldv<CG>(P + c - nx) : 0.f;
+    const float p_right = x + 1 < nx ? ldv<CG>(P + c + 1) : 0.f;
+    const float p_left = x > 0 ? ldv<CG>(P + c - 1) : 0.f;
+    float p_front = 0.f, p_back = 0.f;
+    if constexpr (DIM == 3) {
+        p_front = z + 1 < nz ? ldv<CG>(P + c + nx * ny) : 0.f;
+        p_back = z > 0 ? ldv<CG>(P + c - nx * ny) : 0.f;
     }
     float f_sum = f_top + f_bottom + f_right + f_left;
     if constexpr (DIM == 3) f_sum = f_sum + f_front + f_back;
     if (f_sum == 0.f) return;
-    const T* P = a.p;
-    const float p_top = y + 1 < ny ? ld(P[c + nx]) : 0.f;
-    const float p_bottom = y > 0 ? ld(P[c - nx]) : 0.f;
-    const float p_right = x + 1 < nx ? ld(P[c + 1]) : 0.f;
-    const float p_left = x > 0 ? ld(P[c - 1]) : 0.f;
     float p_sum = p_top * f_top + p_bottom * f_bottom;
     p_sum = p_sum + p_right * f_right;
     p_sum = p_sum + p_left * f_left;
     if constexpr (DIM == 3) {
-        const float p_front = z + 1 < nz ? ld(P[c + nx * ny]) : 0.f;
-        const float p_back = z > 0 ? ld(P[c - nx * ny]) : 0.f;
         p_sum = p_sum + p_front * f_front;
         p_sum = p_sum + p_back * f_back;
     }
     float pn;
     if constexpr (L0) pn = (p_sum - a.rho_h * a.div0[c] / a.dt) / f_sum;
-    else pn = (p_sum - ld(a.r[c]) * a.hh) / f_sum;
+    else pn = (p_sum - r_c * a.hh) / f_sum;
     a.p[c] = st<T>(rnd<R>(pn));
 }
 
@@ -147,7 +182,7 @@ int launch_smooth(ss_sim* s, const StepConsts& c, int L, int iterations, int qui
 // ------------------------------------------------------------------ residual
 // compute_residual.comp:77-130 (2D :72-117): r = b - (sum_f p_nb - f_sum p)/h^2,
 // out of grid = solid; level 0 takes b = rho*div/(dt*h).
-template <int DIM, bool L0, typename T = float>
+template <int DIM, bool L0, typename T = float, bool CG = false>
 SS_D float residual_cell(const MGArgsT<T>& a, int x, int y, int z) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int c = idx3(x, y, z, nx, ny);
@@ -176,36 +211,33 @@ SS_D float residual_cell(const MGArgsT<T>& a, int x, int y, int z) {
         }
     }
     const T* P = a.p;
-    const float p_top = y + 1 < ny ? ld(P[c + nx]) : 0.f;
-    const float p_bottom = y > 0 ? ld(P[c - nx]) : 0.f;
-    const float p_right = x + 1 < nx ? ld(P[c + 1]) : 0.f;
-    const float p_left = x > 0 ? ld(P[c - 1]) : 0.f;
+    const float p_top = y + 1 < ny ? ldv<CG>(P + c + nx) : 0.f;
+    const float p_bottom = y > 0 ? ldv<CG>(P + c - nx) : 0.f;
+    const float p_right = x + 1 < nx ? ldv<CG>(P + c + 1) : 0.f;
+    const float p_left = x > 0 ? ldv<CG>(P + c - 1) : 0.f;
     float p_sum = p_top * f_top + p_bottom * f_bottom;
     p_sum = p_sum + p_right * f_right;
     p_sum = p_sum + p_left * f_left;
     float f_sum = f_top + f_bottom + f_right + f_left;
     if constexpr (DIM == 3) {
-        const float p_front = z + 1 < nz ? ld(P[c + nx * ny]) : 0.f;
-        const float p_back = z > 0 ? ld(P[c - nx * ny]) : 0.f;
+        const float p_front = z + 1 < nz ? ldv<CG>(P + c + nx * ny) : 0.f;
+        const float p_back = z > 0 ? ldv<CG>(P + c - nx * ny) : 0.f;
         p_sum = p_sum + p_front * f_front;
         p_sum = p_sum + p_back * f_back;
         f_sum = f_sum + f_front + f_back;
     }
     float old;
     if constexpr (L0) old = a.rho * a.div0r[c] / a.dt_h;
-    else old = ld(a.r[c]);
-    return old - (p_sum - f_sum * ld(P[c])) / a.hh;
+    else old = ldv<CG>(a.r + c);
+    return old - (p_sum - f_sum * ldv<CG>(P + c)) / a.hh;
 }
 
 // One thread per coarse cell: residual of its 2^DIM children (written in place
 // when WRITE_FINE, the reference's in-place residual), then restrict_residual
 // (restrict_residual.comp:40-64, 2D :40-59) into the next level when
 // WRITE_COARSE.  The grid also covers the fine cells left over by odd sizes.
-template <int DIM, bool L0, bool WRITE_FINE, bool WRITE_COARSE, typename T = float>
-__global__ void __launch_bounds__(256) k_residual_restrict(MGArgsT<T> a, T* __restrict__ rc, int cx, int cy, int cz) {
-    const int X = blockIdx.x * blockDim.x + threadIdx.x;
-    const int Y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int Z = blockIdx.z * blockDim.z + threadIdx.z;
+template <int DIM, bool L0, bool WRITE_FINE, bool WRITE_COARSE, typename T = float, bool CG = false>
+SS_D void residual_restrict_cell(const MGArgsT<T>& a, T* __restrict__ rc, int cx, int cy, int cz, int X, int Y, int Z) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int x0 = 2 * X, y0 = 2 * Y, z0 = DIM == 3 ? 2 * Z : 0;
     if (x0 >= nx || y0 >= ny || z0 >= nz) return;
@@ -219,7 +251,7 @@ __global__ void __launch_bounds__(256) k_residual_restrict(MGArgsT<T> a, T* __re
                 const int x = x0 + dx, y = y0 + dy, z = z0 + dz;
                 float res = 0.f;
                 if (x < nx && y < ny && z < nz) {
-                    res = residual_cell<DIM, L0, T>(a, x, y, z);
+                    res = residual_cell<DIM, L0, T, CG>(a, x, y, z);
                     if constexpr (WRITE_FINE) {
                         a.r[idx3(x, y, z, nx, ny)] = st<T>(res);
                         res = rnd<T>(res);
@@ -240,6 +272,13 @@ __global__ void __launch_bounds__(256) k_residual_restrict(MGArgsT<T> a, T* __re
             rc[idx3(X, Y, Z, cx, cy)] = st<T>(out);
         }
     }
+}
+
+template <int DIM, bool L0, bool WRITE_FINE, bool WRITE_COARSE, typename T = float>
+__global__ void __launch_bounds__(256) k_residual_restrict(MGArgsT<T> a, T* __restrict__ rc, int cx, int cy, int cz) {
+    residual_restrict_cell<DIM, L0, WRITE_FINE, WRITE_COARSE, T>(a, rc, cx, cy, cz, blockIdx.x * blockDim.x + threadIdx.x,
+                                                                 blockIdx.y * blockDim.y + threadIdx.y,
+                                                                 blockIdx.z * blockDim.z + threadIdx.z);
 }
 
 template <int DIM, bool L0>
@@ -309,12 +348,9 @@ int launch_restrict(ss_sim* s, int L, cudaStream_t st) {
 // --------------------------------------------------------------- prolongation
 // prolong_pressure.comp:39-51: p_L += GL_LINEAR, CLAMP_TO_EDGE sample of
 // p_{L+1} at the fine cell centre, on every cell.
-template <int DIM, typename T = float>
-__global__ void __launch_bounds__(256) k_prolong(T* __restrict__ p, int ax, int ay, int az,
-                                                 const T* __restrict__ pc, int cx, int cy, int cz) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+template <int DIM, typename T = float, bool CG = false>
+SS_D void prolong_cell(T* __restrict__ p, int ax, int ay, int az, const T* __restrict__ pc, int cx, int cy, int cz,
+                       int x, int y, int z) {
     if (x >= ax || y >= ay || z >= az) return;
     const float tx = (((float)x + 0.5f) / (float)ax) * (float)cx - 0.5f;
     const float ty = (((float)y + 0.5f) / (float)ay) * (float)cy - 0.5f;
@@ -325,22 +361,29 @@ __global__ void __launch_bounds__(256) k_prolong(T* __restrict__ p, int ax, int 
     const int ya = min(max(y0, 0), cy - 1), yb = min(max(y0 + 1, 0), cy - 1);
     float s;
     if constexpr (DIM == 2) {
-        s = lerp_(lerp_(ld(pc[idx3(xa, ya, 0, cx, cy)]), ld(pc[idx3(xb, ya, 0, cx, cy)]), wx),
-                  lerp_(ld(pc[idx3(xa, yb, 0, cx, cy)]), ld(pc[idx3(xb, yb, 0, cx, cy)]), wx), wy);
+        s = lerp_(lerp_(ldv<CG>(&pc[idx3(xa, ya, 0, cx, cy)]), ldv<CG>(&pc[idx3(xb, ya, 0, cx, cy)]), wx),
+                  lerp_(ldv<CG>(&pc[idx3(xa, yb, 0, cx, cy)]), ldv<CG>(&pc[idx3(xb, yb, 0, cx, cy)]), wx), wy);
     } else {
         const float tz = (((float)z + 0.5f) / (float)az) * (float)cz - 0.5f;
         const float fz = floorf(tz);
         const int z0 = (int)fz;
         const float wz = tz - fz;
         const int za = min(max(z0, 0), cz - 1), zb = min(max(z0 + 1, 0), cz - 1);
-        const float c0 = lerp_(lerp_(ld(pc[idx3(xa, ya, za, cx, cy)]), ld(pc[idx3(xb, ya, za, cx, cy)]), wx),
-                               lerp_(ld(pc[idx3(xa, yb, za, cx, cy)]), ld(pc[idx3(xb, yb, za, cx, cy)]), wx), wy);
-        const float c1 = lerp_(lerp_(ld(pc[idx3(xa, ya, zb, cx, cy)]), ld(pc[idx3(xb, ya, zb, cx, cy)]), wx),
-                               lerp_(ld(pc[idx3(xa, yb, zb, cx, cy)]), ld(pc[idx3(xb, yb, zb, cx, cy)]), wx), wy);
+        const float c0 = lerp_(lerp_(ldv<CG>(&pc[idx3(xa, ya, za, cx, cy)]), ldv<CG>(&pc[idx3(xb, ya, za, cx, cy)]), wx),
+                               lerp_(ldv<CG>(&pc[idx3(xa, yb, za, cx, cy)]), ldv<CG>(&pc[idx3(xb, yb, za, cx, cy)]), wx), wy);
+        const float c1 = lerp_(lerp_(ldv<CG>(&pc[idx3(xa, ya, zb, cx, cy)]), ldv<CG>(&pc[idx3(xb, ya, zb, cx, cy)]), wx),
+                               lerp_(ldv<CG>(&pc[idx3(xa, yb, zb, cx, cy)]), ldv<CG>(&pc[idx3(xb, yb, zb, cx, cy)]), wx), wy);
         s = lerp_(c0, c1, wz);
     }
     const int i = idx3(x, y, z, ax, ay);
-    p[i] = st<T>(ld(p[i]) + s);
+    p[i] = st<T>(ldv<CG>(p + i) + s);
+}
+
+template <int DIM, typename T = float>
+__global__ void __launch_bounds__(256) k_prolong(T* __restrict__ p, int ax, int ay, int az,
+                                                 const T* __restrict__ pc, int cx, int cy, int cz) {
+    prolong_cell<DIM, T>(p, ax, ay, az, pc, cx, cy, cz, blockIdx.x * blockDim.x + threadIdx.x,
+                         blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z * blockDim.z + threadIdx.z);
 }
 
 int launch_prolong(ss_sim* s, int L, cudaStream_t st) {
@@ -858,6 +901,181 @@ int coarse_residual_restrict(ss_sim* s, const StepConsts& c, int L, int prec, cu
 int coarse_prolong(ss_sim* s, int L, int prec, cudaStream_t st) {
     if (prec == SS_PREC_MIXED) return coarse_prolong_t<__half>(s, L, (__half*)s->cp[L], (const __half*)s->cp[L + 1], st);
     return coarse_prolong_t<__nv_bfloat16>(s, L, (__nv_bfloat16*)s->cp[L], (const __nv_bfloat16*)s->cp[L + 1], st);
+}
+
+// ------------------------------------------------- cooperative coarse legs
+// Opt-in (SMOKESIM_COOP_CELLS): the levels between the first with at most
+// coop_cells cells and the bottom solve, where a launch per operator costs
+// about as much as the operator.  Each V-cycle leg of those levels runs as ONE
+// cooperative launch
+// (all blocks co-resident) whose phases - half-sweeps, residual + restriction
+// (with the clearing of the next level's correction), prolongation - are
+// separated by a grid barrier; the per-cell operators are the ones above,
+// with level reads through L2 (other blocks wrote them since this SM may
+// have cached them).  Down leg: pre-smoothing and restriction of each level
+// first .. bottom-1; the bottom kernel runs between the legs; up leg:
+// prolongation and post-smoothing back to level first.  Measured on the
+// 256^3 step it is slower than the graph of separate launches (levels 64^3
+// and 32^3: 91 us against 69 us a V-cycle; with 128^3: 281 us against
+// 166 us): the grid-stride phases have fewer threads in flight than a
+// launch per operator, and a grid barrier costs about what a launch inside
+// a CUDA graph does.  So it is off by default.
+template <typename T>
+struct CoopLevel {
+    MGArgsT<T> sm;   // smoother operands (out-of-grid rule of the smoother)
+    MGArgsT<T> rs;   // residual operands (rule of the residual)
+};
+
+template <typename T>
+struct CoopArgs {
+    CoopLevel<T> lv[SS_MAX_LEVELS];
+    int first, last;        // levels first .. last-1 (last: the bottom level)
+    int n_pre, n_post;
+    unsigned int* bar;      // arrivals, generation
+    int* err;               // bit 1: a grid barrier gave up
+};
+
+// Grid barrier over gridDim.x co-resident blocks (generation counting).  The
+// wait is bounded (about a second); a block that gives up sets the error word
+// and reports false, and every block then stops at its next barrier.
+SS_D bool coop_sync(unsigned int* bar, int* err) {
+    __syncthreads();
+    __shared__ int ok_s;
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = bar + 1;
+        const unsigned int g = *gen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            for (int k = 0; *gen == g; ++k) {
+                if (k > (1 << 23)) {
+                    ok = 0;
+                    atomicOr(err, 2);
+                    break;
+                }
+                if (k > 16) __nanosleep(100);
+            }
+        }
+        __threadfence();
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+template <int DIM, typename T>
+SS_D void coop_smooth(const MGArgsT<T>& a, int parity, int gt, int gs) {
+    const int hx = (a.nx + 1) / 2;
+    const int items = hx * a.ny * a.nz;
+    for (int i = gt; i < items; i += gs) {
+        const int xi = i % hx, t = i / hx, y = t % a.ny, z = t / a.ny;
+        const int x = 2 * xi + ((y + z + parity) & 1);
+        if (x < a.nx) smooth_cell<DIM, false, T, T, true>(a, x, y, z);
+    }
+}
+
+template <int DIM, bool DOWN, typename T>
+__global__ void __launch_bounds__(256) k_coarse_coop(CoopArgs<T> A) {
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    if constexpr (DOWN) {
+        for (int L = A.first; L < A.last; ++L) {
+            const CoopLevel<T>& lv = A.lv[L];
+            for (int it = 0; it < 2 * A.n_pre; ++it) {
+                coop_smooth<DIM, T>(lv.sm, it & 1, gt, gs);
+                if (!coop_sync(A.bar, A.err)) return;
+            }
+            const MGArgsT<T>& nx = A.lv[L + 1].sm;
+            const int hx = (lv.rs.nx + 1) / 2, hy = (lv.rs.ny + 1) / 2, hz = DIM == 3 ? (lv.rs.nz + 1) / 2 : 1;
+            for (int i = gt; i < hx * hy * hz; i += gs) {
+                const int X = i % hx, t = i / hx, Y = t % hy, Z = t / hy;
+                residual_restrict_cell<DIM, false, false, true, T, true>(lv.rs, nx.r, nx.nx, nx.ny, nx.nz, X, Y, Z);
+            }
+            const int nc = nx.nx * nx.ny * nx.nz;
+            for (int i = gt; i < nc; i += gs) nx.p[i] = st<T>(0.f);
+            if (L + 1 < A.last && !coop_sync(A.bar, A.err)) return;
+        }
+    } else {
+        for (int L = A.last - 1; L >= A.first; --L) {
+            const CoopLevel<T>& lv = A.lv[L];
+            const MGArgsT<T>& nx = A.lv[L + 1].sm;
+            const int nf = lv.sm.nx * lv.sm.ny * lv.sm.nz;
+            for (int i = gt; i < nf; i += gs) {
+                const int x = i % lv.sm.nx, t = i / lv.sm.nx, y = t % lv.sm.ny, z = t / lv.sm.ny;
+                prolong_cell<DIM, T, true>(lv.sm.p, lv.sm.nx, lv.sm.ny, lv.sm.nz, nx.p, nx.nx, nx.ny, nx.nz, x, y, z);
+            }
+            for (int it = 0; it < 2 * A.n_post; ++it) {
+                if (!coop_sync(A.bar, A.err)) return;
+                coop_smooth<DIM, T>(lv.sm, it & 1, gt, gs);
+            }
+            if (L > A.first && !coop_sync(A.bar, A.err)) return;
+        }
+    }
+}
+
+// first level of the cooperative legs, or -1 (none: every level runs its own launches)
+int coarse_coop_first(const ss_sim* s) {
+    if (s->coop_cells <= 0 || s->bottom >= s->levels) return -1;
+    for (int L = 1; L < s->bottom && L < s->levels - 1; ++L)
+        if ((long long)s->lv[L].n[0] * s->lv[L].n[1] * s->lv[L].n[2] <= s->coop_cells) return L;
+    return -1;
+}
+
+template <int DIM, bool DOWN, typename T>
+static int launch_coop_t(ss_sim* s, const CoopArgs<T>& A, cudaStream_t st) {
+    static int blocks = 0;
+    if (blocks == 0) {
+        int dev = 0, sms = 0, occ = 0;
+        TRY_CUDA_MG(cudaGetDevice(&dev), "cudaGetDevice");
+        TRY_CUDA_MG(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+        TRY_CUDA_MG(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_coarse_coop<DIM, DOWN, T>, 256, 0),
+                    "occupancy");
+        if (occ < 1) return set_error(SS_E_UNSUPPORTED, "cooperative coarse kernel does not fit an SM");
+        // two blocks an SM: enough threads for a 64^3 half-sweep, few arrivals per barrier
+        blocks = sms * std::min(occ, 2);
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    s->nlaunch += 1;
+    return check_cuda(cudaLaunchKernelEx(&cfg, k_coarse_coop<DIM, DOWN, T>, A), "k_coarse_coop");
+}
+
+template <typename T>
+static int launch_coarse_coop_t(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, bool down, T* const* cp,
+                                T* const* cr, cudaStream_t st) {
+    const int first = coarse_coop_first(s);
+    if (first < 1) return set_error(SS_E_INVALID, "no cooperative coarse levels");
+    CoopArgs<T> A{};
+    A.first = first;
+    A.last = s->bottom;
+    A.n_pre = mg.n_pre;
+    A.n_post = mg.n_post;
+    A.bar = s->coop_bar;
+    A.err = s->d_err;
+    for (int L = first; L <= s->bottom; ++L) {
+        A.lv[L].sm = mg_args_t<T>(s, c, L, smooth_oob(s, 0), cp[L], cr[L]);
+        A.lv[L].rs = mg_args_t<T>(s, c, L, resid_oob(s, 0), cp[L], cr[L]);
+    }
+    if (s->dim == 3) return down ? launch_coop_t<3, true, T>(s, A, st) : launch_coop_t<3, false, T>(s, A, st);
+    return down ? launch_coop_t<2, true, T>(s, A, st) : launch_coop_t<2, false, T>(s, A, st);
+}
+
+int launch_coarse_coop(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int prec, bool down, cudaStream_t st) {
+    if (prec == SS_PREC_MIXED)
+        return launch_coarse_coop_t<__half>(s, c, mg, down, (__half* const*)s->cp, (__half* const*)s->cr, st);
+    return launch_coarse_coop_t<__nv_bfloat16>(s, c, mg, down, (__nv_bfloat16* const*)s->cp,
+                                               (__nv_bfloat16* const*)s->cr, st);
 }
 
 int coarse_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, int prec, cudaStream_t st) {

@@ -110,6 +110,8 @@ struct ss_sim {
     ss_stats st{};
     long long nlaunch = 0;     // kernels launched since the counter was reset
     int* d_err = nullptr;      // device error word: bit 0 = a bounded barrier wait gave up
+    unsigned int* coop_bar = nullptr;   // grid barrier of the cooperative coarse legs: arrivals, generation
+    long long coop_cells = 0;  // coarse levels of at most this many cells run in the cooperative legs (0: none)
     int use_tma = 1;           // TMA tile loads: 1 coarse-level sweeps, 2 also level 0 (where the layout allows)
     // The multigrid part of a solve recorded once as a CUDA graph and replayed
     // (api.cpp, run_graph): slot 0 fixed-count FP32 V-cycles, 1 one FP32
@@ -204,6 +206,8 @@ int run_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* saves);
 bool rb_tma_supported(const ss_sim* s);
 int launch_rb_smooth_tma(ss_sim* s, float* pc, const float* po, const float* rhs, const uint8_t* mask, int colour,
                          cudaStream_t st);
+int coarse_coop_first(const ss_sim* s);
+int launch_coarse_coop(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int prec, bool down, cudaStream_t st);
 int launch_vorticity_field(ss_sim* s, const StepConsts& c, const float* const vel[3], float* out, cudaStream_t st);
 
 // adjoint kernels (k_adjoint.cu)

@@ -40,6 +40,24 @@ def test_mixed_solve_bitwise(name, dim, n, nch, enc, mc, prec):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("coop", ["0", "4096", "100000000"])
+@pytest.mark.parametrize("name,dim,n,nch,enc,mc", [("3d_l1", 3, (64, 48, 48), 1, 1, 4),
+                                                   ("3d_open_odd", 3, (66, 50, 38), 1, 0, 4),
+                                                   ("2d_quad", 2, (128, 96, 1), 1, 1, 4)])
+def test_mixed_cooperative_coarse_legs(monkeypatch, coop, name, dim, n, nch, enc, mc):
+    """Coarse levels of at most SMOKESIM_COOP_CELLS cells run as two
+    cooperative launches per V-cycle (grid barriers between the operators);
+    0 keeps one launch per operator.  Same bits either way."""
+    monkeypatch.setenv("SMOKESIM_COOP_CELLS", coop)
+    g, o = make_pair(dim, n, nch, enc, seed=37, min_coarse=mc)
+    p = scene.workload_params(ref_quirks=0, precision=abi.PREC_MIXED, n_vcycles=3, n_coarse=12)
+    for k in range(2):
+        g.step(p)
+        o.step(p)
+        assert_same(g, o, dim, f"cooperative legs {coop} step {k}")
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_MIXED_BF16])
 def test_mixed_tolerance_matches_oracle(prec):
     g, o = make_pair(3, (32, 24, 20), 1, 1, seed=3, min_coarse=4)
