@@ -404,14 +404,17 @@ def main():
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
+        vc = 0
         for _ in range(args.steps):
             step1(sim, p)
-            _ = sim.stats()
+            vc += sim.stats().vcycles
         torch.cuda.synchronize()
         e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
+        # these steps continue the timed run's simulation, so the state (and
+        # the refinement steps a step needs) differs from the timed steps'
         e2e = {"value": job_rate(world, cells, args.steps, e2e_s * 1e3), "unit": UNIT,
                "h2d_bytes_per_step": C.sizeof(abi.Emitter) * len(sc["emitters"]),
-               "d2h_bytes_per_step": 8 * 8}
+               "d2h_bytes_per_step": 8 * 8, "vcycles_mean": vc / max(1, args.steps)}
 
         # roofline of the dominant kernel: the level-0 red-black smoother
         # (k_rb_smooth4, one colour per launch on the colour-split arrays).
