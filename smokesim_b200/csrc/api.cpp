@@ -94,6 +94,7 @@ static void free_sim(ss_sim* s) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
     cudaFree(s->d_scale);
     cudaFree(s->red.partial_max);
+    cudaFree(s->red.ticket);
     for (int l = 0; l < SS_MAX_LEVELS; ++l) { cudaFree(s->cp[l]); cudaFree(s->cr[l]); }
     cudaFree(s->rhs_r);
     cudaFree(s->red.partial);
@@ -745,6 +746,10 @@ static int ensure_mixed(ss_sim* s, int prec, cudaStream_t st) {
     }
     if (!s->red.partial_max)
         CU(cudaMalloc((void**)&s->red.partial_max, (size_t)s->red.max_blocks * sizeof(double)), "cudaMalloc");
+    if (!s->red.ticket) {
+        CU(cudaMalloc((void**)&s->red.ticket, sizeof(unsigned int)), "cudaMalloc");
+        CU(cudaMemsetAsync(s->red.ticket, 0, sizeof(unsigned int), st), "ticket");
+    }
     if (!s->d_scale) {
         CU(cudaMalloc((void**)&s->d_scale, 2 * sizeof(float)), "cudaMalloc");
         const float one[2] = {1.f, 1.f};
@@ -798,7 +803,9 @@ static int v_cycle_mixed(ss_sim* s, const StepConsts& c, const ss_mg_schedule& m
 // Mixed-precision projection: iterative refinement of the FP64 pressure with
 // FP32 V-cycles on the FP64 residual (k_mixed.cu).  Each refinement step
 // counts as one V-cycle in the statistics.
-static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts& c, cudaStream_t st) {
+// defer_p0: the caller's FP64 velocity update writes the FP32 pressure copy
+static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts& c, cudaStream_t st,
+                                bool defer_p0 = false) {
     const ss_mg_schedule& mg = p->mg;
     if (mg.ref_quirks) return set_error(SS_E_INVALID, "the mixed-precision solve runs the corrected operators (ref_quirks = 0)");
     TRY(ensure_mixed(s, mg.precision, st));
@@ -849,7 +856,7 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
             break;
         }
     }
-    TRY(launch_p0_from_p64(s, st));
+    if (!defer_p0) TRY(launch_p0_from_p64(s, st));
     if (stats) {
         s->st.div_before = db;
         s->st.residual = res;
@@ -860,9 +867,10 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
 }
 
 // multigrid_pressure_solve (common/physics/grid.c:173-175)
-static int pressure_solve(ss_sim* s, const ss_params* p, const StepConsts& c, cudaStream_t st) {
+static int pressure_solve(ss_sim* s, const ss_params* p, const StepConsts& c, cudaStream_t st,
+                          bool defer_p0 = false) {
     const ss_mg_schedule& mg = p->mg;
-    if (mg.precision != SS_PREC_FP32) return pressure_solve_mixed(s, p, c, st);
+    if (mg.precision != SS_PREC_FP32) return pressure_solve_mixed(s, p, c, st, defer_p0);
     s->p64_valid = 0;
     const bool tol_mode = mg.tol > 0.0;
     const bool stats = p->collect_stats || tol_mode;
@@ -952,13 +960,21 @@ static int do_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* sv
     }
     if (sv) TRY(save_vel(s, sv->force_vel, st));
     if (m & SS_STAGE_APPLY_VORTICITY) TRY(launch_vorticity(s, c, st));
+    // a mixed solve followed by the update leaves the FP32 pressure copy to
+    // the update kernel, which reads the FP64 pressure anyway
+    const bool defer_p0 = (m & SS_STAGE_RESOLVE_PRESSURE) && (m & SS_STAGE_UPDATE_VELOCITIES) &&
+                          p->mg.precision != SS_PREC_FP32;
     if (m & SS_STAGE_RESOLVE_PRESSURE) {
-        TRY(pressure_solve(s, p, c, st));
+        TRY(pressure_solve(s, p, c, st, defer_p0));
         if (sv) sv->vcycles = s->st.vcycles;
     }
     if (m & SS_STAGE_UPDATE_VELOCITIES) {
-        if (p->mg.precision != SS_PREC_FP32 && s->p64_valid) TRY(launch_update_velocities_p64(s, c, st));
-        else TRY(launch_update_velocities(s, c, st));
+        if (p->mg.precision != SS_PREC_FP32 && s->p64_valid) {
+            TRY(launch_update_velocities_p64(s, c, st, defer_p0 ? s->p[0] : nullptr));
+        } else {
+            if (defer_p0) TRY(launch_p0_from_p64(s, st));
+            TRY(launch_update_velocities(s, c, st));
+        }
         if ((m & SS_STAGE_RESOLVE_PRESSURE) && (p->collect_stats || p->mg.tol > 0.0)) {
             TRY(launch_divergence(s, false, SLOT_DIV_AFTER, st));
             TRY(read_slots(s, st));

@@ -626,8 +626,11 @@ int launch_vorticity_field(ss_sim* s, const StepConsts& c, const float* const ve
 // flag of the cell below (z-1) carry over from the previous plane.
 constexpr int kUpdPlanes = 8;
 
+// p0_out (FP64 pressure only): also store each cell's pressure rounded to
+// FP32 - the pressure field of the API - in the same pass.
 template <int DIM, typename P = float>
-__global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const P* __restrict__ p, double k64 = 0.0) {
+__global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const P* __restrict__ p, double k64 = 0.0,
+                                                         float* __restrict__ p0_out = nullptr) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
@@ -644,6 +647,7 @@ __global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const P* _
         const bool in = inxy && z < nz;
         const P pc = in ? __ldg(p + idx3(x, y, z, nx, ny)) : P(0);
         const bool sc = in && (a.flags[idx3(x, y, z, nx, ny)] & F_SOLID);
+        if (p0_out && in) p0_out[idx3(x, y, z, nx, ny)] = (float)pc;
 #pragma unroll
         for (int comp = 0; comp < DIM; ++comp) {
             const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
@@ -679,13 +683,13 @@ int launch_update_velocities(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     return check_cuda(cudaGetLastError(), "k_update_velocity");
 }
 
-int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st) {
+int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st, float* p0_out) {
     FluidArgs a = fluid_args(s, c);
     dim3 b(32, 8, 1);
     dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? (s->nz + kUpdPlanes) / kUpdPlanes : 1, b);
     const double k64 = -(double)c.dt / ((double)c.rho * (double)s->h);
-    if (s->dim == 3) k_update_velocity<3, double><<<g, b, 0, st>>>(a, s->p64, k64);
-    else k_update_velocity<2, double><<<g, b, 0, st>>>(a, s->p64, k64);
+    if (s->dim == 3) k_update_velocity<3, double><<<g, b, 0, st>>>(a, s->p64, k64, p0_out);
+    else k_update_velocity<2, double><<<g, b, 0, st>>>(a, s->p64, k64, p0_out);
     for (int d = 0; d < s->dim; ++d) s->vi[d] ^= 1;
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_update_velocity<p64>");
@@ -693,36 +697,41 @@ int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st
 
 // ------------------------------------------------------------ smoke advection
 // advect_smoke (shaders3d/compute/advect_smoke.comp:55-72; 2D :51-68).
+// A thread takes kSmokePlanes cells up z (fewer, longer-lived blocks).
+constexpr int kSmokePlanes = 4;
+
 template <int DIM>
 __global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z * blockDim.z + threadIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    if (x >= nx || y >= ny || z >= nz) return;
-    const int c = idx3(x, y, z, nx, ny);
+    if (x >= nx || y >= ny) return;
+    const int zb = blockIdx.z * kSmokePlanes, ze = min(zb + kSmokePlanes, nz);
     const size_t ncell = (size_t)nx * ny * nz;
-    // the cell's faces always exist: loaded before the solid test
-    float vel[3];
-    vel_at_centre<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
-    if (a.flags[c] & F_SOLID) {
-        for (int ch = 0; ch < a.nch; ++ch) a.dens_o[ch * ncell + c] = 0.f;
-        a.temp_o[c] = a.c.t_amb;
-        return;
+    for (int z = zb; z < ze; ++z) {
+        const int c = idx3(x, y, z, nx, ny);
+        // the cell's faces always exist: loaded before the solid test
+        float vel[3];
+        vel_at_centre<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+        if (a.flags[c] & F_SOLID) {
+            for (int ch = 0; ch < a.nch; ++ch) a.dens_o[ch * ncell + c] = 0.f;
+            a.temp_o[c] = a.c.t_amb;
+            continue;
+        }
+        const float gx = (float)x + 0.5f, gy = (float)y + 0.5f, gz = DIM == 3 ? (float)z + 0.5f : 0.f;
+        const float cfl = a.c.cfl;
+        const float bx = gx - vel[0] * cfl, by = gy - vel[1] * cfl, bz = gz - vel[2] * cfl;
+        const Taps t = make_taps<DIM>(nx, ny, nz, bx - 0.5f, by - 0.5f, bz - 0.5f);
+        for (int ch = 0; ch < a.nch; ++ch)
+            a.dens_o[ch * ncell + c] = sample_taps_fast<DIM>(a.dens + ch * ncell, nx, ny, nz, t, 0.f);
+        a.temp_o[c] = sample_taps_fast<DIM>(a.temp, nx, ny, nz, t, a.c.t_amb);
     }
-    const float gx = (float)x + 0.5f, gy = (float)y + 0.5f, gz = DIM == 3 ? (float)z + 0.5f : 0.f;
-    const float cfl = a.c.cfl;
-    const float bx = gx - vel[0] * cfl, by = gy - vel[1] * cfl, bz = gz - vel[2] * cfl;
-    const Taps t = make_taps<DIM>(nx, ny, nz, bx - 0.5f, by - 0.5f, bz - 0.5f);
-    for (int ch = 0; ch < a.nch; ++ch)
-        a.dens_o[ch * ncell + c] = sample_taps_fast<DIM>(a.dens + ch * ncell, nx, ny, nz, t, 0.f);
-    a.temp_o[c] = sample_taps_fast<DIM>(a.temp, nx, ny, nz, t, a.c.t_amb);
 }
 
 int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     FluidArgs a = fluid_args(s, c);
     dim3 b(32, 8, 1);
-    dim3 g = grid_for(s->nx, s->ny, s->nz, b);
+    dim3 g = grid_for(s->nx, s->ny, (s->nz + kSmokePlanes - 1) / kSmokePlanes, b);
     if (s->dim == 3) k_advect_smoke<3><<<g, b, 0, st>>>(a);
     else k_advect_smoke<2><<<g, b, 0, st>>>(a);
     s->si ^= 1;

@@ -80,7 +80,8 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
     const double* __restrict__ p_in, const float* __restrict__ e, double* __restrict__ p_out,
     const float* __restrict__ div0, const uint8_t* __restrict__ fmask, int nx, int ny, int nz, double k,
     double inv_k, double inv_khh, float* __restrict__ rhs_s, float* __restrict__ rhs_r, double* __restrict__ psum,
-    double* __restrict__ pmax) {
+    double* __restrict__ pmax, unsigned int* __restrict__ ticket, double* __restrict__ out, int slot,
+    float* __restrict__ scale) {
     __shared__ double sP[2][kIrTY + 2][kIrTX + 2];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kIrTX * ty;
     const int x0 = blockIdx.x * kIrTX, y0 = blockIdx.y * kIrTY;
@@ -168,32 +169,50 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
     }
     block_sum_max(acc, amax, psum + blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
                   pmax + blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
-}
-
-// Also derives the power-of-two scale of the coarse storage from max|rho|:
-// with max|rho| / (k h^2) = m * 2^e (m in [0.5, 1)), the restricted residual
-// is multiplied by 2^-e (largest magnitude below 1) on its way to the FP16 /
-// BF16 level and the prolonged correction by 2^e on its way back.
-__global__ void k_reduce_max_final(const double* __restrict__ partial, int n, double* __restrict__ out, int slot,
-                                   double inv_khh, float* __restrict__ scale) {
-    double m = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, partial[i]);
-    __shared__ double sh[1024];
-    sh[threadIdx.x] = m;
+    // The last block to finish folds every block's partials: each thread sums
+    // a fixed stride of them, then a fixed tree - the same order whichever
+    // block is last.  It writes the residual norm (slot >= 0), max |rho| and
+    // the power-of-two scale of the coarse storage derived from it - with
+    // max|rho| / (k h^2) = m * 2^e (m in [0.5, 1)) the restricted residual is
+    // multiplied by 2^-e on its way to the FP16 / BF16 level and the prolonged
+    // correction by 2^e on its way back - and re-arms the ticket for the next
+    // launch.
+    const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
+    __shared__ bool last;
+    if (tid == 0) {
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == nblocks - 1;
+    }
     __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+    if (!last) return;
+    double s = 0.0, mx = 0.0;
+    for (unsigned int i = tid; i < nblocks; i += kIrTX * kIrTY) {
+        s += __ldcg(psum + i);
+        mx = fmax(mx, __ldcg(pmax + i));
+    }
+    __shared__ double fs[kIrTX * kIrTY], fm[kIrTX * kIrTY];
+    fs[tid] = s;
+    fm[tid] = mx;
+    __syncthreads();
+    for (int o = kIrTX * kIrTY / 2; o > 0; o >>= 1) {
+        if (tid < o) {
+            fs[tid] += fs[tid + o];
+            fm[tid] = fmax(fm[tid], fm[tid + o]);
+        }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        out[slot] = sh[0];
+    if (tid == 0) {
+        if (slot >= 0) out[slot] = fs[0];
+        out[SLOT_AMAX] = fm[0];
         int e = 0;
-        frexp(sh[0] * inv_khh, &e);
+        frexp(fm[0] * inv_khh, &e);
         e = max(-100, min(100, e));
         scale[0] = (float)ldexp(1.0, -e);
         scale[1] = (float)ldexp(1.0, e);
+        *ticket = 0u;
     }
 }
+
 
 // p64 += e at every fluid cell (e: the correction, colour-split FP32)
 template <int DIM>
@@ -230,7 +249,8 @@ int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate
     const double inv_k = 1.0 / k;
     const double inv_khh = 1.0 / (k * (double)s->lv[0].hh);
 #define IR_ARGS(ACC) s->p64, s->p_alt[0], s->p64b, s->div0, s->fmask, s->nx, s->ny, s->nz, k, inv_k, inv_khh, \
-                     s->rhs_s, s->rhs_r, s->red.partial, s->red.partial_max
+                     s->rhs_s, s->rhs_r, s->red.partial, s->red.partial_max, s->red.ticket, s->red.out, slot, \
+                     s->d_scale
     if (s->dim == 3) {
         if (accumulate) k_ir_residual<3, true><<<g, b, 0, st>>>(IR_ARGS(true));
         else k_ir_residual<3, false><<<g, b, 0, st>>>(IR_ARGS(false));
@@ -243,18 +263,9 @@ int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate
     int rc = check_cuda(cudaGetLastError(), "k_ir_residual");
     if (rc) return rc;
     // with accumulate the caller swaps s->p64 / s->p64b afterwards (the launch
-    // may be recorded into a graph and replayed, the swap is host state)
-    if (slot >= 0) {
-        rc = launch_reduce_final(s, nblocks, slot, st);
-        if (rc) return rc;
-    }
-    const double* in;
-    int n;
-    rc = reduce_stage1(s, s->red.partial_max, nblocks, true, &in, &n, st);
-    if (rc) return rc;
-    k_reduce_max_final<<<1, 1024, 0, st>>>(in, n, s->red.out, SLOT_AMAX, inv_khh, s->d_scale);
-    s->nlaunch += 1;
-    return check_cuda(cudaGetLastError(), "k_reduce_max_final");
+    // may be recorded into a graph and replayed, the swap is host state); the
+    // norms and the coarse scale are folded by the kernel's last block
+    return rc;
 }
 
 int launch_ir_accumulate(ss_sim* s, cudaStream_t st) {

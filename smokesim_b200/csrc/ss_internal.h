@@ -33,6 +33,7 @@ struct ReduceSlots {
     double* partial;      // per-block partial sums (device scratch)
     double* partial_max = nullptr;  // per-block maxima (mixed-precision solve)
     double* partial2 = nullptr;     // second-stage partials: sums, then maxima (2 * stage2 entries)
+    unsigned int* ticket = nullptr; // blocks finished in the refinement residual (the last one folds)
     int stage2 = 0;
     double* out;          // reduction results (device), SLOT_* below
     double* host;         // pinned mirror of out
@@ -186,7 +187,8 @@ int launch_p64_from_p0(ss_sim* s, cudaStream_t st);
 int launch_p0_from_p64(ss_sim* s, cudaStream_t st);
 int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate, cudaStream_t st);
 int launch_ir_accumulate(ss_sim* s, cudaStream_t st);
-int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st);
+// p0_out: when given, the FP32 copy of the FP64 pressure is written there too
+int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st, float* p0_out = nullptr);
 // first stage of a deterministic reduction over n per-block partials: sums
 // (or maxima) of consecutive groups of 1024; *res / *nres describe what is
 // left for a single final block (the input itself when n <= 1024)
