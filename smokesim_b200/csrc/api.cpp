@@ -262,6 +262,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     A((void**)&s->red.out, SLOT_COUNT * sizeof(double));
     A((void**)&s->d_err, sizeof(int));
     A((void**)&s->coop_bar, 2 * sizeof(unsigned int));
+    A((void**)&s->red.ticket, sizeof(unsigned int));
     if (rc == SS_OK) {
         cudaError_t e = cudaMallocHost((void**)&s->red.host, SLOT_COUNT * sizeof(double));
         if (e != cudaSuccess) rc = check_cuda(e, "cudaMallocHost");
@@ -284,6 +285,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     }
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->d_err, 0, sizeof(int), st), "memset");
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->coop_bar, 0, 2 * sizeof(unsigned int), st), "memset");
+    if (!rc) rc = check_cuda(cudaMemsetAsync(s->red.ticket, 0, sizeof(unsigned int), st), "memset");
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->div0, 0, s->ncell * 4, st), "memset");
     if (!rc && s->div0r != s->div0) rc = check_cuda(cudaMemsetAsync(s->div0r, 0, s->ncell * 4, st), "memset");
     if (!rc && s->rb_mask) rc = rb_init_vector_paths(s, st);
@@ -746,10 +748,7 @@ static int ensure_mixed(ss_sim* s, int prec, cudaStream_t st) {
     }
     if (!s->red.partial_max)
         CU(cudaMalloc((void**)&s->red.partial_max, (size_t)s->red.max_blocks * sizeof(double)), "cudaMalloc");
-    if (!s->red.ticket) {
-        CU(cudaMalloc((void**)&s->red.ticket, sizeof(unsigned int)), "cudaMalloc");
-        CU(cudaMemsetAsync(s->red.ticket, 0, sizeof(unsigned int), st), "ticket");
-    }
+
     if (!s->d_scale) {
         CU(cudaMalloc((void**)&s->d_scale, 2 * sizeof(float)), "cudaMalloc");
         const float one[2] = {1.f, 1.f};
@@ -975,15 +974,20 @@ static int do_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* sv
             if (defer_p0) TRY(launch_p0_from_p64(s, st));
             TRY(launch_update_velocities(s, c, st));
         }
-        if ((m & SS_STAGE_RESOLVE_PRESSURE) && (p->collect_stats || p->mg.tol > 0.0)) {
-            TRY(launch_divergence(s, false, SLOT_DIV_AFTER, st));
-            TRY(read_slots(s, st));
-            s->st.div_after = sqrt(s->red.host[SLOT_DIV_AFTER]);
-            s->st.rel_div = s->st.div_before > 0 ? s->st.div_after / s->st.div_before : 0.0;
-        }
     }
+    // divergence left by the projection (statistics): folded into the smoke
+    // advection, which loads the same faces, when that stage runs next
+    const bool div_after = (m & SS_STAGE_UPDATE_VELOCITIES) && (m & SS_STAGE_RESOLVE_PRESSURE) &&
+                           (p->collect_stats || p->mg.tol > 0.0);
+    const bool div_in_smoke = div_after && (m & SS_STAGE_ADVECT_SMOKE);
+    if (div_after && !div_in_smoke) TRY(launch_divergence(s, false, SLOT_DIV_AFTER, st));
     if (sv) TRY(save_vel(s, sv->proj_vel, st));
-    if (m & SS_STAGE_ADVECT_SMOKE) TRY(launch_advect_smoke(s, c, st));
+    if (m & SS_STAGE_ADVECT_SMOKE) TRY(launch_advect_smoke(s, c, st, div_in_smoke ? SLOT_DIV_AFTER : -1));
+    if (div_after) {
+        TRY(read_slots(s, st));
+        s->st.div_after = sqrt(s->red.host[SLOT_DIV_AFTER]);
+        s->st.rel_div = s->st.div_before > 0 ? s->st.div_after / s->st.div_before : 0.0;
+    }
     if (m & SS_STAGE_OBSTACLES) {
         if (scene_moving(s)) {
             obstacles_update(s, p->time_step);

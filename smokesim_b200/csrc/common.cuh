@@ -276,6 +276,19 @@ template <> SS_D __half st<__half>(float v) { return __float2half_rn(v); }
 template <> SS_D __nv_bfloat16 st<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 template <typename T> SS_D float rnd(float v) { return ld(st<T>(v)); }
 
+// Sum of n per-block partials by one block's threads, each
+// thread keeping eight independent accumulators so its L2 loads are in
+// flight together; the order depends only on n and the thread count.
+SS_D double fold_sum(const double* p, unsigned int n, unsigned int tid, unsigned int nt) {
+    double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    unsigned int i = tid;
+    for (; i + 7 * nt < n; i += 8 * nt) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] += __ldcg(p + i + k * nt);
+    }
+    for (; i < n; i += nt) a[0] += __ldcg(p + i);
+    return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+}
 // a float4 through the read-only path, and lane k of a float4
 SS_D float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 SS_D float f4(const float4& v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }

@@ -698,25 +698,61 @@ int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st
 // ------------------------------------------------------------ smoke advection
 // advect_smoke (shaders3d/compute/advect_smoke.comp:55-72; 2D :51-68).
 // A thread takes kSmokePlanes cells up z (fewer, longer-lived blocks).
+// With DIV the kernel also folds the squared divergence of the velocities it
+// advects with - the projected velocities - into the statistics slot `slot`
+// (the operator of k_divergence below, from the six faces already loaded
+// here); the last block to finish sums the blocks' partials in a fixed order.
 constexpr int kSmokePlanes = 4;
+SS_D double block_sum(double v);
 
-template <int DIM>
-__global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a) {
+struct DivFold {
+    double* partial;
+    unsigned int* ticket;
+    double* out;
+    int slot;
+};
+
+template <int DIM, bool DIV>
+__global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a, DivFold df) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    if (x >= nx || y >= ny) return;
     const int zb = blockIdx.z * kSmokePlanes, ze = min(zb + kSmokePlanes, nz);
     const size_t ncell = (size_t)nx * ny * nz;
-    for (int z = zb; z < ze; ++z) {
+    double acc = 0.0;
+    for (int z = zb; z < ze && x < nx && y < ny; ++z) {
         const int c = idx3(x, y, z, nx, ny);
         // the cell's faces always exist: loaded before the solid test
-        float vel[3];
-        vel_at_centre<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
-        if (a.flags[c] & F_SOLID) {
+        const float f_left = __ldg(a.u + idx3(x, y, z, nx + 1, ny)), f_right = __ldg(a.u + idx3(x + 1, y, z, nx + 1, ny));
+        const float f_bottom = __ldg(a.v + idx3(x, y, z, nx, ny + 1)), f_top = __ldg(a.v + idx3(x, y + 1, z, nx, ny + 1));
+        float f_back = 0.f, f_front = 0.f;
+        if constexpr (DIM == 3) {
+            f_back = __ldg(a.w + idx3(x, y, z, nx, ny));
+            f_front = __ldg(a.w + idx3(x, y, z + 1, nx, ny));
+        }
+        // vel_at_centre's values
+        const float vel[3] = {lerp_(f_left, f_right, 0.5f), lerp_(f_bottom, f_top, 0.5f),
+                              DIM == 3 ? lerp_(f_back, f_front, 0.5f) : 0.f};
+        const uint8_t fl = a.flags[c];
+        if (fl & F_SOLID) {
             for (int ch = 0; ch < a.nch; ++ch) a.dens_o[ch * ncell + c] = 0.f;
             a.temp_o[c] = a.c.t_amb;
             continue;
+        }
+        if constexpr (DIV) {
+            const bool sv = a.sv0 != nullptr;
+            const float v_top = (fl & F_TOP) ? (sv ? a.sv1[c + nx] : 0.f) : f_top;
+            const float v_bottom = (fl & F_BOTTOM) ? (sv ? a.sv1[c - nx] : 0.f) : f_bottom;
+            const float v_right = (fl & F_RIGHT) ? (sv ? a.sv0[c + 1] : 0.f) : f_right;
+            const float v_left = (fl & F_LEFT) ? (sv ? a.sv0[c - 1] : 0.f) : f_left;
+            float d = v_right - v_left + v_top - v_bottom;
+            if constexpr (DIM == 3) {
+                const int pl = nx * ny;
+                const float v_front = (fl & F_FRONT) ? (sv ? a.sv2[c + pl] : 0.f) : f_front;
+                const float v_back = (fl & F_BACK) ? (sv ? a.sv2[c - pl] : 0.f) : f_back;
+                d = d + v_front - v_back;
+            }
+            acc += (double)d * (double)d;
         }
         const float gx = (float)x + 0.5f, gy = (float)y + 0.5f, gz = DIM == 3 ? (float)z + 0.5f : 0.f;
         const float cfl = a.c.cfl;
@@ -726,14 +762,41 @@ __global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a) {
             a.dens_o[ch * ncell + c] = sample_taps_fast<DIM>(a.dens + ch * ncell, nx, ny, nz, t, 0.f);
         a.temp_o[c] = sample_taps_fast<DIM>(a.temp, nx, ny, nz, t, a.c.t_amb);
     }
+    if constexpr (DIV) {
+        const double bs = block_sum(acc);
+        const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+        const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
+        __shared__ bool last;
+        if (tid == 0) {
+            df.partial[bid] = bs;
+            __threadfence();
+            last = atomicAdd(df.ticket, 1u) == nb - 1;
+        }
+        __syncthreads();
+        if (!last) return;
+        const double total = block_sum(fold_sum(df.partial, nb, tid, blockDim.x * blockDim.y));
+        if (tid == 0) {
+            df.out[df.slot] = total;
+            *df.ticket = 0u;
+        }
+    }
 }
 
-int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st) {
+int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st, int div_slot) {
     FluidArgs a = fluid_args(s, c);
     dim3 b(32, 8, 1);
     dim3 g = grid_for(s->nx, s->ny, (s->nz + kSmokePlanes - 1) / kSmokePlanes, b);
-    if (s->dim == 3) k_advect_smoke<3><<<g, b, 0, st>>>(a);
-    else k_advect_smoke<2><<<g, b, 0, st>>>(a);
+    DivFold df{s->red.partial, s->red.ticket, s->red.out, div_slot};
+    if (div_slot >= 0 && (int)(g.x * g.y * g.z) > s->red.max_blocks)
+        return set_error(SS_E_INVALID, "reduction scratch too small");
+    if (s->dim == 3) {
+        if (div_slot >= 0) k_advect_smoke<3, true><<<g, b, 0, st>>>(a, df);
+        else k_advect_smoke<3, false><<<g, b, 0, st>>>(a, df);
+    } else {
+        if (div_slot >= 0) k_advect_smoke<2, true><<<g, b, 0, st>>>(a, df);
+        else k_advect_smoke<2, false><<<g, b, 0, st>>>(a, df);
+    }
     s->si ^= 1;
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_advect_smoke");

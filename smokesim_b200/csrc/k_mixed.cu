@@ -185,6 +185,8 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
     }
     __syncthreads();
     if (!last) return;
+    // (one load in flight per thread: the eight-accumulator fold costs this
+    // kernel registers, and so occupancy, in its main loop)
     double s = 0.0, mx = 0.0;
     for (unsigned int i = tid; i < nblocks; i += kIrTX * kIrTY) {
         s += __ldcg(psum + i);

@@ -143,7 +143,9 @@ int launch_advect_velocities(ss_sim* s, const StepConsts& c, bool fuse_buoyancy,
 int launch_buoyancy(ss_sim* s, const StepConsts& c, cudaStream_t st);
 int launch_vorticity(ss_sim* s, const StepConsts& c, cudaStream_t st);
 int launch_update_velocities(ss_sim* s, const StepConsts& c, cudaStream_t st);
-int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st);
+// div_slot >= 0: also fold the squared divergence of the current velocities
+// into that statistics slot (the k_divergence operator, no right-hand sides)
+int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st, int div_slot = -1);
 // divergence of the current velocities into div0 (+div0r); optional ||div||^2 into slot
 // with sc and quirks >= 0 also the level-0 right-hand sides rhs_s / rhs_r of that boundary rule
 int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st, const StepConsts* sc = nullptr,
