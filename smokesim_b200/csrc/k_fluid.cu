@@ -424,7 +424,7 @@ static bool pow2_normal(float v) {
     return std::frexp(v, &e) == 0.5f && v >= 1.1754944e-38f && v <= 8.5070592e37f;
 }
 
-constexpr int kMX = 32, kMY = 8, kMZ = 32;   // tile and z chunk
+constexpr int kMX = 32, kMY = 8, kMZ = 32;   // tile and largest z chunk
 constexpr int kUW = kMX + 3, kUH = kMY + 4;  // u faces x0-1 .. x0+kMX+1, rows y0-2 .. y0+kMY+1
 constexpr int kVW = kMX + 4, kVH = kMY + 3;  // v faces: cols x0-2 .. x0+kMX+1, face rows y0-1 .. y0+kMY+1
 constexpr int kWW = kMX + 4, kWH = kMY + 4;  // w faces: cols x0-2 .. x0+kMX+1, rows y0-2 .. y0+kMY+1
@@ -443,11 +443,11 @@ struct VortSmem {
 // POW2: 2h and rho are powers of two, so dividing by them is multiplying by
 // their exact reciprocals (inv_2h, inv_rho) - the same correctly rounded value.
 template <bool POW2>
-__global__ void __launch_bounds__(kMT) k_vorticity_march(FluidArgs a, float inv_2h, float inv_rho) {
+__global__ void __launch_bounds__(kMT) k_vorticity_march(FluidArgs a, float inv_2h, float inv_rho, int planes) {
     __shared__ VortSmem S;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY;
-    const int zb = blockIdx.z * kMZ, ze = min(zb + kMZ, nz);
+    const int zb = blockIdx.z * planes, ze = min(zb + planes, nz);
     const int tid = threadIdx.x;
     // in-plane offsets of this thread's loads (-1: outside the face array)
     int ou[kUL], ov[kVL], ow[kWL];
@@ -586,12 +586,14 @@ int launch_vorticity(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     dim3 gc = grid_for(s->nx, s->ny, s->nz, b);
     dim3 gf = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, b);
     if (s->dim == 3) {
-        dim3 gt((s->nx + kMX - 1) / kMX, (s->ny + kMY - 1) / kMY, (s->nz + kMZ - 1) / kMZ);
+        const int tx = (s->nx + kMX - 1) / kMX, ty = (s->ny + kMY - 1) / kMY;
+        const int planes = z_planes((long long)tx * ty, s->nz, kMZ, 4);
+        dim3 gt(tx, ty, (s->nz + planes - 1) / planes);
         const float two_h = 2.f * s->h;
         if (pow2_normal(two_h) && pow2_normal(c.rho))
-            k_vorticity_march<true><<<gt, kMT, 0, st>>>(a, 1.f / two_h, 1.f / c.rho);
+            k_vorticity_march<true><<<gt, kMT, 0, st>>>(a, 1.f / two_h, 1.f / c.rho, planes);
         else
-            k_vorticity_march<false><<<gt, kMT, 0, st>>>(a, 0.f, 0.f);
+            k_vorticity_march<false><<<gt, kMT, 0, st>>>(a, 0.f, 0.f, planes);
         s->nlaunch += 1;
     } else {
         k_vorticity<2><<<gc, b, 0, st>>>(a, s->vort);
@@ -629,13 +631,13 @@ constexpr int kUpdPlanes = 8;
 // p0_out (FP64 pressure only): also store each cell's pressure rounded to
 // FP32 - the pressure field of the API - in the same pass.
 template <int DIM, typename P = float>
-__global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const P* __restrict__ p, double k64 = 0.0,
-                                                         float* __restrict__ p0_out = nullptr) {
+__global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const P* __restrict__ p, int planes,
+                                                         double k64 = 0.0, float* __restrict__ p0_out = nullptr) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const int zb = blockIdx.z * kUpdPlanes;
-    const int zend = min(zb + kUpdPlanes, DIM == 3 ? nz + 1 : 1);
+    const int zb = blockIdx.z * planes;
+    const int zend = min(zb + planes, DIM == 3 ? nz + 1 : 1);
     const bool inxy = x < nx && y < ny;
     P p_back = P(0);
     bool s_back = false;
@@ -675,9 +677,10 @@ __global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const P* _
 int launch_update_velocities(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     FluidArgs a = fluid_args(s, c);
     dim3 b(32, 8, 1);
-    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? (s->nz + kUpdPlanes) / kUpdPlanes : 1, b);
-    if (s->dim == 3) k_update_velocity<3><<<g, b, 0, st>>>(a, s->p[0]);
-    else k_update_velocity<2><<<g, b, 0, st>>>(a, s->p[0]);
+    const int planes = z_planes((long long)((s->nx + 32) / 32) * ((s->ny + 8) / 8), s->nz + 1, kUpdPlanes);
+    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? (s->nz + planes) / planes : 1, b);
+    if (s->dim == 3) k_update_velocity<3><<<g, b, 0, st>>>(a, s->p[0], planes);
+    else k_update_velocity<2><<<g, b, 0, st>>>(a, s->p[0], planes);
     for (int d = 0; d < s->dim; ++d) s->vi[d] ^= 1;
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_update_velocity");
@@ -686,10 +689,11 @@ int launch_update_velocities(ss_sim* s, const StepConsts& c, cudaStream_t st) {
 int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st, float* p0_out) {
     FluidArgs a = fluid_args(s, c);
     dim3 b(32, 8, 1);
-    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? (s->nz + kUpdPlanes) / kUpdPlanes : 1, b);
+    const int planes = z_planes((long long)((s->nx + 32) / 32) * ((s->ny + 8) / 8), s->nz + 1, kUpdPlanes);
+    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->dim == 3 ? (s->nz + planes) / planes : 1, b);
     const double k64 = -(double)c.dt / ((double)c.rho * (double)s->h);
-    if (s->dim == 3) k_update_velocity<3, double><<<g, b, 0, st>>>(a, s->p64, k64, p0_out);
-    else k_update_velocity<2, double><<<g, b, 0, st>>>(a, s->p64, k64, p0_out);
+    if (s->dim == 3) k_update_velocity<3, double><<<g, b, 0, st>>>(a, s->p64, planes, k64, p0_out);
+    else k_update_velocity<2, double><<<g, b, 0, st>>>(a, s->p64, planes, k64, p0_out);
     for (int d = 0; d < s->dim; ++d) s->vi[d] ^= 1;
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_update_velocity<p64>");
@@ -713,11 +717,11 @@ struct DivFold {
 };
 
 template <int DIM, bool DIV>
-__global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a, DivFold df) {
+__global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a, DivFold df, int planes) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const int zb = blockIdx.z * kSmokePlanes, ze = min(zb + kSmokePlanes, nz);
+    const int zb = blockIdx.z * planes, ze = min(zb + planes, nz);
     const size_t ncell = (size_t)nx * ny * nz;
     double acc = 0.0;
     for (int z = zb; z < ze && x < nx && y < ny; ++z) {
@@ -786,16 +790,17 @@ __global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a, DivFold df) {
 int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st, int div_slot) {
     FluidArgs a = fluid_args(s, c);
     dim3 b(32, 8, 1);
-    dim3 g = grid_for(s->nx, s->ny, (s->nz + kSmokePlanes - 1) / kSmokePlanes, b);
+    const int planes = z_planes((long long)((s->nx + 31) / 32) * ((s->ny + 7) / 8), s->nz, kSmokePlanes);
+    dim3 g = grid_for(s->nx, s->ny, (s->nz + planes - 1) / planes, b);
     DivFold df{s->red.partial, s->red.ticket, s->red.out, div_slot};
     if (div_slot >= 0 && (int)(g.x * g.y * g.z) > s->red.max_blocks)
         return set_error(SS_E_INVALID, "reduction scratch too small");
     if (s->dim == 3) {
-        if (div_slot >= 0) k_advect_smoke<3, true><<<g, b, 0, st>>>(a, df);
-        else k_advect_smoke<3, false><<<g, b, 0, st>>>(a, df);
+        if (div_slot >= 0) k_advect_smoke<3, true><<<g, b, 0, st>>>(a, df, planes);
+        else k_advect_smoke<3, false><<<g, b, 0, st>>>(a, df, planes);
     } else {
-        if (div_slot >= 0) k_advect_smoke<2, true><<<g, b, 0, st>>>(a, df);
-        else k_advect_smoke<2, false><<<g, b, 0, st>>>(a, df);
+        if (div_slot >= 0) k_advect_smoke<2, true><<<g, b, 0, st>>>(a, df, planes);
+        else k_advect_smoke<2, false><<<g, b, 0, st>>>(a, df, planes);
     }
     s->si ^= 1;
     s->nlaunch += 1;
@@ -849,14 +854,14 @@ constexpr int kDivPlanes = 8;
 
 template <int DIM>
 __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restrict__ div0, float* __restrict__ div0r,
-                                                    double* __restrict__ partial, RhsOut ro) {
+                                                    double* __restrict__ partial, RhsOut ro, int planes) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int zb = blockIdx.z * kDivPlanes;
+    const int zb = blockIdx.z * planes;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     double acc = 0.0;
     if (x < nx && y < ny) {
-        const int ze = min(zb + kDivPlanes, nz);
+        const int ze = min(zb + planes, nz);
         float f_back = 0.f;
         if constexpr (DIM == 3) f_back = __ldg(a.w + idx3(x, y, zb, nx, ny));
         for (int z = zb; z < ze; ++z) {
@@ -929,13 +934,14 @@ int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st, const St
         ro.r_solid = quirks ? 1 : s->enclosed;
     }
     dim3 b(32, 8, 1);
-    dim3 g = grid_for(s->nx, s->ny, (s->nz + kDivPlanes - 1) / kDivPlanes, b);
+    const int planes = z_planes((long long)((s->nx + 31) / 32) * ((s->ny + 7) / 8), s->nz, kDivPlanes);
+    dim3 g = grid_for(s->nx, s->ny, (s->nz + planes - 1) / planes, b);
     const int nblocks = (int)(g.x * g.y * g.z);
     float* d0 = write ? s->div0 : nullptr;
     float* d0r = (write && s->div0r != s->div0) ? s->div0r : nullptr;
     double* part = slot >= 0 ? s->red.partial : nullptr;
-    if (s->dim == 3) k_divergence<3><<<g, b, 0, st>>>(a, d0, d0r, part, ro);
-    else k_divergence<2><<<g, b, 0, st>>>(a, d0, d0r, part, ro);
+    if (s->dim == 3) k_divergence<3><<<g, b, 0, st>>>(a, d0, d0r, part, ro, planes);
+    else k_divergence<2><<<g, b, 0, st>>>(a, d0, d0r, part, ro, planes);
     s->nlaunch += 1;
     int rc = check_cuda(cudaGetLastError(), "k_divergence");
     if (rc || slot < 0) return rc;

@@ -72,7 +72,7 @@ __global__ void k_f32_from_p64(const double* __restrict__ p64, float* __restrict
 // cell: the column's own values roll through registers (the z neighbours),
 // each plane's tile plus its one-cell x/y rim goes through shared memory (the
 // x and y neighbours), double-buffered so a plane costs one barrier.
-constexpr int kIrTX = 32, kIrTY = 8, kIrChunk = 16;
+constexpr int kIrTX = 32, kIrTY = 8, kIrChunk = 16;   // largest z chunk
 constexpr int kIrRim = 2 * kIrTX + 2 * kIrTY;   // rim cells of a tile (no corners: 5/7-point stencil)
 
 template <int DIM, bool ACC>
@@ -81,12 +81,12 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
     const float* __restrict__ div0, const uint8_t* __restrict__ fmask, int nx, int ny, int nz, double k,
     double inv_k, double inv_khh, float* __restrict__ rhs_s, float* __restrict__ rhs_r, double* __restrict__ psum,
     double* __restrict__ pmax, unsigned int* __restrict__ ticket, double* __restrict__ out, int slot,
-    float* __restrict__ scale) {
+    float* __restrict__ scale, int planes) {
     __shared__ double sP[2][kIrTY + 2][kIrTX + 2];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kIrTX * ty;
     const int x0 = blockIdx.x * kIrTX, y0 = blockIdx.y * kIrTY;
     const int x = x0 + tx, y = y0 + ty;
-    const int zb = blockIdx.z * kIrChunk, ze = min(zb + kIrChunk, nz);
+    const int zb = blockIdx.z * planes, ze = min(zb + planes, nz);
     const bool in = x < nx && y < ny;
     // this thread's rim cell (tid < kIrRim), in tile coordinates
     int hx = 0, hy = 0;
@@ -244,7 +244,9 @@ int launch_p0_from_p64(ss_sim* s, cudaStream_t st) {
 
 int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate, cudaStream_t st) {
     dim3 b(kIrTX, kIrTY, 1);
-    dim3 g((s->nx + kIrTX - 1) / kIrTX, (s->ny + kIrTY - 1) / kIrTY, (s->nz + kIrChunk - 1) / kIrChunk);
+    const int tx = (s->nx + kIrTX - 1) / kIrTX, ty = (s->ny + kIrTY - 1) / kIrTY;
+    const int planes = z_planes((long long)tx * ty, s->nz, kIrChunk);
+    dim3 g(tx, ty, (s->nz + planes - 1) / planes);
     const int nblocks = (int)(g.x * g.y * g.z);
     if (nblocks > s->red.max_blocks) return set_error(SS_E_INVALID, "reduction scratch too small");
     const double k = (double)c.dt / ((double)c.rho * (double)s->h);
@@ -252,7 +254,7 @@ int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate
     const double inv_khh = 1.0 / (k * (double)s->lv[0].hh);
 #define IR_ARGS(ACC) s->p64, s->p_alt[0], s->p64b, s->div0, s->fmask, s->nx, s->ny, s->nz, k, inv_k, inv_khh, \
                      s->rhs_s, s->rhs_r, s->red.partial, s->red.partial_max, s->red.ticket, s->red.out, slot, \
-                     s->d_scale
+                     s->d_scale, planes
     if (s->dim == 3) {
         if (accumulate) k_ir_residual<3, true><<<g, b, 0, st>>>(IR_ARGS(true));
         else k_ir_residual<3, false><<<g, b, 0, st>>>(IR_ARGS(false));

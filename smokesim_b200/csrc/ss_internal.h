@@ -207,6 +207,15 @@ struct StepSaves {
     int vcycles;             // out: V-cycles (or refinement steps) the solve ran
 };
 int run_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* saves);
+// z planes a thread (or a block) of a z-marching kernel takes: at most
+// max_planes (the figure tuned at 256^3), and few enough that small grids
+// still fill the GPU - about `target` blocks for `tiles` blocks a z slab
+inline int z_planes(long long tiles, int nz, int max_planes, int min_planes = 1, long long target = 148LL * 8) {
+    long long p = (tiles * nz + target - 1) / target;
+    if (p > max_planes) p = max_planes;
+    if (p < min_planes) p = min_planes;
+    return (int)p;
+}
 bool rb_tma_supported(const ss_sim* s);
 int launch_rb_smooth_tma(ss_sim* s, float* pc, const float* po, const float* rhs, const uint8_t* mask, int colour,
                          cudaStream_t st);
