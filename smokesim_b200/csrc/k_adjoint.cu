@@ -975,7 +975,9 @@ SS_D void bottom_adj_sweeps(const AdjLevel& a, int iterations) {
     if (iterations <= 0) return;
     const int n = a.nx * a.ny * a.nz;
     int nt = blockDim.x;
-    while (nt > 128 && (n + nt / 2 - 1) / (nt / 2) <= 2) nt /= 2;
+    // the fewest threads that still give every cell its own thread (the
+    // coarsest 8^3 level: 512); measured faster than two cells a thread
+    while (nt > 128 && (n + nt / 2 - 1) / (nt / 2) <= 1) nt /= 2;
     if ((n + nt - 1) / nt <= 2) {
         if ((int)threadIdx.x < nt) bottom_adj_sweeps_cached<DIM, 2>(a, iterations, nt);
         __syncthreads();
