@@ -260,24 +260,29 @@ def run_variant(torch, sim_cls, scene, sc, name, args, stream, barrier, world, d
 
 
 ADJOINT_CASES = [
-    # name, scene, steps, checkpoint interval (= steps: every intermediate kept, no recomputation)
-    ("rollout64", dict(kind="rollout64", n=64), 64, 8),
-    ("rollout64_no_recompute", dict(kind="rollout64", n=64), 64, 64),
-    ("plume128", dict(kind="plume3d", n=128), 200, 14),
+    # name, scene, steps, checkpoint interval (= steps: every intermediate kept,
+    # no recomputation), projection precision of the forward
+    ("rollout64", dict(kind="rollout64", n=64), 64, 8, 0),
+    ("rollout64_no_recompute", dict(kind="rollout64", n=64), 64, 64, 0),
+    ("plume128", dict(kind="plume3d", n=128), 200, 14, 0),
+    # the inverse-control configuration: mixed-precision forward (FP16 coarse
+    # corrections), the recorded refinement steps transposed in the adjoint
+    ("plume128_mixed", dict(kind="plume3d", n=128), 200, 14, 1),
 ]
 
 
 def adjoint_bench(torch, stream):
     """Forward rollout with checkpoints + reverse pass (ss_adjoint_*) against
-    the plain forward steps of the same scene: FP32 projection with the
-    corrected operators, 4 V-cycles per step, L2 loss on the final density."""
+    the plain forward steps of the same scene: FP32 (or mixed-precision)
+    projection with the corrected operators, 4 V-cycles (refinement steps) per
+    step, L2 loss on the final density."""
     from smokesim_b200 import Sim, abi, scene
     from smokesim_b200.adjoint import Rollout
     out = {}
-    for name, sa, nsteps, every in ADJOINT_CASES:
+    for name, sa, nsteps, every, prec in ADJOINT_CASES:
         sc = scene.rollout64(seed=0, n=sa["n"]) if sa["kind"] == "rollout64" else scene.plume3d(seed=0, n=sa["n"])
         sc.pop("rng", None)
-        p = scene.workload_params(ref_quirks=0, n_vcycles=4, collect_stats=0)
+        p = scene.workload_params(ref_quirks=0, n_vcycles=4, collect_stats=0, precision=prec)
         cells = sa["n"] ** 3
         forces = np.zeros((nsteps, 3), np.float32)
         forces[:, 1] = 0.5
@@ -318,6 +323,7 @@ def adjoint_bench(torch, stream):
         ro.close()
         sim.close()
         out[name] = {"grid": [sa["n"]] * 3, "steps": nsteps, "checkpoint_every": every,
+                     "precision": "mixed (f16 coarse)" if prec else "f32",
                      "forward_ms_per_step": fwd_ms, "forward_with_checkpoints_ms_per_step": f_ms,
                      "fwd_adjoint_ms_per_step": fb_ms, "fwd_adjoint_over_forward": fb_ms / fwd_ms,
                      "fwd_adjoint_mcell_steps_per_s": cells / (fb_ms / 1e3) / 1e6,

@@ -257,7 +257,9 @@ int ss_divergence_norm_noalloc(int dim, const int n[3], const float* u, const fl
  * back-traced point, buoyancy, vorticity confinement, the projection update,
  * each V-cycle of the multigrid schedule (red-black sweeps in reverse colour
  * order, residual + restriction, prolongation) and the divergence.  The
- * projection must run the corrected operators (ref_quirks = 0) in FP32;
+ * projection must run the corrected operators (ref_quirks = 0); with the
+ * mixed-precision solve the forward's recorded refinement steps are
+ * transposed as FP32 V-cycles (the same linear map in exact arithmetic);
  * obstacles are treated as fixed geometry.
  *
  * Control force: every step adds dt * force to the face velocities inside

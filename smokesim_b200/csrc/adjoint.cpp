@@ -141,7 +141,15 @@ static int check_adjoint_params(const ss_adjoint* A, const ss_params* p) {
     if (!A || !p) return set_error(SS_E_INVALID, "NULL argument");
     if (p->stage_mask & SS_STAGE_RESOLVE_PRESSURE) {
         if (p->mg.ref_quirks) return set_error(SS_E_UNSUPPORTED, "the adjoint transposes the corrected operators (ref_quirks = 0)");
-        if (p->mg.precision != SS_PREC_FP32) return set_error(SS_E_UNSUPPORTED, "the adjoint transposes the FP32 solve");
+        // The mixed-precision solve's refinement steps are, in exact
+        // arithmetic, the same V-cycles on the pressure as the FP32 solve's
+        // (a linear V-cycle applied to the correction with the residual as its
+        // right-hand side), so the recorded count of them is transposed with
+        // the FP32 adjoint V-cycle: the gradient of the exact-arithmetic map at
+        // the states the mixed forward produced.
+        if (p->mg.precision != SS_PREC_FP32 && p->mg.precision != SS_PREC_MIXED &&
+            p->mg.precision != SS_PREC_MIXED_BF16)
+            return set_error(SS_E_INVALID, "unknown precision mode");
     }
     return SS_OK;
 }

@@ -150,12 +150,16 @@ def test_rollout_checkpointing_consistent():
     assert res[1][2]["checkpoint_bytes"] < res[0][2]["checkpoint_bytes"]
 
 
-def test_rollout_gradient_vs_fp64_fd():
+@pytest.mark.parametrize("prec", [abi.PREC_FP32, abi.PREC_MIXED])
+def test_rollout_gradient_vs_fp64_fd(prec):
     """8-step rollout at 32^3: dL/d(initial velocity) and dL/d(force) on 32
     random control coordinates against FP64 central differences with
     h = 1e-3.  Semi-Lagrangian advection is piecewise smooth: where h = 1e-3
     straddles a kink (the 1e-3 and 1e-4 differences disagree), the h = 1e-4
-    difference is the reference for that coordinate."""
+    difference is the reference for that coordinate.  The GPU forward runs the
+    FP32 or the mixed-precision projection (4 V-cycles / refinement steps a
+    step); the FP64 differences use the FP32 scheme, which is the same map in
+    exact arithmetic."""
     from oracle.oracle import OracleSim
     from smokesim_b200 import Sim
     from smokesim_b200.adjoint import Rollout
@@ -195,12 +199,13 @@ def test_rollout_gradient_vs_fp64_fd():
 
     g = Sim(sc["desc"])
     scene.apply(g, sc)
+    pg = scene.workload_params(ref_quirks=0, n_vcycles=4, precision=prec)
     ro = Rollout(g, nsteps, 3)
-    ro.forward(p, forces)
+    ro.forward(pg, forces)
     rho = torch.from_numpy(g.get_field(abi.FIELD_DENSITY).ravel()).cuda().double()
     gd = (2 * (rho - torch.from_numpy(rho_t).cuda())).float().contiguous()
     torch.cuda.synchronize()
-    gf = ro.backward(p, grad_density=gd.data_ptr())
+    gf = ro.backward(pg, grad_density=gd.data_ptr())
     gvel = {k: ro.grad(k) for k in VEL}
     # 32 coordinates: 24 velocity faces near the plume, 8 force components
     h = 1e-3
