@@ -267,6 +267,14 @@ int ss_divergence_norm_noalloc(int dim, const int n[3], const float* u, const fl
  * sets it for plain steps, the rollout below takes one per step. */
 int ss_set_emitter_force(ss_sim* sim, const float force[3]);
 
+/* Coarse control force field (an extension for inverse control; no
+ * counterpart in the reference): three components on n^3 cell-centred samples
+ * spanning the whole domain, upsampled trilinearly (clamp to edge) to every
+ * face position and added as dt * F to the face velocities after the
+ * emitters, every step.  field: host array of 3*n*n*n floats, component-major
+ * (F_x, then F_y, then F_z), x fastest; n = 0 removes the field.  3D only. */
+int ss_set_force_field(ss_sim* sim, int n, const float* field, void* stream);
+
 typedef struct ss_adjoint ss_adjoint;
 /* A rollout of nsteps steps from the simulation's current state, with the
  * state checkpointed every checkpoint_every steps (0: every step) so the
@@ -293,6 +301,9 @@ int ss_adjoint_get_field(ss_adjoint* adj, int field, float* dst, size_t count, i
 /* Statistics of the last reverse pass: kernel launches and device bytes held
  * by checkpoints and recomputation buffers. */
 int ss_adjoint_info(ss_adjoint* adj, long long* kernel_launches, long long* checkpoint_bytes, long long* workspace_bytes);
+/* dL/d(force field) after ss_adjoint_backward: 3*n^3 floats (host), the layout
+ * of ss_set_force_field; count must match the simulation's field. */
+int ss_adjoint_force_field_grad(ss_adjoint* adj, float* dst, size_t count);
 
 /* ---- headless renderer -------------------------------------------------- */
 /* Replaces the reference's GL fragment shaders with CUDA kernels writing an

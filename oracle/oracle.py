@@ -56,6 +56,10 @@ def load(precision="f32"):
         L.og_set_field_f64.argtypes = [vp, i, C.POINTER(C.c_double), sz]
         L.og_set_emitter_force.argtypes = [vp, C.POINTER(C.c_float * 3)]
         L.og_set_emitter_force_f64.argtypes = [vp, C.POINTER(C.c_double * 3)]
+        L.og_set_force_field.argtypes = [vp, i, C.POINTER(C.c_float)]
+        L.og_set_force_field.restype = None
+        L.og_set_force_field_f64.argtypes = [vp, i, C.POINTER(C.c_double)]
+        L.og_set_force_field_f64.restype = None
         L.og_render.argtypes = [vp, C.POINTER(abi.RenderDesc), C.c_void_p]
         L.og_render.restype = None
         L.og_set_velocity_other.argtypes = [vp, i, C.POINTER(C.c_float), sz]
@@ -145,6 +149,22 @@ class OracleSim:
         out = np.empty((desc.height, desc.width, 4), np.uint8)
         self.L.og_render(self.h, C.byref(desc), out.ctypes.data)
         return out
+
+    def set_force_field(self, field):
+        """Coarse control force field: an array of shape (3, n, n, n) (or
+        None to remove it); float64 input is kept at FP64 precision."""
+        if field is None:
+            self.L.og_set_force_field(self.h, 0, None)
+            return
+        a = np.asarray(field)
+        n = a.shape[-1]
+        assert a.shape == (3, n, n, n), a.shape
+        if a.dtype == np.float64:
+            a = np.ascontiguousarray(a)
+            self.L.og_set_force_field_f64(self.h, n, a.ctypes.data_as(C.POINTER(C.c_double)))
+        else:
+            a = np.ascontiguousarray(a, dtype=np.float32)
+            self.L.og_set_force_field(self.h, n, a.ctypes.data_as(C.POINTER(C.c_float)))
 
     def set_emitter_force(self, force):
         f = (C.c_double * 3)(*[float(x) for x in force])

@@ -70,6 +70,8 @@ typedef struct og_sim {
     int p64_valid;
     int cround;
     real force[3];   /* control force on the faces inside active emitters */
+    real* ff;        /* coarse control force field, 3 * ffn^3 (none: ffn == 0) */
+    int ffn;
 } og_sim;
 
 /* ---------------------------------------------------------------- helpers */
@@ -239,6 +241,7 @@ void og_destroy(og_sim* s) {
     }
     free(s->em); free(s->ob); free(s->bx);
     free(s->p64);
+    free(s->ff);
     free(s);
 }
 
@@ -453,6 +456,55 @@ void og_emitter_velocity(og_sim* s, real dt) {
                     if (forced && inside) a[I3(x, y, z, ax, ay)] = a[I3(x, y, z, ax, ay)] + dt * s->force[comp];
                 }
     }
+}
+
+/* Extension: coarse control force field.  Three components on n^3
+ * cell-centred samples over the domain; each face takes dt times the
+ * GL_LINEAR + CLAMP_TO_EDGE sample of its component at the face position
+ * (texel coordinate (pos / N) * n - 1/2), after the emitters.  3D only. */
+static void og_apply_force_field(og_sim* s, real dt) {
+    if (s->ffn <= 0 || s->dim != 3) return;
+    const int n = s->ffn;
+    const size_t nn = (size_t)n * n * n;
+    for (int comp = 0; comp < 3; ++comp) {
+        int ax = NX + (comp == 0), ay = NY + (comp == 1), az = NZ + (comp == 2);
+        real* a = comp == 0 ? CUR_VX : comp == 1 ? CUR_VY : CUR_VZ;
+        const real* f = s->ff + comp * nn;
+        OMP_FOR
+        for (int z = 0; z < az; ++z)
+            for (int y = 0; y < ay; ++y)
+                for (int x = 0; x < ax; ++x) {
+                    const real xf = (real)x + (comp == 0 ? (real)0 : (real)0.5);
+                    const real yf = (real)y + (comp == 1 ? (real)0 : (real)0.5);
+                    const real zf = (real)z + (comp == 2 ? (real)0 : (real)0.5);
+                    const real tx = (xf / (real)NX) * (real)n - (real)0.5;
+                    const real ty = (yf / (real)NY) * (real)n - (real)0.5;
+                    const real tz = (zf / (real)NZ) * (real)n - (real)0.5;
+                    const real val = sample_edge(f, 3, n, n, n, tx, ty, tz);
+                    a[I3(x, y, z, ax, ay)] = a[I3(x, y, z, ax, ay)] + dt * val;
+                }
+    }
+}
+
+void og_set_force_field(og_sim* s, int n, const float* f) {
+    free(s->ff);
+    s->ff = NULL;
+    s->ffn = 0;
+    if (n <= 0 || !f) return;
+    const size_t cnt = (size_t)3 * n * n * n;
+    s->ff = (real*)malloc(cnt * sizeof(real));
+    for (size_t i = 0; i < cnt; ++i) s->ff[i] = (real)f[i];
+    s->ffn = n;
+}
+void og_set_force_field_f64(og_sim* s, int n, const double* f) {
+    free(s->ff);
+    s->ff = NULL;
+    s->ffn = 0;
+    if (n <= 0 || !f) return;
+    const size_t cnt = (size_t)3 * n * n * n;
+    s->ff = (real*)malloc(cnt * sizeof(real));
+    for (size_t i = 0; i < cnt; ++i) s->ff[i] = (real)f[i];
+    s->ffn = n;
 }
 
 void og_set_emitter_force(og_sim* s, const float f[3]) {
@@ -1330,6 +1382,7 @@ void og_run_physics_step(og_sim* s, const ss_params* prm) {
         og_update_emitters_status(s, prm->current_time);
         og_handle_emitters(s, dt);
         og_emitter_velocity(s, dt);
+        og_apply_force_field(s, dt);
     }
     if (m & SS_STAGE_ADVECT_VELOCITIES) advect_velocities_impl(s, dt, wind);
     if (m & SS_STAGE_APPLY_BUOYANCY) apply_buoyancy_impl(s, dt, tamb, prm->t_weight_coeff, prm->t_temp_coeff);
@@ -1373,6 +1426,7 @@ void og_stage_handle_emitters(og_sim* s, const ss_params* p) {
     og_update_emitters_status(s, p->current_time);
     og_handle_emitters(s, p->time_step);
     og_emitter_velocity(s, p->time_step);
+    og_apply_force_field(s, p->time_step);
 }
 void og_stage_multigrid(og_sim* s, const ss_params* p) { og_multigrid_pressure_solve(s, &p->mg, p->time_step, p->density); }
 void og_stage_obstacles(og_sim* s, const ss_params* p) { og_obstacle_update(s, p->time_step); og_update_solid_map(s); }

@@ -292,7 +292,7 @@ EXPORTED = [
     "ss_compute_residual", "ss_compute_restrict", "ss_prolong_and_add", "ss_update_velocities",
     "ss_advect_smoke", "ss_obstacle_update_step", "ss_update_solid_map", "ss_init_solid_map",
     "ss_get_level", "ss_set_level", "ss_divergence_norm_noalloc",
-    "ss_set_emitter_force", "ss_adjoint_create", "ss_adjoint_destroy", "ss_adjoint_forward",
+    "ss_set_emitter_force", "ss_set_force_field", "ss_adjoint_force_field_grad", "ss_adjoint_create", "ss_adjoint_destroy", "ss_adjoint_forward",
     "ss_adjoint_backward", "ss_adjoint_field_device_ptr", "ss_adjoint_get_field", "ss_adjoint_info",
     "ss_set_field_device", "ss_get_field_device", "ss_render_default", "ss_render",
     "ss_save_state", "ss_load_state",
@@ -335,6 +335,8 @@ def _declare(L):
     L.ss_divergence_norm_noalloc.argtypes = [i, C.POINTER(C.c_int * 3), vp, vp, vp, vp, vp, vp]
     L.ss_set_level.argtypes = [vp, i, i, fp, sz, vp]
     L.ss_set_emitter_force.argtypes = [vp, C.POINTER(C.c_float * 3)]
+    L.ss_set_force_field.argtypes = [vp, C.c_int, C.POINTER(C.c_float), vp]
+    L.ss_adjoint_force_field_grad.argtypes = [vp, C.POINTER(C.c_float), C.c_size_t]
     L.ss_adjoint_create.argtypes = [vp, i, i, C.POINTER(vp)]
     L.ss_adjoint_destroy.argtypes = [vp]
     L.ss_adjoint_forward.argtypes = [vp, C.POINTER(Params), fp, vp]

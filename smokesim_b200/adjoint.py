@@ -72,6 +72,13 @@ class Rollout:
         _check(self.L.ss_adjoint_get_field(self.h, field, C.c_void_p(dst_ptr), n, 1, C.c_void_p(stream)),
                "ss_adjoint_get_field")
 
+    def force_field_grad(self, n):
+        """dL/d(coarse force field) of the last backward pass, shape (3, n, n, n)."""
+        out = np.empty((3, n, n, n), np.float32)
+        _check(self.L.ss_adjoint_force_field_grad(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size),
+               "ss_adjoint_force_field_grad")
+        return out
+
     def info(self):
         a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
         _check(self.L.ss_adjoint_info(self.h, C.byref(a), C.byref(b), C.byref(c)), "ss_adjoint_info")

@@ -59,6 +59,8 @@ struct ss_adjoint {
     float* vc3 = nullptr, *wdir = nullptr, *dbar3 = nullptr, *wbar = nullptr;
     double* fpart = nullptr;
     double* fgrad = nullptr;   // nsteps * 3
+    float* ffgrad = nullptr;   // dL/d(coarse force field), 3 * ff_n^3
+    int ffgrad_n = 0;          // ff_n that ffgrad was sized and last filled for
     std::vector<void*> allocs;
     long long launches = 0, ckpt_bytes = 0, work_bytes = 0;
     bool forward_done = false;
@@ -79,6 +81,7 @@ static int amalloc(ss_adjoint* A, void** p, size_t bytes, long long* counter) {
 
 static void free_adjoint(ss_adjoint* A) {
     if (A->vgraph) cudaGraphExecDestroy(A->vgraph);
+    cudaFree(A->ffgrad);
     for (void* p : A->allocs) cudaFree(p);
     delete A;
 }
@@ -260,6 +263,8 @@ static int adj_step(ss_adjoint* A, const ss_params* p, int k, const Record& R, c
         TRY_ADJ(adj_buoyancy(s, c, A->ub[1], A->db, A->tb, st));
     }
     if (m & SS_STAGE_HANDLE_EMITTERS) {
+        // the force field came after the emitters: its transpose first
+        if (s->ff_n > 0) TRY_ADJ(adj_force_field(s, c, A->ub, A->ffgrad, st));
         // the emitter records of this step (their status changes over time)
         if (!R.em.empty())
             TRY_ADJ(check_cuda(cudaMemcpyAsync(s->d_em, R.em.data(), R.em.size() * sizeof(ss_emitter),
@@ -378,6 +383,17 @@ int ss_adjoint_backward(ss_adjoint* A, const ss_params* p, const float* grad_den
     else TRY_ADJ(check_cuda(cudaMemsetAsync(A->tb, 0, s->ncell * 4, st), "memset"));
     TRY_ADJ(check_cuda(cudaMemsetAsync(A->w.pbar[0], 0, s->ncell * 4, st), "memset"));
     TRY_ADJ(check_cuda(cudaMemsetAsync(A->fgrad, 0, (size_t)A->n * 3 * sizeof(double), st), "memset"));
+    if (s->ff_n > 0) {
+        const size_t nff = (size_t)3 * s->ff_n * s->ff_n * s->ff_n;
+        if (A->ffgrad_n != s->ff_n) {
+            cudaFree(A->ffgrad);
+            A->ffgrad = nullptr;
+            A->ffgrad_n = 0;
+            TRY_ADJ(check_cuda(cudaMalloc((void**)&A->ffgrad, nff * sizeof(float)), "cudaMalloc(force field gradient)"));
+            A->ffgrad_n = s->ff_n;
+        }
+        TRY_ADJ(check_cuda(cudaMemsetAsync(A->ffgrad, 0, nff * sizeof(float), st), "memset"));
+    }
     const int nseg = (A->n + A->every - 1) / A->every;
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int k0 = sg * A->every, k1 = std::min(A->n, k0 + A->every);
@@ -391,6 +407,8 @@ int ss_adjoint_backward(ss_adjoint* A, const ss_params* p, const float* grad_den
     TRY_ADJ(restore_state(s, A->ckpt[0], st));
     for (int d = 0; d < 3; ++d) s->force[d] = 0.f;
     A->launches = s->nlaunch;
+    // the force-field gradient is read back with a plain copy afterwards
+    if (s->ff_n > 0) TRY_ADJ(check_cuda(cudaStreamSynchronize(st), "adjoint sync"));
     if (grad_forces) {
         std::vector<double> g((size_t)A->n * 3);
         TRY_ADJ(check_cuda(cudaMemcpyAsync(g.data(), A->fgrad, g.size() * sizeof(double), cudaMemcpyDeviceToHost, st),
@@ -431,6 +449,16 @@ int ss_adjoint_get_field(ss_adjoint* A, int field, float* dst, size_t count, int
     TRY_ADJ(check_cuda(cudaMemcpyAsync(dst, d, n * sizeof(float), dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st),
                        "adjoint field"));
     if (!dst_on_device) TRY_ADJ(check_cuda(cudaStreamSynchronize(st), "adjoint field sync"));
+    return SS_OK;
+}
+
+int ss_adjoint_force_field_grad(ss_adjoint* A, float* dst, size_t count) {
+    if (!A || !dst) return set_error(SS_E_INVALID, "NULL argument");
+    const int n = A->ffgrad_n;
+    if (n <= 0 || !A->ffgrad) return set_error(SS_E_INVALID, "no force field gradient (no field, or no backward pass yet)");
+    const size_t nff = (size_t)3 * n * n * n;
+    if (count != nff) return set_error(SS_E_INVALID, "count differs from 3 * n^3 of the force field");
+    TRY_ADJ(check_cuda(cudaMemcpy(dst, A->ffgrad, nff * sizeof(float), cudaMemcpyDeviceToHost), "force field gradient"));
     return SS_OK;
 }
 

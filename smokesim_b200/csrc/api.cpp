@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <string>
 #include <vector>
 
@@ -90,6 +91,7 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->p64);
     cudaFree(s->p64b);
     cudaFree(s->render_buf);
+    cudaFree(s->ffield);
     for (auto& g : s->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     cudaFree(s->d_scale);
@@ -944,6 +946,7 @@ static int do_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* sv
         emitters_status(s, p->current_time);
         TRY(upload_array((void**)&s->d_em, &s->cap_em, s->em.data(), sizeof(ss_emitter), (int)s->em.size(), st));
         TRY(launch_emitters(s, c, st));
+        TRY(launch_force_field(s, c, st));
     }
     if (sv) {
         TRY(save_vel(s, sv->emit_vel, st));
@@ -1014,6 +1017,30 @@ int ss_run_physics_step(ss_sim* s, const ss_params* p, int nsteps, void* stream)
     return SS_OK;
 }
 
+int ss_set_force_field(ss_sim* s, int n, const float* field, void* stream) {
+    if (!s) return set_error(SS_E_INVALID, "NULL handle");
+    if (n < 0 || n > 256) return set_error(SS_E_INVALID, "force field size out of range (0..256)");
+    if (n > 0 && s->dim != 3) return set_error(SS_E_UNSUPPORTED, "the force field is 3D only");
+    if (n > 0 && !field) return set_error(SS_E_INVALID, "NULL field");
+    cudaStream_t st = as_stream(stream);
+    const size_t count = (size_t)3 * n * n * n;
+    for (size_t i = 0; i < count; ++i)
+        if (!std::isfinite(field[i])) return set_error(SS_E_NONFINITE, "force field");
+    if (n != s->ff_n) {
+        if (s->ffield) CU(cudaStreamSynchronize(st), "force field sync");
+        cudaFree(s->ffield);
+        s->ffield = nullptr;
+        s->ff_n = 0;
+        if (n > 0) CU(cudaMalloc((void**)&s->ffield, count * sizeof(float)), "cudaMalloc(force field)");
+    }
+    if (n > 0) {
+        CU(cudaMemcpyAsync(s->ffield, field, count * sizeof(float), cudaMemcpyHostToDevice, st), "force field");
+        CU(cudaStreamSynchronize(st), "force field sync");
+    }
+    s->ff_n = n;
+    return SS_OK;
+}
+
 int ss_get_stats(ss_sim* s, ss_stats* out) {
     if (!s || !out) return set_error(SS_E_INVALID, "NULL argument");
     *out = s->st;
@@ -1031,7 +1058,8 @@ int ss_handle_emitters(ss_sim* s, const ss_params* p, void* stream) {
     TRY(check_params(s, p));
     cudaStream_t st = as_stream(stream);
     TRY(upload_array((void**)&s->d_em, &s->cap_em, s->em.data(), sizeof(ss_emitter), (int)s->em.size(), st));
-    return launch_emitters(s, make_consts(s, p), st);
+    TRY(launch_emitters(s, make_consts(s, p), st));
+    return launch_force_field(s, make_consts(s, p), st);
 }
 
 int ss_advect_velocities(ss_sim* s, const ss_params* p, void* stream) {

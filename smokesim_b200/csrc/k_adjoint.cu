@@ -1204,6 +1204,62 @@ int adj_advect_velocity(ss_sim* s, const StepConsts& c, bool buoy, const float* 
     return check_cuda(cudaGetLastError(), "adjoint of advect_velocities");
 }
 
+// Adjoint of the coarse control force field (k_force_field): the face
+// velocities pass their adjoint through unchanged, and each face scatters
+// dt * ubar times its eight trilinear weights into the field's gradient (the
+// weights of the forward's lerp chain; clamped taps that coincide add up).
+SS_D void ff_taps(int n, float t, int* a, int* b, float* w) {
+    const float f = floorf(t);
+    const int i = (int)f;
+    *w = t - f;
+    *a = min(max(i, 0), n - 1);
+    *b = min(max(i + 1, 0), n - 1);
+}
+
+__global__ void __launch_bounds__(256) k_adj_force_field(const float* __restrict__ ub, const float* __restrict__ vb,
+                                                         const float* __restrict__ wb, int nx, int ny, int nz,
+                                                         float* __restrict__ G, int n, float dt) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const size_t nn = (size_t)n * n * n;
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        const float* bar = comp == 0 ? ub : comp == 1 ? vb : wb;
+        const float g = dt * bar[idx3(x, y, z, ax, ay)];
+        if (g == 0.f) continue;
+        const float xf = (float)x + (comp == 0 ? 0.f : 0.5f);
+        const float yf = (float)y + (comp == 1 ? 0.f : 0.5f);
+        const float zf = (float)z + (comp == 2 ? 0.f : 0.5f);
+        int xa, xb, ya, yb, za, zb;
+        float wx, wy, wz;
+        ff_taps(n, (xf / (float)nx) * (float)n - 0.5f, &xa, &xb, &wx);
+        ff_taps(n, (yf / (float)ny) * (float)n - 0.5f, &ya, &yb, &wy);
+        ff_taps(n, (zf / (float)nz) * (float)n - 0.5f, &za, &zb, &wz);
+        float* gc = G + comp * nn;
+        const float ax0 = 1.f - wx, ay0 = 1.f - wy, az0 = 1.f - wz;
+        atomicAdd(gc + idx3(xa, ya, za, n, n), g * ax0 * ay0 * az0);
+        atomicAdd(gc + idx3(xb, ya, za, n, n), g * wx * ay0 * az0);
+        atomicAdd(gc + idx3(xa, yb, za, n, n), g * ax0 * wy * az0);
+        atomicAdd(gc + idx3(xb, yb, za, n, n), g * wx * wy * az0);
+        atomicAdd(gc + idx3(xa, ya, zb, n, n), g * ax0 * ay0 * wz);
+        atomicAdd(gc + idx3(xb, ya, zb, n, n), g * wx * ay0 * wz);
+        atomicAdd(gc + idx3(xa, yb, zb, n, n), g * ax0 * wy * wz);
+        atomicAdd(gc + idx3(xb, yb, zb, n, n), g * wx * wy * wz);
+    }
+}
+
+int adj_force_field(ss_sim* s, const StepConsts& c, float* const ub[3], float* grad, cudaStream_t st) {
+    if (s->ff_n <= 0 || s->dim != 3) return SS_OK;
+    dim3 b(32, 8, 1);
+    dim3 g = grid_of(s->nx + 1, s->ny + 1, s->nz + 1, b);
+    k_adj_force_field<<<g, b, 0, st>>>(ub[0], ub[1], ub[2], s->nx, s->ny, s->nz, grad, s->ff_n, c.dt);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_adj_force_field");
+}
+
 int adj_buoyancy(ss_sim* s, const StepConsts& c, float* vbar, float* dbar, float* tbar, cudaStream_t st) {
     const float* vel[3] = {nullptr, nullptr, nullptr};
     AdjFluid a = adj_fluid(s, c, vel, nullptr, nullptr);

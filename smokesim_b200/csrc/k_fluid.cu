@@ -178,6 +178,69 @@ int launch_emitters(ss_sim* s, const StepConsts& c, cudaStream_t st) {
     return check_cuda(cudaGetLastError(), "k_emitters");
 }
 
+// ------------------------------------------------- coarse control force field
+// Extension (inverse control): F, three components on n^3 cell-centred samples
+// over the domain, sampled at each face position with GL_LINEAR +
+// CLAMP_TO_EDGE arithmetic (the pressure prolongation's) and added as dt * F.
+SS_D void coarse_taps(int n, float t, int* a, int* b, float* w) {
+    const float f = floorf(t);
+    const int i = (int)f;
+    *w = t - f;
+    *a = min(max(i, 0), n - 1);
+    *b = min(max(i + 1, 0), n - 1);
+}
+
+// face (x, y, z) of axis comp in the coarse texel frame
+SS_D void force_field_coords(int comp, int x, int y, int z, int nx, int ny, int nz, int n, float* tx, float* ty,
+                             float* tz) {
+    const float xf = (float)x + (comp == 0 ? 0.f : 0.5f);
+    const float yf = (float)y + (comp == 1 ? 0.f : 0.5f);
+    const float zf = (float)z + (comp == 2 ? 0.f : 0.5f);
+    *tx = (xf / (float)nx) * (float)n - 0.5f;
+    *ty = (yf / (float)ny) * (float)n - 0.5f;
+    *tz = (zf / (float)nz) * (float)n - 0.5f;
+}
+
+__global__ void __launch_bounds__(256) k_force_field(float* __restrict__ u, float* __restrict__ v,
+                                                     float* __restrict__ w, int nx, int ny, int nz,
+                                                     const float* __restrict__ F, int n, float dt) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const size_t nn = (size_t)n * n * n;
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        float tx, ty, tz;
+        force_field_coords(comp, x, y, z, nx, ny, nz, n, &tx, &ty, &tz);
+        int xa, xb, ya, yb, za, zb;
+        float wx, wy, wz;
+        coarse_taps(n, tx, &xa, &xb, &wx);
+        coarse_taps(n, ty, &ya, &yb, &wy);
+        coarse_taps(n, tz, &za, &zb, &wz);
+        const float* f = F + comp * nn;
+        const float c0 = lerp_(lerp_(__ldg(f + idx3(xa, ya, za, n, n)), __ldg(f + idx3(xb, ya, za, n, n)), wx),
+                               lerp_(__ldg(f + idx3(xa, yb, za, n, n)), __ldg(f + idx3(xb, yb, za, n, n)), wx), wy);
+        const float c1 = lerp_(lerp_(__ldg(f + idx3(xa, ya, zb, n, n)), __ldg(f + idx3(xb, ya, zb, n, n)), wx),
+                               lerp_(__ldg(f + idx3(xa, yb, zb, n, n)), __ldg(f + idx3(xb, yb, zb, n, n)), wx), wy);
+        const float val = lerp_(c0, c1, wz);
+        float* dst = comp == 0 ? u : comp == 1 ? v : w;
+        const int i = idx3(x, y, z, ax, ay);
+        dst[i] = dst[i] + dt * val;
+    }
+}
+
+int launch_force_field(ss_sim* s, const StepConsts& c, cudaStream_t st) {
+    if (s->ff_n <= 0 || s->dim != 3) return SS_OK;
+    dim3 b(32, 8, 1);
+    dim3 g = grid_for(s->nx + 1, s->ny + 1, s->nz + 1, b);
+    k_force_field<<<g, b, 0, st>>>(s->vel[0][s->vi[0]], s->vel[1][s->vi[1]], s->vel[2][s->vi[2]], s->nx, s->ny, s->nz,
+                                   s->ffield, s->ff_n, c.dt);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_force_field");
+}
+
 // ------------------------------------------------------- velocity advection
 // advect_vx / advect_vy / advect_vz (shaders3d/compute/advect_vx.comp:54-77,
 // advect_vy.comp:55-79, advect_vz.comp:55-78; 2D advect_vx.comp:50-73,

@@ -93,6 +93,8 @@ struct ss_sim {
     void* cr[SS_MAX_LEVELS] = {};       // coarse right-hand side / residual
     float* d_scale = nullptr;           // [scale, 1/scale] of the coarse storage (device)
     float force[3] = {0.f, 0.f, 0.f};   // control force on the faces inside active emitters
+    float* ffield = nullptr;            // coarse control force field, 3 * ff_n^3 (none: ff_n == 0)
+    int ff_n = 0;
     void* render_buf = nullptr;         // device image of ss_render with a host destination
     size_t render_bytes = 0;
     int rb_vec = 0;                     // level-0 kernels may work on 4 cells per thread (nx % 8 == 0)
@@ -221,6 +223,8 @@ int launch_rb_smooth_tma(ss_sim* s, float* pc, const float* po, const float* rhs
                          cudaStream_t st);
 int coarse_coop_first(const ss_sim* s);
 int launch_coarse_coop(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int prec, bool down, cudaStream_t st);
+int launch_force_field(ss_sim* s, const StepConsts& c, cudaStream_t st);
+int adj_force_field(ss_sim* s, const StepConsts& c, float* const ub[3], float* grad, cudaStream_t st);
 int launch_vorticity_field(ss_sim* s, const StepConsts& c, const float* const vel[3], float* out, cudaStream_t st);
 
 // adjoint kernels (k_adjoint.cu)

@@ -135,6 +135,18 @@ class Sim:
         f = (C.c_float * 3)(*[float(x) for x in force])
         _check(self.L.ss_set_emitter_force(self.h, C.byref(f)), "ss_set_emitter_force")
 
+    def set_force_field(self, field):
+        """Coarse control force field, shape (3, n, n, n) (None removes it)."""
+        if field is None:
+            _check(self.L.ss_set_force_field(self.h, 0, None, self.stream), "ss_set_force_field")
+            return
+        a = np.ascontiguousarray(field, dtype=np.float32)
+        n = a.shape[-1]
+        if a.shape != (3, n, n, n):
+            raise ValueError(f"force field must have shape (3, n, n, n), got {a.shape}")
+        _check(self.L.ss_set_force_field(self.h, n, a.ctypes.data_as(C.POINTER(C.c_float)), self.stream),
+               "ss_set_force_field")
+
     def clear_grid(self, t_ambient):
         _check(self.L.ss_clear_grid(self.h, C.c_float(t_ambient), self.stream), "ss_clear_grid")
 

@@ -330,3 +330,23 @@ def test_vorticity_divisor_paths(h, rho):
         g.step(p)
         o.step(p)
     assert_same(g, o, 3, f"vorticity h={h} rho={rho}")
+
+
+@pytest.mark.parametrize("n,enc,nf", [((19, 17, 13), 1, 4), ((24, 20, 18), 0, 16)])
+def test_force_field_step_bitwise(n, enc, nf):
+    """Coarse control force field (trilinear, clamp to edge, added after the
+    emitters every step): full steps match the oracle bit for bit."""
+    g, o = make_pair(3, n, 1, enc, seed=43, min_coarse=3)
+    field = np.random.default_rng(3).standard_normal((3, nf, nf, nf)).astype(np.float32) * 0.5
+    g.set_force_field(field)
+    o.set_force_field(field)
+    p = scene.workload_params(ref_quirks=0, n_coarse=10)
+    for k in range(3):
+        g.step(p)
+        o.step(p)
+        assert_same(g, o, 3, f"force field step {k}")
+    g.set_force_field(None)
+    o.set_force_field(None)
+    g.step(p)
+    o.step(p)
+    assert_same(g, o, 3, "force field removed")
