@@ -52,6 +52,12 @@ def parse():
                     help="no timing: set up, run --profile-steps steps and a few level-0 smoother sweeps (for ncu)")
     ap.add_argument("--profile-steps", type=int, default=1,
                     help="steps of the --profile run (the first one starts from the GRF state)")
+    ap.add_argument("--inverse", action="store_true",
+                    help="instead of the benchmark: the inverse-control run (plume scene at --inverse-n, per-step emitter "
+                         "forces + a 16^3 force field fitted by Adam to a target density)")
+    ap.add_argument("--inverse-n", type=int, default=128)
+    ap.add_argument("--inverse-steps", type=int, default=200)
+    ap.add_argument("--inverse-iters", type=int, default=50)
     return ap.parse_args()
 
 
@@ -332,6 +338,79 @@ def adjoint_bench(torch, stream):
     return out
 
 
+def inverse_control(args, torch, stream):
+    """Inverse control on the plume scene: per-step 3-vector emitter forces and
+    a 16^3 coarse force field, fitted with Adam (lr 1e-2) so that the final
+    density after --inverse-steps steps matches a target run whose emitters
+    are moved 10 cells apart in x.  Mixed-precision projection (FP16 coarse
+    corrections, tolerance 1e-6) in the forward; the adjoint transposes the
+    recorded refinement steps; checkpoints every ~sqrt(steps)."""
+    from smokesim_b200 import Sim, abi, scene
+    from smokesim_b200.adjoint import Rollout
+    n, nsteps, iters, nf = args.inverse_n, args.inverse_steps, args.inverse_iters, 16
+    every = max(1, int(round(nsteps ** 0.5)))
+    p = scene.workload_params(ref_quirks=0, precision=abi.PREC_MIXED, tol=1e-6, n_vcycles=40, collect_stats=0)
+    sc = scene.plume3d(seed=0, n=n)
+    sc.pop("rng", None)
+    tgt = scene.plume3d(seed=0, n=n)
+    tgt.pop("rng", None)
+    tgt["emitters"][0].pos[0] -= 5.0
+    tgt["emitters"][1].pos[0] += 5.0
+    free0, total = torch.cuda.mem_get_info()
+    ts = Sim(tgt["desc"], stream=stream.cuda_stream)
+    scene.apply(ts, tgt)
+    ts.step(p, nsteps)
+    rho_t = torch.from_numpy(ts.get_field(abi.FIELD_DENSITY).ravel()).cuda()
+    ts.close()
+    sim = Sim(sc["desc"], stream=stream.cuda_stream)
+    scene.apply(sim, sc)
+    ro = Rollout(sim, nsteps, every)
+    forces = torch.zeros((nsteps, 3), dtype=torch.float32, requires_grad=True)
+    field = torch.zeros((3, nf, nf, nf), dtype=torch.float32, requires_grad=True)
+    opt = torch.optim.Adam([forces, field], lr=1e-2)
+    rho = torch.empty(abi.field_count(3, sim.n, abi.FIELD_DENSITY), device="cuda")
+    losses, ms = [], []
+    peak_used = 0
+    e0, e_mid, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    fwd_ms, bwd_ms = [], []
+    for it in range(iters):
+        sim.set_force_field(field.detach().numpy())
+        torch.cuda.synchronize()
+        e0.record(stream)
+        ro.forward(p, forces.detach().numpy(), stream=stream.cuda_stream)
+        e_mid.record(stream)
+        sim.L.ss_get_field_device(sim.h, abi.FIELD_DENSITY, C.c_void_p(rho.data_ptr()), rho.numel(),
+                                  C.c_void_p(stream.cuda_stream))
+        with torch.cuda.stream(stream):
+            diff = rho - rho_t
+            loss = float((diff * diff).sum())
+            gd = (2.0 * diff).contiguous()
+        gf = ro.backward(p, grad_density=gd.data_ptr(), stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fwd_ms.append(e0.elapsed_time(e_mid) / nsteps)
+        bwd_ms.append(e0.elapsed_time(e1) / nsteps)
+        peak_used = max(peak_used, free0 - torch.cuda.mem_get_info()[0])
+        losses.append(loss)
+        forces.grad = torch.from_numpy(np.ascontiguousarray(gf, dtype=np.float32))
+        field.grad = torch.from_numpy(ro.force_field_grad(nf))
+        opt.step()
+        opt.zero_grad()
+    info = ro.info()
+    ro.close()
+    sim.close()
+    return {"inverse_control": {
+        "grid": [n] * 3, "steps": nsteps, "checkpoint_every": every, "iterations": iters,
+        "controls": f"{nsteps} x 3 emitter forces + 3 x {nf}^3 force field", "optimizer": "Adam lr 1e-2",
+        "precision": "mixed (f64 residual/refinement, f16 coarse), tolerance 1e-6",
+        "loss_first": losses[0], "loss_last": losses[-1], "loss_min": min(losses),
+        "loss_curve": losses,
+        "forward_with_checkpoints_ms_per_step": float(np.median(fwd_ms)),
+        "fwd_adjoint_ms_per_step": float(np.median(bwd_ms)),
+        "device_bytes_in_use_peak": int(peak_used),
+        "checkpoint_bytes": info["checkpoint_bytes"], "workspace_bytes": info["workspace_bytes"]}}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -357,6 +436,11 @@ def main():
     def barrier():
         if world > 1:
             dist.barrier()
+
+    if args.inverse:
+        out = inverse_control(args, torch, stream)
+        print(json.dumps(out))
+        return 0
 
     if args.profile_adjoint:
         from smokesim_b200.adjoint import Rollout
