@@ -267,13 +267,15 @@ def run_variant(torch, sim_cls, scene, sc, name, args, stream, barrier, world, d
 
 ADJOINT_CASES = [
     # name, scene, steps, checkpoint interval (= steps: every intermediate kept,
-    # no recomputation), projection precision of the forward
-    ("rollout64", dict(kind="rollout64", n=64), 64, 8, 0),
-    ("rollout64_no_recompute", dict(kind="rollout64", n=64), 64, 64, 0),
-    ("plume128", dict(kind="plume3d", n=128), 200, 14, 0),
+    # no recomputation), projection precision of the forward, owner-computes
+    # (deterministic) scatter-adds in the reverse pass
+    ("rollout64", dict(kind="rollout64", n=64), 64, 8, 0, False),
+    ("rollout64_no_recompute", dict(kind="rollout64", n=64), 64, 64, 0, False),
+    ("plume128", dict(kind="plume3d", n=128), 200, 14, 0, False),
     # the inverse-control configuration: mixed-precision forward (FP16 coarse
     # corrections), the recorded refinement steps transposed in the adjoint
-    ("plume128_mixed", dict(kind="plume3d", n=128), 200, 14, 1),
+    ("plume128_mixed", dict(kind="plume3d", n=128), 200, 14, 1, False),
+    ("plume128_deterministic", dict(kind="plume3d", n=128), 200, 14, 0, True),
 ]
 
 
@@ -285,7 +287,7 @@ def adjoint_bench(torch, stream):
     from smokesim_b200 import Sim, abi, scene
     from smokesim_b200.adjoint import Rollout
     out = {}
-    for name, sa, nsteps, every, prec in ADJOINT_CASES:
+    for name, sa, nsteps, every, prec, det in ADJOINT_CASES:
         sc = scene.rollout64(seed=0, n=sa["n"]) if sa["kind"] == "rollout64" else scene.plume3d(seed=0, n=sa["n"])
         sc.pop("rng", None)
         p = scene.workload_params(ref_quirks=0, n_vcycles=4, collect_stats=0, precision=prec)
@@ -309,7 +311,7 @@ def adjoint_bench(torch, stream):
         # the reverse pass leaves the simulation in the rollout's initial state)
         sim = Sim(sc["desc"], stream=stream.cuda_stream)
         scene.apply(sim, sc)
-        ro = Rollout(sim, nsteps, every)
+        ro = Rollout(sim, nsteps, every, deterministic=det)
         rho = torch.empty(abi.field_count(3, sim.n, abi.FIELD_DENSITY), device="cuda")
         for _ in range(2):
             torch.cuda.synchronize()
@@ -330,6 +332,7 @@ def adjoint_bench(torch, stream):
         sim.close()
         out[name] = {"grid": [sa["n"]] * 3, "steps": nsteps, "checkpoint_every": every,
                      "precision": "mixed (f16 coarse)" if prec else "f32",
+                     "scatter": "owner-computes" if det else "atomic",
                      "forward_ms_per_step": fwd_ms, "forward_with_checkpoints_ms_per_step": f_ms,
                      "fwd_adjoint_ms_per_step": fb_ms, "fwd_adjoint_over_forward": fb_ms / fwd_ms,
                      "fwd_adjoint_mcell_steps_per_s": cells / (fb_ms / 1e3) / 1e6,

@@ -298,6 +298,13 @@ int ss_adjoint_backward(ss_adjoint* adj, const ss_params* params, const float* g
 int ss_adjoint_field_device_ptr(ss_adjoint* adj, int field, void** dptr, size_t* count);
 /* the same copied to dst (device memory when dst_on_device, else host) */
 int ss_adjoint_get_field(ss_adjoint* adj, int field, float* dst, size_t count, int dst_on_device, void* stream);
+/* Scatter-adds of the reverse pass: on = 0 (default) sums with atomicAdd, so
+ * two reverse passes agree only to rounding; on = 1 switches to the
+ * owner-computes variant (each destination enumerates the sources whose
+ * trilinear taps cover it and sums them in a fixed order), which gives
+ * bitwise-identical gradients run to run at a higher cost.  Allocates its
+ * scratch (32 bytes per face) on first use. */
+int ss_adjoint_set_deterministic(ss_adjoint* adj, int on);
 /* Statistics of the last reverse pass: kernel launches and device bytes held
  * by checkpoints and recomputation buffers. */
 int ss_adjoint_info(ss_adjoint* adj, long long* kernel_launches, long long* checkpoint_bytes, long long* workspace_bytes);

@@ -17,15 +17,22 @@ from .sim import Sim, _check
 
 class Rollout:
     """nsteps steps of `sim` from its current state, checkpointed every
-    `checkpoint_every` steps."""
+    `checkpoint_every` steps.  deterministic=True makes the reverse pass's
+    scatter-adds owner-computes (bitwise-repeatable gradients) instead of
+    atomic."""
 
-    def __init__(self, sim: Sim, nsteps: int, checkpoint_every: int = 0):
+    def __init__(self, sim: Sim, nsteps: int, checkpoint_every: int = 0, deterministic: bool = False):
         self.sim = sim
         self.L = sim.L
         self.nsteps = nsteps
         h = C.c_void_p()
         _check(self.L.ss_adjoint_create(sim.h, nsteps, checkpoint_every, C.byref(h)), "ss_adjoint_create")
         self.h = h
+        if deterministic:
+            self.set_deterministic(True)
+
+    def set_deterministic(self, on: bool = True):
+        _check(self.L.ss_adjoint_set_deterministic(self.h, int(bool(on))), "ss_adjoint_set_deterministic")
 
     def close(self):
         if getattr(self, "h", None):

@@ -63,6 +63,8 @@ struct ss_adjoint {
     int ffgrad_n = 0;          // ff_n that ffgrad was sized and last filled for
     std::vector<void*> allocs;
     long long launches = 0, ckpt_bytes = 0, work_bytes = 0;
+    AdjOwner own{};                // owner-computes scratch (allocated when first enabled)
+    bool deterministic = false;    // owner-computes scatters instead of atomics
     bool forward_done = false;
     bool last_recorded = false;   // rec holds the last segment, written by the forward pass
     // the transposed V-cycles of one step, recorded once as a CUDA graph
@@ -237,11 +239,12 @@ static int adj_step(ss_adjoint* A, const ss_params* p, int k, const Record& R, c
     const StepConsts c = make_consts(s, p);
     const int m = p->stage_mask;
     const size_t ncell = s->ncell;
+    const AdjOwner* own = A->deterministic ? &A->own : nullptr;
     if (m & SS_STAGE_ADVECT_SMOKE) {
         TRY_ADJ(check_cuda(cudaMemsetAsync(A->db2, 0, ncell * s->nch * 4, st), "memset"));
         TRY_ADJ(check_cuda(cudaMemsetAsync(A->tb2, 0, ncell * 4, st), "memset"));
         const float* vel[3] = {R.un[0], R.un[1], R.un[2]};
-        TRY_ADJ(adj_advect_smoke(s, c, vel, R.dens_e, R.temp_e, A->db, A->tb, A->db2, A->tb2, A->vc3, A->ub, st));
+        TRY_ADJ(adj_advect_smoke(s, c, vel, R.dens_e, R.temp_e, A->db, A->tb, A->db2, A->tb2, A->vc3, A->ub, st, own));
         std::swap(A->db, A->db2);
         std::swap(A->tb, A->tb2);
     }
@@ -257,14 +260,14 @@ static int adj_step(ss_adjoint* A, const ss_params* p, int k, const Record& R, c
         const float* vel[3] = {R.ue[0], R.ue[1], R.ue[2]};
         const float* gin[3] = {A->ub[0], A->ub[1], A->ub[2]};
         TRY_ADJ(adj_advect_velocity(s, c, (m & SS_STAGE_APPLY_BUOYANCY) != 0, vel, R.dens_e, R.temp_e, gin, A->ub2,
-                                    A->db, A->tb, st));
+                                    A->db, A->tb, st, own));
         for (int d = 0; d < 3; ++d) std::swap(A->ub[d], A->ub2[d]);
     } else if (m & SS_STAGE_APPLY_BUOYANCY) {
-        TRY_ADJ(adj_buoyancy(s, c, A->ub[1], A->db, A->tb, st));
+        TRY_ADJ(adj_buoyancy(s, c, A->ub[1], A->db, A->tb, st, own));
     }
     if (m & SS_STAGE_HANDLE_EMITTERS) {
         // the force field came after the emitters: its transpose first
-        if (s->ff_n > 0) TRY_ADJ(adj_force_field(s, c, A->ub, A->ffgrad, st));
+        if (s->ff_n > 0) TRY_ADJ(adj_force_field(s, c, A->ub, A->ffgrad, st, own));
         // the emitter records of this step (their status changes over time)
         if (!R.em.empty())
             TRY_ADJ(check_cuda(cudaMemcpyAsync(s->d_em, R.em.data(), R.em.size() * sizeof(ss_emitter),
@@ -394,6 +397,7 @@ int ss_adjoint_backward(ss_adjoint* A, const ss_params* p, const float* grad_den
         }
         TRY_ADJ(check_cuda(cudaMemsetAsync(A->ffgrad, 0, nff * sizeof(float), st), "memset"));
     }
+    if (A->deterministic) TRY_ADJ(check_cuda(cudaMemsetAsync(A->own.win, 0, 24 * sizeof(int), st), "memset"));
     const int nseg = (A->n + A->every - 1) / A->every;
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int k0 = sg * A->every, k1 = std::min(A->n, k0 + A->every);
@@ -415,6 +419,14 @@ int ss_adjoint_backward(ss_adjoint* A, const ss_params* p, const float* grad_den
                            "force gradient"));
         TRY_ADJ(check_cuda(cudaStreamSynchronize(st), "adjoint sync"));
         for (size_t i = 0; i < g.size(); ++i) grad_forces[i] = (float)g[i];
+    }
+    if (A->deterministic) {
+        int err = 0;
+        TRY_ADJ(check_cuda(cudaMemcpyAsync(&err, A->own.win + 23, sizeof(int), cudaMemcpyDeviceToHost, st), "reach flag"));
+        TRY_ADJ(check_cuda(cudaStreamSynchronize(st), "adjoint sync"));
+        if (err)
+            return set_error(SS_E_INVALID, "a back-traced point lies more than 8 cells from its source: the "
+                                           "owner-computes scatters enumerate at most 8; use the atomic ones");
     }
     return check_cuda(cudaGetLastError(), "adjoint backward");
 }
@@ -459,6 +471,20 @@ int ss_adjoint_force_field_grad(ss_adjoint* A, float* dst, size_t count) {
     const size_t nff = (size_t)3 * n * n * n;
     if (count != nff) return set_error(SS_E_INVALID, "count differs from 3 * n^3 of the force field");
     TRY_ADJ(check_cuda(cudaMemcpy(dst, A->ffgrad, nff * sizeof(float), cudaMemcpyDeviceToHost), "force field gradient"));
+    return SS_OK;
+}
+
+int ss_adjoint_set_deterministic(ss_adjoint* A, int on) {
+    if (!A) return set_error(SS_E_INVALID, "NULL handle");
+    if (on && !A->own.win) {
+        ss_sim* s = A->s;
+        for (int d = 0; d < s->dim; ++d) {
+            TRY_ADJ(amalloc(A, &A->own.tr[d], s->nv[d] * 16, &A->work_bytes));
+            TRY_ADJ(amalloc(A, &A->own.vq[d], s->nv[d] * 16, &A->work_bytes));
+        }
+        TRY_ADJ(amalloc(A, (void**)&A->own.win, 24 * sizeof(int), &A->work_bytes));
+    }
+    A->deterministic = on != 0;
     return SS_OK;
 }
 

@@ -115,6 +115,46 @@ struct AdjFluid {
 // solid cells set to (0, t_amb).  Adjoint: scatter into din/tin, and the
 // position gradient into a per-cell velocity adjoint (vcb, 3 arrays), spread to
 // the faces by k_adj_centre_to_faces.
+// Per-cell part, shared with the owner-computes trace pass: the position
+// gradient vb, the back-traced point clamped as make_taps clamps it (tc), and,
+// when din / tin are given, the scatter of the adjoints into them.  Returns
+// false for a solid cell, which scatters nothing.
+template <int DIM>
+SS_D bool smoke_cell_adj(const AdjFluid& a, int x, int y, int z, const float* __restrict__ dout,
+                         const float* __restrict__ tout, float* din, float* tin, float vb[3], float tc[3]) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int c = idx3(x, y, z, nx, ny);
+    const size_t ncell = (size_t)nx * ny * nz;
+    vb[0] = vb[1] = vb[2] = 0.f;
+    if (a.flags[c] & F_SOLID) return false;
+    float vel[3];
+    vel_at_centre<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+    const float cfl = a.c.cfl;
+    const float gx = (float)x + 0.5f, gy = (float)y + 0.5f, gz = DIM == 3 ? (float)z + 0.5f : 0.f;
+    const float tx = gx - vel[0] * cfl - 0.5f, ty = gy - vel[1] * cfl - 0.5f, tz = gz - vel[2] * cfl - 0.5f;
+    const Taps t = make_taps<DIM>(nx, ny, nz, tx, ty, tz);
+    float bb[3] = {0.f, 0.f, 0.f};
+    float dw[3];
+    for (int ch = 0; ch <= a.nch; ++ch) {
+        const bool is_t = ch == a.nch;
+        const float g = is_t ? tout[c] : dout[ch * ncell + c];
+        if (g == 0.f) continue;
+        const float* src = is_t ? a.temp : a.dens + ch * ncell;
+        float* dst = din ? (is_t ? tin : din + ch * ncell) : nullptr;
+        adj_sample<DIM>(src, dst, nx, ny, nz, t, is_t ? a.c.t_amb : 0.f, g, dw);
+        bb[0] += g * dw[0];
+        bb[1] += g * dw[1];
+        bb[2] += g * dw[2];
+    }
+    vb[0] = -cfl * bb[0] * clamp_grad(tx, nx);
+    vb[1] = -cfl * bb[1] * clamp_grad(ty, ny);
+    vb[2] = DIM == 3 ? -cfl * bb[2] * clamp_grad(tz, nz) : 0.f;
+    tc[0] = clampt(tx, -2.f, (float)(nx + 1));
+    tc[1] = clampt(ty, -2.f, (float)(ny + 1));
+    tc[2] = DIM == 3 ? clampt(tz, -2.f, (float)(nz + 1)) : 0.f;
+    return true;
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(256) k_adj_advect_smoke(AdjFluid a, const float* __restrict__ dout, const float* __restrict__ tout,
                                                           float* __restrict__ din, float* __restrict__ tin,
@@ -126,31 +166,8 @@ __global__ void __launch_bounds__(256) k_adj_advect_smoke(AdjFluid a, const floa
     if (x >= nx || y >= ny || z >= nz) return;
     const int c = idx3(x, y, z, nx, ny);
     const size_t ncell = (size_t)nx * ny * nz;
-    float vb[3] = {0.f, 0.f, 0.f};
-    if (!(a.flags[c] & F_SOLID)) {
-        float vel[3];
-        vel_at_centre<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
-        const float cfl = a.c.cfl;
-        const float gx = (float)x + 0.5f, gy = (float)y + 0.5f, gz = DIM == 3 ? (float)z + 0.5f : 0.f;
-        const float tx = gx - vel[0] * cfl - 0.5f, ty = gy - vel[1] * cfl - 0.5f, tz = gz - vel[2] * cfl - 0.5f;
-        const Taps t = make_taps<DIM>(nx, ny, nz, tx, ty, tz);
-        float bb[3] = {0.f, 0.f, 0.f};
-        float dw[3];
-        for (int ch = 0; ch <= a.nch; ++ch) {
-            const bool is_t = ch == a.nch;
-            const float g = is_t ? tout[c] : dout[ch * ncell + c];
-            if (g == 0.f) continue;
-            const float* src = is_t ? a.temp : a.dens + ch * ncell;
-            float* dst = is_t ? tin : din + ch * ncell;
-            adj_sample<DIM>(src, dst, nx, ny, nz, t, is_t ? a.c.t_amb : 0.f, g, dw);
-            bb[0] += g * dw[0];
-            bb[1] += g * dw[1];
-            bb[2] += g * dw[2];
-        }
-        vb[0] = -cfl * bb[0] * clamp_grad(tx, nx);
-        vb[1] = -cfl * bb[1] * clamp_grad(ty, ny);
-        vb[2] = DIM == 3 ? -cfl * bb[2] * clamp_grad(tz, nz) : 0.f;
-    }
+    float vb[3], tc[3];
+    smoke_cell_adj<DIM>(a, x, y, z, dout, tout, din, tin, vb, tc);
     vcb[c] = vb[0];
     vcb[ncell + c] = vb[1];
     if (DIM == 3) vcb[2 * ncell + c] = vb[2];
@@ -573,6 +590,52 @@ __global__ void __launch_bounds__(256) k_adj_vort3(const float* __restrict__ wba
 // Forward: k_advect_velocity<DIM, BUOY>.  gin: adjoint of the advected
 // (and buoyancy-forced) velocity; outputs accumulate (atomically) into
 // ubar/vbar/wbar (input velocity) and dbar/tbar (smoke, through buoyancy).
+//
+// Per-face part, shared with the owner-computes trace pass: what the face of
+// axis comp with adjoint g != 0 passes back, as flags: kKeep (a y face next
+// to solid keeps its pre-advection value: g goes to the face itself), kBuoy
+// (the y face's buoyancy: g goes to the two cells' smoke), kSample (a traced
+// sample: tc = the back-traced point clamped as make_taps clamps it, vb = the
+// position gradient; with srcb the sample's adjoint is scattered into it).
+enum { kKeep = 1, kBuoy = 2, kSample = 4 };
+template <int DIM, bool BUOY>
+SS_D int vel_face_adj(const AdjFluid& a, int comp, int x, int y, int z, float g, bool s_c, float* srcb, float tc[3],
+                      float vb[3]) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+    int f = 0;
+    if (BUOY && comp == 1) {
+        if (solid0(a.flags, x, y, z, nx, ny, nz) || solid0(a.flags, x, y - 1, z, nx, ny, nz)) return kKeep;
+        f = kBuoy;
+    }
+    const int id = comp == 0 ? x : comp == 1 ? y : z;
+    if (id == 0 && a.c.wind[comp] != 0.f) return f;
+    if (s_c || solid1(a.flags, x - (comp == 0), y - (comp == 1), z - (comp == 2), nx, ny, nz)) return f;
+    const float cfl = a.c.cfl;
+    const float* src = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
+    float vel[3];
+    if (comp == 0) vel_at_xface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+    else if (comp == 1) vel_at_yface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+    else vel_at_zface(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+    const float gx = (float)x + (comp == 0 ? 0.f : 0.5f);
+    const float gy = (float)y + (comp == 1 ? 0.f : 0.5f);
+    const float gz = DIM == 3 ? (float)z + (comp == 2 ? 0.f : 0.5f) : 0.f;
+    const float tx = gx - vel[0] * cfl - (comp == 0 ? 0.f : 0.5f);
+    const float ty = gy - vel[1] * cfl - (comp == 1 ? 0.f : 0.5f);
+    const float tz = gz - vel[2] * cfl - (comp == 2 ? 0.f : 0.5f);
+    const Taps t = make_taps<DIM>(ax, ay, az, tx, ty, tz);
+    float dw[3];
+    adj_sample<DIM>(src, srcb, ax, ay, az, t, 0.f, g, dw);
+    // back-trace position -> the velocity that traced it
+    vb[0] = -cfl * g * dw[0] * clamp_grad(tx, ax);
+    vb[1] = -cfl * g * dw[1] * clamp_grad(ty, ay);
+    vb[2] = DIM == 3 ? -cfl * g * dw[2] * clamp_grad(tz, az) : 0.f;
+    tc[0] = clampt(tx, -2.f, (float)(ax + 1));
+    tc[1] = clampt(ty, -2.f, (float)(ay + 1));
+    tc[2] = DIM == 3 ? clampt(tz, -2.f, (float)(az + 1)) : 0.f;
+    return f | kSample;
+}
+
 template <int DIM, bool BUOY>
 __global__ void __launch_bounds__(256) k_adj_advect_velocity(AdjFluid a, const float* __restrict__ gu, const float* __restrict__ gv,
                                                              const float* __restrict__ gw, float* __restrict__ ub,
@@ -582,7 +645,6 @@ __global__ void __launch_bounds__(256) k_adj_advect_velocity(AdjFluid a, const f
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const float cfl = a.c.cfl;
     const bool s_c = solid1(a.flags, x, y, z, nx, ny, nz);
 #pragma unroll
     for (int comp = 0; comp < DIM; ++comp) {
@@ -591,14 +653,11 @@ __global__ void __launch_bounds__(256) k_adj_advect_velocity(AdjFluid a, const f
         const int i = idx3(x, y, z, ax, ay);
         const float g = (comp == 0 ? gu : comp == 1 ? gv : gw)[i];
         if (g == 0.f) continue;
-        const int id = comp == 0 ? x : comp == 1 ? y : z;
         float* srcb = comp == 0 ? ub : comp == 1 ? vbar : wb;
-        const float* src = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
-        if (BUOY && comp == 1) {
-            if (solid0(a.flags, x, y, z, nx, ny, nz) || solid0(a.flags, x, y - 1, z, nx, ny, nz)) {
-                atomicAdd(srcb + i, g);   // the face keeps its pre-advection value
-                continue;
-            }
+        float tc[3], vb[3];
+        const int f = vel_face_adj<DIM, BUOY>(a, comp, x, y, z, g, s_c, srcb, tc, vb);
+        if (f & kKeep) atomicAdd(srcb + i, g);
+        if (f & kBuoy) {
             // buoyancy: dt*(-alpha*sum_ch mean(dens) + beta*(mean(T) - t_amb)), means over the cells y-1, y
             const size_t ncell = (size_t)nx * ny * nz;
             const float gd = -a.c.alpha * g * a.c.dt * 0.5f;
@@ -610,28 +669,10 @@ __global__ void __launch_bounds__(256) k_adj_advect_velocity(AdjFluid a, const f
             scatter(tbar, nx, ny, nz, x, y - 1, z, gt);
             scatter(tbar, nx, ny, nz, x, y, z, gt);
         }
-        if (id == 0 && a.c.wind[comp] != 0.f) continue;
-        if (s_c || solid1(a.flags, x - (comp == 0), y - (comp == 1), z - (comp == 2), nx, ny, nz)) continue;
-        float vel[3];
-        if (comp == 0) vel_at_xface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
-        else if (comp == 1) vel_at_yface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
-        else vel_at_zface(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
-        const float gx = (float)x + (comp == 0 ? 0.f : 0.5f);
-        const float gy = (float)y + (comp == 1 ? 0.f : 0.5f);
-        const float gz = DIM == 3 ? (float)z + (comp == 2 ? 0.f : 0.5f) : 0.f;
-        const float tx = gx - vel[0] * cfl - (comp == 0 ? 0.f : 0.5f);
-        const float ty = gy - vel[1] * cfl - (comp == 1 ? 0.f : 0.5f);
-        const float tz = gz - vel[2] * cfl - (comp == 2 ? 0.f : 0.5f);
-        const Taps t = make_taps<DIM>(ax, ay, az, tx, ty, tz);
-        float dw[3];
-        adj_sample<DIM>(src, srcb, ax, ay, az, t, 0.f, g, dw);
-        // back-trace position -> the velocity that traced it
-        const float vb0 = -cfl * g * dw[0] * clamp_grad(tx, ax);
-        const float vb1 = -cfl * g * dw[1] * clamp_grad(ty, ay);
-        const float vb2 = DIM == 3 ? -cfl * g * dw[2] * clamp_grad(tz, az) : 0.f;
-        const float q0 = 0.25f * vb0, q1 = 0.25f * vb1, q2 = 0.25f * vb2;
+        if (!(f & kSample)) continue;
+        const float q0 = 0.25f * vb[0], q1 = 0.25f * vb[1], q2 = 0.25f * vb[2];
         if (comp == 0) {
-            atomicAdd(ub + i, vb0);
+            atomicAdd(ub + i, vb[0]);
             // v at (i-1/2, j+1/2, k): v(i-1,j), v(i,j), v(i-1,j+1), v(i,j+1)
             scatter(vbar, nx, ny + 1, nz, x - 1, y, z, q1); scatter(vbar, nx, ny + 1, nz, x, y, z, q1);
             scatter(vbar, nx, ny + 1, nz, x - 1, y + 1, z, q1); scatter(vbar, nx, ny + 1, nz, x, y + 1, z, q1);
@@ -640,7 +681,7 @@ __global__ void __launch_bounds__(256) k_adj_advect_velocity(AdjFluid a, const f
                 scatter(wb, nx, ny, nz + 1, x - 1, y, z + 1, q2); scatter(wb, nx, ny, nz + 1, x, y, z + 1, q2);
             }
         } else if (comp == 1) {
-            atomicAdd(vbar + i, vb1);
+            atomicAdd(vbar + i, vb[1]);
             scatter(ub, nx + 1, ny, nz, x, y - 1, z, q0); scatter(ub, nx + 1, ny, nz, x + 1, y - 1, z, q0);
             scatter(ub, nx + 1, ny, nz, x, y, z, q0); scatter(ub, nx + 1, ny, nz, x + 1, y, z, q0);
             if (DIM == 3) {
@@ -648,7 +689,7 @@ __global__ void __launch_bounds__(256) k_adj_advect_velocity(AdjFluid a, const f
                 scatter(wb, nx, ny, nz + 1, x, y - 1, z + 1, q2); scatter(wb, nx, ny, nz + 1, x, y, z + 1, q2);
             }
         } else {
-            atomicAdd(wb + i, vb2);
+            atomicAdd(wb + i, vb[2]);
             scatter(ub, nx + 1, ny, nz, x, y, z - 1, q0); scatter(ub, nx + 1, ny, nz, x + 1, y, z - 1, q0);
             scatter(ub, nx + 1, ny, nz, x, y, z, q0); scatter(ub, nx + 1, ny, nz, x + 1, y, z, q0);
             scatter(vbar, nx, ny + 1, nz, x, y, z - 1, q1); scatter(vbar, nx, ny + 1, nz, x, y + 1, z - 1, q1);
@@ -757,6 +798,299 @@ __global__ void k_sum3(const double* __restrict__ part, int n, double* __restric
         for (int q = 0; q < 3; ++q) out[q] = sh[q][0];
 }
 
+// ------------------------------------------ deterministic owner-computes
+// The scatter-adds above sum in the order the atomics land, so two reverse
+// passes agree only to rounding.  The owner-computes variant fixes the order:
+// a trace pass stores, per source element, its back-traced point clamped as
+// make_taps clamps it (w = 0 when the element scatters nothing) and the
+// per-axis reach of its taps (block maxima of s - x0 and x0 - s, where x0 =
+// floor of the point); a gather pass then lets every destination element d
+// enumerate the box of sources whose taps can cover it (the inverse footprint:
+// s in [d - max(x0 - s) - 1, d + max(s - x0)] per axis), in a fixed order,
+// and add their weighted adjoints itself.  Integer maxima commute, so the
+// boxes do not depend on the order the blocks finish in either.
+
+// block maximum of the tap reaches, into win[0..5]: s - x0 per axis, then x0 - s
+SS_D void reach_max(int* win, const int v[6]) {
+    __shared__ int sw[6];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    if (tid < 6) sw[tid] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const int m = __reduce_max_sync(0xffffffffu, v[q]);
+        if ((tid & 31) == 0 && m > 0) atomicMax(&sw[q], m);
+    }
+    __syncthreads();
+    if (tid < 6 && sw[tid] > 0) atomicMax(win + tid, sw[tid]);
+}
+
+SS_D void reach_of(const float tc[3], int x, int y, int z, int dim, int v[6]) {
+    const int p[3] = {x, y, z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int x0 = d < dim ? (int)floorf(tc[d]) : p[d];
+        v[d] = p[d] - x0;
+        v[3 + d] = x0 - p[d];
+    }
+}
+
+// Longest tap reach the gather passes enumerate (boxes of at most 2 * 8 + 2
+// sources per axis); longer back-traces set the error word kOwnerErr of the
+// reach array, which the host reports, instead of running for minutes.
+constexpr int kOwnerMaxReach = 8;
+constexpr int kOwnerErr = 23;
+
+// the box of sources whose taps can cover the element (x, y, z) of an
+// (ax, ay, az) array, from the reaches win[0..5]; false (and the error word
+// err set) when a reach exceeds kOwnerMaxReach
+SS_D bool owner_box(const int* __restrict__ win, int* err, int x, int y, int z, int ax, int ay, int az, int dim,
+                    int lo[3], int hi[3]) {
+    const int p[3] = {x, y, z}, n[3] = {ax, ay, az};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (d >= dim) { lo[d] = hi[d] = p[d]; continue; }
+        const int back = __ldg(win + 3 + d), fwd = __ldg(win + d);
+        if (back > kOwnerMaxReach || fwd > kOwnerMaxReach) {
+            *err = 1;
+            return false;
+        }
+        lo[d] = max(p[d] - back - 1, 0);
+        hi[d] = min(p[d] + fwd, n[d] - 1);
+    }
+    return true;
+}
+
+// trilinear weight with which the sample at the traced point t covers the
+// element (x, y, z); false when it is not one of the sample's taps
+template <int DIM>
+SS_D bool cover(const float4& t, int x, int y, int z, float* w) {
+    const float fx = floorf(t.x), fy = floorf(t.y);
+    const int ix = x - (int)fx, iy = y - (int)fy;
+    if ((unsigned)ix > 1u || (unsigned)iy > 1u) return false;
+    const float wx = t.x - fx, wy = t.y - fy;
+    float r = (ix ? wx : 1.f - wx) * (iy ? wy : 1.f - wy);
+    if constexpr (DIM == 3) {
+        const float fz = floorf(t.z);
+        const int iz = z - (int)fz;
+        if ((unsigned)iz > 1u) return false;
+        const float wz = t.z - fz;
+        r = r * (iz ? wz : 1.f - wz);
+    }
+    *w = r;
+    return true;
+}
+
+// smoke advection, trace pass: vcb as k_adj_advect_smoke writes it, tr = the
+// cell's clamped back-traced point (w = 1; 0 for a solid cell), reaches into win
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_trace_smoke(AdjFluid a, const float* __restrict__ dout,
+                                                         const float* __restrict__ tout, float* __restrict__ vcb,
+                                                         float4* __restrict__ tr, int* __restrict__ win) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    int v[6] = {0, 0, 0, 0, 0, 0};
+    if (x < nx && y < ny && z < nz) {
+        const int c = idx3(x, y, z, nx, ny);
+        const size_t ncell = (size_t)nx * ny * nz;
+        float vb[3], tc[3];
+        const bool live = smoke_cell_adj<DIM>(a, x, y, z, dout, tout, nullptr, nullptr, vb, tc);
+        vcb[c] = vb[0];
+        vcb[ncell + c] = vb[1];
+        if (DIM == 3) vcb[2 * ncell + c] = vb[2];
+        tr[c] = live ? make_float4(tc[0], tc[1], tc[2], 1.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (live) reach_of(tc, x, y, z, DIM, v);
+    }
+    reach_max(win, v);
+}
+
+// smoke advection, gather pass: every cell adds the sampled adjoints of the
+// cells whose back-traced sample covers it, sources in z, y, x order
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_gather_smoke(const float4* __restrict__ tr, const int* __restrict__ win,
+                                                          int* __restrict__ err, int nx, int ny, int nz, int nch,
+                                                          const float* __restrict__ dout, const float* __restrict__ tout,
+                                                          float* __restrict__ din, float* __restrict__ tin) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (x >= nx || y >= ny || z >= nz) return;
+    const size_t ncell = (size_t)nx * ny * nz;
+    int lo[3], hi[3];
+    if (!owner_box(win, err, x, y, z, nx, ny, nz, DIM, lo, hi)) return;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};   // channels 0..2, temperature
+    for (int sz = lo[2]; sz <= hi[2]; ++sz)
+        for (int sy = lo[1]; sy <= hi[1]; ++sy)
+            for (int sx = lo[0]; sx <= hi[0]; ++sx) {
+                const int s = idx3(sx, sy, sz, nx, ny);
+                const float4 t = __ldg(tr + s);
+                float w;
+                if (t.w == 0.f || !cover<DIM>(t, x, y, z, &w)) continue;
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) {
+                    if (ch >= nch) break;
+                    const float g = __ldg(dout + ch * ncell + s);
+                    if (g != 0.f) acc[ch] += g * w;
+                }
+                const float g = __ldg(tout + s);
+                if (g != 0.f) acc[3] += g * w;
+            }
+    const int c = idx3(x, y, z, nx, ny);
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch)
+        if (ch < nch) din[ch * ncell + c] += acc[ch];
+    tin[c] += acc[3];
+}
+
+struct OwnerFaces {
+    float4* tr[3];   // per face: clamped back-traced point, w = g (0: no sample)
+    float4* vq[3];   // per face: position gradient (x, y, z), w = g kept by the face itself
+    int* win;        // 6 reaches per component
+};
+
+// velocity advection, trace pass: per face the outcome of vel_face_adj,
+// nothing scattered
+template <int DIM, bool BUOY>
+__global__ void __launch_bounds__(256) k_adj_trace_velocity(AdjFluid a, const float* __restrict__ gu, const float* __restrict__ gv,
+                                                            const float* __restrict__ gw, OwnerFaces o) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const bool s_c = solid1(a.flags, x, y, z, nx, ny, nz);
+#pragma unroll
+    for (int comp = 0; comp < DIM; ++comp) {
+        const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+        int v[6] = {0, 0, 0, 0, 0, 0};
+        if (x < ax && y < ay && z < az) {
+            const int i = idx3(x, y, z, ax, ay);
+            const float g = (comp == 0 ? gu : comp == 1 ? gv : gw)[i];
+            float4 t = make_float4(0.f, 0.f, 0.f, 0.f), q = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (g != 0.f) {
+                float tc[3], vb[3];
+                const int f = vel_face_adj<DIM, BUOY>(a, comp, x, y, z, g, s_c, nullptr, tc, vb);
+                if (f & kKeep) q.w = g;
+                if (f & kSample) {
+                    t = make_float4(tc[0], tc[1], tc[2], g);
+                    q.x = vb[0]; q.y = vb[1]; q.z = vb[2];
+                    reach_of(tc, x, y, z, DIM, v);
+                }
+            }
+            o.tr[comp][i] = t;
+            o.vq[comp][i] = q;
+        }
+        reach_max(o.win + 6 * comp, v);
+    }
+}
+
+SS_D float comp_of(const float4& q, int d) { return d == 0 ? q.x : d == 1 ? q.y : q.z; }
+
+// velocity advection, gather pass: every face adds, in this order, the
+// sampled adjoints of the faces of its axis whose sample covers it (sources
+// in z, y, x order), its own position gradient, the quarter position
+// gradients of the four faces of each other axis whose interpolated velocity
+// it entered (offsets +a e_c - b e_d), and the value a solid-adjacent y face
+// keeps; every cell then adds the buoyancy of its y faces y and y + 1.
+template <int DIM, bool BUOY>
+__global__ void __launch_bounds__(256) k_adj_gather_velocity(AdjFluid a, const float* __restrict__ gv, OwnerFaces o,
+                                                             float* __restrict__ ub, float* __restrict__ vbar,
+                                                             float* __restrict__ wb, float* __restrict__ dbar,
+                                                             float* __restrict__ tbar) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        const int ax = nx + (d == 0), ay = ny + (d == 1), az = nz + (d == 2);
+        if (x >= ax || y >= ay || z >= az) continue;
+        const int i = idx3(x, y, z, ax, ay);
+        float* dst = d == 0 ? ub : d == 1 ? vbar : wb;
+        float acc = dst[i];
+        int lo[3], hi[3];
+        if (!owner_box(o.win + 6 * d, o.win + kOwnerErr, x, y, z, ax, ay, az, DIM, lo, hi)) return;
+        const float4* tr = o.tr[d];
+        for (int sz = lo[2]; sz <= hi[2]; ++sz)
+            for (int sy = lo[1]; sy <= hi[1]; ++sy)
+                for (int sx = lo[0]; sx <= hi[0]; ++sx) {
+                    const float4 t = __ldg(tr + idx3(sx, sy, sz, ax, ay));
+                    float w;
+                    if (t.w != 0.f && cover<DIM>(t, x, y, z, &w)) acc += t.w * w;
+                }
+        const float4 own = __ldg(o.vq[d] + i);
+        acc += comp_of(own, d);
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+            if (c == d) continue;
+            const int cx = nx + (c == 0), cy = ny + (c == 1), cz = nz + (c == 2);
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int sx = x + (c == 0 ? e : 0) - (d == 0 ? b : 0);
+                    const int sy = y + (c == 1 ? e : 0) - (d == 1 ? b : 0);
+                    const int sz = z + (c == 2 ? e : 0) - (d == 2 ? b : 0);
+                    if (!in3(sx, sy, sz, cx, cy, cz)) continue;
+                    const float qv = 0.25f * comp_of(__ldg(o.vq[c] + idx3(sx, sy, sz, cx, cy)), d);
+                    if (qv != 0.f) acc += qv;
+                }
+        }
+        if (BUOY && d == 1) acc += own.w;
+        dst[i] = acc;
+    }
+    if (BUOY && x < nx && y < ny && z < nz) {
+        const size_t ncell = (size_t)nx * ny * nz;
+        const int c = idx3(x, y, z, nx, ny);
+        float dsum = 0.f, tsum = 0.f;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int fy = y + k;   // the face below, then the face above the cell
+            const float g = gv[idx3(x, fy, z, nx, ny + 1)];
+            if (g == 0.f) continue;
+            if (solid0(a.flags, x, fy, z, nx, ny, nz) || solid0(a.flags, x, fy - 1, z, nx, ny, nz)) continue;
+            dsum += -a.c.alpha * g * a.c.dt * 0.5f;
+            tsum += a.c.beta * g * a.c.dt * 0.5f;
+        }
+        if (dsum != 0.f)
+            for (int ch = 0; ch < a.nch; ++ch) dbar[ch * ncell + c] += dsum;
+        if (tsum != 0.f) tbar[c] += tsum;
+    }
+}
+
+// stand-alone buoyancy^T, owner-computes: each cell gathers its two y faces
+// (read before any face is cleared: a face is cleared only when it touches
+// solid, and then it contributes nothing)
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_buoyancy_owner(AdjFluid a, float* __restrict__ vbar, float* __restrict__ dbar,
+                                                            float* __restrict__ tbar) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    if (x >= nx || y >= ny + 1 || z >= nz) return;
+    const bool solid_face = solid0(a.flags, x, y, z, nx, ny, nz) || solid0(a.flags, x, y - 1, z, nx, ny, nz);
+    if (y < ny) {
+        const size_t ncell = (size_t)nx * ny * nz;
+        const int c = idx3(x, y, z, nx, ny);
+        float dsum = 0.f, tsum = 0.f;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int fy = y + k;
+            if (solid0(a.flags, x, fy, z, nx, ny, nz) || solid0(a.flags, x, fy - 1, z, nx, ny, nz)) continue;
+            const float g = vbar[idx3(x, fy, z, nx, ny + 1)];
+            if (g == 0.f) continue;
+            dsum += -a.c.alpha * g * a.c.dt * 0.5f;
+            tsum += a.c.beta * g * a.c.dt * 0.5f;
+        }
+        if (dsum != 0.f)
+            for (int ch = 0; ch < a.nch; ++ch) dbar[ch * ncell + c] += dsum;
+        if (tsum != 0.f) tbar[c] += tsum;
+    }
+    if (solid_face) vbar[idx3(x, y, z, nx, ny + 1)] = 0.f;
+}
+
 // ------------------------------------------------------------------- host
 static AdjFluid adj_fluid(const ss_sim* s, const StepConsts& c, const float* const vel[3], const float* dens,
                           const float* temp) {
@@ -773,10 +1107,25 @@ static const dim3 kB(32, 8, 1);
 
 int adj_advect_smoke(ss_sim* s, const StepConsts& c, const float* const vel[3], const float* dens, const float* temp,
                      const float* dout, const float* tout, float* din, float* tin, float* vcb, float* const vb[3],
-                     cudaStream_t st) {
+                     cudaStream_t st, const AdjOwner* own) {
     AdjFluid a = adj_fluid(s, c, vel, dens, temp);
     dim3 g = grid_of(s->nx, s->ny, s->nz, kB);
     dim3 gf = grid_of(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, kB);
+    if (own) {
+        float4* tr = (float4*)own->tr[0];
+        TRY_ADJ(check_cuda(cudaMemsetAsync(own->win, 0, 6 * sizeof(int), st), "memset"));
+        if (s->dim == 3) {
+            k_adj_trace_smoke<3><<<g, kB, 0, st>>>(a, dout, tout, vcb, tr, own->win);
+            k_adj_gather_smoke<3><<<g, kB, 0, st>>>(tr, own->win, own->win + kOwnerErr, s->nx, s->ny, s->nz, s->nch, dout, tout, din, tin);
+            k_adj_centre_to_faces<3><<<gf, kB, 0, st>>>(vcb, s->nx, s->ny, s->nz, vb[0], vb[1], vb[2]);
+        } else {
+            k_adj_trace_smoke<2><<<g, kB, 0, st>>>(a, dout, tout, vcb, tr, own->win);
+            k_adj_gather_smoke<2><<<g, kB, 0, st>>>(tr, own->win, own->win + kOwnerErr, s->nx, s->ny, s->nz, s->nch, dout, tout, din, tin);
+            k_adj_centre_to_faces<2><<<gf, kB, 0, st>>>(vcb, s->nx, s->ny, s->nz, vb[0], vb[1], nullptr);
+        }
+        s->nlaunch += 3;
+        return check_cuda(cudaGetLastError(), "adjoint of advect_smoke (owner-computes)");
+    }
     if (s->dim == 3) {
         k_adj_advect_smoke<3><<<g, kB, 0, st>>>(a, dout, tout, din, tin, vcb);
         k_adj_centre_to_faces<3><<<gf, kB, 0, st>>>(vcb, s->nx, s->ny, s->nz, vb[0], vb[1], vb[2]);
@@ -1190,9 +1539,35 @@ int adj_vorticity(ss_sim* s, const StepConsts& c, const float* vort, float* cons
 
 int adj_advect_velocity(ss_sim* s, const StepConsts& c, bool buoy, const float* const vel[3], const float* dens,
                         const float* temp, const float* const gin[3], float* const vb[3], float* dbar, float* tbar,
-                        cudaStream_t st) {
+                        cudaStream_t st, const AdjOwner* own) {
     AdjFluid a = adj_fluid(s, c, vel, dens, temp);
     dim3 gf = grid_of(s->nx + 1, s->ny + 1, s->dim == 3 ? s->nz + 1 : 1, kB);
+    if (own) {
+        OwnerFaces o;
+        for (int d = 0; d < 3; ++d) {
+            o.tr[d] = (float4*)own->tr[d];
+            o.vq[d] = (float4*)own->vq[d];
+        }
+        o.win = own->win;
+        TRY_ADJ(check_cuda(cudaMemsetAsync(own->win, 0, 18 * sizeof(int), st), "memset"));
+        if (s->dim == 3) {
+            if (buoy) {
+                k_adj_trace_velocity<3, true><<<gf, kB, 0, st>>>(a, gin[0], gin[1], gin[2], o);
+                k_adj_gather_velocity<3, true><<<gf, kB, 0, st>>>(a, gin[1], o, vb[0], vb[1], vb[2], dbar, tbar);
+            } else {
+                k_adj_trace_velocity<3, false><<<gf, kB, 0, st>>>(a, gin[0], gin[1], gin[2], o);
+                k_adj_gather_velocity<3, false><<<gf, kB, 0, st>>>(a, gin[1], o, vb[0], vb[1], vb[2], dbar, tbar);
+            }
+        } else if (buoy) {
+            k_adj_trace_velocity<2, true><<<gf, kB, 0, st>>>(a, gin[0], gin[1], nullptr, o);
+            k_adj_gather_velocity<2, true><<<gf, kB, 0, st>>>(a, gin[1], o, vb[0], vb[1], nullptr, dbar, tbar);
+        } else {
+            k_adj_trace_velocity<2, false><<<gf, kB, 0, st>>>(a, gin[0], gin[1], nullptr, o);
+            k_adj_gather_velocity<2, false><<<gf, kB, 0, st>>>(a, gin[1], o, vb[0], vb[1], nullptr, dbar, tbar);
+        }
+        s->nlaunch += 2;
+        return check_cuda(cudaGetLastError(), "adjoint of advect_velocities (owner-computes)");
+    }
     if (s->dim == 3) {
         if (buoy) k_adj_advect_velocity<3, true><<<gf, kB, 0, st>>>(a, gin[0], gin[1], gin[2], vb[0], vb[1], vb[2], dbar, tbar);
         else k_adj_advect_velocity<3, false><<<gf, kB, 0, st>>>(a, gin[0], gin[1], gin[2], vb[0], vb[1], vb[2], dbar, tbar);
@@ -1251,21 +1626,91 @@ __global__ void __launch_bounds__(256) k_adj_force_field(const float* __restrict
     }
 }
 
-int adj_force_field(ss_sim* s, const StepConsts& c, float* const ub[3], float* grad, cudaStream_t st) {
+// Owner-computes variant: one block per (coarse sample, component) sums
+// dt * ubar times the sample's weight over the faces whose taps include it,
+// each thread over a fixed subset in a fixed order, then a fixed tree.
+// Candidate faces along an axis: t = ((i + off) / na) * n - 0.5 in
+// [ci - 1, ci + 1) (every face below / above for the end samples, where the
+// taps clamp), widened by 2 for rounding; ff_taps decides exactly.
+SS_D void ff_range(int ci, int n, int na, float off, int a, int* lo, int* hi) {
+    const float sc = (float)na / (float)n;
+    int l = (int)floorf(((float)ci - 0.5f) * sc - off) - 2, h = (int)ceilf(((float)ci + 1.5f) * sc - off) + 2;
+    if (ci == 0) l = 0;
+    if (ci == n - 1) h = a - 1;
+    *lo = max(l, 0);
+    *hi = min(h, a - 1);
+}
+SS_D float ff_weight(int ci, int n, float t) {
+    int ta, tb;
+    float w;
+    ff_taps(n, t, &ta, &tb, &w);
+    return (ta == ci ? 1.f - w : 0.f) + (tb == ci ? w : 0.f);
+}
+
+__global__ void __launch_bounds__(256) k_adj_force_field_owner(const float* __restrict__ ub, const float* __restrict__ vb,
+                                                               const float* __restrict__ wb, int nx, int ny, int nz,
+                                                               float* __restrict__ G, int n, float dt) {
+    const int node = blockIdx.x, comp = blockIdx.y;
+    const int ci = node % n, cj = (node / n) % n, ck = node / (n * n);
+    const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+    const float ox = comp == 0 ? 0.f : 0.5f, oy = comp == 1 ? 0.f : 0.5f, oz = comp == 2 ? 0.f : 0.5f;
+    int lx, hx, ly, hy, lz, hz;
+    ff_range(ci, n, nx, ox, ax, &lx, &hx);
+    ff_range(cj, n, ny, oy, ay, &ly, &hy);
+    ff_range(ck, n, nz, oz, az, &lz, &hz);
+    const int ex = hx - lx + 1, ey = hy - ly + 1, ez = hz - lz + 1;
+    const float* bar = comp == 0 ? ub : comp == 1 ? vb : wb;
+    float acc = 0.f;
+    const int total = ex * ey * ez;
+    for (int k = threadIdx.x; k < total; k += blockDim.x) {
+        const int x = lx + k % ex, y = ly + (k / ex) % ey, z = lz + k / (ex * ey);
+        const float g = dt * bar[idx3(x, y, z, ax, ay)];
+        if (g == 0.f) continue;
+        const float wx = ff_weight(ci, n, (((float)x + ox) / (float)nx) * (float)n - 0.5f);
+        const float wy = ff_weight(cj, n, (((float)y + oy) / (float)ny) * (float)n - 0.5f);
+        const float wz = ff_weight(ck, n, (((float)z + oz) / (float)nz) * (float)n - 0.5f);
+        const float w = wx * wy * wz;
+        if (w != 0.f) acc += g * w;
+    }
+    __shared__ float sh[256];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && sh[0] != 0.f) G[(size_t)comp * n * n * n + node] += sh[0];
+}
+
+int adj_force_field(ss_sim* s, const StepConsts& c, float* const ub[3], float* grad, cudaStream_t st,
+                    const AdjOwner* own) {
     if (s->ff_n <= 0 || s->dim != 3) return SS_OK;
-    dim3 b(32, 8, 1);
-    dim3 g = grid_of(s->nx + 1, s->ny + 1, s->nz + 1, b);
-    k_adj_force_field<<<g, b, 0, st>>>(ub[0], ub[1], ub[2], s->nx, s->ny, s->nz, grad, s->ff_n, c.dt);
+    if (own) {
+        const int n = s->ff_n;
+        k_adj_force_field_owner<<<dim3((unsigned)(n * n * n), 3), 256, 0, st>>>(ub[0], ub[1], ub[2], s->nx, s->ny,
+                                                                              s->nz, grad, n, c.dt);
+    } else {
+        dim3 b(32, 8, 1);
+        dim3 g = grid_of(s->nx + 1, s->ny + 1, s->nz + 1, b);
+        k_adj_force_field<<<g, b, 0, st>>>(ub[0], ub[1], ub[2], s->nx, s->ny, s->nz, grad, s->ff_n, c.dt);
+    }
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_adj_force_field");
 }
 
-int adj_buoyancy(ss_sim* s, const StepConsts& c, float* vbar, float* dbar, float* tbar, cudaStream_t st) {
+int adj_buoyancy(ss_sim* s, const StepConsts& c, float* vbar, float* dbar, float* tbar, cudaStream_t st,
+                 const AdjOwner* own) {
     const float* vel[3] = {nullptr, nullptr, nullptr};
     AdjFluid a = adj_fluid(s, c, vel, nullptr, nullptr);
     dim3 g = grid_of(s->nx, s->ny + 1, s->nz, kB);
-    if (s->dim == 3) k_adj_buoyancy<3><<<g, kB, 0, st>>>(a, vbar, dbar, tbar);
-    else k_adj_buoyancy<2><<<g, kB, 0, st>>>(a, vbar, dbar, tbar);
+    if (own) {
+        if (s->dim == 3) k_adj_buoyancy_owner<3><<<g, kB, 0, st>>>(a, vbar, dbar, tbar);
+        else k_adj_buoyancy_owner<2><<<g, kB, 0, st>>>(a, vbar, dbar, tbar);
+    } else if (s->dim == 3) {
+        k_adj_buoyancy<3><<<g, kB, 0, st>>>(a, vbar, dbar, tbar);
+    } else {
+        k_adj_buoyancy<2><<<g, kB, 0, st>>>(a, vbar, dbar, tbar);
+    }
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "adjoint of apply_buoyancy");
 }

@@ -224,7 +224,6 @@ int launch_rb_smooth_tma(ss_sim* s, float* pc, const float* po, const float* rhs
 int coarse_coop_first(const ss_sim* s);
 int launch_coarse_coop(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int prec, bool down, cudaStream_t st);
 int launch_force_field(ss_sim* s, const StepConsts& c, cudaStream_t st);
-int adj_force_field(ss_sim* s, const StepConsts& c, float* const ub[3], float* grad, cudaStream_t st);
 int launch_vorticity_field(ss_sim* s, const StepConsts& c, const float* const vel[3], float* out, cudaStream_t st);
 
 // adjoint kernels (k_adjoint.cu)
@@ -233,6 +232,15 @@ struct AdjScratch {
     float* bbar[SS_MAX_LEVELS];
     float* T[SS_MAX_LEVELS];
 };
+// Scratch of the deterministic (owner-computes) adjoint scatters; a null
+// AdjOwner selects the atomic scatter-adds.
+struct AdjOwner {
+    void* tr[3];   // float4 per face of each axis: clamped back-traced point, w = weight of the source (the smoke pass uses tr[0])
+    void* vq[3];   // float4 per face of each axis: position gradient, w = value the face keeps
+    int* win;      // tap reaches: 6 per face axis (the smoke pass uses the first 6); win[23]: error word
+};
+int adj_force_field(ss_sim* s, const StepConsts& c, float* const ub[3], float* grad, cudaStream_t st,
+                    const AdjOwner* own = nullptr);
 #define TRY_ADJ(x)                          \
     do {                                    \
         int _rc = (x);                      \
@@ -240,7 +248,7 @@ struct AdjScratch {
     } while (0)
 int adj_advect_smoke(ss_sim* s, const StepConsts& c, const float* const vel[3], const float* dens, const float* temp,
                      const float* dout, const float* tout, float* din, float* tin, float* vcb, float* const vb[3],
-                     cudaStream_t st);
+                     cudaStream_t st, const AdjOwner* own = nullptr);
 int adj_update(ss_sim* s, const StepConsts& c, float* const vb[3], float* pbar, cudaStream_t st);
 int adj_divergence(ss_sim* s, const float* dbar, float* const vb[3], cudaStream_t st);
 int adj_v_cycle(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, const AdjScratch& w, cudaStream_t st);
@@ -249,8 +257,9 @@ int adj_vorticity(ss_sim* s, const StepConsts& c, const float* vort, float* cons
                   float* wbar, cudaStream_t st);
 int adj_advect_velocity(ss_sim* s, const StepConsts& c, bool buoy, const float* const vel[3], const float* dens,
                         const float* temp, const float* const gin[3], float* const vb[3], float* dbar, float* tbar,
-                        cudaStream_t st);
-int adj_buoyancy(ss_sim* s, const StepConsts& c, float* vbar, float* dbar, float* tbar, cudaStream_t st);
+                        cudaStream_t st, const AdjOwner* own = nullptr);
+int adj_buoyancy(ss_sim* s, const StepConsts& c, float* vbar, float* dbar, float* tbar, cudaStream_t st,
+                 const AdjOwner* own = nullptr);
 int adj_emitters(ss_sim* s, const StepConsts& c, int forced, float* const vb[3], double* fpart, double* fout,
                  const ss_emitter* em, int ne, cudaStream_t st);
 int adj_force_blocks(const ss_sim* s);

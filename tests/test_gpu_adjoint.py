@@ -59,7 +59,7 @@ def _oracle_loss(desc, em, ob, f, p, ybar, x_dir, eps, force, dim, nch, n):
     return tot
 
 
-def _directional(dim, n, nch, enc, mask, seed=1, force=(0.0, 0.0, 0.0), eps=1e-4, tol=2e-3):
+def _directional(dim, n, nch, enc, mask, seed=1, force=(0.0, 0.0, 0.0), eps=1e-4, tol=2e-3, deterministic=False):
     from smokesim_b200.adjoint import Rollout
     import torch
     desc, em, ob, f, p, g = _setup(dim, n, nch, enc, seed, mask)
@@ -68,7 +68,7 @@ def _directional(dim, n, nch, enc, mask, seed=1, force=(0.0, 0.0, 0.0), eps=1e-4
     ybar = {k: rng.standard_normal(abi.field_count(dim, n, k, nch)).astype(np.float32) for k in outs}
     ins = _fields(dim)
     x_dir = {k: rng.standard_normal(abi.field_count(dim, n, k, nch)) for k in ins}
-    ro = Rollout(g, 1)
+    ro = Rollout(g, 1, deterministic=deterministic)
     fr = np.array([force], np.float32)
     ro.forward(p, fr)
     dev = {k: torch.from_numpy(v).cuda() for k, v in ybar.items()}
@@ -332,3 +332,98 @@ def test_force_field_gradient_vs_fp64_fd():
     assert err.max() <= 1e-3, (err.max(), list(zip(adj, fd)))
     ro.close()
     g.close()
+
+
+# ------------------------------------------------ owner-computes scatter-adds
+def _stage_grads(dim, n, nch, enc, mask, deterministic, seed=3, state_scale=1.0):
+    """Adjoint of one step of the given stages for a random output seed: the
+    gradients of every input field and of the control force."""
+    from smokesim_b200.adjoint import Rollout
+    import torch
+    desc, em, ob, f, p, g = _setup(dim, n, nch, enc, seed, mask, state_scale=state_scale)
+    rng = np.random.default_rng(seed + 100)
+    outs = VEL[:dim] + [abi.FIELD_DENSITY, abi.FIELD_TEMPERATURE]
+    ybar = {k: rng.standard_normal(abi.field_count(dim, n, k, nch)).astype(np.float32) for k in outs}
+    ro = Rollout(g, 1, deterministic=deterministic)
+    force = np.array([(0.3, -0.2, 0.1)[:dim] + (0.0,) * (3 - dim)], np.float32)
+    ro.forward(p, force)
+    dev = {k: torch.from_numpy(v).cuda() for k, v in ybar.items()}
+    torch.cuda.synchronize()
+    gf = ro.backward(p, grad_density=dev[abi.FIELD_DENSITY].data_ptr(),
+                     grad_temperature=dev[abi.FIELD_TEMPERATURE].data_ptr(),
+                     grad_velocity=[dev[k].data_ptr() for k in VEL[:dim]])
+    out = {k: ro.grad(k).copy() for k in _fields(dim)}
+    out["force"] = np.asarray(gf, np.float32).copy()
+    ro.close()
+    g.close()
+    return out
+
+
+OWNER_STAGES = [
+    ("advect", abi.STAGE_ADVECT_VELOCITIES),
+    ("advect_buoyancy", abi.STAGE_ADVECT_VELOCITIES | abi.STAGE_APPLY_BUOYANCY),
+    ("buoyancy", abi.STAGE_APPLY_BUOYANCY),
+    ("smoke", abi.STAGE_ADVECT_SMOKE),
+    ("full", abi.STAGE_ALL),
+]
+
+
+@pytest.mark.parametrize("gname,dim,n,nch,enc", GRIDS)
+@pytest.mark.parametrize("stage,mask", OWNER_STAGES)
+@pytest.mark.parametrize("scale", [1.0, 4.0])
+def test_owner_computes_matches_atomic(gname, dim, n, nch, enc, stage, mask, scale):
+    """The owner-computes scatter-adds give the atomic variant's gradients up
+    to summation order, and bitwise the same gradients run to run.  scale 4
+    multiplies the random velocities (back-traces several cells long, so the
+    inverse-footprint boxes are wide)."""
+    a = _stage_grads(dim, n, nch, enc, mask, False, state_scale=scale)
+    b = _stage_grads(dim, n, nch, enc, mask, True, state_scale=scale)
+    c = _stage_grads(dim, n, nch, enc, mask, True, state_scale=scale)
+    for k in a:
+        assert b[k].tobytes() == c[k].tobytes(), k
+        tol = 1e-5 * max(float(np.abs(a[k]).max()), 1e-30)
+        assert np.allclose(b[k], a[k], rtol=1e-5, atol=tol), (k, float(np.abs(b[k] - a[k]).max()), tol)
+
+
+def test_owner_computes_stage_matches_fd():
+    """Full step, owner-computes scatters, against FP64 central differences."""
+    _directional(3, (16, 14, 12), 1, 1, abi.STAGE_ALL, seed=3, force=(0.3, -0.2, 0.1), deterministic=True)
+
+
+def test_rollout_deterministic_bitwise():
+    """A 32^3 rollout of 8 steps (checkpoint every 3) with per-step forces and
+    a 4^3 control force field: two reverse passes with the owner-computes
+    scatters give bitwise-identical gradients of the initial velocity, smoke,
+    forces and force field; the atomic variant agrees with them to rounding."""
+    from smokesim_b200 import Sim
+    from smokesim_b200.adjoint import Rollout
+    import torch
+    n, nsteps, nf = 32, 8, 4
+    sc = scene.rollout64(seed=4, n=n)
+    p = scene.workload_params(ref_quirks=0, n_vcycles=4)
+    rng = np.random.default_rng(5)
+    forces = (rng.standard_normal((nsteps, 3)) * 0.2).astype(np.float32)
+    field = (rng.standard_normal((3, nf, nf, nf)) * 0.3).astype(np.float32)
+
+    def run(det):
+        g = Sim(sc["desc"])
+        scene.apply(g, sc)
+        g.set_force_field(field)
+        ro = Rollout(g, nsteps, 3, deterministic=det)
+        ro.forward(p, forces)
+        rho = torch.from_numpy(g.get_field(abi.FIELD_DENSITY).ravel()).cuda()
+        gd = (2 * (rho - 0.05)).contiguous()
+        torch.cuda.synchronize()
+        gf = ro.backward(p, grad_density=gd.data_ptr())
+        out = {k: ro.grad(k).copy() for k in VEL + [abi.FIELD_DENSITY, abi.FIELD_TEMPERATURE]}
+        out["force"] = np.asarray(gf, np.float32).copy()
+        out["field"] = ro.force_field_grad(nf).copy()
+        ro.close()
+        g.close()
+        return out
+
+    d1, d2, at = run(True), run(True), run(False)
+    for k in d1:
+        assert d1[k].tobytes() == d2[k].tobytes(), k
+        scale = max(float(np.abs(at[k]).max()), 1e-30)
+        assert np.allclose(d1[k], at[k], rtol=1e-3, atol=1e-5 * scale), (k, float(np.abs(d1[k] - at[k]).max()), scale)
