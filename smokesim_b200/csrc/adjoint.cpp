@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -63,6 +64,8 @@ struct ss_adjoint {
     int ffgrad_n = 0;          // ff_n that ffgrad was sized and last filled for
     std::vector<void*> allocs;
     long long launches = 0, ckpt_bytes = 0, work_bytes = 0;
+    float* cresp = nullptr;        // response matrix of the coarsest level's sweeps, cresp_n^2
+    int cresp_n = 0;
     AdjOwner own{};                // owner-computes scratch (allocated when first enabled)
     bool deterministic = false;    // owner-computes scatters instead of atomics
     bool forward_done = false;
@@ -323,6 +326,17 @@ int ss_adjoint_create(ss_sim* s, int nsteps, int every, ss_adjoint** out) {
     }
     W((void**)&A->fpart, (size_t)adj_force_blocks(s) * 3 * sizeof(double));
     W((void**)&A->fgrad, (size_t)nsteps * 3 * sizeof(double));
+    // the bottom solve's adjoint applies the coarsest sweeps as one matrix
+    // (SMOKESIM_ADJ_COARSE_SWEEPS=1 transposes them sweep by sweep instead)
+    {
+        const ss::Level& lc = s->lv[s->levels - 1];
+        const long long nc = (long long)lc.n[0] * lc.n[1] * lc.n[2];
+        const char* e = getenv("SMOKESIM_ADJ_COARSE_SWEEPS");
+        if (s->levels >= 2 && nc <= kCoarseResponseMax && !(e && atoi(e) != 0)) {
+            W((void**)&A->cresp, (size_t)(nc * nc) * 4);
+            A->cresp_n = (int)nc;
+        }
+    }
     if (rc) {
         free_adjoint(A);
         return rc;
@@ -398,6 +412,12 @@ int ss_adjoint_backward(ss_adjoint* A, const ss_params* p, const float* grad_den
         TRY_ADJ(check_cuda(cudaMemsetAsync(A->ffgrad, 0, nff * sizeof(float), st), "memset"));
     }
     if (A->deterministic) TRY_ADJ(check_cuda(cudaMemsetAsync(A->own.win, 0, 24 * sizeof(int), st), "memset"));
+    // this call's coarsest-level map (schedule and solid fractions as they are now)
+    A->w.cresp = nullptr;
+    if (A->cresp) {
+        TRY_ADJ(launch_coarse_response(s, p->mg.n_coarse, A->cresp, st));
+        A->w.cresp = A->cresp;
+    }
     const int nseg = (A->n + A->every - 1) / A->every;
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int k0 = sg * A->every, k1 = std::min(A->n, k0 + A->every);

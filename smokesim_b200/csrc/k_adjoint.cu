@@ -1217,6 +1217,7 @@ struct AdjBottomArgs {
     int total;
     int n_pre, n_post, n_coarse;
     float oobA;
+    const float* cresp;   // coarsest level's response matrix, or null
 };
 
 SS_D AdjLevel bottom_adj_level(const AdjBottomArgs& b, int l, float* sp, float* sb, float* sT) {
@@ -1387,7 +1388,43 @@ __global__ void __launch_bounds__(1024) k_adj_bottom(AdjBottomArgs b) {
         }
         __syncthreads();
     }
-    bottom_adj_sweeps<DIM>(bottom_adj_level(b, last, sp, sb, sT), b.n_coarse);
+    if (b.cresp) {
+        // the coarsest sweeps as one product: bbar += D^T pbar, D = d(p after
+        // the sweeps)/d(right-hand side); the adjoint of their initial guess
+        // (zero) is not needed.  Threads split the sum over j into `parts`
+        // slices whose partial sums meet in the T arrays (unused outside the
+        // sweeps), then add in slice order.
+        const AdjLevel ac = bottom_adj_level(b, last, sp, sb, sT);
+        const int n = ac.nx * ac.ny * ac.nz;
+        int parts = (int)blockDim.x / n;
+        if (parts > b.total / n) parts = b.total / n;
+        if (parts < 1) parts = 1;
+        const int chunk = (n + parts - 1) / parts;
+        for (int t = threadIdx.x; t < n * parts; t += blockDim.x) {
+            const int i = t % n, part = t / n;
+            const int j0 = part * chunk, j1 = min(j0 + chunk, n);
+            const float* col = b.cresp + i;
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+            int j = j0;
+            for (; j + 4 <= j1; j += 4) {
+                s0 += __ldg(col + (size_t)j * n) * ac.pbar[j];
+                s1 += __ldg(col + (size_t)(j + 1) * n) * ac.pbar[j + 1];
+                s2 += __ldg(col + (size_t)(j + 2) * n) * ac.pbar[j + 2];
+                s3 += __ldg(col + (size_t)(j + 3) * n) * ac.pbar[j + 3];
+            }
+            for (; j < j1; ++j) s0 += __ldg(col + (size_t)j * n) * ac.pbar[j];
+            sT[t] = (s0 + s1) + (s2 + s3);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            float acc = 0.f;
+            for (int part = 0; part < parts; ++part) acc += sT[part * n + i];
+            ac.bbar[i] += acc;
+        }
+        __syncthreads();
+    } else {
+        bottom_adj_sweeps<DIM>(bottom_adj_level(b, last, sp, sb, sT), b.n_coarse);
+    }
     // up: residual + restriction^T, then pre-smoothing^T
     for (int l = last - 1; l >= 0; --l) {
         const AdjLevel a = bottom_adj_level(b, l, sp, sb, sT);
@@ -1438,6 +1475,7 @@ static int adj_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, const AdjScrat
     b.bbar0 = w.bbar[L];
     b.n_pre = mg.n_pre; b.n_post = mg.n_post; b.n_coarse = mg.n_coarse;
     b.oobA = s->enclosed ? 1.f : 0.f;
+    b.cresp = w.cresp;
     const size_t smem = (size_t)3 * off * sizeof(float);
     if (smem > (size_t)kBottomSmemBytes) return set_error(SS_E_INVALID, "adjoint bottom levels exceed shared memory");
     cudaError_t e = s->dim == 3

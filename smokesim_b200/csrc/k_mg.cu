@@ -836,6 +836,53 @@ int launch_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, cudaStream_t st) {
     return launch_bottom_t<float, float>(s, mg, L, s->p, s->r, st);
 }
 
+// Response of the coarsest level's smoothing to unit right-hand sides, for
+// the adjoint (which applies its transpose as one matrix-vector product
+// instead of transposing the sweeps one by one): block i runs the bottom
+// solve's `iters` red-black iterations from p = 0 with r = e_i (corrected
+// out-of-grid rule, FP32 stores) and writes the result into column i of D,
+// D[j * n + i] = dp_j / dr_i.
+template <int DIM>
+__global__ void __launch_bounds__(1024) k_coarse_response(BottomLevel lv, const float* __restrict__ alpha, float oobA,
+                                                          int iters, float* __restrict__ D) {
+    extern __shared__ float sm[];
+    const int n = lv.n[0] * lv.n[1] * lv.n[2];
+    float* sp = sm;
+    float* sr = sm + n;
+    float* sa = sm + 2 * n;
+    const int i = blockIdx.x;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        sp[c] = 0.f;
+        sr[c] = c == i ? 1.f : 0.f;
+        sa[c] = alpha[c];
+    }
+    __syncthreads();
+    MGArgs a;
+    a.p = sp; a.r = sr; a.alpha = sa;
+    a.flags = nullptr; a.div0 = nullptr; a.div0r = nullptr;
+    a.nx = lv.n[0]; a.ny = lv.n[1]; a.nz = lv.n[2];
+    a.oobA = oobA;
+    a.hh = lv.hh;
+    a.rho_h = 0.f; a.dt = 1.f; a.rho = 1.f; a.dt_h = 1.f;
+    bottom_smooth<DIM, float>(a, iters);
+    for (int c = threadIdx.x; c < n; c += blockDim.x) D[(size_t)c * n + i] = sp[c];
+}
+
+int launch_coarse_response(ss_sim* s, int iters, float* D, cudaStream_t st) {
+    const ss::Level& lv = s->lv[s->levels - 1];
+    const int n = lv.n[0] * lv.n[1] * lv.n[2];
+    if (n > kCoarseResponseMax) return set_error(SS_E_INVALID, "coarsest level too large for its response matrix");
+    BottomLevel b{};
+    b.n[0] = lv.n[0]; b.n[1] = lv.n[1]; b.n[2] = lv.n[2];
+    b.off = 0;
+    b.hh = lv.hh;
+    const size_t smem = (size_t)3 * n * sizeof(float);
+    if (s->dim == 3) k_coarse_response<3><<<n, 1024, smem, st>>>(b, s->alpha[s->levels - 1], smooth_oob(s, 0), iters, D);
+    else k_coarse_response<2><<<n, 1024, smem, st>>>(b, s->alpha[s->levels - 1], smooth_oob(s, 0), iters, D);
+    s->nlaunch += 1;
+    return check_cuda(cudaGetLastError(), "k_coarse_response");
+}
+
 // ---------------------------------------------------- coarse-storage variants
 // The coarse levels of the mixed-precision correction solve: the same
 // operators as above (out-of-grid rule of the corrected mode) on FP16 or BF16

@@ -231,7 +231,13 @@ struct AdjScratch {
     float* pbar[SS_MAX_LEVELS];
     float* bbar[SS_MAX_LEVELS];
     float* T[SS_MAX_LEVELS];
+    // response matrix of the coarsest level's sweeps (launch_coarse_response);
+    // null: the bottom solve's adjoint transposes the sweeps one by one
+    const float* cresp;
 };
+// coarsest levels up to this many cells get a response matrix (4 MiB)
+constexpr int kCoarseResponseMax = 1024;
+int launch_coarse_response(ss_sim* s, int iters, float* D, cudaStream_t st);
 // Scratch of the deterministic (owner-computes) adjoint scatters; a null
 // AdjOwner selects the atomic scatter-adds.
 struct AdjOwner {

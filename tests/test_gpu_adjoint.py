@@ -427,3 +427,46 @@ def test_rollout_deterministic_bitwise():
         assert d1[k].tobytes() == d2[k].tobytes(), k
         scale = max(float(np.abs(at[k]).max()), 1e-30)
         assert np.allclose(d1[k], at[k], rtol=1e-3, atol=1e-5 * scale), (k, float(np.abs(d1[k] - at[k]).max()), scale)
+
+
+def test_coarse_response_matches_sweeps(monkeypatch):
+    """The bottom solve's adjoint applies the coarsest level's sweeps as one
+    product with their response matrix (default); transposing them sweep by
+    sweep (SMOKESIM_ADJ_COARSE_SWEEPS=1) gives the same gradients to
+    rounding (8-step 32^3 rollout, 4 V-cycles a step, forces)."""
+    from smokesim_b200 import Sim
+    from smokesim_b200.adjoint import Rollout
+    import torch
+    n, nsteps = 32, 8
+    sc = scene.rollout64(seed=6, n=n)
+    p = scene.workload_params(ref_quirks=0, n_vcycles=4)
+    forces = (np.random.default_rng(7).standard_normal((nsteps, 3)) * 0.2).astype(np.float32)
+
+    def run(sweeps):
+        if sweeps:
+            monkeypatch.setenv("SMOKESIM_ADJ_COARSE_SWEEPS", "1")
+        else:
+            monkeypatch.delenv("SMOKESIM_ADJ_COARSE_SWEEPS", raising=False)
+        g = Sim(sc["desc"])
+        scene.apply(g, sc)
+        ro = Rollout(g, nsteps, 4)
+        ro.forward(p, forces)
+        rho = torch.from_numpy(g.get_field(abi.FIELD_DENSITY).ravel()).cuda()
+        gd = (2 * (rho - 0.05)).contiguous()
+        torch.cuda.synchronize()
+        gf = ro.backward(p, grad_density=gd.data_ptr())
+        out = {k: ro.grad(k).copy() for k in VEL + [abi.FIELD_DENSITY, abi.FIELD_TEMPERATURE, abi.FIELD_PRESSURE]}
+        out["force"] = np.asarray(gf, np.float32).copy()
+        info = ro.info()
+        ro.close()
+        g.close()
+        return out, info
+
+    (a, ia), (b, ib) = run(False), run(True)
+    assert ia["workspace_bytes"] > ib["workspace_bytes"]   # the matrix was allocated
+    # the warm-start pressure's gradient is tiny (the V-cycles damp the initial
+    # guess), so rounding is measured against the largest state gradient
+    scale = max(float(np.abs(b[k]).max()) for k in b if k != "force")
+    for k in a:
+        s_k = max(float(np.abs(b[k]).max()), 1e-30) if k == "force" else scale
+        assert np.allclose(a[k], b[k], rtol=1e-4, atol=1e-5 * s_k), (k, float(np.abs(a[k] - b[k]).max()), s_k)
