@@ -275,6 +275,9 @@ ADJOINT_CASES = [
     # the inverse-control configuration: mixed-precision forward (FP16 coarse
     # corrections), the recorded refinement steps transposed in the adjoint
     ("plume128_mixed", dict(kind="plume3d", n=128), 200, 14, 1, False),
+    # the same with every intermediate kept (25 GB of records at 128^3: HBM
+    # holds them, so nothing is recomputed)
+    ("plume128_mixed_no_recompute", dict(kind="plume3d", n=128), 200, 200, 1, False),
     ("plume128_deterministic", dict(kind="plume3d", n=128), 200, 14, 0, True),
 ]
 

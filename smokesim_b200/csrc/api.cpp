@@ -202,6 +202,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     // SMOKESIM_COOP_CELLS: coarse levels of at most this many cells run as two
     // cooperative launches per V-cycle (default 0: one launch per operator)
     if (const char* e = getenv("SMOKESIM_COOP_CELLS")) s->coop_cells = atoll(e);
+    if (const char* e = getenv("SMOKESIM_ADJ_ZM")) s->adj_zm = atoi(e);
     s->nv[0] = (size_t)(s->nx + 1) * s->ny * s->nz;
     s->nv[1] = (size_t)s->nx * (s->ny + 1) * s->nz;
     s->nv[2] = s->dim == 3 ? (size_t)s->nx * s->ny * (s->nz + 1) : 0;

@@ -116,6 +116,7 @@ struct ss_sim {
     unsigned int* coop_bar = nullptr;   // grid barrier of the cooperative coarse legs: arrivals, generation
     long long coop_cells = 0;  // coarse levels of at most this many cells run in the cooperative legs (0: none)
     int use_tma = 1;           // TMA tile loads: 1 coarse-level sweeps, 2 also level 0 (where the layout allows)
+    int adj_zm = 0;            // adjoint sweeps of 3D levels with even nx: z-marching pair kernel with at most this many planes a block (0: one cell a thread)
     // The multigrid part of a solve recorded once as a CUDA graph and replayed
     // (api.cpp, run_graph): slot 0 fixed-count FP32 V-cycles, 1 one FP32
     // tolerance cycle, 2/3 one mixed refinement step per FP64 buffer parity.
