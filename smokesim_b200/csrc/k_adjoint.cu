@@ -490,36 +490,41 @@ SS_D float prolong_coef(int x, int af, int cf, int K) {
 }
 
 // Transpose of p_f += trilinear(p_c): p_c_bar(K) = sum over the fine cells
-// whose interpolation stencil holds K
-template <int DIM>
+// whose interpolation stencil holds K.  W = 6 takes the fine window
+// [2K-2, 2K+3] of any size ratio; W = 4 the window [2K-1, 2K+2], which holds
+// every nonzero coefficient when each fine extent is exactly twice the
+// coarse one (the two outer cells of the 6-window then weigh 0), so both
+// give the same sums.
+template <int DIM, int W>
 __global__ void __launch_bounds__(256) k_adj_prolong(const float* __restrict__ pfb, int ax, int ay, int az,
                                                      float* __restrict__ pcb, int cx, int cy, int cz) {
     const int X = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y * blockDim.y + threadIdx.y;
     const int Z = blockIdx.z * blockDim.z + threadIdx.z;
     if (X >= cx || Y >= cy || Z >= cz) return;
-    // per-axis coefficients of the fine window [2K-2, 2K+3] (0 outside the grid)
-    float wx[6], wy[6], wz[6];
+    constexpr int o = W == 4 ? 1 : 2;
+    // per-axis coefficients of the fine window (0 outside the grid)
+    float wx[W], wy[W], wz[W];
 #pragma unroll
-    for (int j = 0; j < 6; ++j) {
-        const int x = 2 * X - 2 + j, y = 2 * Y - 2 + j, z = 2 * Z - 2 + j;
+    for (int j = 0; j < W; ++j) {
+        const int x = 2 * X - o + j, y = 2 * Y - o + j, z = 2 * Z - o + j;
         wx[j] = (x >= 0 && x < ax) ? prolong_coef(x, ax, cx, X) : 0.f;
         wy[j] = (y >= 0 && y < ay) ? prolong_coef(y, ay, cy, Y) : 0.f;
-        wz[j] = DIM == 3 ? ((z >= 0 && z < az) ? prolong_coef(z, az, cz, Z) : 0.f) : (j == 2 ? 1.f : 0.f);
+        wz[j] = DIM == 3 ? ((z >= 0 && z < az) ? prolong_coef(z, az, cz, Z) : 0.f) : (j == o ? 1.f : 0.f);
     }
     float s = 0.f;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
+    for (int k = 0; k < W; ++k) {
         if (wz[k] == 0.f) continue;
-        const int z = DIM == 3 ? 2 * Z - 2 + k : 0;
+        const int z = DIM == 3 ? 2 * Z - o + k : 0;
 #pragma unroll
-        for (int j = 0; j < 6; ++j) {
+        for (int j = 0; j < W; ++j) {
             if (wy[j] == 0.f) continue;
-            const int y = 2 * Y - 2 + j;
+            const int y = 2 * Y - o + j;
             float row = 0.f;
 #pragma unroll
-            for (int i = 0; i < 6; ++i)
-                if (wx[i] != 0.f) row += wx[i] * pfb[idx3(2 * X - 2 + i, y, z, ax, ay)];
+            for (int i = 0; i < W; ++i)
+                if (wx[i] != 0.f) row += wx[i] * pfb[idx3(2 * X - o + i, y, z, ax, ay)];
             s += wz[k] * wy[j] * row;
         }
     }
@@ -1466,19 +1471,27 @@ __global__ void __launch_bounds__(1024) k_adj_bottom(AdjBottomArgs b) {
         float* pc = sp + b.off[l + 1];
         for (int q = threadIdx.x; q < cx * cy * cz; q += blockDim.x) {
             const int X = q % cx, t = q / cx, Y = t % cy, Z = t / cy;
+            // per-axis coefficients of the fine window [2K-2, 2K+3] (0 outside the grid)
+            float wx[6], wy[6], wz[6];
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                const int x = 2 * X - 2 + j, y = 2 * Y - 2 + j, z = 2 * Z - 2 + j;
+                wx[j] = (x >= 0 && x < a.nx) ? prolong_coef(x, a.nx, cx, X) : 0.f;
+                wy[j] = (y >= 0 && y < a.ny) ? prolong_coef(y, a.ny, cy, Y) : 0.f;
+                wz[j] = DIM == 3 ? ((z >= 0 && z < a.nz) ? prolong_coef(z, a.nz, cz, Z) : 0.f) : (j == 2 ? 1.f : 0.f);
+            }
             float s = 0.f;
-            const int z0 = DIM == 3 ? 2 * Z - 2 : 0, z1 = DIM == 3 ? 2 * Z + 3 : 0;
-            for (int z = max(z0, 0); z <= min(z1, a.nz - 1); ++z) {
-                const float wz = DIM == 3 ? prolong_coef(z, a.nz, cz, Z) : 1.f;
-                if (wz == 0.f) continue;
-                for (int y = max(2 * Y - 2, 0); y <= min(2 * Y + 3, a.ny - 1); ++y) {
-                    const float wy = prolong_coef(y, a.ny, cy, Y);
-                    if (wy == 0.f) continue;
-                    for (int x = max(2 * X - 2, 0); x <= min(2 * X + 3, a.nx - 1); ++x) {
-                        const float wx = prolong_coef(x, a.nx, cx, X);
-                        if (wx == 0.f) continue;
-                        s += wx * wy * wz * a.pbar[idx3(x, y, z, a.nx, a.ny)];
-                    }
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                if (wz[k] == 0.f) continue;
+                const int z = DIM == 3 ? 2 * Z - 2 + k : 0;
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    if (wy[j] == 0.f) continue;
+                    const int y = 2 * Y - 2 + j;
+#pragma unroll
+                    for (int i = 0; i < 6; ++i)
+                        if (wx[i] != 0.f) s += wx[i] * wy[j] * wz[k] * a.pbar[idx3(2 * X - 2 + i, y, z, a.nx, a.ny)];
                 }
             }
             pc[q] = s;
@@ -1598,8 +1611,15 @@ static int adj_v_cycle_rec(ss_sim* s, const StepConsts& c, const ss_mg_schedule&
     const size_t nc = (size_t)cx * cy * cz;
     // p_L += P p_{L+1}  ->  pbar_{L+1} = P^T pbar_L
     dim3 gc = grid_of(cx, cy, cz, kB);
-    if (s->dim == 3) k_adj_prolong<3><<<gc, kB, 0, st>>>(a.pbar, a.nx, a.ny, a.nz, w.pbar[L + 1], cx, cy, cz);
-    else k_adj_prolong<2><<<gc, kB, 0, st>>>(a.pbar, a.nx, a.ny, a.nz, w.pbar[L + 1], cx, cy, cz);
+    const bool halves = a.nx == 2 * cx && a.ny == 2 * cy && (s->dim == 2 || a.nz == 2 * cz);
+    if (s->dim == 3) {
+        if (halves) k_adj_prolong<3, 4><<<gc, kB, 0, st>>>(a.pbar, a.nx, a.ny, a.nz, w.pbar[L + 1], cx, cy, cz);
+        else k_adj_prolong<3, 6><<<gc, kB, 0, st>>>(a.pbar, a.nx, a.ny, a.nz, w.pbar[L + 1], cx, cy, cz);
+    } else if (halves) {
+        k_adj_prolong<2, 4><<<gc, kB, 0, st>>>(a.pbar, a.nx, a.ny, a.nz, w.pbar[L + 1], cx, cy, cz);
+    } else {
+        k_adj_prolong<2, 6><<<gc, kB, 0, st>>>(a.pbar, a.nx, a.ny, a.nz, w.pbar[L + 1], cx, cy, cz);
+    }
     s->nlaunch += 1;
     TRY_ADJ(check_cuda(cudaMemsetAsync(w.bbar[L + 1], 0, nc * sizeof(float), st), "memset"));
     TRY_ADJ(adj_v_cycle_rec(s, c, mg, L + 1, w, st));
