@@ -26,7 +26,9 @@ _lock = threading.Lock()
 def build(force=False):
     """Compile liboracle_f32.so / liboracle_f64.so with the committed Makefile."""
     targets = [os.path.join(ORACLE_DIR, f) for f in ("liboracle_f32.so", "liboracle_f64.so")]
-    if not force and all(os.path.exists(t) for t in targets):
+    sources = [os.path.join(ORACLE_DIR, "smokesim_oracle.c"), os.path.join(ORACLE_DIR, "..", "include", "smokesim.h")]
+    newest = max(os.path.getmtime(f) for f in sources if os.path.exists(f))
+    if not force and all(os.path.exists(t) and os.path.getmtime(t) >= newest for t in targets):
         return
     env = dict(os.environ)
     env.pop("CC", None)

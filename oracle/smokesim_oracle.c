@@ -72,6 +72,13 @@ typedef struct og_sim {
     real force[3];   /* control force on the faces inside active emitters */
     real* ff;        /* coarse control force field, 3 * ffn^3 (none: ffn == 0) */
     int ffn;
+    /* mixed solve: response matrix of the coarsest level's sweeps,
+     * cm[i * cm_n + j] = dp_j / dr_i, with the solid fractions and iteration
+     * count it was built for */
+    real* cm;
+    real* cm_alpha;
+    size_t cm_n;
+    int cm_iters;
 } og_sim;
 
 /* ---------------------------------------------------------------- helpers */
@@ -241,6 +248,8 @@ void og_destroy(og_sim* s) {
     }
     free(s->em); free(s->ob); free(s->bx);
     free(s->p64);
+    free(s->cm);
+    free(s->cm_alpha);
     free(s->ff);
     free(s);
 }
@@ -904,10 +913,71 @@ void og_prolong_and_add(og_sim* s, int L) {
 /* v_cycle (common/physics/grid.c:177-209).  With ref_quirks == 0 the level's
  * right-hand side is kept aside so the post-smoother solves the same system
  * as the pre-smoother, and both operators use one out-of-grid rule. */
+/* The mixed solve's coarsest level (levels >= 2, at most 1024 cells) is not
+ * swept: its n_coarse red-black iterations from p = 0 are a linear map of the
+ * right-hand side, applied as a matrix (k_mg.cu k_bottom / coarse_product).
+ * The matrix is the iterations' response to unit right-hand sides in FP32
+ * without the coarse-storage rounding, rebuilt when the level's solid
+ * fractions or the iteration count change; p_j = cstore(sum_i cm[i n + j] r_i)
+ * in the summation order of the CUDA product. */
+static int og_coarse_matrix_applies(const og_sim* s, int L) {
+    const size_t n = (size_t)s->ls[L][0] * s->ls[L][1] * s->ls[L][2];
+    return s->cround != 0 && L >= 1 && L == s->levels - 1 && n <= 1024;
+}
+
+static void og_coarse_matrix(og_sim* s, int L, const ss_mg_schedule* mg, real dt, real rho) {
+    const size_t n = (size_t)s->ls[L][0] * s->ls[L][1] * s->ls[L][2];
+    const real* A = s->solid[L][3];
+    real* P = s->p[L];
+    real* R = s->r[L];
+    if (!s->cm || s->cm_n != n || s->cm_iters != mg->n_coarse || memcmp(s->cm_alpha, A, n * sizeof(real)) != 0) {
+        free(s->cm);
+        free(s->cm_alpha);
+        s->cm = (real*)malloc(n * n * sizeof(real));
+        s->cm_alpha = (real*)malloc(n * sizeof(real));
+        real* keep_r = (real*)malloc(n * sizeof(real));
+        memcpy(keep_r, R, n * sizeof(real));
+        const int cr = s->cround;
+        s->cround = 0;
+        for (size_t i = 0; i < n; ++i) {
+            memset(P, 0, n * sizeof(real));
+            memset(R, 0, n * sizeof(real));
+            R[i] = (real)1;
+            og_smooth_mode(s, L, mg->n_coarse, dt, rho, mg->ref_quirks);
+            memcpy(s->cm + i * n, P, n * sizeof(real));
+        }
+        s->cround = cr;
+        memcpy(R, keep_r, n * sizeof(real));
+        free(keep_r);
+        memcpy(s->cm_alpha, A, n * sizeof(real));
+        s->cm_n = n;
+        s->cm_iters = mg->n_coarse;
+    }
+    /* `parts` slices of i per value (the largest power of two <= 32 with
+     * parts * n <= 1024), each with eight round-robin partial sums added
+     * pairwise, the slices folded as a tree: v[q] += v[q + o], o = parts/2 .. 1 */
+    size_t parts = 1;
+    while (parts < 32 && parts * 2 * n <= 1024) parts *= 2;
+    const size_t chunk = (n + parts - 1) / parts;
+    for (size_t j = 0; j < n; ++j) {
+        real v[32];
+        for (size_t q = 0; q < parts; ++q) {
+            real a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            const size_t i0 = q * chunk, i1 = i0 + chunk < n ? i0 + chunk : n;
+            for (size_t i = i0; i < i1; ++i) a[(i - i0) & 7] = a[(i - i0) & 7] + s->cm[i * n + j] * R[i];
+            v[q] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+        }
+        for (size_t o = parts / 2; o >= 1; o /= 2)
+            for (size_t q = 0; q < o; ++q) v[q] = v[q] + v[q + o];
+        P[j] = cstore(s, v[0]);
+    }
+}
+
 void og_v_cycle(og_sim* s, int L, const ss_mg_schedule* mg, real dt, real rho) {
     const int q = mg->ref_quirks;
     if (L == s->levels - 1) {
-        og_smooth_mode(s, L, mg->n_coarse, dt, rho, q);
+        if (og_coarse_matrix_applies(s, L)) og_coarse_matrix(s, L, mg, dt, rho);
+        else og_smooth_mode(s, L, mg->n_coarse, dt, rho, q);
         return;
     }
     og_smooth_mode(s, L, mg->n_pre, dt, rho, q);

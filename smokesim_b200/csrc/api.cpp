@@ -92,6 +92,9 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->p64b);
     cudaFree(s->render_buf);
     cudaFree(s->ffield);
+    cudaFree(s->cmat);
+    cudaFree(s->cmat_alpha);
+    cudaFree(s->cmat_state);
     for (auto& g : s->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     cudaFree(s->d_scale);
@@ -203,6 +206,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     // cooperative launches per V-cycle (default 0: one launch per operator)
     if (const char* e = getenv("SMOKESIM_COOP_CELLS")) s->coop_cells = atoll(e);
     if (const char* e = getenv("SMOKESIM_ADJ_ZM")) s->adj_zm = atoi(e);
+    if (const char* e = getenv("SMOKESIM_COARSE_SWEEPS")) s->coarse_matrix = atoi(e) ? 0 : 1;
     s->nv[0] = (size_t)(s->nx + 1) * s->ny * s->nz;
     s->nv[1] = (size_t)s->nx * (s->ny + 1) * s->nz;
     s->nv[2] = s->dim == 3 ? (size_t)s->nx * s->ny * (s->nz + 1) : 0;
@@ -769,6 +773,19 @@ static int ensure_mixed(ss_sim* s, int prec, cudaStream_t st) {
             CU(cudaMemsetAsync(s->cr[l], 0, n * 2, st), "memset");
         }
     }
+    if (s->coarse_matrix && !s->cmat && s->bottom <= s->levels - 1) {
+        const ss::Level& lc = s->lv[s->levels - 1];
+        const long long nc = (long long)lc.n[0] * lc.n[1] * lc.n[2];
+        if (nc <= kCoarseResponseMax) {
+            CU(cudaMalloc((void**)&s->cmat, (size_t)(nc * nc) * sizeof(float)), "cudaMalloc(coarse matrix)");
+            CU(cudaMalloc((void**)&s->cmat_alpha, (size_t)nc * sizeof(float)), "cudaMalloc(coarse matrix)");
+            CU(cudaMalloc((void**)&s->cmat_state, 2 * sizeof(int)), "cudaMalloc(coarse matrix)");
+            CU(cudaMemsetAsync(s->cmat_state, 0xff, 2 * sizeof(int), st), "memset");
+            s->cmat_n = (int)nc;
+            s->cmat_dirty = 1;
+            s->cmat_iters = -1;
+        }
+    }
     s->cstore = prec;
     return SS_OK;
 }
@@ -812,6 +829,7 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
     if (mg.ref_quirks) return set_error(SS_E_INVALID, "the mixed-precision solve runs the corrected operators (ref_quirks = 0)");
     TRY(ensure_mixed(s, mg.precision, st));
     TRY(ensure_pyramid(s, st));
+    TRY(update_coarse_matrix(s, mg, st));
     const bool tol_mode = mg.tol > 0.0;
     const bool stats = p->collect_stats || tol_mode;
     TRY(launch_divergence(s, true, stats ? SLOT_DIV_BEFORE : -1, st));

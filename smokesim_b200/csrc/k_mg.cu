@@ -441,6 +441,7 @@ int launch_solid_pyramid(ss_sim* s, cudaStream_t st) {
         }
     }
     s->pyramid_dirty = 0;
+    s->cmat_dirty = 1;
     s->nlaunch += s->levels - 1;
     return check_cuda(cudaGetLastError(), "k_restrict_alpha");
 }
@@ -537,6 +538,7 @@ struct BottomArgsT {
     int total;
     int n_pre, n_post, n_coarse, quirks;
     float oob_smooth, oob_resid;
+    const float* cmat;   // coarsest level by its response matrix (mixed solve), or null: sweeps
 };
 
 template <typename T>
@@ -679,6 +681,37 @@ SS_D void bottom_smooth(const MGArgs& a, int iterations) {
 
 // T: storage type of the global level arrays; R: rounding of every value the
 // solve stores (T, or float for the FP32 solve).
+// Part of p_j = sum_i E[i n + j] r_i over i in [i0, i1), where E[i n + j] =
+// dp_j / dr_i of the coarsest level's n_coarse sweeps from p = 0
+// (k_coarse_response, layout 1): eight partial sums taken round-robin
+// ((i - i0) mod 8), added pairwise, so the oracle can repeat the order.  Two
+// rounds of eight independent loads are in flight per step (the matrix
+// streams from L2).
+SS_D float coarse_product(const float* __restrict__ E, const float* r, int n, int j, int i0, int i1) {
+    float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float* e = E + j;
+    int i = i0;
+    for (; i + 16 <= i1; i += 16) {
+        float v[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = __ldg(e + (size_t)(i + k) * n);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) a[k & 7] += v[k] * r[i + k];
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+        if (i + k < i1) a[k & 7] += __ldg(e + (size_t)(i + k) * n) * r[i + k];
+    return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+}
+
+// Threads per coarse value in the bottom's matrix product: the largest power
+// of two (at most 32) with parts * n <= the block's 1024 threads.
+SS_D int coarse_parts(int n) {
+    int parts = 1;
+    while (parts < 32 && parts * 2 * n <= 1024) parts *= 2;
+    return parts;
+}
+
 template <int DIM, typename T, typename R>
 __global__ void __launch_bounds__(1024) k_bottom(BottomArgsT<T> b) {
     extern __shared__ float sm[];
@@ -738,7 +771,23 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgsT<T> b) {
         __syncthreads();
     }
     // coarsest level
-    bottom_smooth<DIM, R>(bottom_level(b, sp, sr, sa, b.nlev - 1, b.oob_smooth), b.n_coarse);
+    if (b.cmat) {
+        // p = E r: `parts` adjacent lanes per value, each over a contiguous
+        // slice of i, their sums folded by a shuffle tree (lane q += lane q + o
+        // for o = parts/2 .. 1)
+        const MGArgs ac = bottom_level(b, sp, sr, sa, b.nlev - 1, b.oob_smooth);
+        const int n = ac.nx * ac.ny * ac.nz;
+        const int parts = coarse_parts(n), chunk = (n + parts - 1) / parts;
+        const int t = threadIdx.x, j = t / parts, part = t % parts;
+        const bool on = t < n * parts;
+        float v = 0.f;
+        if (on) v = coarse_product(b.cmat, ac.r, n, j, part * chunk, min(n, (part + 1) * chunk));
+        for (int o = parts / 2; o >= 1; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (on && part == 0) ac.p[j] = rnd<R>(v);
+        __syncthreads();
+    } else {
+        bottom_smooth<DIM, R>(bottom_level(b, sp, sr, sa, b.nlev - 1, b.oob_smooth), b.n_coarse);
+    }
     // up: prolongation + post-smoothing
     for (int l = b.nlev - 2; l >= 0; --l) {
         const MGArgs a = bottom_level(b, sp, sr, sa, l, b.oob_smooth);
@@ -819,6 +868,7 @@ static int launch_bottom_t(ss_sim* s, const ss_mg_schedule& mg, int L, T* const*
     b.quirks = mg.ref_quirks ? 1 : 0;
     b.oob_smooth = smooth_oob(s, mg.ref_quirks);
     b.oob_resid = resid_oob(s, mg.ref_quirks);
+    b.cmat = sizeof(T) == 2 ? s->cmat : nullptr;   // the mixed solve's coarse storage
     const size_t smem = (size_t)3 * off * sizeof(float);
     if (smem > (size_t)kBottomSmemBytes) return set_error(SS_E_INVALID, "bottom levels exceed shared memory");
     // the attribute is per function; setting it on every launch is cheap
@@ -836,15 +886,18 @@ int launch_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, cudaStream_t st) {
     return launch_bottom_t<float, float>(s, mg, L, s->p, s->r, st);
 }
 
-// Response of the coarsest level's smoothing to unit right-hand sides, for
-// the adjoint (which applies its transpose as one matrix-vector product
-// instead of transposing the sweeps one by one): block i runs the bottom
-// solve's `iters` red-black iterations from p = 0 with r = e_i (corrected
-// out-of-grid rule, FP32 stores) and writes the result into column i of D,
-// D[j * n + i] = dp_j / dr_i.
+// Response of the coarsest level's smoothing to unit right-hand sides: block
+// i runs the bottom solve's `iters` red-black iterations from p = 0 with
+// r = e_i (corrected out-of-grid rule, FP32 stores) and writes the result p
+// as D[j * n + i] = dp_j / dr_i (layout 0: the adjoint applies D^T, reading
+// consecutive i) or D[i * n + j] (layout 1: the mixed solve's bottom applies
+// D, reading consecutive j).  With `state`, blocks do nothing unless
+// state[1] (set by k_coarse_check) asks for a rebuild.
 template <int DIM>
 __global__ void __launch_bounds__(1024) k_coarse_response(BottomLevel lv, const float* __restrict__ alpha, float oobA,
-                                                          int iters, float* __restrict__ D) {
+                                                          int iters, float* __restrict__ D, int layout,
+                                                          const int* __restrict__ state) {
+    if (state && state[1] == 0) return;
     extern __shared__ float sm[];
     const int n = lv.n[0] * lv.n[1] * lv.n[2];
     float* sp = sm;
@@ -865,10 +918,25 @@ __global__ void __launch_bounds__(1024) k_coarse_response(BottomLevel lv, const 
     a.hh = lv.hh;
     a.rho_h = 0.f; a.dt = 1.f; a.rho = 1.f; a.dt_h = 1.f;
     bottom_smooth<DIM, float>(a, iters);
-    for (int c = threadIdx.x; c < n; c += blockDim.x) D[(size_t)c * n + i] = sp[c];
+    for (int c = threadIdx.x; c < n; c += blockDim.x) D[layout ? (size_t)i * n + c : (size_t)c * n + i] = sp[c];
 }
 
-int launch_coarse_response(ss_sim* s, int iters, float* D, cudaStream_t st) {
+// One block: state[1] = 1 when the coarsest level's solid fractions or the
+// iteration count differ from the ones the matrix was built for (state[0];
+// -1 before the first build), and the new ones are kept.
+__global__ void __launch_bounds__(1024) k_coarse_check(const float* __restrict__ alpha, float* __restrict__ kept, int n,
+                                                       int iters, int* __restrict__ state) {
+    int diff = 0;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) diff |= alpha[c] != kept[c];
+    diff = __syncthreads_or(diff) || state[0] != iters;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) kept[c] = alpha[c];
+    if (threadIdx.x == 0) {
+        state[0] = iters;
+        state[1] = diff;
+    }
+}
+
+static int launch_response(ss_sim* s, int iters, float* D, int layout, const int* state, cudaStream_t st) {
     const ss::Level& lv = s->lv[s->levels - 1];
     const int n = lv.n[0] * lv.n[1] * lv.n[2];
     if (n > kCoarseResponseMax) return set_error(SS_E_INVALID, "coarsest level too large for its response matrix");
@@ -877,10 +945,32 @@ int launch_coarse_response(ss_sim* s, int iters, float* D, cudaStream_t st) {
     b.off = 0;
     b.hh = lv.hh;
     const size_t smem = (size_t)3 * n * sizeof(float);
-    if (s->dim == 3) k_coarse_response<3><<<n, 1024, smem, st>>>(b, s->alpha[s->levels - 1], smooth_oob(s, 0), iters, D);
-    else k_coarse_response<2><<<n, 1024, smem, st>>>(b, s->alpha[s->levels - 1], smooth_oob(s, 0), iters, D);
+    const float* alpha = s->alpha[s->levels - 1];
+    if (s->dim == 3) k_coarse_response<3><<<n, 1024, smem, st>>>(b, alpha, smooth_oob(s, 0), iters, D, layout, state);
+    else k_coarse_response<2><<<n, 1024, smem, st>>>(b, alpha, smooth_oob(s, 0), iters, D, layout, state);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_coarse_response");
+}
+
+int launch_coarse_response(ss_sim* s, int iters, float* D, cudaStream_t st) {
+    return launch_response(s, iters, D, 0, nullptr, st);
+}
+
+// The mixed solve's coarsest-level matrix, rebuilt where the solid pyramid
+// or the coarse iteration count changed since it was built.
+int update_coarse_matrix(ss_sim* s, const ss_mg_schedule& mg, cudaStream_t st) {
+    if (!s->cmat) return SS_OK;
+    if (!s->cmat_dirty && s->cmat_iters == mg.n_coarse) return SS_OK;
+    const ss::Level& lv = s->lv[s->levels - 1];
+    const int n = lv.n[0] * lv.n[1] * lv.n[2];
+    k_coarse_check<<<1, 1024, 0, st>>>(s->alpha[s->levels - 1], s->cmat_alpha, n, mg.n_coarse, s->cmat_state);
+    s->nlaunch += 1;
+    int rc = check_cuda(cudaGetLastError(), "k_coarse_check");
+    if (rc == SS_OK) rc = launch_response(s, mg.n_coarse, s->cmat, 1, s->cmat_state, st);
+    if (rc != SS_OK) return rc;
+    s->cmat_dirty = 0;
+    s->cmat_iters = mg.n_coarse;
+    return SS_OK;
 }
 
 // ---------------------------------------------------- coarse-storage variants

@@ -117,6 +117,13 @@ struct ss_sim {
     long long coop_cells = 0;  // coarse levels of at most this many cells run in the cooperative legs (0: none)
     int use_tma = 1;           // TMA tile loads: 1 coarse-level sweeps, 2 also level 0 (where the layout allows)
     int adj_zm = 0;            // adjoint sweeps of 3D levels with even nx: z-marching pair kernel with at most this many planes a block (0: one cell a thread)
+    // mixed solve: the coarsest level by its response matrix instead of its
+    // n_coarse sweeps (levels of at most kCoarseResponseMax cells)
+    int coarse_matrix = 1;       // SMOKESIM_COARSE_SWEEPS=1 sets 0
+    float* cmat = nullptr;       // cmat_n^2: E[i n + j] = dp_j / dr_i
+    float* cmat_alpha = nullptr; // solid fractions it was built for
+    int* cmat_state = nullptr;   // device: [0] iteration count it was built for, [1] rebuild flag
+    int cmat_n = 0, cmat_iters = -1, cmat_dirty = 1;
     // The multigrid part of a solve recorded once as a CUDA graph and replayed
     // (api.cpp, run_graph): slot 0 fixed-count FP32 V-cycles, 1 one FP32
     // tolerance cycle, 2/3 one mixed refinement step per FP64 buffer parity.
@@ -239,6 +246,7 @@ struct AdjScratch {
 // coarsest levels up to this many cells get a response matrix (4 MiB)
 constexpr int kCoarseResponseMax = 1024;
 int launch_coarse_response(ss_sim* s, int iters, float* D, cudaStream_t st);
+int update_coarse_matrix(ss_sim* s, const ss_mg_schedule& mg, cudaStream_t st);
 // Scratch of the deterministic (owner-computes) adjoint scatters; a null
 // AdjOwner selects the atomic scatter-adds.
 struct AdjOwner {
