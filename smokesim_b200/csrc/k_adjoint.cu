@@ -8,9 +8,10 @@
 // no derivatives; the forward operators they transpose are restatements of
 // its shaders (cited at the forward kernels).
 //
-//  - advection: the trilinear gather becomes a scatter-add (atomicAdd) into
-//    the advected array, plus the chain rule through the back-traced point
-//    into the velocity that traced it;
+//  - advection: the trilinear gather becomes a scatter-add into the advected
+//    array (atomicAdd, warp-aggregated along x for the smoke; or the
+//    deterministic owner-computes gather below), plus the chain rule through
+//    the back-traced point into the velocity that traced it;
 //  - buoyancy: a 2-tap average per y face, transposed into the two cells;
 //  - vorticity confinement: f = N x w with N = grad|w| / (|grad|w|| + 1e-20),
 //    w = curl of the cell-centred velocity; its Jacobian-transpose in three
@@ -155,6 +156,40 @@ SS_D bool smoke_cell_adj(const AdjFluid& a, int x, int y, int z, const float* __
     return true;
 }
 
+// Warp-aggregated scatter of one tap row: c0 into (x0, y, z), c1 into
+// (x0 + 1, y, z).  The 32 lanes of a warp hold consecutive x of one row, so a
+// lane's x0 + 1 is usually the next lane's x0: that lane then adds the
+// previous lane's c1 to its own c0 and one atomic serves both.  The merge
+// decision (row_merge, from the lanes' packed tap coordinates; key < 0: no
+// sample) is shared by every array scattered through the same taps; every
+// lane of the warp makes both calls.
+struct RowMerge {
+    bool take, given;
+};
+SS_D long long row_key(bool live, int x0, int y, int z) {
+    return live ? (((long long)(z + 2) << 42) | ((long long)(y + 2) << 21) | (long long)(x0 + 2)) : -1;
+}
+SS_D RowMerge row_merge(long long key) {
+    const int lane = threadIdx.x & 31;
+    const long long pk = __shfl_up_sync(0xffffffffu, key, 1);
+    RowMerge m;
+    m.take = lane > 0 && key >= 0 && pk >= 0 && pk + 1 == key;
+    m.given = __shfl_down_sync(0xffffffffu, (int)m.take, 1) != 0 && lane < 31;
+    return m;
+}
+SS_D void row_scatter(float* a, int ax, int ay, int az, int x0, int y, int z, float c0, float c1, bool live,
+                      const RowMerge& m) {
+    const float pc1 = __shfl_up_sync(0xffffffffu, c1, 1);
+    if (m.take) c0 += pc1;
+    if (live) {
+        scatter(a, ax, ay, az, x0, y, z, c0);
+        if (!m.given) scatter(a, ax, ay, az, x0 + 1, y, z, c1);
+    }
+}
+
+// Atomic variant: the per-cell part without its scatter, then the samples'
+// adjoints of every channel through warp-aggregated tap rows (blocks of 32
+// lanes along x; no early exit, every lane takes part in the shuffles).
 template <int DIM>
 __global__ void __launch_bounds__(256) k_adj_advect_smoke(AdjFluid a, const float* __restrict__ dout, const float* __restrict__ tout,
                                                           float* __restrict__ din, float* __restrict__ tin,
@@ -163,14 +198,45 @@ __global__ void __launch_bounds__(256) k_adj_advect_smoke(AdjFluid a, const floa
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    if (x >= nx || y >= ny || z >= nz) return;
-    const int c = idx3(x, y, z, nx, ny);
+    const bool in = x < nx && y < ny && z < nz;
+    const int c = in ? idx3(x, y, z, nx, ny) : 0;
     const size_t ncell = (size_t)nx * ny * nz;
-    float vb[3], tc[3];
-    smoke_cell_adj<DIM>(a, x, y, z, dout, tout, din, tin, vb, tc);
-    vcb[c] = vb[0];
-    vcb[ncell + c] = vb[1];
-    if (DIM == 3) vcb[2 * ncell + c] = vb[2];
+    float vb[3] = {0.f, 0.f, 0.f}, tc[3] = {0.f, 0.f, 0.f};
+    const bool live = in && smoke_cell_adj<DIM>(a, x, y, z, dout, tout, nullptr, nullptr, vb, tc);
+    if (in) {
+        vcb[c] = vb[0];
+        vcb[ncell + c] = vb[1];
+        if (DIM == 3) vcb[2 * ncell + c] = vb[2];
+    }
+    const float fx = floorf(tc[0]), fy = floorf(tc[1]), fz = DIM == 3 ? floorf(tc[2]) : 0.f;
+    const int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
+    const float wx = tc[0] - fx, wy = tc[1] - fy, wz = tc[2] - fz;
+    constexpr int KZ = DIM == 3 ? 2 : 1;
+    RowMerge m[KZ][2];
+#pragma unroll
+    for (int k = 0; k < KZ; ++k)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) m[k][j] = row_merge(row_key(live, x0, y0 + j, z0 + k));
+    for (int ch = 0; ch <= a.nch; ++ch) {
+        const bool is_t = ch == a.nch;
+        const float g = live ? (is_t ? tout[c] : dout[ch * ncell + c]) : 0.f;
+        float* dst = is_t ? tin : din + ch * ncell;
+#pragma unroll
+        for (int k = 0; k < KZ; ++k)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                float c0, c1;
+                if constexpr (DIM == 3) {
+                    const float wyz = j ? wy : 1.f - wy, wzk = k ? wz : 1.f - wz;
+                    c0 = g * ((1.f - wx) * wyz * wzk);
+                    c1 = g * (wx * wyz * wzk);
+                } else {
+                    c0 = g * (1.f - wx) * (j ? wy : 1.f - wy);
+                    c1 = g * wx * (j ? wy : 1.f - wy);
+                }
+                row_scatter(dst, nx, ny, DIM == 3 ? nz : 1, x0, y0 + j, z0 + k, c0, c1, live, m[k][j]);
+            }
+    }
 }
 
 // faces += 0.5 * (per-cell velocity adjoint of the two cells sharing the face)
