@@ -58,6 +58,8 @@ def load(precision="f32"):
         L.og_set_field_f64.argtypes = [vp, i, C.POINTER(C.c_double), sz]
         L.og_set_emitter_force.argtypes = [vp, C.POINTER(C.c_float * 3)]
         L.og_set_emitter_force_f64.argtypes = [vp, C.POINTER(C.c_double * 3)]
+        L.og_set_coarse_matrix.argtypes = [vp, i]
+        L.og_set_coarse_matrix.restype = None
         L.og_set_force_field.argtypes = [vp, i, C.POINTER(C.c_float)]
         L.og_set_force_field.restype = None
         L.og_set_force_field_f64.argtypes = [vp, i, C.POINTER(C.c_double)]
@@ -167,6 +169,11 @@ class OracleSim:
         else:
             a = np.ascontiguousarray(a, dtype=np.float32)
             self.L.og_set_force_field(self.h, n, a.ctypes.data_as(C.POINTER(C.c_float)))
+
+    def set_coarse_matrix(self, on):
+        """Mixed solve: coarsest level by its response matrix (default, as
+        the CUDA path) or swept (the CUDA path's SMOKESIM_COARSE_SWEEPS=1)."""
+        self.L.og_set_coarse_matrix(self.h, int(bool(on)))
 
     def set_emitter_force(self, force):
         f = (C.c_double * 3)(*[float(x) for x in force])

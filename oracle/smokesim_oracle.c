@@ -79,6 +79,7 @@ typedef struct og_sim {
     real* cm_alpha;
     size_t cm_n;
     int cm_iters;
+    int cm_off;      /* 1: sweep the coarsest level (the CUDA path's SMOKESIM_COARSE_SWEEPS=1) */
 } og_sim;
 
 /* ---------------------------------------------------------------- helpers */
@@ -922,8 +923,10 @@ void og_prolong_and_add(og_sim* s, int L) {
  * in the summation order of the CUDA product. */
 static int og_coarse_matrix_applies(const og_sim* s, int L) {
     const size_t n = (size_t)s->ls[L][0] * s->ls[L][1] * s->ls[L][2];
-    return s->cround != 0 && L >= 1 && L == s->levels - 1 && n <= 1024;
+    return !s->cm_off && s->cround != 0 && L >= 1 && L == s->levels - 1 && n <= 1024;
 }
+
+void og_set_coarse_matrix(og_sim* s, int on) { s->cm_off = on ? 0 : 1; }
 
 static void og_coarse_matrix(og_sim* s, int L, const ss_mg_schedule* mg, real dt, real rho) {
     const size_t n = (size_t)s->ls[L][0] * s->ls[L][1] * s->ls[L][2];

@@ -151,3 +151,18 @@ def test_mixed_stage_subsets(stages):
         pairs.append((sg.div_after, so.div_after))
     for a, b in pairs:
         assert abs(a - b) <= 1e-9 * max(1.0, abs(b))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,dim,n,nch,enc,mc", [MIXED_GRIDS[0], MIXED_GRIDS[1], MIXED_GRIDS[5]])
+def test_mixed_coarse_sweeps_bitwise(monkeypatch, name, dim, n, nch, enc, mc):
+    """SMOKESIM_COARSE_SWEEPS=1 sweeps the coarsest level instead of applying
+    its response matrix; the oracle's sweeping form matches it bit for bit."""
+    monkeypatch.setenv("SMOKESIM_COARSE_SWEEPS", "1")
+    g, o = make_pair(dim, n, nch, enc, seed=41, min_coarse=mc)
+    o.set_coarse_matrix(False)
+    p = scene.workload_params(ref_quirks=0, precision=abi.PREC_MIXED, n_vcycles=3, n_coarse=12)
+    for k in range(2):
+        g.step(p)
+        o.step(p)
+        assert_same(g, o, dim, f"coarse sweeps step {k}")

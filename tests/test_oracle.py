@@ -242,6 +242,31 @@ def test_mixed_precision_refinement_reaches_tolerance(oracle_mod):
     assert err < 1e-4, err
 
 
+@pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_MIXED_BF16])
+def test_mixed_coarse_matrix_matches_sweeps(oracle_mod, prec):
+    """The mixed solve's coarsest level as one product with the response
+    matrix of its sweeps (default) against the sweeps themselves (GRF scene at
+    32^3, coarsest 4^3, 80 iterations): the same linear map up to rounding,
+    so the two solves take the same refinement steps (within one) to 1e-6 and
+    their pressures agree to what that tolerance fixes (a 1e-6 relative
+    residual leaves ~1e-4 in the pressure on this grid)."""
+    res = {}
+    for on in (True, False):
+        sc = scene.grf256(seed=0, n=32)
+        o = oracle_mod.OracleSim(sc["desc"], "f32")
+        scene.apply(o, sc)
+        o.set_coarse_matrix(on)
+        for _ in range(2):
+            o.step(scene.workload_params(ref_quirks=0, tol=1e-6, n_vcycles=40, precision=prec))
+        st = o.stats()
+        res[on] = (st.converged, st.vcycles, o.get_field(abi.FIELD_PRESSURE, f64=True))
+        fluid = o.get_field(abi.FIELD_SOLID) == 0
+    assert res[True][0] == res[False][0] == 1
+    assert abs(res[True][1] - res[False][1]) <= 1
+    a, b = res[True][2][fluid], res[False][2][fluid]
+    assert rel_l2(a - a.mean(), b - b.mean()) < 1e-3
+
+
 def test_render_known_answers(oracle_mod):
     """The render restatement: an empty 3D grid leaves every pixel transparent
     (the ray marches through zero density); an empty 2D grid shows the ambient
