@@ -211,6 +211,14 @@ int ss_clear_grid(ss_sim* sim, float t_ambient, void* stream);
 /* ---- the step ------------------------------------------------------------------ */
 /* Reference run_physics_step (common/physics/physics.c:72-101), nsteps times. */
 int ss_run_physics_step(ss_sim* sim, const ss_params* params, int nsteps, void* stream);
+/* Statistics of the last ss_run_physics_step call.  Every bounded wait inside
+ * a kernel that gave up (bit 0 of the simulation's device error word: a
+ * coarse-level sweep whose TMA tile loads did not arrive in time) is reported
+ * as SS_E_CUDA by the next call that reads the device back - ss_get_stats,
+ * ss_get_field with a host destination, or the step itself when it collects
+ * statistics or solves to a tolerance - and then cleared.  A step that neither
+ * collects statistics nor solves to a tolerance returns SS_OK before its
+ * kernels ran, so check one of those calls before trusting its fields. */
 int ss_get_stats(ss_sim* sim, ss_stats* out);
 
 /* ---- individual stages (reference common/physics/grid.h:37-68) -------------- */
@@ -245,9 +253,11 @@ int ss_init_solid_map(ss_sim* sim, void* stream);                               
  * Allocates nothing: its scratch (16384 FP64 partial sums, 128 KiB) is a
  * static device array that every GPU loading this library holds until exit.
  * At most 67,108,864 cells; larger grids return SS_E_INVALID.  The first call
- * on each device looks up that array's address (a one-time set-up); make that
- * first call before any stream capture begins.  All calls share the scratch,
- * so calls that overlap on the GPU (different streams, no ordering) race. */
+ * on each device looks up that array's address (a one-time set-up, repeated
+ * only when the device's CUDA context changed, e.g. after cudaDeviceReset);
+ * make that first call before any stream capture begins.  All calls share the
+ * scratch, so calls that overlap on the GPU (different streams, no ordering)
+ * race. */
 int ss_divergence_norm_noalloc(int dim, const int n[3], const float* u, const float* v, const float* w,
                                const uint8_t* solid, double* out_norm, void* stream);
 

@@ -86,6 +86,8 @@ def load(precision="f32"):
         L.og_divergence_norm.restype = C.c_double
         L.og_projected_residual_norm.argtypes = [vp, real, real]
         L.og_projected_residual_norm.restype = C.c_double
+        L.og_update_emitters_status.argtypes = [vp, C.c_float]
+        L.og_update_emitters_status.restype = None
         L.og_init_solid_map.argtypes = [vp]
         L.og_update_solid_map.argtypes = [vp]
         L.og_num_threads.restype = i
@@ -221,6 +223,9 @@ class OracleSim:
     # single stages
     def stage(self, name, params):
         getattr(self.L, "og_stage_" + name)(self.h, C.byref(params))
+
+    def update_emitters_status(self, params):
+        self.L.og_update_emitters_status(self.h, params.current_time)
 
     def smooth(self, level, iterations, params):
         self.L.og_smooth_mode(self.h, level, iterations, params.time_step, params.density, params.mg.ref_quirks)

@@ -8,7 +8,6 @@ from __future__ import annotations
 
 import ctypes as C
 import os
-import subprocess
 import threading
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))

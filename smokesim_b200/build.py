@@ -17,7 +17,7 @@ CSRC = os.path.join(PKG_DIR, "csrc")
 OUT = os.path.join(PKG_DIR, "libsmokesim.so")
 BUILD_DIR = os.path.join(PKG_DIR, "_build")
 
-SOURCES = ["api.cpp", "k_fluid.cu", "k_mg.cu", "k_rbgs.cu", "k_rbgs_tma.cu", "k_rb.cu", "k_rb_tma.cu", "k_scene.cu", "k_mixed.cu", "k_adjoint.cu", "adjoint.cpp", "k_render.cu", "state_io.cpp", "k_noalloc.cu"]
+SOURCES = ["api.cpp", "k_fluid.cu", "k_mg.cu", "k_rbgs.cu", "k_rbgs_tma.cu", "k_rb.cu", "k_scene.cu", "k_mixed.cu", "k_adjoint.cu", "adjoint.cpp", "k_render.cu", "state_io.cpp", "k_noalloc.cu"]
 HEADERS = ["common.cuh", "ss_internal.h", "tma.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -43,13 +43,21 @@ def build(force=False, verbose=False):
     # the image's CC/CXX wrappers lack libgomp; nvcc drives the system g++
     env.pop("CC", None)
     env.pop("CXX", None)
-    objs = []
-    for src in SOURCES:
+    def compile_one(src):
         obj = os.path.join(BUILD_DIR, os.path.splitext(src)[0] + ".o")
         cmd = [NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         r = subprocess.run(cmd, env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+        return src, obj, r
+
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    jobs = max(1, min(len(SOURCES), os.cpu_count() or 1))
+    with ThreadPoolExecutor(jobs) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    objs = []
+    for src, obj, r in results:
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}")
         if verbose and r.stdout:

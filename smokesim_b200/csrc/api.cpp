@@ -61,6 +61,9 @@ StepConsts make_consts(const ss_sim* s, const ss_params* p) {
 #define CU(x, what) TRY(check_cuda((x), what))
 
 static cudaStream_t as_stream(void* st) { return (cudaStream_t)st; }
+extern "C" {
+static int check_device_error(ss_sim* s, cudaStream_t st);
+}
 
 static int dalloc(void** p, size_t bytes) {
     if (bytes == 0) bytes = 16;
@@ -110,7 +113,6 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->d_ob);
     cudaFree(s->d_bx);
     cudaFree(s->d_err);
-    cudaFree(s->coop_bar);
     delete s;
 }
 
@@ -198,14 +200,10 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     s->h = d->cell_size;
     s->t_amb0 = d->t_ambient;
     s->ncell = (size_t)s->nx * s->ny * s->nz;
-    // SMOKESIM_TMA: 0 keeps every sweep on per-thread loads, 1 (default) feeds
-    // the coarse-level tiled sweeps with TMA, 2 also the level-0 colour sweeps
-    // (the warp-specialised pipeline of k_rb_tma.cu); the results are the same
-    if (const char* e = getenv("SMOKESIM_TMA")) s->use_tma = atoi(e);
-    // SMOKESIM_COOP_CELLS: coarse levels of at most this many cells run as two
-    // cooperative launches per V-cycle (default 0: one launch per operator)
-    if (const char* e = getenv("SMOKESIM_COOP_CELLS")) s->coop_cells = atoll(e);
-    if (const char* e = getenv("SMOKESIM_ADJ_ZM")) s->adj_zm = atoi(e);
+    // SMOKESIM_TMA=0 keeps the coarse-level tiled sweeps on per-thread loads
+    // (the form every grid whose rows TMA cannot tile takes anyway); the
+    // default 1 feeds them with TMA.  The results are the same.
+    if (const char* e = getenv("SMOKESIM_TMA")) s->use_tma = atoi(e) ? 1 : 0;
     if (const char* e = getenv("SMOKESIM_COARSE_SWEEPS")) s->coarse_matrix = atoi(e) ? 0 : 1;
     s->nv[0] = (size_t)(s->nx + 1) * s->ny * s->nz;
     s->nv[1] = (size_t)s->nx * (s->ny + 1) * s->nz;
@@ -268,7 +266,6 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     A((void**)&s->red.partial2, (size_t)2 * s->red.stage2 * sizeof(double));
     A((void**)&s->red.out, SLOT_COUNT * sizeof(double));
     A((void**)&s->d_err, sizeof(int));
-    A((void**)&s->coop_bar, 2 * sizeof(unsigned int));
     A((void**)&s->red.ticket, sizeof(unsigned int));
     if (rc == SS_OK) {
         cudaError_t e = cudaMallocHost((void**)&s->red.host, SLOT_COUNT * sizeof(double));
@@ -291,7 +288,6 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
         if (!rc) rc = check_cuda(cudaMemsetAsync(s->r[l], 0, n * 4, st), "memset");
     }
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->d_err, 0, sizeof(int), st), "memset");
-    if (!rc) rc = check_cuda(cudaMemsetAsync(s->coop_bar, 0, 2 * sizeof(unsigned int), st), "memset");
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->red.ticket, 0, sizeof(unsigned int), st), "memset");
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->div0, 0, s->ncell * 4, st), "memset");
     if (!rc && s->div0r != s->div0) rc = check_cuda(cudaMemsetAsync(s->div0r, 0, s->ncell * 4, st), "memset");
@@ -547,7 +543,7 @@ int ss_get_field(ss_sim* s, int f, float* host, size_t count, void* stream) {
     if (count != n) return set_error(SS_E_INVALID, "element count does not match the field");
     CU(cudaMemcpyAsync(host, d, n * sizeof(float), cudaMemcpyDeviceToHost, st), "get_field");
     CU(cudaStreamSynchronize(st), "get_field sync");
-    return SS_OK;
+    return check_device_error(s, st);
 }
 
 int ss_field_device_ptr(ss_sim* s, int f, void** dptr, size_t* count) {
@@ -656,11 +652,23 @@ static int v_cycle_rec(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg,
     return SS_OK;
 }
 
+// The device error word collects the bounded waits that gave up (bit 0: a
+// coarse-level sweep's TMA tile load did not arrive in time, so that sweep
+// skipped its cells).  It is read here - by every statistics read of a step,
+// ss_get_stats and ss_get_field - reported once and cleared, so the next
+// report concerns later launches only.
 static int check_device_error(ss_sim* s, cudaStream_t st) {
     int err = 0;
     CU(cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "error word");
     CU(cudaStreamSynchronize(st), "error word sync");
-    if (err) return set_error(SS_E_CUDA, "a kernel gave up waiting for its tile loads (bounded barrier wait)");
+    if (err) {
+        CU(cudaMemsetAsync(s->d_err, 0, sizeof(int), st), "error word clear");
+        CU(cudaStreamSynchronize(st), "error word clear");
+        if (err & 1)
+            return set_error(SS_E_CUDA, "a coarse-level sweep gave up waiting for its TMA tile loads (bounded wait); "
+                                        "the pressure of that solve is not valid");
+        return set_error(SS_E_CUDA, "unknown bit set in the device error word");
+    }
     return SS_OK;
 }
 
@@ -804,12 +812,6 @@ static int v_cycle_mixed(ss_sim* s, const StepConsts& c, const ss_mg_schedule& m
     }
     if (L >= s->bottom) return coarse_bottom(s, mg, L, prec, st);
     if (L == s->levels - 1) return coarse_smooth(s, c, L, mg.n_coarse, prec, st);
-    if (L == coarse_coop_first(s)) {
-        // levels L .. bottom-1 in one cooperative launch per leg
-        TRY(launch_coarse_coop(s, c, mg, prec, true, st));
-        TRY(coarse_bottom(s, mg, s->bottom, prec, st));
-        return launch_coarse_coop(s, c, mg, prec, false, st);
-    }
     TRY(coarse_smooth(s, c, L, mg.n_pre, prec, st));
     TRY(coarse_residual_restrict(s, c, L, prec, st));
     const size_t nc = (size_t)s->lv[L + 1].n[0] * s->lv[L + 1].n[1] * s->lv[L + 1].n[2];
@@ -834,7 +836,6 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
     const bool stats = p->collect_stats || tol_mode;
     TRY(launch_divergence(s, true, stats ? SLOT_DIV_BEFORE : -1, st));
     if (!s->p64_valid) TRY(launch_p64_from_p0(s, st));
-    CU(cudaMemsetAsync(s->coop_bar, 0, 2 * sizeof(unsigned int), st), "clear grid barrier");
     const int cap = mg.n_vcycles > 0 ? mg.n_vcycles : 1;
     int done = 0;
     double db = 0.0, res = 0.0;

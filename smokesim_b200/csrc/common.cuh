@@ -295,8 +295,12 @@ SS_D float f4(const float4& v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k =
 
 // a / f for an integer count f in 1..6, value-identical to the IEEE quotient
 // (the same value; -0 may come back as +0): q0 = a*RN(1/f) followed by one
-// residual correction with fused multiply-adds, verified exhaustively against
-// IEEE division over every finite float a for f = 1..5 (tests/division_check.c).
+// residual correction with fused multiply-adds - the FMA-based correctly
+// rounded division of P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990, with the
+// exact reciprocal of a small integer as its start value - verified
+// exhaustively against IEEE division over every finite float a for f = 1..5
+// (tests/division_check.c).
 // For f = 6 it divides a/2 by 3, exact except where a/2 is subnormal, which
 // takes the IEEE path.
 SS_D float div_by_count(float a, int f) {

@@ -418,96 +418,6 @@ __global__ void __launch_bounds__(256) k_adj_smooth(AdjLevel a, int colour, int 
 }
 
 // residual adjoint of a fine cell from its coarse parent
-// z-marching form of k_adj_smooth (3D, even nx): thread (i, y) owns the cell
-// pair x = 2i, 2i + 1 of row y for `planes` z planes and updates the one of
-// this colour in each.  T of the planes z - 1, z, z + 1 at the pair stays in
-// registers, plane z is shared with the block for the x and y neighbours, and
-// pbar, bbar and T move as 8-byte pairs (the partner keeps its loaded value:
-// no thread writes the other colour in a half-step).  Same operations in the
-// same order as k_adj_smooth, so the results are identical.
-template <bool L0>
-__global__ void __launch_bounds__(256) k_adj_smooth_zm(AdjLevel a, int colour, int do_b, int do_a, int planes) {
-    __shared__ float2 sT[10][34];   // plane z: rows y0 - 1 .. y0 + 8, pairs i0 - 1 .. i0 + 32
-    const int lx = threadIdx.x, ly = threadIdx.y;
-    const int i = blockIdx.x * 32 + lx, y = blockIdx.y * 8 + ly;
-    const int nx = a.nx, ny = a.ny, nz = a.nz, np = nx >> 1;
-    const int z0 = blockIdx.z * planes, z1 = min(z0 + planes, nz);
-    const bool act = i < np && y < ny;
-    float2* __restrict__ T2 = reinterpret_cast<float2*>(a.T);
-    float2* __restrict__ P2 = reinterpret_cast<float2*>(a.pbar);
-    float2* __restrict__ B2 = reinterpret_cast<float2*>(a.bbar);
-    const float2 zero = make_float2(0.f, 0.f);
-    auto pq = [&](int pi, int py, int pz) { return (pz * ny + py) * np + pi; };   // pair index
-    float2 prev = zero, cur = zero, next = zero;
-    if (do_b && act) {
-        if (z0 > 0) prev = T2[pq(i, y, z0 - 1)];
-        cur = T2[pq(i, y, z0)];
-    }
-    for (int z = z0; z < z1; ++z) {
-        if (do_b) {
-            if (act && z + 1 < nz) next = T2[pq(i, y, z + 1)];
-            __syncthreads();   // the previous plane's readers are done
-            if (act) sT[ly + 1][lx + 1] = cur;
-            if (i < np) {
-                const int y0 = blockIdx.y * 8;
-                if (ly == 0 && y0 > 0) sT[0][lx + 1] = T2[pq(i, y0 - 1, z)];
-                if (ly == 7 && y0 + 8 < ny) sT[9][lx + 1] = T2[pq(i, y0 + 8, z)];
-            }
-            if (y < ny) {
-                if (lx == 0 && i > 0) sT[ly + 1][0] = T2[pq(i - 1, y, z)];
-                if (lx == 31 && i + 1 < np) sT[ly + 1][33] = T2[pq(i + 1, y, z)];
-            }
-            __syncthreads();
-        }
-        if (act) {
-            const int par = (y + z + colour) & 1;
-            const int x = 2 * i + par;
-            const int q = pq(i, y, z);
-            float wself, d;
-            bool fluid;
-            cell_weights<3, L0>(a, x, y, z, wself, d, fluid);
-            float2 p2 = P2[q];
-            float pb = par ? p2.y : p2.x;
-            if (do_b) {
-                float sum = 0.f;
-                if (y + 1 < ny) sum += par ? sT[ly + 2][lx + 1].y : sT[ly + 2][lx + 1].x;
-                if (y > 0) sum += par ? sT[ly][lx + 1].y : sT[ly][lx + 1].x;
-                if (x + 1 < nx) sum += par ? sT[ly + 1][lx + 2].x : cur.y;
-                if (x > 0) sum += par ? cur.x : sT[ly + 1][lx].y;
-                if (z + 1 < nz) sum += par ? next.y : next.x;
-                if (z > 0) sum += par ? prev.y : prev.x;
-                pb += wself * sum;
-            }
-            if (do_a) {
-                float t = 0.f;
-                if (fluid && d != 0.f) {
-                    t = pb / d;
-                    pb = 0.f;
-                    float2 b2 = B2[q];
-                    if (par) b2.y -= a.beta * t;
-                    else b2.x -= a.beta * t;
-                    B2[q] = b2;
-                }
-                if (do_b) {
-                    float2 t2 = cur;
-                    if (par) t2.y = t;
-                    else t2.x = t;
-                    T2[q] = t2;
-                } else {
-                    a.T[2 * q + par] = t;
-                }
-            }
-            if (par) p2.y = pb;
-            else p2.x = pb;
-            P2[q] = p2;
-        }
-        if (do_b) {
-            prev = cur;
-            cur = next;
-        }
-    }
-}
-
 template <int DIM, bool L0>
 SS_D float res_bar(const AdjLevel& a, const float* __restrict__ rcb, int cx, int cy, int cz, int x, int y, int z) {
     const int X = x >> 1, Y = y >> 1, Z = DIM == 3 ? z >> 1 : 0;
@@ -1339,17 +1249,10 @@ static AdjLevel adj_level(ss_sim* s, const StepConsts& c, int L, const AdjScratc
 static int adj_sweeps(ss_sim* s, const AdjLevel& a, int L, int iterations, cudaStream_t st) {
     if (iterations <= 0) return SS_OK;
     dim3 g = grid_of((a.nx + 1) / 2, a.ny, a.nz, kB);
-    const bool zm = s->dim == 3 && s->adj_zm && (a.nx & 1) == 0;
-    const long long tiles = (long long)((a.nx / 2 + 31) / 32) * ((a.ny + 7) / 8);
-    const int planes = z_planes(tiles, a.nz, s->adj_zm > 0 ? s->adj_zm : 1);
-    const dim3 gz((a.nx / 2 + 31) / 32, (a.ny + 7) / 8, (a.nz + planes - 1) / planes);
     // forward: per sweep colour 0 then 1; transpose: per sweep colour 1 then 0,
     // each colour's gather half fused with the next colour's update half
     auto launch = [&](int colour, int do_b, int do_a) {
-        if (zm) {
-            if (L == 0) k_adj_smooth_zm<true><<<gz, kB, 0, st>>>(a, colour, do_b, do_a, planes);
-            else k_adj_smooth_zm<false><<<gz, kB, 0, st>>>(a, colour, do_b, do_a, planes);
-        } else if (s->dim == 3) {
+        if (s->dim == 3) {
             if (L == 0) k_adj_smooth<3, true><<<g, kB, 0, st>>>(a, colour, do_b, do_a);
             else k_adj_smooth<3, false><<<g, kB, 0, st>>>(a, colour, do_b, do_a);
         } else {

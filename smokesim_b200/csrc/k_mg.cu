@@ -67,8 +67,8 @@ static MGArgs mg_args(ss_sim* s, const StepConsts& c, int L, float oobA) {
 
 // ------------------------------------------------------------------ smoother
 // A level value as float; CG reads through L2 only (ld.global.cg), for
-// arrays other blocks of the same cooperative launch wrote since this SM last
-// cached them (L1 is not coherent across SMs).
+// arrays that other blocks of the same launch may have written since this SM
+// last cached them (L1 is not coherent across SMs).
 template <bool CG, typename T>
 SS_D float ldv(const T* p) {
     if constexpr (CG) return ld(__ldcg(p));
@@ -1040,181 +1040,6 @@ int coarse_residual_restrict(ss_sim* s, const StepConsts& c, int L, int prec, cu
 int coarse_prolong(ss_sim* s, int L, int prec, cudaStream_t st) {
     if (prec == SS_PREC_MIXED) return coarse_prolong_t<__half>(s, L, (__half*)s->cp[L], (const __half*)s->cp[L + 1], st);
     return coarse_prolong_t<__nv_bfloat16>(s, L, (__nv_bfloat16*)s->cp[L], (const __nv_bfloat16*)s->cp[L + 1], st);
-}
-
-// ------------------------------------------------- cooperative coarse legs
-// Opt-in (SMOKESIM_COOP_CELLS): the levels between the first with at most
-// coop_cells cells and the bottom solve, where a launch per operator costs
-// about as much as the operator.  Each V-cycle leg of those levels runs as ONE
-// cooperative launch
-// (all blocks co-resident) whose phases - half-sweeps, residual + restriction
-// (with the clearing of the next level's correction), prolongation - are
-// separated by a grid barrier; the per-cell operators are the ones above,
-// with level reads through L2 (other blocks wrote them since this SM may
-// have cached them).  Down leg: pre-smoothing and restriction of each level
-// first .. bottom-1; the bottom kernel runs between the legs; up leg:
-// prolongation and post-smoothing back to level first.  Measured on the
-// 256^3 step it is slower than the graph of separate launches (levels 64^3
-// and 32^3: 91 us against 69 us a V-cycle; with 128^3: 281 us against
-// 166 us): the grid-stride phases have fewer threads in flight than a
-// launch per operator, and a grid barrier costs about what a launch inside
-// a CUDA graph does.  So it is off by default.
-template <typename T>
-struct CoopLevel {
-    MGArgsT<T> sm;   // smoother operands (out-of-grid rule of the smoother)
-    MGArgsT<T> rs;   // residual operands (rule of the residual)
-};
-
-template <typename T>
-struct CoopArgs {
-    CoopLevel<T> lv[SS_MAX_LEVELS];
-    int first, last;        // levels first .. last-1 (last: the bottom level)
-    int n_pre, n_post;
-    unsigned int* bar;      // arrivals, generation
-    int* err;               // bit 1: a grid barrier gave up
-};
-
-// Grid barrier over gridDim.x co-resident blocks (generation counting).  The
-// wait is bounded (about a second); a block that gives up sets the error word
-// and reports false, and every block then stops at its next barrier.
-SS_D bool coop_sync(unsigned int* bar, int* err) {
-    __syncthreads();
-    __shared__ int ok_s;
-    if (threadIdx.x == 0) {
-        volatile unsigned int* gen = bar + 1;
-        const unsigned int g = *gen;
-        __threadfence();
-        int ok = 1;
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            for (int k = 0; *gen == g; ++k) {
-                if (k > (1 << 23)) {
-                    ok = 0;
-                    atomicOr(err, 2);
-                    break;
-                }
-                if (k > 16) __nanosleep(100);
-            }
-        }
-        __threadfence();
-        ok_s = ok;
-    }
-    __syncthreads();
-    return ok_s != 0;
-}
-
-template <int DIM, typename T>
-SS_D void coop_smooth(const MGArgsT<T>& a, int parity, int gt, int gs) {
-    const int hx = (a.nx + 1) / 2;
-    const int items = hx * a.ny * a.nz;
-    for (int i = gt; i < items; i += gs) {
-        const int xi = i % hx, t = i / hx, y = t % a.ny, z = t / a.ny;
-        const int x = 2 * xi + ((y + z + parity) & 1);
-        if (x < a.nx) smooth_cell<DIM, false, T, T, true>(a, x, y, z);
-    }
-}
-
-template <int DIM, bool DOWN, typename T>
-__global__ void __launch_bounds__(256) k_coarse_coop(CoopArgs<T> A) {
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
-    if constexpr (DOWN) {
-        for (int L = A.first; L < A.last; ++L) {
-            const CoopLevel<T>& lv = A.lv[L];
-            for (int it = 0; it < 2 * A.n_pre; ++it) {
-                coop_smooth<DIM, T>(lv.sm, it & 1, gt, gs);
-                if (!coop_sync(A.bar, A.err)) return;
-            }
-            const MGArgsT<T>& nx = A.lv[L + 1].sm;
-            const int hx = (lv.rs.nx + 1) / 2, hy = (lv.rs.ny + 1) / 2, hz = DIM == 3 ? (lv.rs.nz + 1) / 2 : 1;
-            for (int i = gt; i < hx * hy * hz; i += gs) {
-                const int X = i % hx, t = i / hx, Y = t % hy, Z = t / hy;
-                residual_restrict_cell<DIM, false, false, true, T, true>(lv.rs, nx.r, nx.nx, nx.ny, nx.nz, X, Y, Z);
-            }
-            const int nc = nx.nx * nx.ny * nx.nz;
-            for (int i = gt; i < nc; i += gs) nx.p[i] = st<T>(0.f);
-            if (L + 1 < A.last && !coop_sync(A.bar, A.err)) return;
-        }
-    } else {
-        for (int L = A.last - 1; L >= A.first; --L) {
-            const CoopLevel<T>& lv = A.lv[L];
-            const MGArgsT<T>& nx = A.lv[L + 1].sm;
-            const int nf = lv.sm.nx * lv.sm.ny * lv.sm.nz;
-            for (int i = gt; i < nf; i += gs) {
-                const int x = i % lv.sm.nx, t = i / lv.sm.nx, y = t % lv.sm.ny, z = t / lv.sm.ny;
-                prolong_cell<DIM, T, true>(lv.sm.p, lv.sm.nx, lv.sm.ny, lv.sm.nz, nx.p, nx.nx, nx.ny, nx.nz, x, y, z);
-            }
-            for (int it = 0; it < 2 * A.n_post; ++it) {
-                if (!coop_sync(A.bar, A.err)) return;
-                coop_smooth<DIM, T>(lv.sm, it & 1, gt, gs);
-            }
-            if (L > A.first && !coop_sync(A.bar, A.err)) return;
-        }
-    }
-}
-
-// first level of the cooperative legs, or -1 (none: every level runs its own launches)
-int coarse_coop_first(const ss_sim* s) {
-    if (s->coop_cells <= 0 || s->bottom >= s->levels) return -1;
-    for (int L = 1; L < s->bottom && L < s->levels - 1; ++L)
-        if ((long long)s->lv[L].n[0] * s->lv[L].n[1] * s->lv[L].n[2] <= s->coop_cells) return L;
-    return -1;
-}
-
-template <int DIM, bool DOWN, typename T>
-static int launch_coop_t(ss_sim* s, const CoopArgs<T>& A, cudaStream_t st) {
-    static int blocks = 0;
-    if (blocks == 0) {
-        int dev = 0, sms = 0, occ = 0;
-        TRY_CUDA_MG(cudaGetDevice(&dev), "cudaGetDevice");
-        TRY_CUDA_MG(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-        TRY_CUDA_MG(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_coarse_coop<DIM, DOWN, T>, 256, 0),
-                    "occupancy");
-        if (occ < 1) return set_error(SS_E_UNSUPPORTED, "cooperative coarse kernel does not fit an SM");
-        // two blocks an SM: enough threads for a 64^3 half-sweep, few arrivals per barrier
-        blocks = sms * std::min(occ, 2);
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(blocks);
-    cfg.blockDim = dim3(256);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    s->nlaunch += 1;
-    return check_cuda(cudaLaunchKernelEx(&cfg, k_coarse_coop<DIM, DOWN, T>, A), "k_coarse_coop");
-}
-
-template <typename T>
-static int launch_coarse_coop_t(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, bool down, T* const* cp,
-                                T* const* cr, cudaStream_t st) {
-    const int first = coarse_coop_first(s);
-    if (first < 1) return set_error(SS_E_INVALID, "no cooperative coarse levels");
-    CoopArgs<T> A{};
-    A.first = first;
-    A.last = s->bottom;
-    A.n_pre = mg.n_pre;
-    A.n_post = mg.n_post;
-    A.bar = s->coop_bar;
-    A.err = s->d_err;
-    for (int L = first; L <= s->bottom; ++L) {
-        A.lv[L].sm = mg_args_t<T>(s, c, L, smooth_oob(s, 0), cp[L], cr[L]);
-        A.lv[L].rs = mg_args_t<T>(s, c, L, resid_oob(s, 0), cp[L], cr[L]);
-    }
-    if (s->dim == 3) return down ? launch_coop_t<3, true, T>(s, A, st) : launch_coop_t<3, false, T>(s, A, st);
-    return down ? launch_coop_t<2, true, T>(s, A, st) : launch_coop_t<2, false, T>(s, A, st);
-}
-
-int launch_coarse_coop(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int prec, bool down, cudaStream_t st) {
-    if (prec == SS_PREC_MIXED)
-        return launch_coarse_coop_t<__half>(s, c, mg, down, (__half* const*)s->cp, (__half* const*)s->cr, st);
-    return launch_coarse_coop_t<__nv_bfloat16>(s, c, mg, down, (__nv_bfloat16* const*)s->cp,
-                                               (__nv_bfloat16* const*)s->cr, st);
 }
 
 int coarse_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, int prec, cudaStream_t st) {

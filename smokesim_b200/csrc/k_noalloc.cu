@@ -33,7 +33,29 @@ constexpr long long kMaxCells = kCellsPerBlock * kMaxPartials;               // 
 __device__ __align__(256) double g_noalloc_partials[kMaxPartials];
 
 std::mutex g_setup_mu;
-double* g_partials_addr[256] = {};   // device address of g_noalloc_partials, per device ordinal
+// Device address of g_noalloc_partials per device ordinal, with the CUDA
+// context it was looked up in: after cudaDeviceReset (or under another
+// context on that device) the module is loaded again, possibly elsewhere, so
+// a changed context means a new look-up.
+double* g_partials_addr[256] = {};
+void* g_partials_ctx[256] = {};
+
+// The calling thread's current CUDA context (driver cuCtxGetCurrent, found
+// through the runtime so that no driver library is linked); null if unknown.
+void* current_context() {
+    using Fn = int (*)(void**);
+    static Fn fn = []() -> Fn {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            return reinterpret_cast<Fn>(p);
+        return nullptr;
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
 
 __device__ __forceinline__ double block_sum_noalloc(double v) {
 #pragma unroll
@@ -105,19 +127,22 @@ __global__ void __launch_bounds__(1024) k_div_norm_noalloc_final(const double* _
     if (threadIdx.x == 0) *out = sqrt(sh[0]);
 }
 
-// Set-up, once per device and with that device current: the host-side name
-// g_noalloc_partials is only a stand-in, so look up the array's device address.
+// Set-up, once per device (and again only if that device's context changed),
+// with the device current: the host-side name g_noalloc_partials is only a
+// stand-in, so look up the array's device address.
 int scratch_address(double** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return check_cuda(e, "cudaGetDevice");
     if (dev < 0 || dev >= 256) return set_error(SS_E_UNSUPPORTED, "device ordinal out of range");
+    const void* ctx = current_context();
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_partials_addr[dev]) {
+    if (!g_partials_addr[dev] || !ctx || ctx != g_partials_ctx[dev]) {
         void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        e = cudaGetSymbolAddress(&p, g_noalloc_partials);   // also makes the device's context current
         if (e != cudaSuccess) return check_cuda(e, "cudaGetSymbolAddress(g_noalloc_partials)");
         g_partials_addr[dev] = static_cast<double*>(p);
+        g_partials_ctx[dev] = current_context();
     }
     *out = g_partials_addr[dev];
     return SS_OK;

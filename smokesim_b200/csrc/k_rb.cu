@@ -495,13 +495,9 @@ int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st) {
         planes = (int)std::max(1LL, std::min(16LL, per_plane * g.nz / (148LL * 4 * 3)));
     }
     dim3 gr4(gr.x, gr.y, (g.nz + planes - 1) / planes);
-    const bool tma = rb_tma_supported(s);
     for (int it = 0; it < iterations; ++it)
         for (int c = 0; c < 2; ++c) {
-            if (tma) {
-                const int rc = launch_rb_smooth_tma(s, p[c], p[1 - c], rhs[c], mask[c], c, st);
-                if (rc) return rc;
-            } else if (s->rb_vec) {
+            if (s->rb_vec) {
                 if (s->dim == 3) k_rb_smooth4<3><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
                 else k_rb_smooth4<2><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
             } else {

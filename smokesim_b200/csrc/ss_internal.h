@@ -113,10 +113,7 @@ struct ss_sim {
     ss_stats st{};
     long long nlaunch = 0;     // kernels launched since the counter was reset
     int* d_err = nullptr;      // device error word: bit 0 = a bounded barrier wait gave up
-    unsigned int* coop_bar = nullptr;   // grid barrier of the cooperative coarse legs: arrivals, generation
-    long long coop_cells = 0;  // coarse levels of at most this many cells run in the cooperative legs (0: none)
-    int use_tma = 1;           // TMA tile loads: 1 coarse-level sweeps, 2 also level 0 (where the layout allows)
-    int adj_zm = 0;            // adjoint sweeps of 3D levels with even nx: z-marching pair kernel with at most this many planes a block (0: one cell a thread)
+    int use_tma = 1;           // TMA tile loads of the coarse-level tiled sweeps (0: per-thread loads)
     // mixed solve: the coarsest level by its response matrix instead of its
     // n_coarse sweeps (levels of at most kCoarseResponseMax cells)
     int coarse_matrix = 1;       // SMOKESIM_COARSE_SWEEPS=1 sets 0
@@ -226,11 +223,6 @@ inline int z_planes(long long tiles, int nz, int max_planes, int min_planes = 1,
     if (p < min_planes) p = min_planes;
     return (int)p;
 }
-bool rb_tma_supported(const ss_sim* s);
-int launch_rb_smooth_tma(ss_sim* s, float* pc, const float* po, const float* rhs, const uint8_t* mask, int colour,
-                         cudaStream_t st);
-int coarse_coop_first(const ss_sim* s);
-int launch_coarse_coop(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int prec, bool down, cudaStream_t st);
 int launch_force_field(ss_sim* s, const StepConsts& c, cudaStream_t st);
 int launch_vorticity_field(ss_sim* s, const StepConsts& c, const float* const vel[3], float* out, cudaStream_t st);
 

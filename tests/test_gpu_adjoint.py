@@ -470,19 +470,3 @@ def test_coarse_response_matches_sweeps(monkeypatch):
     for k in a:
         s_k = max(float(np.abs(b[k]).max()), 1e-30) if k == "force" else scale
         assert np.allclose(a[k], b[k], rtol=1e-4, atol=1e-5 * s_k), (k, float(np.abs(a[k] - b[k]).max()), s_k)
-
-
-@pytest.mark.parametrize("stage,mask", [("projection", abi.STAGE_RESOLVE_PRESSURE | abi.STAGE_UPDATE_VELOCITIES),
-                                        ("full", abi.STAGE_ALL)])
-def test_zmarch_adjoint_sweeps_identical(monkeypatch, stage, mask):
-    """The opt-in z-marching adjoint smoother (SMOKESIM_ADJ_ZM=16: pairs of
-    cells, two planes a block at 128 x 128 x 64) gives bitwise the gradients
-    of the default one-cell-a-thread kernel; owner-computes scatters make both
-    runs reproducible."""
-    n = (128, 128, 64)
-    monkeypatch.delenv("SMOKESIM_ADJ_ZM", raising=False)
-    a = _stage_grads(3, n, 1, 1, mask, True)
-    monkeypatch.setenv("SMOKESIM_ADJ_ZM", "16")
-    b = _stage_grads(3, n, 1, 1, mask, True)
-    for k in a:
-        assert a[k].tobytes() == b[k].tobytes(), k

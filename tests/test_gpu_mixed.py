@@ -20,7 +20,7 @@ MIXED_GRIDS = [
     ("3d_tma", 3, (32, 24, 20), 1, 1, 4),
     ("3d_l1", 3, (64, 48, 48), 1, 1, 8),
     ("3d_even_not_quad", 3, (20, 18, 14), 1, 0, 4),   # nx % 8 != 0: one cell per thread
-    ("3d_two_segments", 3, (512, 12, 10), 1, 1, 4),    # TMA-fed level-0 sweep, two row segments
+    ("3d_long_rows", 3, (512, 12, 10), 1, 1, 4),       # colour rows of 256 cells
 ]
 
 
@@ -37,24 +37,6 @@ def test_mixed_solve_bitwise(name, dim, n, nch, enc, mc, prec):
     sg, so = g.stats(), o.stats()
     assert sg.vcycles == so.vcycles == 3
     assert abs(sg.residual - so.residual) <= 1e-9 * max(1e-30, so.residual)
-
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("coop", ["0", "4096", "100000000"])
-@pytest.mark.parametrize("name,dim,n,nch,enc,mc", [("3d_l1", 3, (64, 48, 48), 1, 1, 4),
-                                                   ("3d_open_odd", 3, (66, 50, 38), 1, 0, 4),
-                                                   ("2d_quad", 2, (128, 96, 1), 1, 1, 4)])
-def test_mixed_cooperative_coarse_legs(monkeypatch, coop, name, dim, n, nch, enc, mc):
-    """Coarse levels of at most SMOKESIM_COOP_CELLS cells run as two
-    cooperative launches per V-cycle (grid barriers between the operators);
-    0 keeps one launch per operator.  Same bits either way."""
-    monkeypatch.setenv("SMOKESIM_COOP_CELLS", coop)
-    g, o = make_pair(dim, n, nch, enc, seed=37, min_coarse=mc)
-    p = scene.workload_params(ref_quirks=0, precision=abi.PREC_MIXED, n_vcycles=3, n_coarse=12)
-    for k in range(2):
-        g.step(p)
-        o.step(p)
-        assert_same(g, o, dim, f"cooperative legs {coop} step {k}")
 
 
 @pytest.mark.gpu

@@ -27,9 +27,9 @@ GRIDS = [
     # taller than two z chunks and wider than one x tile of the fused
     # vorticity kernel (32 x 8 cells, 32 planes per block)
     ("3d_tall_open", 3, (35, 10, 70), 1, 0),
-    # colour rows of 256 cells: the TMA-fed level-0 sweep runs two 128-wide
-    # segments per row and a row block (8 rows) that straddles the grid edge
-    ("3d_two_segments", 3, (512, 12, 10), 1, 1),
+    # colour rows of 256 cells and a row block (8 rows) that straddles the
+    # grid edge
+    ("3d_long_rows", 3, (512, 12, 10), 1, 1),
 ]
 
 
@@ -285,19 +285,18 @@ def test_full_step_bitwise_tma(name, dim, n, nch, enc, mc):
         assert_same(g, o, dim, f"tma full step {k}")
 
 
-# Level-0 colour sweeps on every path: per-thread loads (SMOKESIM_TMA=0 and
-# the default) and the warp-specialised TMA pipeline (SMOKESIM_TMA=2), which
-# runs where the colour rows are whole 16-byte units of mask bytes.
+# Full steps with the coarse-level sweeps on TMA tiles (default) and on
+# per-thread loads (SMOKESIM_TMA=0), FP32 and mixed precision.
 L0_TMA_GRIDS = [
     ("3d_tma", 3, (32, 24, 20), 1, 1, 4),
     ("3d_tma_l1", 3, (64, 48, 48), 1, 1, 8),
-    ("3d_two_segments", 3, (512, 12, 10), 1, 1, 4),
-    ("3d_two_segments_open", 3, (512, 20, 9), 1, 0, 4),
+    ("3d_long_rows", 3, (512, 12, 10), 1, 1, 4),
+    ("3d_long_rows_open", 3, (512, 20, 9), 1, 0, 4),
 ]
 
 
 @pytest.mark.parametrize("name,dim,n,nch,enc,mc", L0_TMA_GRIDS)
-@pytest.mark.parametrize("tma", ["0", "2"])
+@pytest.mark.parametrize("tma", ["0", "1"])
 @pytest.mark.parametrize("prec", [abi.PREC_FP32, abi.PREC_MIXED])
 def test_full_step_bitwise_level0_paths(monkeypatch, name, dim, n, nch, enc, mc, tma, prec):
     monkeypatch.setenv("SMOKESIM_TMA", tma)
