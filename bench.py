@@ -313,6 +313,11 @@ ADJOINT_CASES = [
     ("plume128_mixed_no_recompute", dict(kind="plume3d", n=128), 200, 200, 1, False),
     ("plume128_deterministic", dict(kind="plume3d", n=128), 200, 14, 0, True),
 ]
+# cases whose forward pass also stores every step's solved pressure, so the
+# reverse pass recomputes segments without solving (ss_adjoint_set_pressure_store)
+PRESSURE_STORE_CASES = [
+    ("plume128_mixed_pressure_store", dict(kind="plume3d", n=128), 200, 14, 1, False),
+]
 
 
 def adjoint_bench(torch, stream):
@@ -323,7 +328,8 @@ def adjoint_bench(torch, stream):
     from smokesim_b200 import Sim, abi, scene
     from smokesim_b200.adjoint import Rollout
     out = {}
-    for name, sa, nsteps, every, prec, det in ADJOINT_CASES:
+    cases = [c + (False,) for c in ADJOINT_CASES] + [c + (True,) for c in PRESSURE_STORE_CASES]
+    for name, sa, nsteps, every, prec, det, pstore in cases:
         sc = scene.rollout64(seed=0, n=sa["n"]) if sa["kind"] == "rollout64" else scene.plume3d(seed=0, n=sa["n"])
         sc.pop("rng", None)
         p = scene.workload_params(ref_quirks=0, n_vcycles=4, collect_stats=0, precision=prec)
@@ -347,7 +353,7 @@ def adjoint_bench(torch, stream):
         # the reverse pass leaves the simulation in the rollout's initial state)
         sim = Sim(sc["desc"], stream=stream.cuda_stream)
         scene.apply(sim, sc)
-        ro = Rollout(sim, nsteps, every, deterministic=det)
+        ro = Rollout(sim, nsteps, every, deterministic=det, store_pressure=pstore)
         rho = torch.empty(abi.field_count(3, sim.n, abi.FIELD_DENSITY), device="cuda")
         for _ in range(2):
             torch.cuda.synchronize()
@@ -369,11 +375,50 @@ def adjoint_bench(torch, stream):
         out[name] = {"grid": [sa["n"]] * 3, "steps": nsteps, "checkpoint_every": every,
                      "precision": "mixed (f16 coarse)" if prec else "f32",
                      "scatter": "owner-computes" if det else "atomic",
+                     "recompute": ("segments replay the stored pressures (no solve)" if pstore else
+                                   "segments re-run every stage") if every < nsteps else "none",
                      "forward_ms_per_step": fwd_ms, "forward_with_checkpoints_ms_per_step": f_ms,
                      "fwd_adjoint_ms_per_step": fb_ms, "fwd_adjoint_over_forward": fb_ms / fwd_ms,
                      "fwd_adjoint_mcell_steps_per_s": cells / (fb_ms / 1e3) / 1e6,
                      "reverse_kernel_launches": info["kernel_launches"],
                      "checkpoint_bytes": info["checkpoint_bytes"], "workspace_bytes": info["workspace_bytes"]}
+    return out
+
+
+def config_runs(torch, stream, cpu):
+    """The plain-method configurations at their own sizes and step counts
+    (FP32, 4 V-cycles of 2+2 sweeps to 8, the reference's boundary rules):
+    the 2D 256^2 plume for 200 steps and the 3D 128^3 plume for 500 steps,
+    timed with CUDA events on the simulation's stream after 5 warm-up steps,
+    each with the C/OpenMP oracle on a bounded sample of the same steps."""
+    from smokesim_b200 import Sim, scene
+    out = {}
+    for name, sc, steps, sample in (("plume2d_256", scene.plume2d(seed=0, n=256), 200, 20),
+                                    ("plume3d_128", scene.plume3d(seed=0, n=128), 500, 4)):
+        sc.pop("rng", None)
+        p = sc["params"]
+        sim = Sim(sc["desc"], stream=stream.cuda_stream)
+        scene.apply(sim, sc)
+        sim.step(p, 5)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.step(p, steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        n = sc["desc"].n
+        cells = n[0] * n[1] * (n[2] if sc["desc"].dim == 3 else 1)
+        line = {"grid": [n[0], n[1]] + ([n[2]] if sc["desc"].dim == 3 else []), "steps": steps,
+                "ms_per_step": ms, "mcell_steps_per_s": cells / (ms / 1e3) / 1e6,
+                "schedule": "FP32, 4 V-cycles, 2+2 sweeps, 80 coarsest, down to 8, reference boundary rules"}
+        sim.close()
+        if cpu:
+            cv, csec, threads, _ = cpu_step_rate(sc, sample, 1)
+            line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
+                                    "ms_per_step": csec * 1e3,
+                                    "sample": f"median of {sample} steps after 1 warm-up from the initial state"}
+        out[name] = line
     return out
 
 
@@ -403,7 +448,7 @@ def inverse_control(args, torch, stream):
     ts.close()
     sim = Sim(sc["desc"], stream=stream.cuda_stream)
     scene.apply(sim, sc)
-    ro = Rollout(sim, nsteps, every)
+    ro = Rollout(sim, nsteps, every, store_pressure=True)
     forces = torch.zeros((nsteps, 3), dtype=torch.float32, requires_grad=True)
     field = torch.zeros((3, nf, nf, nf), dtype=torch.float32, requires_grad=True)
     opt = torch.optim.Adam([forces, field], lr=1e-2)
@@ -442,6 +487,7 @@ def inverse_control(args, torch, stream):
         "grid": [n] * 3, "steps": nsteps, "checkpoint_every": every, "iterations": iters,
         "controls": f"{nsteps} x 3 emitter forces + 3 x {nf}^3 force field", "optimizer": "Adam lr 1e-2",
         "precision": "mixed (f64 residual/refinement, f16 coarse), tolerance 1e-6",
+        "recompute": "checkpoint every ~sqrt(steps) steps; segments recomputed with the stored per-step pressures",
         "loss_first": losses[0], "loss_last": losses[-1], "loss_min": min(losses),
         "loss_curve": losses,
         "forward_with_checkpoints_ms_per_step": float(np.median(fwd_ms)),
@@ -631,8 +677,13 @@ def main():
                   "step_size": d.step_size, "shadow_steps": d.shadow_steps}
 
     adjoint = None
-    if not args.no_adjoint:
+    inverse = None
+    configs = None
+    if not args.no_adjoint and world == 1:
         adjoint = adjoint_bench(torch, stream)
+        inverse = inverse_control(args, torch, stream)["inverse_control"]
+    if world == 1:
+        configs = config_runs(torch, stream, rank == 0 and not args.no_cpu_baseline)
 
     line = {
         "impl": "b200", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -641,7 +692,9 @@ def main():
         "data": "synthetic (seeded scene + GRF)",
         "config": workload_config(args, sc), "gpu_launches": int(head["gpu_launches"]), "clocks": clocks,
         "variants": variants,
+        "configs": configs,
         "adjoint": adjoint,
+        "inverse_control": inverse,
         "render": render,
         "e2e": e2e, "roofline": roofline,
     }

@@ -317,6 +317,14 @@ int ss_adjoint_get_field(ss_adjoint* adj, int field, float* dst, size_t count, i
 int ss_adjoint_set_deterministic(ss_adjoint* adj, int on);
 /* Statistics of the last reverse pass: kernel launches and device bytes held
  * by checkpoints and recomputation buffers. */
+/* Pressure store (off by default): with on != 0 the next ss_adjoint_forward
+ * also keeps every step's solved pressure (nsteps fields, FP64 with the
+ * mixed-precision solve, FP32 otherwise), and ss_adjoint_backward's
+ * recomputation of a segment takes the stored pressure instead of running the
+ * pressure solve again.  The recomputed states - and so the gradients - are
+ * the same; the reverse pass saves one pressure solve per recomputed step for
+ * nsteps * ncell * 8 bytes of device memory (counted in checkpoint_bytes). */
+int ss_adjoint_set_pressure_store(ss_adjoint* adj, int on);
 int ss_adjoint_info(ss_adjoint* adj, long long* kernel_launches, long long* checkpoint_bytes, long long* workspace_bytes);
 /* dL/d(force field) after ss_adjoint_backward: 3*n^3 floats (host), the layout
  * of ss_set_force_field; count must match the simulation's field. */

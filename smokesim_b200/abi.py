@@ -293,7 +293,7 @@ EXPORTED = [
     "ss_get_level", "ss_set_level", "ss_divergence_norm_noalloc",
     "ss_set_emitter_force", "ss_set_force_field", "ss_adjoint_force_field_grad", "ss_adjoint_create", "ss_adjoint_destroy", "ss_adjoint_forward",
     "ss_adjoint_backward", "ss_adjoint_field_device_ptr", "ss_adjoint_get_field", "ss_adjoint_info",
-    "ss_adjoint_set_deterministic",
+    "ss_adjoint_set_deterministic", "ss_adjoint_set_pressure_store",
     "ss_set_field_device", "ss_get_field_device", "ss_render_default", "ss_render",
     "ss_save_state", "ss_load_state",
 ]
@@ -344,6 +344,7 @@ def _declare(L):
     L.ss_adjoint_field_device_ptr.argtypes = [vp, i, C.POINTER(vp), C.POINTER(sz)]
     L.ss_adjoint_info.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     L.ss_adjoint_set_deterministic.argtypes = [vp, i]
+    L.ss_adjoint_set_pressure_store.argtypes = [vp, i]
     L.ss_adjoint_get_field.argtypes = [vp, i, vp, sz, i, vp]
     L.ss_set_field_device.argtypes = [vp, i, vp, sz, vp]
     L.ss_render_default.argtypes = [vp, i, i, C.POINTER(RenderDesc)]

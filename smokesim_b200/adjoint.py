@@ -21,7 +21,8 @@ class Rollout:
     scatter-adds owner-computes (bitwise-repeatable gradients) instead of
     atomic."""
 
-    def __init__(self, sim: Sim, nsteps: int, checkpoint_every: int = 0, deterministic: bool = False):
+    def __init__(self, sim: Sim, nsteps: int, checkpoint_every: int = 0, deterministic: bool = False,
+                 store_pressure: bool = False):
         self.sim = sim
         self.L = sim.L
         self.nsteps = nsteps
@@ -30,9 +31,16 @@ class Rollout:
         self.h = h
         if deterministic:
             self.set_deterministic(True)
+        if store_pressure:
+            self.set_pressure_store(True)
 
     def set_deterministic(self, on: bool = True):
         _check(self.L.ss_adjoint_set_deterministic(self.h, int(bool(on))), "ss_adjoint_set_deterministic")
+
+    def set_pressure_store(self, on: bool = True):
+        """Keep every step's solved pressure in the forward pass, so the reverse
+        pass recomputes segments without solving again (same gradients)."""
+        _check(self.L.ss_adjoint_set_pressure_store(self.h, int(bool(on))), "ss_adjoint_set_pressure_store")
 
     def close(self):
         if getattr(self, "h", None):

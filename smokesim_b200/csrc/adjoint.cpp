@@ -30,6 +30,8 @@ struct State {
     float* dens = nullptr;
     float* temp = nullptr;
     float* p = nullptr;
+    double* p64 = nullptr;      // the mixed solve's FP64 pressure (allocated when a mixed forward saves one)
+    bool p64_valid = false;
     std::vector<ss_emitter> em;
     std::vector<ss_obstacle> ob;
 };
@@ -70,6 +72,13 @@ struct ss_adjoint {
     bool deterministic = false;    // owner-computes scatters instead of atomics
     bool forward_done = false;
     bool last_recorded = false;   // rec holds the last segment, written by the forward pass
+    // optional: the solved pressure of every step (FP64 with the mixed solve),
+    // so that recomputing a segment replays it instead of solving again
+    bool store_p = false;
+    std::vector<void*> pstore;
+    std::vector<int> pstore_vc;
+    size_t pstore_elem = 0;        // bytes per cell of the stored pressures
+    long long pstore_bytes = 0;
     // the transposed V-cycles of one step, recorded once as a CUDA graph
     cudaGraphExec_t vgraph = nullptr;
     unsigned char vkey[64] = {};
@@ -88,6 +97,7 @@ static void free_adjoint(ss_adjoint* A) {
     if (A->vgraph) cudaGraphExecDestroy(A->vgraph);
     cudaFree(A->ffgrad);
     for (void* p : A->allocs) cudaFree(p);
+    for (void* p : A->pstore) cudaFree(p);
     delete A;
 }
 
@@ -118,12 +128,20 @@ static int copy_d2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
     return check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st), "state copy");
 }
 
-static int save_state(ss_sim* s, State& S, cudaStream_t st) {
+static int save_state(ss_adjoint* A, State& S, cudaStream_t st) {
+    ss_sim* s = A->s;
     for (int d = 0; d < s->dim; ++d) TRY_ADJ(copy_d2d(S.vel[d], s->vel[d][s->vi[d]], s->nv[d] * 4, st));
     TRY_ADJ(copy_d2d(S.v_other, s->vel[1][1 - s->vi[1]], s->nv[1] * 4, st));
     TRY_ADJ(copy_d2d(S.dens, s->dens[s->si], s->ncell * s->nch * 4, st));
     TRY_ADJ(copy_d2d(S.temp, s->temp[s->si], s->ncell * 4, st));
     TRY_ADJ(copy_d2d(S.p, s->p[0], s->ncell * 4, st));
+    // the mixed solve warm-starts from its FP64 pressure: keep it exactly, so
+    // that a recomputed segment repeats the forward pass bit for bit
+    S.p64_valid = s->p64_valid && s->p64;
+    if (S.p64_valid) {
+        if (!S.p64) TRY_ADJ(amalloc(A, (void**)&S.p64, s->ncell * sizeof(double), &A->ckpt_bytes));
+        TRY_ADJ(copy_d2d(S.p64, s->p64, s->ncell * sizeof(double), st));
+    }
     S.em = s->em;
     S.ob = s->ob;
     return SS_OK;
@@ -136,6 +154,10 @@ static int restore_state(ss_sim* s, const State& S, cudaStream_t st) {
     TRY_ADJ(copy_d2d(s->temp[s->si], S.temp, s->ncell * 4, st));
     TRY_ADJ(copy_d2d(s->p[0], S.p, s->ncell * 4, st));
     s->p64_valid = 0;
+    if (S.p64_valid && s->p64) {
+        TRY_ADJ(copy_d2d(s->p64, S.p64, s->ncell * sizeof(double), st));
+        s->p64_valid = 1;
+    }
     s->em = S.em;
     s->ob = S.ob;
     return SS_OK;
@@ -213,10 +235,47 @@ static int adj_solve(ss_adjoint* A, const ss_params* p, const StepConsts& c, int
     return check_cuda(cudaGraphLaunch(A->vgraph, st), "cudaGraphLaunch");
 }
 
+// Size the per-step pressure store for this forward pass's precision.
+static int ensure_pstore(ss_adjoint* A, const ss_params* p) {
+    if (!A->store_p || !(p->stage_mask & SS_STAGE_RESOLVE_PRESSURE)) return SS_OK;
+    const size_t elem = p->mg.precision != SS_PREC_FP32 ? sizeof(double) : sizeof(float);
+    if (A->pstore_elem == elem && (int)A->pstore.size() == A->n) return SS_OK;
+    for (void* q : A->pstore) cudaFree(q);
+    A->pstore.clear();
+    A->pstore_bytes = 0;
+    A->pstore_elem = 0;
+    A->pstore.assign(A->n, nullptr);
+    A->pstore_vc.assign(A->n, 0);
+    for (int k = 0; k < A->n; ++k) {
+        const cudaError_t e = cudaMalloc(&A->pstore[k], A->s->ncell * elem);
+        if (e != cudaSuccess) {
+            for (void* q : A->pstore) cudaFree(q);
+            A->pstore.clear();
+            return check_cuda(e, "cudaMalloc(pressure store)");
+        }
+        A->pstore_bytes += (long long)(A->s->ncell * elem);
+    }
+    A->pstore_elem = elem;
+    return SS_OK;
+}
+
+// the pressure-store part of a step's saves: save in the forward pass,
+// replay when a segment is recomputed
+static void pstore_saves(ss_adjoint* A, int k, bool replay, StepSaves& sv) {
+    if (!A->store_p || A->pstore.empty()) return;
+    if (replay) {
+        sv.pres_restore = A->pstore[k];
+        sv.vcycles_restore = A->pstore_vc[k];
+    } else {
+        sv.pres_save = A->pstore[k];
+    }
+}
+
 // Forward step k keeping what its adjoint reads.
-static int record_step(ss_adjoint* A, const ss_params* p, int k, Record& R, cudaStream_t st) {
+static int record_step(ss_adjoint* A, const ss_params* p, int k, Record& R, cudaStream_t st, bool replay = false) {
     ss_sim* s = A->s;
     StepSaves sv{};
+    pstore_saves(A, k, replay, sv);
     for (int d = 0; d < s->dim; ++d) {
         sv.emit_vel[d] = R.ue[d];
         sv.force_vel[d] = R.ua[d];
@@ -227,6 +286,7 @@ static int record_step(ss_adjoint* A, const ss_params* p, int k, Record& R, cuda
     set_force(A, k);
     TRY_ADJ(run_step(s, p, st, &sv));
     R.vcycles = sv.vcycles;
+    if (!replay && !A->pstore.empty()) A->pstore_vc[k] = sv.vcycles;
     R.em = s->em;
     if (p->stage_mask & SS_STAGE_APPLY_VORTICITY) {
         const float* ua[3] = {R.ua[0], R.ua[1], R.ua[2]};
@@ -365,15 +425,19 @@ int ss_adjoint_forward(ss_adjoint* A, const ss_params* p, const float* forces, v
     }
     s->nlaunch = 0;
     A->last_recorded = false;
+    TRY_ADJ(ensure_pstore(A, p));
     const int last0 = ((A->n - 1) / A->every) * A->every;   // first step of the last segment
     for (int k = 0; k < A->n; ++k) {
-        if (k % A->every == 0) TRY_ADJ(save_state(s, A->ckpt[k / A->every], st));
+        if (k % A->every == 0) TRY_ADJ(save_state(A, A->ckpt[k / A->every], st));
         // the last segment keeps its intermediates now: the reverse pass
         // starts there without recomputing it
         if (k >= last0) TRY_ADJ(record_step(A, p, k, A->rec[k - last0], st));
         else {
             set_force(A, k);
-            TRY_ADJ(run_step(s, p, st, nullptr));
+            StepSaves sv{};
+            pstore_saves(A, k, false, sv);
+            TRY_ADJ(run_step(s, p, st, sv.pres_save ? &sv : nullptr));
+            if (sv.pres_save) A->pstore_vc[k] = sv.vcycles;
         }
     }
     for (int d = 0; d < 3; ++d) s->force[d] = 0.f;
@@ -423,7 +487,7 @@ int ss_adjoint_backward(ss_adjoint* A, const ss_params* p, const float* grad_den
         const int k0 = sg * A->every, k1 = std::min(A->n, k0 + A->every);
         if (!(sg == nseg - 1 && A->last_recorded)) {
             TRY_ADJ(restore_state(s, A->ckpt[sg], st));
-            for (int k = k0; k < k1; ++k) TRY_ADJ(record_step(A, p, k, A->rec[k - k0], st));
+            for (int k = k0; k < k1; ++k) TRY_ADJ(record_step(A, p, k, A->rec[k - k0], st, true));
         }
         A->last_recorded = false;   // rec now holds this segment
         for (int k = k1 - 1; k >= k0; --k) TRY_ADJ(adj_step(A, p, k, A->rec[k - k0], st));
@@ -508,10 +572,24 @@ int ss_adjoint_set_deterministic(ss_adjoint* A, int on) {
     return SS_OK;
 }
 
+int ss_adjoint_set_pressure_store(ss_adjoint* A, int on) {
+    if (!A) return set_error(SS_E_INVALID, "NULL handle");
+    A->store_p = on != 0;
+    if (!A->store_p) {
+        for (void* q : A->pstore) cudaFree(q);
+        A->pstore.clear();
+        A->pstore_vc.clear();
+        A->pstore_bytes = 0;
+        A->pstore_elem = 0;
+    }
+    A->forward_done = false;   // the next backward needs a forward that filled (or not) the store
+    return SS_OK;
+}
+
 int ss_adjoint_info(ss_adjoint* A, long long* launches, long long* ckpt_bytes, long long* work_bytes) {
     if (!A) return set_error(SS_E_INVALID, "NULL handle");
     if (launches) *launches = A->launches;
-    if (ckpt_bytes) *ckpt_bytes = A->ckpt_bytes;
+    if (ckpt_bytes) *ckpt_bytes = A->ckpt_bytes + A->pstore_bytes;
     if (work_bytes) *work_bytes = A->work_bytes;
     return SS_OK;
 }

@@ -802,13 +802,16 @@ static int ensure_mixed(ss_sim* s, int prec, cudaStream_t st) {
 // coarse levels FP16/BF16), corrected operators (ref_quirks = 0).
 static int v_cycle_mixed(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int L, int prec, cudaStream_t st) {
     if (L == 0) {
-        TRY(launch_rb_sweep(s, mg.n_pre, st));
+        // e starts at 0 and the prolongation zeroes non-fluid cells: the
+        // half-sweeps may take the select-free form where that prolongation runs
+        const bool z = rb_zero_form(s);
+        TRY(launch_rb_sweep(s, mg.n_pre, st, z));
         TRY(launch_rb_residual_restrict_mixed(s, prec, st));
         const size_t nc = (size_t)s->lv[1].n[0] * s->lv[1].n[1] * s->lv[1].n[2];
         CU(cudaMemsetAsync(s->cp[1], 0, nc * 2, st), "clear coarse p");
         TRY(v_cycle_mixed(s, c, mg, 1, prec, st));
         TRY(launch_rb_prolong_mixed(s, prec, st));
-        return launch_rb_sweep(s, mg.n_post, st);
+        return launch_rb_sweep(s, mg.n_post, st, z);
     }
     if (L >= s->bottom) return coarse_bottom(s, mg, L, prec, st);
     if (L == s->levels - 1) return coarse_smooth(s, c, L, mg.n_coarse, prec, st);
@@ -987,8 +990,33 @@ static int do_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* sv
     const bool defer_p0 = (m & SS_STAGE_RESOLVE_PRESSURE) && (m & SS_STAGE_UPDATE_VELOCITIES) &&
                           p->mg.precision != SS_PREC_FP32;
     if (m & SS_STAGE_RESOLVE_PRESSURE) {
-        TRY(pressure_solve(s, p, c, st, defer_p0));
-        if (sv) sv->vcycles = s->st.vcycles;
+        const bool f64 = p->mg.precision != SS_PREC_FP32;
+        if (sv && sv->pres_restore) {
+            // the pressure this step's solve produced in an earlier run
+            if (f64) {
+                TRY(ensure_mixed(s, p->mg.precision, st));
+                CU(cudaMemcpyAsync(s->p64, sv->pres_restore, s->ncell * sizeof(double), cudaMemcpyDeviceToDevice, st),
+                   "pressure restore");
+                s->p64_valid = 1;
+                if (!defer_p0) TRY(launch_p0_from_p64(s, st));
+            } else {
+                CU(cudaMemcpyAsync(s->p[0], sv->pres_restore, s->ncell * sizeof(float), cudaMemcpyDeviceToDevice, st),
+                   "pressure restore");
+                s->p64_valid = 0;
+            }
+            s->st.vcycles = sv->vcycles_restore;
+            s->st.converged = 1;
+            sv->vcycles = sv->vcycles_restore;
+        } else {
+            TRY(pressure_solve(s, p, c, st, defer_p0));
+            if (sv) sv->vcycles = s->st.vcycles;
+            if (sv && sv->pres_save) {
+                if (f64) CU(cudaMemcpyAsync(sv->pres_save, s->p64, s->ncell * sizeof(double), cudaMemcpyDeviceToDevice, st),
+                            "pressure save");
+                else CU(cudaMemcpyAsync(sv->pres_save, s->p[0], s->ncell * sizeof(float), cudaMemcpyDeviceToDevice, st),
+                        "pressure save");
+            }
+        }
     }
     if (m & SS_STAGE_UPDATE_VELOCITIES) {
         if (p->mg.precision != SS_PREC_FP32 && s->p64_valid) {

@@ -992,6 +992,7 @@ int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st, const St
     if (write && sc && quirks >= 0 && rb_supported(s, quirks)) {
         ro.rhs_s = s->rhs_s;
         ro.rhs_r = s->rhs_r;
+        s->rhs_r_is_s = 0;   // both forms written, each with its own out-of-grid rule
         ro.rho_h = sc->rho_h; ro.dt = sc->dt; ro.rho = sc->rho; ro.dt_h = sc->dt_h;
         ro.s_solid = quirks ? 0 : s->enclosed;
         ro.r_solid = quirks ? 1 : s->enclosed;

@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
                 p_out[c] = p_in[c];
             }
             rhs_s[q] = s_out;
-            rhs_r[q] = r_out;
+            if (rhs_r) rhs_r[q] = r_out;
         }
         pm = p0;
         p0 = pp;
@@ -252,8 +252,12 @@ int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate
     const double k = (double)c.dt / ((double)c.rho * (double)s->h);
     const double inv_k = 1.0 / k;
     const double inv_khh = 1.0 / (k * (double)s->lv[0].hh);
+    // with h^2 == 1 the residual form rho/(k h^2) is the smoother form rho/k
+    // to the bit: only rhs_s is written, and the level-0 residual reads it
+    s->rhs_r_is_s = s->lv[0].hh == 1.0f ? 1 : 0;
+    float* rhs_r = s->rhs_r_is_s ? nullptr : s->rhs_r;
 #define IR_ARGS(ACC) s->p64, s->p_alt[0], s->p64b, s->div0, s->fmask, s->nx, s->ny, s->nz, k, inv_k, inv_khh, \
-                     s->rhs_s, s->rhs_r, s->red.partial, s->red.partial_max, s->red.ticket, s->red.out, slot, \
+                     s->rhs_s, rhs_r, s->red.partial, s->red.partial_max, s->red.ticket, s->red.out, slot, \
                      s->d_scale, planes
     if (s->dim == 3) {
         if (accumulate) k_ir_residual<3, true><<<g, b, 0, st>>>(IR_ARGS(true));

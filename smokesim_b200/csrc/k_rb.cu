@@ -199,7 +199,11 @@ struct RbPlane {
     float extra;
 };
 
-template <int DIM>
+// ZERO: every non-fluid cell of the other colour holds +0 (the mixed solve's
+// correction: it starts at 0 and its prolongation zeroes non-fluid cells), so
+// a neighbour needs no select - a +0 term in the same place of the sum is
+// the value the select gives.
+template <int DIM, bool ZERO = false>
 __global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, const float* __restrict__ po,
                                                     const float* __restrict__ rhs_c, const uint8_t* __restrict__ mask_c,
                                                     RBLevel g, int colour, int planes) {
@@ -243,12 +247,23 @@ __global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, cons
             wr[k] = (m & M_FLUID) && fs != 0;
             const float left = par ? f4(pm, k) : (k ? f4(pm, k - 1) : cur.extra);
             const float right = par ? (k < 3 ? f4(pm, k + 1) : cur.extra) : f4(pm, k);
-            float sum = ((m & M_TOP) ? f4(cur.pt, k) : 0.f) + ((m & M_BOTTOM) ? f4(cur.pb, k) : 0.f);
-            sum = sum + ((m & M_RIGHT) ? right : 0.f);
-            sum = sum + ((m & M_LEFT) ? left : 0.f);
-            if constexpr (DIM == 3) {
-                sum = sum + ((m & M_FRONT) ? f4(cur.pf, k) : 0.f);
-                sum = sum + ((m & M_BACK) ? f4(pk, k) : 0.f);
+            float sum;
+            if constexpr (ZERO) {
+                sum = f4(cur.pt, k) + f4(cur.pb, k);
+                sum = sum + right;
+                sum = sum + left;
+                if constexpr (DIM == 3) {
+                    sum = sum + f4(cur.pf, k);
+                    sum = sum + f4(pk, k);
+                }
+            } else {
+                sum = ((m & M_TOP) ? f4(cur.pt, k) : 0.f) + ((m & M_BOTTOM) ? f4(cur.pb, k) : 0.f);
+                sum = sum + ((m & M_RIGHT) ? right : 0.f);
+                sum = sum + ((m & M_LEFT) ? left : 0.f);
+                if constexpr (DIM == 3) {
+                    sum = sum + ((m & M_FRONT) ? f4(cur.pf, k) : 0.f);
+                    sum = sum + ((m & M_BACK) ? f4(pk, k) : 0.f);
+                }
             }
             out[k] = wr[k] ? div_by_count(sum - f4(cur.rhs, k), fs) : 0.f;
         }
@@ -268,7 +283,7 @@ __global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, cons
 // Residual of the fine cells under four consecutive coarse cells of a row,
 // restricted: per fine row the even-x cells sit in one colour array and the
 // odd-x cells in the other, both at the coarse x index.
-template <int DIM, bool POW2, typename T = float>
+template <int DIM, bool POW2, typename T = float, bool ZERO = false>
 __global__ void __launch_bounds__(256, 3) k_rb_residual_restrict4(const float* __restrict__ p_red, const float* __restrict__ p_black,
                                                                const float* __restrict__ rr_red, const float* __restrict__ rr_black,
                                                                const uint8_t* __restrict__ m_red, const uint8_t* __restrict__ m_black,
@@ -328,12 +343,23 @@ __global__ void __launch_bounds__(256, 3) k_rb_residual_restrict4(const float* _
                             if constexpr (DIM == 3) { front = f4(o_f, k); back = f4(o_k, k); }
                             own = f4(o_m, k); rr = f4(ro, k);
                         }
-                        float sum = ((m & M_TOP) ? top : 0.f) + ((m & M_BOTTOM) ? bot : 0.f);
-                        sum = sum + ((m & M_RIGHT) ? right : 0.f);
-                        sum = sum + ((m & M_LEFT) ? left : 0.f);
-                        if constexpr (DIM == 3) {
-                            sum = sum + ((m & M_FRONT) ? front : 0.f);
-                            sum = sum + ((m & M_BACK) ? back : 0.f);
+                        float sum;
+                        if constexpr (ZERO) {   // non-fluid neighbours hold +0
+                            sum = top + bot;
+                            sum = sum + right;
+                            sum = sum + left;
+                            if constexpr (DIM == 3) {
+                                sum = sum + front;
+                                sum = sum + back;
+                            }
+                        } else {
+                            sum = ((m & M_TOP) ? top : 0.f) + ((m & M_BOTTOM) ? bot : 0.f);
+                            sum = sum + ((m & M_RIGHT) ? right : 0.f);
+                            sum = sum + ((m & M_LEFT) ? left : 0.f);
+                            if constexpr (DIM == 3) {
+                                sum = sum + ((m & M_FRONT) ? front : 0.f);
+                                sum = sum + ((m & M_BACK) ? back : 0.f);
+                            }
                         }
                         const float f_sum = (float)__popc(m & 0x7Eu);
                         const float lap = sum - f_sum * own;
@@ -367,10 +393,14 @@ __global__ void __launch_bounds__(256, 3) k_rb_residual_restrict4(const float* _
 // computed with the same float expression as k_rb_prolong (whose lower
 // coarse index is x/2 - 1 + (x & 1), checked on the host when the tables are
 // made).
-template <int DIM, typename T = float>
+// ZERO: non-fluid cells get +0 instead (the mixed solve's correction there
+// is never read; the select-free operators above rely on it being +0)
+template <int DIM, typename T = float, bool ZERO = false>
 __global__ void __launch_bounds__(256) k_rb_prolong4(float* __restrict__ p_red, float* __restrict__ p_black, RBLevel g,
                                                      const T* __restrict__ pc, int cx, int cy, int cz,
-                                                     const float* __restrict__ pw, const float* __restrict__ scale) {
+                                                     const float* __restrict__ pw, const float* __restrict__ scale,
+                                                     const uint8_t* __restrict__ m_red = nullptr,
+                                                     const uint8_t* __restrict__ m_black = nullptr) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y * blockDim.y + threadIdx.y;
     const int Z = blockIdx.z;
@@ -430,9 +460,17 @@ __global__ void __launch_bounds__(256) k_rb_prolong4(float* __restrict__ p_red, 
             const int i = (z * g.ny + y) * g.half + X0;
             float4 a = *reinterpret_cast<const float4*>(E + i);
             a.x = a.x + se[0]; a.y = a.y + se[1]; a.z = a.z + se[2]; a.w = a.w + se[3];
-            *reinterpret_cast<float4*>(E + i) = a;
             float4 b = *reinterpret_cast<const float4*>(O + i);
             b.x = b.x + so[0]; b.y = b.y + so[1]; b.z = b.z + so[2]; b.w = b.w + so[3];
+            if constexpr (ZERO) {
+                const uint32_t me = __ldg(reinterpret_cast<const uint32_t*>((c0 ? m_black : m_red) + i));
+                const uint32_t mo = __ldg(reinterpret_cast<const uint32_t*>((c0 ? m_red : m_black) + i));
+                a.x = (me & 0x1u) ? a.x : 0.f; a.y = (me & 0x100u) ? a.y : 0.f;
+                a.z = (me & 0x10000u) ? a.z : 0.f; a.w = (me & 0x1000000u) ? a.w : 0.f;
+                b.x = (mo & 0x1u) ? b.x : 0.f; b.y = (mo & 0x100u) ? b.y : 0.f;
+                b.z = (mo & 0x10000u) ? b.z : 0.f; b.w = (mo & 0x1000000u) ? b.w : 0.f;
+            }
+            *reinterpret_cast<float4*>(E + i) = a;
             *reinterpret_cast<float4*>(O + i) = b;
         }
     }
@@ -479,7 +517,7 @@ int launch_rb_split_mask(ss_sim* s, cudaStream_t st) {
     return check_cuda(cudaGetLastError(), "k_rb_split_any");
 }
 
-int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st) {
+int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st, bool zero) {
     const RBLevel g = rb_level(s);
     const size_t h = s->ncell / 2;
     float* p[2] = {s->p_alt[0], s->p_alt[0] + h};
@@ -498,8 +536,13 @@ int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st) {
     for (int it = 0; it < iterations; ++it)
         for (int c = 0; c < 2; ++c) {
             if (s->rb_vec) {
-                if (s->dim == 3) k_rb_smooth4<3><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
-                else k_rb_smooth4<2><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
+                if (s->dim == 3) {
+                    if (zero) k_rb_smooth4<3, true><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
+                    else k_rb_smooth4<3><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
+                } else {
+                    if (zero) k_rb_smooth4<2, true><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
+                    else k_rb_smooth4<2><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
+                }
             } else {
                 if (s->dim == 3) k_rb_smooth<3><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
                 else k_rb_smooth<2><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
@@ -516,7 +559,7 @@ static bool pow2f(float v) {
 }
 
 template <typename T>
-static int rb_residual_restrict_t(ss_sim* s, T* rc, const float* scale, cudaStream_t st) {
+static int rb_residual_restrict_t(ss_sim* s, T* rc, const float* scale, cudaStream_t st, bool zero = false) {
     const RBLevel g = rb_level(s);
     const size_t h = s->ncell / 2;
     const int cx = s->lv[1].n[0], cy = s->lv[1].n[1], cz = s->lv[1].n[2];
@@ -526,12 +569,15 @@ static int rb_residual_restrict_t(ss_sim* s, T* rc, const float* scale, cudaStre
     dim3 b, gr;
     const float* pr = s->p_alt[0];
     const float* pb = pr + h;
-    const float* rr = s->rhs_r;
+    const float* rr = s->rhs_r_is_s ? s->rhs_s : s->rhs_r;
     const uint8_t* mr = s->rb_mask;
     const uint8_t* mb = s->rb_mask + h;
     if (s->rb_vec) {
         row_launch(cx / 4, cy, cz, b, gr);
-        if (s->dim == 3) {
+        if (s->dim == 3 && zero) {
+            if (p2) k_rb_residual_restrict4<3, true, T, true><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
+            else k_rb_residual_restrict4<3, false, T, true><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
+        } else if (s->dim == 3) {
             if (p2) k_rb_residual_restrict4<3, true, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
             else k_rb_residual_restrict4<3, false, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
         } else {
@@ -554,14 +600,17 @@ static int rb_residual_restrict_t(ss_sim* s, T* rc, const float* scale, cudaStre
 }
 
 template <typename T>
-static int rb_prolong_t(ss_sim* s, const T* pc, const float* scale, cudaStream_t st) {
+static int rb_prolong_t(ss_sim* s, const T* pc, const float* scale, cudaStream_t st, bool zero = false) {
     const RBLevel g = rb_level(s);
     const size_t h = s->ncell / 2;
     const int cx = s->lv[1].n[0], cy = s->lv[1].n[1], cz = s->lv[1].n[2];
     if (s->rb_prolong_vec) {
         dim3 b, gr;
         row_launch(cx / 4, cy, cz, b, gr);
-        if (s->dim == 3) k_rb_prolong4<3, T><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw, scale);
+        if (s->dim == 3 && zero)
+            k_rb_prolong4<3, T, true><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw, scale,
+                                                          s->rb_mask, s->rb_mask + h);
+        else if (s->dim == 3) k_rb_prolong4<3, T><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw, scale);
         else k_rb_prolong4<2, T><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw, scale);
         s->nlaunch += 1;
         return check_cuda(cudaGetLastError(), "k_rb_prolong4");
@@ -577,14 +626,21 @@ int launch_rb_residual_restrict(ss_sim* s, cudaStream_t st) { return rb_residual
 
 int launch_rb_prolong(ss_sim* s, cudaStream_t st) { return rb_prolong_t<float>(s, s->p[1], nullptr, st); }
 
+// The correction solve's level 0 may take the select-free operators when
+// its prolongation zeroes non-fluid cells (the four-cells-a-thread forms of
+// all three operators, 3D).
+bool rb_zero_form(const ss_sim* s) { return s->dim == 3 && s->rb_vec && s->rb_prolong_vec; }
+
 int launch_rb_residual_restrict_mixed(ss_sim* s, int prec, cudaStream_t st) {
-    if (prec == SS_PREC_MIXED) return rb_residual_restrict_t<__half>(s, (__half*)s->cr[1], s->d_scale, st);
-    return rb_residual_restrict_t<__nv_bfloat16>(s, (__nv_bfloat16*)s->cr[1], s->d_scale, st);
+    const bool z = rb_zero_form(s);
+    if (prec == SS_PREC_MIXED) return rb_residual_restrict_t<__half>(s, (__half*)s->cr[1], s->d_scale, st, z);
+    return rb_residual_restrict_t<__nv_bfloat16>(s, (__nv_bfloat16*)s->cr[1], s->d_scale, st, z);
 }
 
 int launch_rb_prolong_mixed(ss_sim* s, int prec, cudaStream_t st) {
-    if (prec == SS_PREC_MIXED) return rb_prolong_t<__half>(s, (const __half*)s->cp[1], s->d_scale, st);
-    return rb_prolong_t<__nv_bfloat16>(s, (const __nv_bfloat16*)s->cp[1], s->d_scale, st);
+    const bool z = rb_zero_form(s);
+    if (prec == SS_PREC_MIXED) return rb_prolong_t<__half>(s, (const __half*)s->cp[1], s->d_scale, st, z);
+    return rb_prolong_t<__nv_bfloat16>(s, (const __nv_bfloat16*)s->cp[1], s->d_scale, st, z);
 }
 
 // Per-axis weight of the fine cell's coarse interpolation, the float

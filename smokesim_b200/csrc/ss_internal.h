@@ -81,6 +81,7 @@ struct ss_sim {
     float* vort = nullptr;              // 3*ncell (2D: ncell) vorticity scratch
     float* rhs_s = nullptr;             // level-0 rho*h*div/dt of the current solve, colour-split (k_rb.cu)
     float* rhs_r = nullptr;             // level-0 rho*div/(dt*h) of the current solve, colour-split
+    int rhs_r_is_s = 0;                 // the mixed solve's residual right-hand side equals rhs_s (h^2 == 1): rhs_r unused
     uint8_t* rb_mask = nullptr;         // colour-split copy of fmask
     float* rb_pw = nullptr;             // level-0 prolongation weights per axis (x, then y, then z)
     // mixed-precision solve: FP64 level-0 pressure, FP16/BF16 coarse levels
@@ -180,7 +181,9 @@ int launch_rbgs_sweep_tma(ss_sim* s, const StepConsts& c, int L, int quirks, boo
 bool rb_supported(const ss_sim* s, int quirks);
 int launch_rb_convert(ss_sim* s, bool split, cudaStream_t st);
 int launch_rb_split_mask(ss_sim* s, cudaStream_t st);
-int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st);
+// zero: the select-free half-sweep (every non-fluid cell of the other colour holds +0)
+int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st, bool zero = false);
+bool rb_zero_form(const ss_sim* s);
 int launch_rb_residual_restrict(ss_sim* s, cudaStream_t st);
 int launch_rb_prolong(ss_sim* s, cudaStream_t st);
 int rb_init_vector_paths(ss_sim* s, cudaStream_t st);
@@ -191,6 +194,7 @@ int coarse_residual_restrict(ss_sim* s, const StepConsts& c, int L, int prec, cu
 int coarse_prolong(ss_sim* s, int L, int prec, cudaStream_t st);
 int coarse_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, int prec, cudaStream_t st);
 int launch_rb_residual_restrict_mixed(ss_sim* s, int prec, cudaStream_t st);
+
 int launch_rb_prolong_mixed(ss_sim* s, int prec, cudaStream_t st);
 int launch_p64_from_p0(ss_sim* s, cudaStream_t st);
 int launch_p0_from_p64(ss_sim* s, cudaStream_t st);
@@ -212,6 +216,12 @@ struct StepSaves {
     float* force_vel[3];     // velocity after advection (+ buoyancy), before vorticity confinement
     float* proj_vel[3];      // velocity after the projection update
     int vcycles;             // out: V-cycles (or refinement steps) the solve ran
+    // the projection's result: pres_save receives the solved pressure (FP64
+    // with the mixed-precision solve, else FP32); with pres_restore set the
+    // step skips the solve and takes that pressure and vcycles_restore instead
+    void* pres_save;
+    const void* pres_restore;
+    int vcycles_restore;
 };
 int run_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* saves);
 // z planes a thread (or a block) of a z-marching kernel takes: at most

@@ -150,29 +150,41 @@ def test_rollout_checkpointing_consistent():
     assert res[1][2]["checkpoint_bytes"] < res[0][2]["checkpoint_bytes"]
 
 
+# Coordinates whose derivative is at least this fraction of the largest one
+# are held to the relative bound one by one; smaller ones (where the FP32
+# gradient's absolute rounding dominates) to the same absolute error as a
+# coordinate at the floor.
+FD_FLOOR = 1e-2
+FD_REL = 1e-3
+
+
 @pytest.mark.parametrize("prec", [abi.PREC_FP32, abi.PREC_MIXED])
 def test_rollout_gradient_vs_fp64_fd(prec):
-    """8-step rollout at 32^3: dL/d(initial velocity) and dL/d(force) on 32
-    random control coordinates against FP64 central differences with
-    h = 1e-3.  Semi-Lagrangian advection is piecewise smooth: where h = 1e-3
-    straddles a kink (the 1e-3 and 1e-4 differences disagree), the h = 1e-4
+    """The differentiable-rollout configuration at 32^3: 64 steps, checkpoint
+    every 8, 4 V-cycles (refinement steps) a step, L2 loss between the final
+    density and a target run whose emitter is shifted 6 cells in x.
+    dL/d(initial velocity) and dL/d(per-step force) on 32 random control
+    coordinates against FP64 central differences with h = 1e-3, coordinate by
+    coordinate: relative error <= 1e-3 wherever |dL/dx| >= 1e-2 max |dL/dx|,
+    absolute error <= 1e-5 max |dL/dx| below that floor.  Semi-Lagrangian
+    advection is piecewise smooth: where h = 1e-3 straddles a kink (the 1e-3
+    and 1e-4 differences disagree by more than the bound) the h = 1e-4
     difference is the reference for that coordinate.  The GPU forward runs the
-    FP32 or the mixed-precision projection (4 V-cycles / refinement steps a
-    step); the FP64 differences use the FP32 scheme, which is the same map in
-    exact arithmetic."""
+    FP32 or the mixed-precision projection; the FP64 differences use the FP32
+    scheme, the same map in exact arithmetic."""
     from oracle.oracle import OracleSim
     from smokesim_b200 import Sim
     from smokesim_b200.adjoint import Rollout
     import torch
-    n, nsteps = 32, 8
+    n, nsteps, every = 32, 64, 8
     sc = scene.rollout64(seed=5, n=n)
     p = scene.workload_params(ref_quirks=0, n_vcycles=4)
     rng = np.random.default_rng(7)
     forces = (rng.standard_normal((nsteps, 3)) * 0.2).astype(np.float32)
     target = scene.rollout64(seed=6, n=n)
-    # target density: a rollout with the emitter shifted by 3 cells in x
+    # target density: a rollout with the emitter shifted by 6 cells (x 32/64) in x
     tsim = OracleSim(target["desc"], "f64")
-    target["emitters"][0].pos[0] += 3.0
+    target["emitters"][0].pos[0] += 6.0 * n / 64
     scene.apply(tsim, target)
     for _ in range(nsteps):
         tsim.step(p)
@@ -200,16 +212,14 @@ def test_rollout_gradient_vs_fp64_fd(prec):
     g = Sim(sc["desc"])
     scene.apply(g, sc)
     pg = scene.workload_params(ref_quirks=0, n_vcycles=4, precision=prec)
-    ro = Rollout(g, nsteps, 3)
+    ro = Rollout(g, nsteps, every)
     ro.forward(pg, forces)
     rho = torch.from_numpy(g.get_field(abi.FIELD_DENSITY).ravel()).cuda().double()
     gd = (2 * (rho - torch.from_numpy(rho_t).cuda())).float().contiguous()
     torch.cuda.synchronize()
     gf = ro.backward(pg, grad_density=gd.data_ptr())
     gvel = {k: ro.grad(k) for k in VEL}
-    # 32 coordinates: 24 velocity faces near the plume, 8 force components
-    h = 1e-3
-    errs = []
+    # 32 coordinates: 24 initial face velocities, 8 force components
     nv = {k: abi.field_count(3, (n, n, n), k) for k in VEL}
     picks = []
     for _ in range(24):
@@ -217,25 +227,35 @@ def test_rollout_gradient_vs_fp64_fd(prec):
         picks.append(("v", k, int(rng.integers(0, nv[k]))))
     for _ in range(8):
         picks.append(("f", int(rng.integers(0, nsteps)), int(rng.integers(0, 3))))
+
     def central(kind, a, b, hh):
         if kind == "v":
             return (loss_fp64({a: b}, None, hh) - loss_fp64({a: b}, None, -hh)) / (2 * hh)
         return (loss_fp64({}, (a, b), hh) - loss_fp64({}, (a, b), -hh)) / (2 * hh)
 
     adj = np.array([gvel[a][b] if kind == "v" else gf[a, b] for kind, a, b in picks], np.float64)
-    fd = np.array([central(kind, a, b, h) for kind, a, b in picks])
+    fd = np.array([central(kind, a, b, 1e-3) for kind, a, b in picks])
     scale = np.abs(fd).max()
     assert scale > 0
+
+    def bad(x, ref):
+        return abs(x - ref) > (FD_REL * abs(ref) if abs(ref) >= FD_FLOOR * scale else FD_REL * FD_FLOOR * scale)
+
     kinks = 0
     for i, (kind, a, b) in enumerate(picks):
-        if abs(adj[i] - fd[i]) > 1e-3 * scale:
+        if bad(adj[i], fd[i]):
             fd4 = central(kind, a, b, 1e-4)
-            if abs(fd4 - fd[i]) > 1e-3 * scale:   # h = 1e-3 crosses a kink
+            if bad(fd[i], fd4):   # h = 1e-3 crosses a kink
                 fd[i] = fd4
                 kinks += 1
-    err = np.abs(adj - fd) / scale
-    assert err.max() <= 1e-3, (err.max(), list(zip(adj, fd)))
-    assert kinks <= 4, kinks
+    above = np.abs(fd) >= FD_FLOOR * scale
+    rel = np.abs(adj - fd) / np.maximum(np.abs(fd), 1e-300)
+    absn = np.abs(adj - fd) / scale
+    report = [(kind, float(x), float(y)) for (kind, _, _), x, y in zip(picks, adj, fd)]
+    assert above.sum() >= 16, (int(above.sum()), report)
+    assert rel[above].max() <= FD_REL, (float(rel[above].max()), report)
+    assert (~above).sum() == 0 or absn[~above].max() <= FD_REL * FD_FLOOR, (float(absn[~above].max()), report)
+    assert kinks <= 6, (kinks, report)
     ro.close()
     g.close()
 
@@ -334,6 +354,93 @@ def test_force_field_gradient_vs_fp64_fd():
     g.close()
 
 
+def test_inverse_control_gradient_vs_fp64_fd():
+    """The inverse-control configuration at its full size, first iteration:
+    plume scene at 128^3, controls = per-step emitter forces + a 16^3 coarse
+    force field (all zero, as Adam starts), mixed-precision projection in the
+    forward, checkpoints every 14 steps, loss = L2 to the density of a run
+    whose two emitters sit 10 cells further apart in x.  The gradient on four
+    control coordinates (two force components, two field coefficients by the
+    emitters) against FP64 central differences of the oracle, coordinate by
+    coordinate to 1e-3 relative.  The FP64 differences over 200 steps at 128^3
+    take hours on the host, so the horizon here is 28 steps (two checkpoint
+    segments, the recomputation included) at a fixed 6 refinement steps a
+    step (the tolerance solve's typical count), the FP64 run using the FP32
+    scheme's 6 V-cycles - the same map in exact arithmetic."""
+    from oracle.oracle import OracleSim
+    from smokesim_b200 import Sim
+    from smokesim_b200.adjoint import Rollout
+    import torch
+    n, nsteps, every, nf, ncyc = 128, 28, 14, 16, 6
+    sc = scene.plume3d(seed=0, n=n)
+    sc.pop("rng", None)
+    tgt = scene.plume3d(seed=0, n=n)
+    tgt.pop("rng", None)
+    tgt["emitters"][0].pos[0] -= 5.0
+    tgt["emitters"][1].pos[0] += 5.0
+    p64 = scene.workload_params(ref_quirks=0, n_vcycles=ncyc)
+    pg = scene.workload_params(ref_quirks=0, n_vcycles=ncyc, precision=abi.PREC_MIXED)
+    to = OracleSim(tgt["desc"], "f64")
+    scene.apply(to, tgt)
+    for _ in range(nsteps):
+        to.step(p64)
+    rho_t = to.get_field(abi.FIELD_DENSITY, f64=True).ravel()
+    to.close()
+    forces = np.zeros((nsteps, 3), np.float32)
+    field = np.zeros((3, nf, nf, nf), np.float32)
+
+    def loss_fp64(dforce, dfield, h):
+        o = OracleSim(sc["desc"], "f64")
+        scene.apply(o, sc)
+        f = field.astype(np.float64).copy()
+        if dfield is not None:
+            f[dfield] += h
+        o.set_force_field(f)
+        for s_ in range(nsteps):
+            fo = forces[s_].astype(np.float64).copy()
+            if dforce is not None and dforce[0] == s_:
+                fo[dforce[1]] += h
+            o.set_emitter_force(fo)
+            o.step(p64)
+        r = o.get_field(abi.FIELD_DENSITY, f64=True).ravel()
+        o.close()
+        return float(np.sum((r - rho_t) ** 2))
+
+    g = Sim(sc["desc"])
+    scene.apply(g, sc)
+    g.set_force_field(field)
+    ro = Rollout(g, nsteps, every)
+    ro.forward(pg, forces)
+    rho = torch.from_numpy(g.get_field(abi.FIELD_DENSITY).ravel()).cuda().double()
+    gd = (2 * (rho - torch.from_numpy(rho_t).cuda())).float().contiguous()
+    torch.cuda.synchronize()
+    gf = ro.backward(pg, grad_density=gd.data_ptr())
+    gfield = ro.force_field_grad(nf)
+    # the coarse cells holding the two emitters (cell-centred samples of n/nf cells)
+    ex = [int(e.pos[0] * nf / n) for e in sc["emitters"]]
+    ez = [int(e.pos[2] * nf / n) for e in sc["emitters"]]
+    ey = int(sc["emitters"][0].pos[1] * nf / n)
+    picks = [("f", 5, 1), ("f", 17, 0), ("ff", (1, ez[0], ey + 1, ex[0])), ("ff", (0, ez[1], ey + 1, ex[1]))]
+
+    def central(pk, hh):
+        if pk[0] == "f":
+            return (loss_fp64((pk[1], pk[2]), None, hh) - loss_fp64((pk[1], pk[2]), None, -hh)) / (2 * hh)
+        return (loss_fp64(None, pk[1], hh) - loss_fp64(None, pk[1], -hh)) / (2 * hh)
+
+    adj = np.array([gf[pk[1], pk[2]] if pk[0] == "f" else gfield[pk[1]] for pk in picks], np.float64)
+    fd = np.array([central(pk, 1e-3) for pk in picks])
+    for i, pk in enumerate(picks):
+        if abs(adj[i] - fd[i]) > FD_REL * abs(fd[i]):
+            fd4 = central(pk, 1e-4)
+            if abs(fd4 - fd[i]) > FD_REL * abs(fd4):   # h = 1e-3 crosses an advection kink
+                fd[i] = fd4
+    rel = np.abs(adj - fd) / np.abs(fd)
+    assert np.all(np.abs(fd) > 0)
+    assert rel.max() <= FD_REL, (rel.tolist(), list(zip(adj.tolist(), fd.tolist())))
+    ro.close()
+    g.close()
+
+
 # ------------------------------------------------ owner-computes scatter-adds
 def _stage_grads(dim, n, nch, enc, mask, deterministic, seed=3, state_scale=1.0):
     """Adjoint of one step of the given stages for a random output seed: the
@@ -427,6 +534,43 @@ def test_rollout_deterministic_bitwise():
         assert d1[k].tobytes() == d2[k].tobytes(), k
         scale = max(float(np.abs(at[k]).max()), 1e-30)
         assert np.allclose(d1[k], at[k], rtol=1e-3, atol=1e-5 * scale), (k, float(np.abs(d1[k] - at[k]).max()), scale)
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP32, abi.PREC_MIXED])
+def test_pressure_store_same_gradients(prec):
+    """ss_adjoint_set_pressure_store: the reverse pass recomputes each
+    segment with the pressures the forward pass stored instead of solving
+    again.  With owner-computes scatters the gradients are bitwise those of
+    the plain recomputation (32^3, 9 steps, checkpoint every 3, FP32 or mixed
+    projection - whose checkpoints keep the FP64 warm-start pressure)."""
+    from smokesim_b200 import Sim
+    from smokesim_b200.adjoint import Rollout
+    import torch
+    n, nsteps = 32, 9
+    sc = scene.rollout64(seed=6, n=n)
+    p = scene.workload_params(ref_quirks=0, n_vcycles=4, precision=prec)
+    forces = (np.random.default_rng(7).standard_normal((nsteps, 3)) * 0.2).astype(np.float32)
+
+    def run(store):
+        g = Sim(sc["desc"])
+        scene.apply(g, sc)
+        ro = Rollout(g, nsteps, 3, deterministic=True, store_pressure=store)
+        ro.forward(p, forces)
+        rho = torch.from_numpy(g.get_field(abi.FIELD_DENSITY).ravel()).cuda()
+        gd = (2 * (rho - 0.05)).contiguous()
+        torch.cuda.synchronize()
+        gf = ro.backward(p, grad_density=gd.data_ptr())
+        out = {k: ro.grad(k).copy() for k in VEL + [abi.FIELD_DENSITY, abi.FIELD_TEMPERATURE]}
+        out["force"] = np.asarray(gf, np.float32).copy()
+        info = ro.info()
+        ro.close()
+        g.close()
+        return out, info
+
+    (a, ia), (b, ib) = run(False), run(True)
+    for k in a:
+        assert a[k].tobytes() == b[k].tobytes(), k
+    assert ib["kernel_launches"] < ia["kernel_launches"]
 
 
 def test_coarse_response_matches_sweeps(monkeypatch):

@@ -39,6 +39,48 @@ def test_mixed_solve_bitwise(name, dim, n, nch, enc, mc, prec):
     assert abs(sg.residual - so.residual) <= 1e-9 * max(1e-30, so.residual)
 
 
+# Grids where the correction solve's level 0 takes the select-free
+# four-cells-a-thread operators (even sizes with a whole number of quads per
+# colour row): several z slabs of blocks, open and enclosed, three density
+# channels, 256-cell rows, h^2 != 1 (the residual's own right-hand side).
+ZERO_FORM_GRIDS = [
+    ("3d_cube", 3, (32, 32, 32), 1, 1, 4, 1.0),
+    ("3d_open_rgb", 3, (64, 40, 34), 3, 0, 4, 1.0),
+    ("3d_tall_rows", 3, (32, 120, 12), 1, 1, 4, 1.0),
+    ("3d_wide", 3, (256, 52, 10), 1, 1, 4, 1.0),
+    ("3d_wide_open", 3, (128, 30, 22), 1, 0, 4, 1.0),
+    ("3d_h_half", 3, (64, 32, 24), 1, 1, 4, 0.5),
+    ("3d_h_03", 3, (64, 32, 24), 1, 1, 4, 0.3),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,dim,n,nch,enc,mc,h", ZERO_FORM_GRIDS)
+@pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_MIXED_BF16])
+def test_mixed_select_free_level0_bitwise(name, dim, n, nch, enc, mc, h, prec):
+    from oracle.oracle import OracleSim
+    from smokesim_b200 import Sim
+    desc = abi.make_desc(dim, n, cell_size=h, density_channels=nch, enclosed=enc, min_coarse=mc)
+    g, o = Sim(desc), OracleSim(desc)
+    rng = scene.Rng(47)
+    from test_gpu_parity import _scene_for
+    em, ob, bx = _scene_for(dim, n, rng)
+    for s_ in (g, o):
+        s_.set_scene(em, ob, bx)
+    for k, a in scene.random_state(rng, dim, n, nch).items():
+        if k == abi.FIELD_DENSITY:
+            a = a[: int(np.prod(g.shape(k)))]
+        g.set_field(k, a)
+        o.set_field(k, a)
+    p = scene.workload_params(ref_quirks=0, precision=prec, n_vcycles=3, n_coarse=12)
+    for k in range(2):
+        g.step(p)
+        o.step(p)
+        assert_same(g, o, dim, f"select-free level 0 step {k}")
+    sg, so = g.stats(), o.stats()
+    assert sg.vcycles == so.vcycles == 3
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_MIXED_BF16])
 def test_mixed_tolerance_matches_oracle(prec):

@@ -115,6 +115,39 @@ def test_single_stage_bitwise(name, dim, n, nch, enc, stage, mask):
         assert_same(g, o, dim, f"{stage} step {k}")
 
 
+# 3D advection reads its taps from shared-memory tiles with a two-cell rim;
+# velocities of up to ~40 cells a second (displacements of several cells at
+# dt = 0.1) send many back-traces outside the tile, onto the array path.
+LONG_TRACE_GRIDS = [g for g in GRIDS if g[1] == 3]
+
+
+@pytest.mark.parametrize("name,dim,n,nch,enc", LONG_TRACE_GRIDS)
+@pytest.mark.parametrize("stage,mask", [("advect_velocities+buoyancy", abi.STAGE_ADVECT_VELOCITIES | abi.STAGE_APPLY_BUOYANCY),
+                                        ("advect_velocities", abi.STAGE_ADVECT_VELOCITIES),
+                                        ("advect_smoke", abi.STAGE_ADVECT_SMOKE),
+                                        ("apply_vorticity", abi.STAGE_APPLY_VORTICITY)])
+@pytest.mark.parametrize("vel_scale", [4.0, 15.0])
+def test_long_backtrace_bitwise(name, dim, n, nch, enc, stage, mask, vel_scale):
+    from oracle.oracle import OracleSim
+    from smokesim_b200 import Sim
+    desc = abi.make_desc(dim, n, cell_size=1.0, density_channels=nch, enclosed=enc, min_coarse=3, t_ambient=0.3)
+    g, o = Sim(desc), OracleSim(desc)
+    rng = scene.Rng(101)
+    em, ob, bx = _scene_for(dim, n, rng)
+    for s in (g, o):
+        s.set_scene(em, ob, bx)
+    for k, a in scene.random_state(rng, dim, n, nch, vel_scale=vel_scale).items():
+        if k == abi.FIELD_DENSITY:
+            a = a[: int(np.prod(g.shape(k)))]
+        g.set_field(k, a)
+        o.set_field(k, a)
+    p = scene.workload_params(stage_mask=mask, t_ambient=0.3, wind=(0.7, 0.0, 0.0) if not enc else (0, 0, 0))
+    for k in range(2):
+        g.step(p)
+        o.step(p)
+        assert_same(g, o, dim, f"{stage} x{vel_scale} step {k}")
+
+
 @pytest.mark.parametrize("name,dim,n,nch,enc", GRIDS)
 @pytest.mark.parametrize("quirks", [1, 0])
 def test_multigrid_levels_bitwise(name, dim, n, nch, enc, quirks):
