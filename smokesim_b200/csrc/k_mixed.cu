@@ -115,16 +115,25 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
         const int sl = z & 1;
         sP[sl][ty + 1][tx + 1] = p0;
         if (tid < kIrRim) sP[sl][hy][hx] = h0;
-        // the next planes' values, in flight across the barrier and this plane's work
+        // the next planes' values, in flight across the barrier and this
+        // plane's work: kept as loaded (pressure and correction apart) and
+        // combined only when they rotate in, so no instruction here waits
         double pn = 0.0, hn = 0.0;
+        float en = 0.f, hen = 0.f;
         uint8_t mn = 0;
         float dvn = 0.f;
         if (in && z + 1 < ze) {
-            if (z + 2 < nz) pn = P(x, y, z + 2);
+            if (z + 2 < nz) {
+                pn = p_in[idx3(x, y, z + 2, nx, ny)];
+                if (ACC) en = e[rb_pos(x, y, z + 2, nx, ny, nz)];
+            }
             mn = fmask[idx3(x, y, z + 1, nx, ny)];
             dvn = div0[idx3(x, y, z + 1, nx, ny)];
         }
-        if (hin && z + 1 < ze) hn = P(gx, gy, z + 1);
+        if (hin && z + 1 < ze) {
+            hn = p_in[idx3(gx, gy, z + 1, nx, ny)];
+            if (ACC) hen = e[rb_pos(gx, gy, z + 1, nx, ny, nz)];
+        }
         const int c = idx3(x, y, z, nx, ny);
         __syncthreads();
         if (in) {
@@ -162,8 +171,8 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
         }
         pm = p0;
         p0 = pp;
-        pp = pn;
-        h0 = hn;
+        pp = ACC ? pn + (double)en : pn;   // P(x, y, z + 2): the same value P() forms
+        h0 = ACC ? hn + (double)hen : hn;
         m = mn;
         dv = dvn;
     }
