@@ -205,6 +205,10 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     // default 1 feeds them with TMA.  The results are the same.
     if (const char* e = getenv("SMOKESIM_TMA")) s->use_tma = atoi(e) ? 1 : 0;
     if (const char* e = getenv("SMOKESIM_COARSE_SWEEPS")) s->coarse_matrix = atoi(e) ? 0 : 1;
+    // SMOKESIM_PDL=0 launches the solve's kernels without programmatic
+    // dependent launch (each waits for the previous one to finish before it
+    // is scheduled); the results are the same.
+    if (const char* e = getenv("SMOKESIM_PDL")) s->pdl = atoi(e) ? 1 : 0;
     s->nv[0] = (size_t)(s->nx + 1) * s->ny * s->nz;
     s->nv[1] = (size_t)s->nx * (s->ny + 1) * s->nz;
     s->nv[2] = s->dim == 3 ? (size_t)s->nx * s->ny * (s->nz + 1) : 0;
@@ -805,10 +809,8 @@ static int v_cycle_mixed(ss_sim* s, const StepConsts& c, const ss_mg_schedule& m
         // e starts at 0 and the prolongation zeroes non-fluid cells: the
         // half-sweeps may take the select-free form where that prolongation runs
         const bool z = rb_zero_form(s);
-        TRY(launch_rb_sweep(s, mg.n_pre, st, z));
-        TRY(launch_rb_residual_restrict_mixed(s, prec, st));
-        const size_t nc = (size_t)s->lv[1].n[0] * s->lv[1].n[1] * s->lv[1].n[2];
-        CU(cudaMemsetAsync(s->cp[1], 0, nc * 2, st), "clear coarse p");
+        TRY(launch_rb_sweep(s, mg.n_pre, st, z, true));   // e starts at 0
+        TRY(launch_rb_residual_restrict_mixed(s, prec, st));   // also clears level 1's p
         TRY(v_cycle_mixed(s, c, mg, 1, prec, st));
         TRY(launch_rb_prolong_mixed(s, prec, st));
         return launch_rb_sweep(s, mg.n_post, st, z);
@@ -816,9 +818,7 @@ static int v_cycle_mixed(ss_sim* s, const StepConsts& c, const ss_mg_schedule& m
     if (L >= s->bottom) return coarse_bottom(s, mg, L, prec, st);
     if (L == s->levels - 1) return coarse_smooth(s, c, L, mg.n_coarse, prec, st);
     TRY(coarse_smooth(s, c, L, mg.n_pre, prec, st));
-    TRY(coarse_residual_restrict(s, c, L, prec, st));
-    const size_t nc = (size_t)s->lv[L + 1].n[0] * s->lv[L + 1].n[1] * s->lv[L + 1].n[2];
-    CU(cudaMemsetAsync(s->cp[L + 1], 0, nc * 2, st), "clear coarse p");
+    TRY(coarse_residual_restrict(s, c, L, prec, st));   // also clears level L+1's p
     TRY(v_cycle_mixed(s, c, mg, L + 1, prec, st));
     TRY(coarse_prolong(s, L, prec, st));
     return coarse_smooth(s, c, L, mg.n_post, prec, st);
@@ -852,7 +852,6 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
             // residual in one pass, recorded as one graph per buffer parity
             const int slot = stats ? SLOT_RESIDUAL : -1;
             TRY(run_graph(s, 2 + s->p64_parity, graph_key(s, 2, s->p64_parity, slot, 1, p), st, [&]() -> int {
-                CU(cudaMemsetAsync(s->p_alt[0], 0, s->ncell * sizeof(float), st), "clear correction");
                 TRY(v_cycle_mixed(s, c, mg, 0, mg.precision, st));
                 return launch_ir_residual(s, c, slot, true, st);
             }));
@@ -873,7 +872,6 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
         pending = true;   // the V-cycle runs at the top of the next pass
         ++done;
         if (!tol_mode && done == cap && !stats) {
-            CU(cudaMemsetAsync(s->p_alt[0], 0, s->ncell * sizeof(float), st), "clear correction");
             TRY(v_cycle_mixed(s, c, mg, 0, mg.precision, st));
             TRY(launch_ir_accumulate(s, st));
             pending = false;

@@ -35,6 +35,15 @@ struct Grid {
 
 SS_HD int idx3(int x, int y, int z, int ax, int ay) { return (z * ay + y) * ax + x; }
 
+// Entry of a kernel that may be launched as a programmatic dependent (launch_k):
+// wait until the grid before it on the stream has completed and its memory
+// is visible, then allow the grid after it to be scheduled (it waits the same
+// way).  No effect in a plain launch.
+SS_D void pdl_entry() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 SS_D float lerp_(float a, float b, float t) { return a * (1.f - t) + b * t; }
 
 SS_D float clampt(float t, float lo, float hi) { return fminf(fmaxf(t, lo), hi); }

@@ -150,6 +150,7 @@ SS_D void smooth_cell(const MGArgsT<T>& a, int x, int y, int z) {
 
 template <int DIM, bool L0, typename T = float>
 __global__ void __launch_bounds__(256) k_smooth(MGArgsT<T> a, int parity) {
+    pdl_entry();
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((y + z + parity) & 1);
@@ -168,11 +169,11 @@ int launch_smooth(ss_sim* s, const StepConsts& c, int L, int iterations, int qui
     for (int it = 0; it < 2 * iterations; ++it) {
         const int parity = it & 1;
         if (s->dim == 3) {
-            if (L == 0) k_smooth<3, true><<<g, b, 0, st>>>(a, parity);
-            else k_smooth<3, false><<<g, b, 0, st>>>(a, parity);
+            if (L == 0) launch_k(s->pdl, g, b, 0, st, k_smooth<3, true>, a, parity);
+            else launch_k(s->pdl, g, b, 0, st, k_smooth<3, false>, a, parity);
         } else {
-            if (L == 0) k_smooth<2, true><<<g, b, 0, st>>>(a, parity);
-            else k_smooth<2, false><<<g, b, 0, st>>>(a, parity);
+            if (L == 0) launch_k(s->pdl, g, b, 0, st, k_smooth<2, true>, a, parity);
+            else launch_k(s->pdl, g, b, 0, st, k_smooth<2, false>, a, parity);
         }
     }
     s->nlaunch += 2 * iterations;
@@ -237,7 +238,8 @@ SS_D float residual_cell(const MGArgsT<T>& a, int x, int y, int z) {
 // (restrict_residual.comp:40-64, 2D :40-59) into the next level when
 // WRITE_COARSE.  The grid also covers the fine cells left over by odd sizes.
 template <int DIM, bool L0, bool WRITE_FINE, bool WRITE_COARSE, typename T = float, bool CG = false>
-SS_D void residual_restrict_cell(const MGArgsT<T>& a, T* __restrict__ rc, int cx, int cy, int cz, int X, int Y, int Z) {
+SS_D void residual_restrict_cell(const MGArgsT<T>& a, T* __restrict__ rc, int cx, int cy, int cz, int X, int Y, int Z,
+                                 T* __restrict__ pz = nullptr) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int x0 = 2 * X, y0 = 2 * Y, z0 = DIM == 3 ? 2 * Z : 0;
     if (x0 >= nx || y0 >= ny || z0 >= nz) return;
@@ -270,23 +272,27 @@ SS_D void residual_restrict_cell(const MGArgsT<T>& a, T* __restrict__ rc, int cx
                 out = (v[0][0][0] + v[0][0][1] + v[0][1][0] + v[0][1][1]) / 4.f;
             }
             rc[idx3(X, Y, Z, cx, cy)] = st<T>(out);
+            if (pz) pz[idx3(X, Y, Z, cx, cy)] = st<T>(0.f);   // the coarse initial guess
         }
     }
 }
 
+// pz: also set the next level's pressure (its initial guess) to +0
 template <int DIM, bool L0, bool WRITE_FINE, bool WRITE_COARSE, typename T = float>
-__global__ void __launch_bounds__(256) k_residual_restrict(MGArgsT<T> a, T* __restrict__ rc, int cx, int cy, int cz) {
+__global__ void __launch_bounds__(256) k_residual_restrict(MGArgsT<T> a, T* __restrict__ rc, int cx, int cy, int cz,
+                                                           T* __restrict__ pz) {
+    pdl_entry();
     residual_restrict_cell<DIM, L0, WRITE_FINE, WRITE_COARSE, T>(a, rc, cx, cy, cz, blockIdx.x * blockDim.x + threadIdx.x,
                                                                  blockIdx.y * blockDim.y + threadIdx.y,
-                                                                 blockIdx.z * blockDim.z + threadIdx.z);
+                                                                 blockIdx.z * blockDim.z + threadIdx.z, pz);
 }
 
 template <int DIM, bool L0>
-static void launch_rr(const MGArgs& a, float* rc, int cx, int cy, int cz, bool wf, bool wc, dim3 g, dim3 b,
+static void launch_rr(bool pdl, const MGArgs& a, float* rc, int cx, int cy, int cz, bool wf, bool wc, dim3 g, dim3 b,
                       cudaStream_t st) {
-    if (wf && wc) k_residual_restrict<DIM, L0, true, true><<<g, b, 0, st>>>(a, rc, cx, cy, cz);
-    else if (wf) k_residual_restrict<DIM, L0, true, false><<<g, b, 0, st>>>(a, rc, cx, cy, cz);
-    else k_residual_restrict<DIM, L0, false, true><<<g, b, 0, st>>>(a, rc, cx, cy, cz);
+    if (wf && wc) launch_k(pdl, g, b, 0, st, k_residual_restrict<DIM, L0, true, true>, a, rc, cx, cy, cz, nullptr);
+    else if (wf) launch_k(pdl, g, b, 0, st, k_residual_restrict<DIM, L0, true, false>, a, rc, cx, cy, cz, nullptr);
+    else launch_k(pdl, g, b, 0, st, k_residual_restrict<DIM, L0, false, true>, a, rc, cx, cy, cz, nullptr);
 }
 
 int launch_residual(ss_sim* s, const StepConsts& c, int L, bool write_fine, bool write_coarse, int quirks,
@@ -301,11 +307,11 @@ int launch_residual(ss_sim* s, const StepConsts& c, int L, bool write_fine, bool
     dim3 b(32, 8, 1);
     dim3 g = grid_for((a.nx + 1) / 2, (a.ny + 1) / 2, s->dim == 3 ? (a.nz + 1) / 2 : 1, b);
     if (s->dim == 3) {
-        if (L == 0) launch_rr<3, true>(a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
-        else launch_rr<3, false>(a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
+        if (L == 0) launch_rr<3, true>(s->pdl != 0, a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
+        else launch_rr<3, false>(s->pdl != 0, a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
     } else {
-        if (L == 0) launch_rr<2, true>(a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
-        else launch_rr<2, false>(a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
+        if (L == 0) launch_rr<2, true>(s->pdl != 0, a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
+        else launch_rr<2, false>(s->pdl != 0, a, rc, cx, cy, cz, write_fine, write_coarse, g, b, st);
     }
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_residual_restrict");
@@ -382,6 +388,7 @@ SS_D void prolong_cell(T* __restrict__ p, int ax, int ay, int az, const T* __res
 template <int DIM, typename T = float>
 __global__ void __launch_bounds__(256) k_prolong(T* __restrict__ p, int ax, int ay, int az,
                                                  const T* __restrict__ pc, int cx, int cy, int cz) {
+    pdl_entry();
     prolong_cell<DIM, T>(p, ax, ay, az, pc, cx, cy, cz, blockIdx.x * blockDim.x + threadIdx.x,
                          blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z * blockDim.z + threadIdx.z);
 }
@@ -392,8 +399,8 @@ int launch_prolong(ss_sim* s, int L, cudaStream_t st) {
     const int* cc = s->lv[next].n;
     dim3 b(32, 8, 1);
     dim3 g = grid_for(f[0], f[1], f[2], b);
-    if (s->dim == 3) k_prolong<3><<<g, b, 0, st>>>(s->p[L], f[0], f[1], f[2], s->p[next], cc[0], cc[1], cc[2]);
-    else k_prolong<2><<<g, b, 0, st>>>(s->p[L], f[0], f[1], f[2], s->p[next], cc[0], cc[1], cc[2]);
+    if (s->dim == 3) launch_k(s->pdl, g, b, 0, st, k_prolong<3>, s->p[L], f[0], f[1], f[2], s->p[next], cc[0], cc[1], cc[2]);
+    else launch_k(s->pdl, g, b, 0, st, k_prolong<2>, s->p[L], f[0], f[1], f[2], s->p[next], cc[0], cc[1], cc[2]);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_prolong");
 }
@@ -714,6 +721,7 @@ SS_D int coarse_parts(int n) {
 
 template <int DIM, typename T, typename R>
 __global__ void __launch_bounds__(1024) k_bottom(BottomArgsT<T> b) {
+    pdl_entry();
     extern __shared__ float sm[];
     float* sp = sm;
     float* sr = sm + b.total;
@@ -876,8 +884,8 @@ static int launch_bottom_t(ss_sim* s, const ss_mg_schedule& mg, int L, T* const*
         ? cudaFuncSetAttribute(k_bottom<3, T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBytes)
         : cudaFuncSetAttribute(k_bottom<2, T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBytes);
     if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute(k_bottom)");
-    if (s->dim == 3) k_bottom<3, T, R><<<1, 1024, smem, st>>>(b);
-    else k_bottom<2, T, R><<<1, 1024, smem, st>>>(b);
+    if (s->dim == 3) launch_k(s->pdl, 1, 1024, smem, st, k_bottom<3, T, R>, b);
+    else launch_k(s->pdl, 1, 1024, smem, st, k_bottom<2, T, R>, b);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_bottom");
 }
@@ -994,21 +1002,21 @@ static int coarse_smooth_t(ss_sim* s, const StepConsts& c, int L, int iterations
     dim3 b(32, 8, 1);
     dim3 g = grid_for((a.nx + 1) / 2, a.ny, a.nz, b);
     for (int it = 0; it < 2 * iterations; ++it) {
-        if (s->dim == 3) k_smooth<3, false, T><<<g, b, 0, st>>>(a, it & 1);
-        else k_smooth<2, false, T><<<g, b, 0, st>>>(a, it & 1);
+        if (s->dim == 3) launch_k(s->pdl, g, b, 0, st, k_smooth<3, false, T>, a, it & 1);
+        else launch_k(s->pdl, g, b, 0, st, k_smooth<2, false, T>, a, it & 1);
     }
     s->nlaunch += 2 * iterations;
     return check_cuda(cudaGetLastError(), "k_smooth (coarse storage)");
 }
 
 template <typename T>
-static int coarse_residual_restrict_t(ss_sim* s, const StepConsts& c, int L, T* p, T* r, T* rc, cudaStream_t st) {
+static int coarse_residual_restrict_t(ss_sim* s, const StepConsts& c, int L, T* p, T* r, T* rc, T* pz, cudaStream_t st) {
     MGArgsT<T> a = mg_args_t<T>(s, c, L, resid_oob(s, 0), p, r);
     const int cx = s->lv[L + 1].n[0], cy = s->lv[L + 1].n[1], cz = s->lv[L + 1].n[2];
     dim3 b(32, 8, 1);
     dim3 g = grid_for((a.nx + 1) / 2, (a.ny + 1) / 2, s->dim == 3 ? (a.nz + 1) / 2 : 1, b);
-    if (s->dim == 3) k_residual_restrict<3, false, false, true, T><<<g, b, 0, st>>>(a, rc, cx, cy, cz);
-    else k_residual_restrict<2, false, false, true, T><<<g, b, 0, st>>>(a, rc, cx, cy, cz);
+    if (s->dim == 3) launch_k(s->pdl, g, b, 0, st, k_residual_restrict<3, false, false, true, T>, a, rc, cx, cy, cz, pz);
+    else launch_k(s->pdl, g, b, 0, st, k_residual_restrict<2, false, false, true, T>, a, rc, cx, cy, cz, pz);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_residual_restrict (coarse storage)");
 }
@@ -1019,8 +1027,8 @@ static int coarse_prolong_t(ss_sim* s, int L, T* p, const T* pc, cudaStream_t st
     const int* cc = s->lv[L + 1].n;
     dim3 b(32, 8, 1);
     dim3 g = grid_for(f[0], f[1], f[2], b);
-    if (s->dim == 3) k_prolong<3, T><<<g, b, 0, st>>>(p, f[0], f[1], f[2], pc, cc[0], cc[1], cc[2]);
-    else k_prolong<2, T><<<g, b, 0, st>>>(p, f[0], f[1], f[2], pc, cc[0], cc[1], cc[2]);
+    if (s->dim == 3) launch_k(s->pdl, g, b, 0, st, k_prolong<3, T>, p, f[0], f[1], f[2], pc, cc[0], cc[1], cc[2]);
+    else launch_k(s->pdl, g, b, 0, st, k_prolong<2, T>, p, f[0], f[1], f[2], pc, cc[0], cc[1], cc[2]);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_prolong (coarse storage)");
 }
@@ -1032,9 +1040,10 @@ int coarse_smooth(ss_sim* s, const StepConsts& c, int L, int iterations, int pre
 
 int coarse_residual_restrict(ss_sim* s, const StepConsts& c, int L, int prec, cudaStream_t st) {
     if (prec == SS_PREC_MIXED)
-        return coarse_residual_restrict_t<__half>(s, c, L, (__half*)s->cp[L], (__half*)s->cr[L], (__half*)s->cr[L + 1], st);
+        return coarse_residual_restrict_t<__half>(s, c, L, (__half*)s->cp[L], (__half*)s->cr[L], (__half*)s->cr[L + 1],
+                                                  (__half*)s->cp[L + 1], st);
     return coarse_residual_restrict_t<__nv_bfloat16>(s, c, L, (__nv_bfloat16*)s->cp[L], (__nv_bfloat16*)s->cr[L],
-                                                      (__nv_bfloat16*)s->cr[L + 1], st);
+                                                      (__nv_bfloat16*)s->cr[L + 1], (__nv_bfloat16*)s->cp[L + 1], st);
 }
 
 int coarse_prolong(ss_sim* s, int L, int prec, cudaStream_t st) {

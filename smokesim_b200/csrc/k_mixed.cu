@@ -82,6 +82,7 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
     double inv_k, double inv_khh, float* __restrict__ rhs_s, float* __restrict__ rhs_r, double* __restrict__ psum,
     double* __restrict__ pmax, unsigned int* __restrict__ ticket, double* __restrict__ out, int slot,
     float* __restrict__ scale, int planes) {
+    pdl_entry();
     __shared__ double sP[2][kIrTY + 2][kIrTX + 2];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kIrTX * ty;
     const int x0 = blockIdx.x * kIrTX, y0 = blockIdx.y * kIrTY;
@@ -269,11 +270,11 @@ int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate
                      s->rhs_s, rhs_r, s->red.partial, s->red.partial_max, s->red.ticket, s->red.out, slot, \
                      s->d_scale, planes
     if (s->dim == 3) {
-        if (accumulate) k_ir_residual<3, true><<<g, b, 0, st>>>(IR_ARGS(true));
-        else k_ir_residual<3, false><<<g, b, 0, st>>>(IR_ARGS(false));
+        if (accumulate) launch_k(s->pdl, g, b, 0, st, k_ir_residual<3, true>, IR_ARGS(true));
+        else launch_k(s->pdl, g, b, 0, st, k_ir_residual<3, false>, IR_ARGS(false));
     } else {
-        if (accumulate) k_ir_residual<2, true><<<g, b, 0, st>>>(IR_ARGS(true));
-        else k_ir_residual<2, false><<<g, b, 0, st>>>(IR_ARGS(false));
+        if (accumulate) launch_k(s->pdl, g, b, 0, st, k_ir_residual<2, true>, IR_ARGS(true));
+        else launch_k(s->pdl, g, b, 0, st, k_ir_residual<2, false>, IR_ARGS(false));
     }
 #undef IR_ARGS
     s->nlaunch += 1;

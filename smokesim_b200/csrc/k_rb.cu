@@ -81,6 +81,7 @@ template <int DIM>
 __global__ void __launch_bounds__(256) k_rb_smooth(float* __restrict__ pc, const float* __restrict__ po,
                                                    const float* __restrict__ rhs_c, const uint8_t* __restrict__ mask_c,
                                                    RBLevel g, int colour) {
+    pdl_entry();
     const int xh = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z;
@@ -105,6 +106,7 @@ __global__ void __launch_bounds__(256) k_rb_residual_restrict(const float* __res
                                                               const uint8_t* __restrict__ m_red, const uint8_t* __restrict__ m_black,
                                                               RBLevel g, T* __restrict__ rc, int cx, int cy, int cz,
                                                               float hh, float inv_hh, const float* __restrict__ scale) {
+    pdl_entry();
     const int X = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y * blockDim.y + threadIdx.y;
     const int Z = blockIdx.z;
@@ -146,6 +148,7 @@ template <int DIM, typename T = float>
 __global__ void __launch_bounds__(256) k_rb_prolong(float* __restrict__ p_red, float* __restrict__ p_black, RBLevel g,
                                                     const T* __restrict__ pc, int cx, int cy, int cz,
                                                     const float* __restrict__ scale) {
+    pdl_entry();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
@@ -203,10 +206,16 @@ struct RbPlane {
 // correction: it starts at 0 and its prolongation zeroes non-fluid cells), so
 // a neighbour needs no select - a +0 term in the same place of the sum is
 // the value the select gives.
-template <int DIM, bool ZERO = false>
+// INIT: the first half-sweep from a zero pressure.  Every neighbour is +0, so
+// the neighbour sum is +0 and the other colour is not read; the kernel writes
+// all of its own colour (+0 where the cell is not updated) and +0 over the
+// other colour (zo) - the values a clear of both arrays followed by the plain
+// half-sweep leaves.
+template <int DIM, bool ZERO = false, bool INIT = false>
 __global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, const float* __restrict__ po,
                                                     const float* __restrict__ rhs_c, const uint8_t* __restrict__ mask_c,
-                                                    RBLevel g, int colour, int planes) {
+                                                    RBLevel g, int colour, int planes, float* __restrict__ zo) {
+    pdl_entry();
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (q >= (g.half >> 2) || y >= g.ny) return;
@@ -221,17 +230,23 @@ __global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, cons
         const int i = (z * g.ny + y) * g.half + xh0;
         const int par = (y + z + colour) & 1;   // x = 2*xh + par
         P.m4 = __ldg(reinterpret_cast<const uint32_t*>(mask_c + i));
+        P.rhs = ldg4(rhs_c + i);
+        if constexpr (INIT) return;
         P.pt = up ? ldg4(po + i + g.half) : zero;
         P.pb = dn ? ldg4(po + i - g.half) : zero;
         P.pf = (DIM == 3 && z + 1 < g.nz) ? ldg4(po + i + pl) : zero;
         // row-end neighbour: left of the first cell (par 0) or right of the last (par 1)
         P.extra = par == 0 ? (xh0 > 0 ? __ldg(po + i - 1) : 0.f) : (xh0 + 4 < g.half ? __ldg(po + i + 4) : 0.f);
-        P.rhs = ldg4(rhs_c + i);
     };
     const int i0 = (zb * g.ny + y) * g.half + xh0;
-    float4 pm = ldg4(po + i0);
-    float4 pk = (DIM == 3 && zb > 0) ? ldg4(po + i0 - pl) : zero;
+    float4 pm = zero, pk = zero;
     RbPlane cur, nxt;
+    cur.pt = cur.pb = cur.pf = zero;
+    cur.extra = 0.f;
+    if constexpr (!INIT) {
+        pm = ldg4(po + i0);
+        pk = (DIM == 3 && zb > 0) ? ldg4(po + i0 - pl) : zero;
+    }
     load(zb, cur);
     nxt = cur;
     for (int z = zb; z < ze; ++z) {
@@ -248,7 +263,9 @@ __global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, cons
             const float left = par ? f4(pm, k) : (k ? f4(pm, k - 1) : cur.extra);
             const float right = par ? (k < 3 ? f4(pm, k + 1) : cur.extra) : f4(pm, k);
             float sum;
-            if constexpr (ZERO) {
+            if constexpr (INIT) {
+                sum = 0.f;
+            } else if constexpr (ZERO) {
                 sum = f4(cur.pt, k) + f4(cur.pb, k);
                 sum = sum + right;
                 sum = sum + left;
@@ -267,7 +284,10 @@ __global__ void __launch_bounds__(256) k_rb_smooth4(float* __restrict__ pc, cons
             }
             out[k] = wr[k] ? div_by_count(sum - f4(cur.rhs, k), fs) : 0.f;
         }
-        if (wr[0] && wr[1] && wr[2] && wr[3]) {
+        if (INIT) {
+            *reinterpret_cast<float4*>(pc + i) = make_float4(out[0], out[1], out[2], out[3]);
+            *reinterpret_cast<float4*>(zo + i) = zero;
+        } else if (wr[0] && wr[1] && wr[2] && wr[3]) {
             *reinterpret_cast<float4*>(pc + i) = make_float4(out[0], out[1], out[2], out[3]);
         } else {
 #pragma unroll
@@ -288,7 +308,9 @@ __global__ void __launch_bounds__(256, 3) k_rb_residual_restrict4(const float* _
                                                                const float* __restrict__ rr_red, const float* __restrict__ rr_black,
                                                                const uint8_t* __restrict__ m_red, const uint8_t* __restrict__ m_black,
                                                                RBLevel g, T* __restrict__ rc, int cx, int cy,
-                                                               float hh, float inv_hh, const float* __restrict__ scale) {
+                                                               float hh, float inv_hh, const float* __restrict__ scale,
+                                                               T* __restrict__ pz) {
+    pdl_entry();
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y * blockDim.y + threadIdx.y;
     const int Z = blockIdx.z;
@@ -386,6 +408,12 @@ __global__ void __launch_bounds__(256, 3) k_rb_residual_restrict4(const float* _
 #pragma unroll
         for (int k = 0; k < 4; ++k) dst[k] = st<T>(out[k] * scale[0]);
     }
+    // the coarse level's initial guess (+0), in place of a separate clear
+    if (pz) {
+        T* zp = pz + (Z * cy + Y) * cx + X0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) zp[k] = st<T>(0.f);
+    }
 }
 
 // prolong_pressure.comp:39-51 for the fine cells under four consecutive
@@ -401,6 +429,7 @@ __global__ void __launch_bounds__(256) k_rb_prolong4(float* __restrict__ p_red, 
                                                      const float* __restrict__ pw, const float* __restrict__ scale,
                                                      const uint8_t* __restrict__ m_red = nullptr,
                                                      const uint8_t* __restrict__ m_black = nullptr) {
+    pdl_entry();
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y * blockDim.y + threadIdx.y;
     const int Z = blockIdx.z;
@@ -517,7 +546,7 @@ int launch_rb_split_mask(ss_sim* s, cudaStream_t st) {
     return check_cuda(cudaGetLastError(), "k_rb_split_any");
 }
 
-int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st, bool zero) {
+int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st, bool zero, bool from_zero) {
     const RBLevel g = rb_level(s);
     const size_t h = s->ncell / 2;
     float* p[2] = {s->p_alt[0], s->p_alt[0] + h};
@@ -533,19 +562,33 @@ int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st, bool zero) {
         planes = (int)std::max(1LL, std::min(16LL, per_plane * g.nz / (148LL * 4 * 3)));
     }
     dim3 gr4(gr.x, gr.y, (g.nz + planes - 1) / planes);
+    // from a zero pressure: the first red half-sweep of the four-cell kernel
+    // clears the black array itself; otherwise both arrays are cleared first
+    const bool init = from_zero && s->rb_vec && iterations > 0;
+    if (from_zero && !init) {
+        const cudaError_t e = cudaMemsetAsync(s->p_alt[0], 0, s->ncell * sizeof(float), st);
+        if (e != cudaSuccess) return check_cuda(e, "clear level-0 pressure");
+    }
     for (int it = 0; it < iterations; ++it)
         for (int c = 0; c < 2; ++c) {
-            if (s->rb_vec) {
+            if (init && it == 0 && c == 0) {
                 if (s->dim == 3) {
-                    if (zero) k_rb_smooth4<3, true><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
-                    else k_rb_smooth4<3><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
+                    if (zero) launch_k(s->pdl, gr4, b, 0, st, k_rb_smooth4<3, true, true>, p[c], p[1 - c], rhs[c], mask[c], g, c, planes, p[1 - c]);
+                    else launch_k(s->pdl, gr4, b, 0, st, k_rb_smooth4<3, false, true>, p[c], p[1 - c], rhs[c], mask[c], g, c, planes, p[1 - c]);
                 } else {
-                    if (zero) k_rb_smooth4<2, true><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
-                    else k_rb_smooth4<2><<<gr4, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c, planes);
+                    launch_k(s->pdl, gr4, b, 0, st, k_rb_smooth4<2, false, true>, p[c], p[1 - c], rhs[c], mask[c], g, c, planes, p[1 - c]);
+                }
+            } else if (s->rb_vec) {
+                if (s->dim == 3) {
+                    if (zero) launch_k(s->pdl, gr4, b, 0, st, k_rb_smooth4<3, true>, p[c], p[1 - c], rhs[c], mask[c], g, c, planes, nullptr);
+                    else launch_k(s->pdl, gr4, b, 0, st, k_rb_smooth4<3>, p[c], p[1 - c], rhs[c], mask[c], g, c, planes, nullptr);
+                } else {
+                    if (zero) launch_k(s->pdl, gr4, b, 0, st, k_rb_smooth4<2, true>, p[c], p[1 - c], rhs[c], mask[c], g, c, planes, nullptr);
+                    else launch_k(s->pdl, gr4, b, 0, st, k_rb_smooth4<2>, p[c], p[1 - c], rhs[c], mask[c], g, c, planes, nullptr);
                 }
             } else {
-                if (s->dim == 3) k_rb_smooth<3><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
-                else k_rb_smooth<2><<<gr, b, 0, st>>>(p[c], p[1 - c], rhs[c], mask[c], g, c);
+                if (s->dim == 3) launch_k(s->pdl, gr, b, 0, st, k_rb_smooth<3>, p[c], p[1 - c], rhs[c], mask[c], g, c);
+                else launch_k(s->pdl, gr, b, 0, st, k_rb_smooth<2>, p[c], p[1 - c], rhs[c], mask[c], g, c);
             }
         }
     s->nlaunch += 2 * iterations;
@@ -558,8 +601,10 @@ static bool pow2f(float v) {
     return frexpf(v, &e) == 0.5f && v >= 1.1754944e-38f && v <= 1e30f;
 }
 
+// pz: also set the next level's pressure (its initial guess) to +0
 template <typename T>
-static int rb_residual_restrict_t(ss_sim* s, T* rc, const float* scale, cudaStream_t st, bool zero = false) {
+static int rb_residual_restrict_t(ss_sim* s, T* rc, const float* scale, cudaStream_t st, bool zero = false,
+                                  T* pz = nullptr) {
     const RBLevel g = rb_level(s);
     const size_t h = s->ncell / 2;
     const int cx = s->lv[1].n[0], cy = s->lv[1].n[1], cz = s->lv[1].n[2];
@@ -575,25 +620,29 @@ static int rb_residual_restrict_t(ss_sim* s, T* rc, const float* scale, cudaStre
     if (s->rb_vec) {
         row_launch(cx / 4, cy, cz, b, gr);
         if (s->dim == 3 && zero) {
-            if (p2) k_rb_residual_restrict4<3, true, T, true><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
-            else k_rb_residual_restrict4<3, false, T, true><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
+            if (p2) launch_k(s->pdl, gr, b, 0, st, k_rb_residual_restrict4<3, true, T, true>, pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale, pz);
+            else launch_k(s->pdl, gr, b, 0, st, k_rb_residual_restrict4<3, false, T, true>, pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale, pz);
         } else if (s->dim == 3) {
-            if (p2) k_rb_residual_restrict4<3, true, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
-            else k_rb_residual_restrict4<3, false, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
+            if (p2) launch_k(s->pdl, gr, b, 0, st, k_rb_residual_restrict4<3, true, T>, pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale, pz);
+            else launch_k(s->pdl, gr, b, 0, st, k_rb_residual_restrict4<3, false, T>, pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale, pz);
         } else {
-            if (p2) k_rb_residual_restrict4<2, true, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
-            else k_rb_residual_restrict4<2, false, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale);
+            if (p2) launch_k(s->pdl, gr, b, 0, st, k_rb_residual_restrict4<2, true, T>, pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale, pz);
+            else launch_k(s->pdl, gr, b, 0, st, k_rb_residual_restrict4<2, false, T>, pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, hh, ih, scale, pz);
         }
         s->nlaunch += 1;
         return check_cuda(cudaGetLastError(), "k_rb_residual_restrict4");
     }
+    if (pz) {
+        const cudaError_t e = cudaMemsetAsync(pz, 0, (size_t)cx * cy * cz * sizeof(T), st);
+        if (e != cudaSuccess) return check_cuda(e, "clear coarse p");
+    }
     row_launch(cx, cy, cz, b, gr);
     if (s->dim == 3) {
-        if (p2) k_rb_residual_restrict<3, true, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
-        else k_rb_residual_restrict<3, false, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
+        if (p2) launch_k(s->pdl, gr, b, 0, st, k_rb_residual_restrict<3, true, T>, pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
+        else launch_k(s->pdl, gr, b, 0, st, k_rb_residual_restrict<3, false, T>, pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
     } else {
-        if (p2) k_rb_residual_restrict<2, true, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
-        else k_rb_residual_restrict<2, false, T><<<gr, b, 0, st>>>(pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
+        if (p2) launch_k(s->pdl, gr, b, 0, st, k_rb_residual_restrict<2, true, T>, pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
+        else launch_k(s->pdl, gr, b, 0, st, k_rb_residual_restrict<2, false, T>, pr, pb, rr, rr + h, mr, mb, g, rc, cx, cy, cz, hh, ih, scale);
     }
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_rb_residual_restrict");
@@ -608,16 +657,20 @@ static int rb_prolong_t(ss_sim* s, const T* pc, const float* scale, cudaStream_t
         dim3 b, gr;
         row_launch(cx / 4, cy, cz, b, gr);
         if (s->dim == 3 && zero)
-            k_rb_prolong4<3, T, true><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw, scale,
-                                                          s->rb_mask, s->rb_mask + h);
-        else if (s->dim == 3) k_rb_prolong4<3, T><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw, scale);
-        else k_rb_prolong4<2, T><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw, scale);
+            launch_k(s->pdl, gr, b, 0, st, k_rb_prolong4<3, T, true>, s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw,
+                     scale, s->rb_mask, s->rb_mask + h);
+        else if (s->dim == 3)
+            launch_k(s->pdl, gr, b, 0, st, k_rb_prolong4<3, T>, s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw,
+                     scale, nullptr, nullptr);
+        else
+            launch_k(s->pdl, gr, b, 0, st, k_rb_prolong4<2, T>, s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, s->rb_pw,
+                     scale, nullptr, nullptr);
         s->nlaunch += 1;
         return check_cuda(cudaGetLastError(), "k_rb_prolong4");
     }
     dim3 b(128), gr((g.nx + 127) / 128, g.ny, g.nz);
-    if (s->dim == 3) k_rb_prolong<3, T><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, scale);
-    else k_rb_prolong<2, T><<<gr, b, 0, st>>>(s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, scale);
+    if (s->dim == 3) launch_k(s->pdl, gr, b, 0, st, k_rb_prolong<3, T>, s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, scale);
+    else launch_k(s->pdl, gr, b, 0, st, k_rb_prolong<2, T>, s->p_alt[0], s->p_alt[0] + h, g, pc, cx, cy, cz, scale);
     s->nlaunch += 1;
     return check_cuda(cudaGetLastError(), "k_rb_prolong");
 }
@@ -633,8 +686,10 @@ bool rb_zero_form(const ss_sim* s) { return s->dim == 3 && s->rb_vec && s->rb_pr
 
 int launch_rb_residual_restrict_mixed(ss_sim* s, int prec, cudaStream_t st) {
     const bool z = rb_zero_form(s);
-    if (prec == SS_PREC_MIXED) return rb_residual_restrict_t<__half>(s, (__half*)s->cr[1], s->d_scale, st, z);
-    return rb_residual_restrict_t<__nv_bfloat16>(s, (__nv_bfloat16*)s->cr[1], s->d_scale, st, z);
+    if (prec == SS_PREC_MIXED)
+        return rb_residual_restrict_t<__half>(s, (__half*)s->cr[1], s->d_scale, st, z, (__half*)s->cp[1]);
+    return rb_residual_restrict_t<__nv_bfloat16>(s, (__nv_bfloat16*)s->cr[1], s->d_scale, st, z,
+                                                 (__nv_bfloat16*)s->cp[1]);
 }
 
 int launch_rb_prolong_mixed(ss_sim* s, int prec, cudaStream_t st) {

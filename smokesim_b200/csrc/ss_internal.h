@@ -5,11 +5,34 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/smokesim.h"
 
 namespace ss {
+
+// Launch a kernel, with programmatic dependent launch allowed when `pdl` is
+// set: the kernel may then be scheduled while the kernel before it on the
+// stream (or in the captured graph) drains.  Every kernel launched this way
+// calls pdl_entry() (common.cuh) before it touches global memory; that waits
+// until the preceding kernel has completed and its writes are visible, so the
+// results are those of a plain launch.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(bool pdl, dim3 grid, dim3 block, size_t smem, cudaStream_t st, void (*kernel)(KArgs...),
+                            Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 struct Level {
     int n[3];
@@ -132,6 +155,8 @@ struct ss_sim {
     };
     SolveGraph graphs[4];
     int use_graphs = 1;
+    // programmatic dependent launch of the solve's kernel chain (SMOKESIM_PDL=0 sets 0)
+    int pdl = 1;
     int rb_active = 0;         // level-0 pressure currently lives colour-split in p_alt[0]
     std::vector<ss::TensorMapEntry> tmaps;
     cudaStream_t stream0 = nullptr;
@@ -182,7 +207,9 @@ bool rb_supported(const ss_sim* s, int quirks);
 int launch_rb_convert(ss_sim* s, bool split, cudaStream_t st);
 int launch_rb_split_mask(ss_sim* s, cudaStream_t st);
 // zero: the select-free half-sweep (every non-fluid cell of the other colour holds +0)
-int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st, bool zero = false);
+// from_zero: the sweeps start from a zero level-0 pressure (cleared here or
+// by the first half-sweep)
+int launch_rb_sweep(ss_sim* s, int iterations, cudaStream_t st, bool zero = false, bool from_zero = false);
 bool rb_zero_form(const ss_sim* s);
 int launch_rb_residual_restrict(ss_sim* s, cudaStream_t st);
 int launch_rb_prolong(ss_sim* s, cudaStream_t st);
