@@ -112,29 +112,39 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
     uint8_t m = in ? fmask[idx3(x, y, zb, nx, ny)] : 0;
     float dv = in ? div0[idx3(x, y, zb, nx, ny)] : 0.f;
     double acc = 0.0, amax = 0.0;
+    // The values the next two planes rotate in are in flight across each
+    // plane's barrier and work: queue A holds what plane z+1 needs (its mask,
+    // divergence and rim, and the pressure of plane z+2), queue B the same one
+    // plane further, issued at the top of plane z.  They stay as loaded
+    // (pressure and correction apart) and are combined only when they rotate
+    // in, so no instruction waits on them early.
+    struct Ahead {
+        double p = 0.0, h = 0.0;
+        float e = 0.f, he = 0.f, dv = 0.f;
+        uint8_t m = 0;
+    };
+    auto fetch = [&](int zn, Ahead& A) {   // zn: the plane whose mask and rim the entry holds
+        if (in && zn < ze) {
+            if (zn + 1 < nz) {
+                A.p = p_in[idx3(x, y, zn + 1, nx, ny)];
+                if (ACC) A.e = e[rb_pos(x, y, zn + 1, nx, ny, nz)];
+            }
+            A.m = fmask[idx3(x, y, zn, nx, ny)];
+            A.dv = div0[idx3(x, y, zn, nx, ny)];
+        }
+        if (hin && zn < ze) {
+            A.h = p_in[idx3(gx, gy, zn, nx, ny)];
+            if (ACC) A.he = e[rb_pos(gx, gy, zn, nx, ny, nz)];
+        }
+    };
+    Ahead qa;
+    fetch(zb + 1, qa);
     for (int z = zb; z < ze; ++z) {
         const int sl = z & 1;
         sP[sl][ty + 1][tx + 1] = p0;
         if (tid < kIrRim) sP[sl][hy][hx] = h0;
-        // the next planes' values, in flight across the barrier and this
-        // plane's work: kept as loaded (pressure and correction apart) and
-        // combined only when they rotate in, so no instruction here waits
-        double pn = 0.0, hn = 0.0;
-        float en = 0.f, hen = 0.f;
-        uint8_t mn = 0;
-        float dvn = 0.f;
-        if (in && z + 1 < ze) {
-            if (z + 2 < nz) {
-                pn = p_in[idx3(x, y, z + 2, nx, ny)];
-                if (ACC) en = e[rb_pos(x, y, z + 2, nx, ny, nz)];
-            }
-            mn = fmask[idx3(x, y, z + 1, nx, ny)];
-            dvn = div0[idx3(x, y, z + 1, nx, ny)];
-        }
-        if (hin && z + 1 < ze) {
-            hn = p_in[idx3(gx, gy, z + 1, nx, ny)];
-            if (ACC) hen = e[rb_pos(gx, gy, z + 1, nx, ny, nz)];
-        }
+        Ahead qb;
+        fetch(z + 2, qb);
         const int c = idx3(x, y, z, nx, ny);
         __syncthreads();
         if (in) {
@@ -172,10 +182,11 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
         }
         pm = p0;
         p0 = pp;
-        pp = ACC ? pn + (double)en : pn;   // P(x, y, z + 2): the same value P() forms
-        h0 = ACC ? hn + (double)hen : hn;
-        m = mn;
-        dv = dvn;
+        pp = ACC ? qa.p + (double)qa.e : qa.p;   // P(x, y, z + 2): the same value P() forms
+        h0 = ACC ? qa.h + (double)qa.he : qa.h;
+        m = qa.m;
+        dv = qa.dv;
+        qa = qb;
     }
     block_sum_max(acc, amax, psum + blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
                   pmax + blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
