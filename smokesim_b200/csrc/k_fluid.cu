@@ -708,32 +708,62 @@ __global__ void __launch_bounds__(256) k_update_velocity(FluidArgs a, const P* _
         p_back = __ldg(p + idx3(x, y, zb - 1, nx, ny));
         s_back = a.flags[idx3(x, y, zb - 1, nx, ny)] & F_SOLID;
     }
-    for (int z = zb; z < zend; ++z) {
+    // a plane's loads, issued one plane ahead so they are in flight across
+    // the plane before: the cell's pressure and solid flag, and per x / y face
+    // the face velocity and the lower cell's pressure and flag (z faces take
+    // the lower cell from the previous plane); every address is in range
+    struct Plane {
+        P pc, plo[2];
+        float src[3];
+        bool sc, slo[2];
+    };
+    auto fetch = [&](int z, Plane& L) {
         const bool in = inxy && z < nz;
-        const P pc = in ? __ldg(p + idx3(x, y, z, nx, ny)) : P(0);
-        const bool sc = in && (a.flags[idx3(x, y, z, nx, ny)] & F_SOLID);
+        L.pc = in ? __ldg(p + idx3(x, y, z, nx, ny)) : P(0);
+        L.sc = in && (a.flags[idx3(x, y, z, nx, ny)] & F_SOLID);
+#pragma unroll
+        for (int comp = 0; comp < DIM; ++comp) {
+            const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
+            L.src[comp] = 0.f;
+            if (comp < 2) { L.plo[comp] = P(0); L.slo[comp] = false; }
+            if (x >= ax || y >= ay || z >= az) continue;
+            const float* __restrict__ src = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
+            L.src[comp] = __ldg(src + idx3(x, y, z, ax, ay));
+            if (comp < 2) {
+                const int xm = x - (comp == 0), ym = y - (comp == 1);
+                L.slo[comp] = solid_oob0(a.flags, xm, ym, z, nx, ny, nz);
+                L.plo[comp] = (xm < 0 || ym < 0) ? P(0) : __ldg(p + idx3(xm, ym, z, nx, ny));
+            }
+        }
+    };
+    Plane cur;
+    fetch(zb, cur);
+    for (int z = zb; z < zend; ++z) {
+        Plane nxt = cur;
+        if (z + 1 < zend) fetch(z + 1, nxt);
+        const bool in = inxy && z < nz;
+        const P pc = cur.pc;
+        const bool sc = cur.sc;
         if (p0_out && in) p0_out[idx3(x, y, z, nx, ny)] = (float)pc;
 #pragma unroll
         for (int comp = 0; comp < DIM; ++comp) {
             const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
             if (x >= ax || y >= ay || z >= az) continue;
-            const int xm = x - (comp == 0), ym = y - (comp == 1), zm = z - (comp == 2);
-            const float* __restrict__ src = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
             float* __restrict__ dst = comp == 0 ? a.uo : comp == 1 ? a.vo : a.wo;
             const int i = idx3(x, y, z, ax, ay);
-            const bool s_lo = comp == 2 ? s_back : solid_oob0(a.flags, xm, ym, zm, nx, ny, nz);
+            const bool s_lo = comp == 2 ? s_back : cur.slo[comp < 2 ? comp : 0];
             if (sc || s_lo) {
                 const float* sv = comp == 0 ? a.sv0 : comp == 1 ? a.sv1 : a.sv2;
                 dst[i] = (in && sv) ? sv[idx3(x, y, z, nx, ny)] : 0.f;
                 continue;
             }
-            const P plo = comp == 2 ? p_back
-                                    : ((xm < 0 || ym < 0) ? P(0) : __ldg(p + idx3(xm, ym, zm, nx, ny)));
-            if constexpr (std::is_same<P, double>::value) dst[i] = (float)((double)__ldg(src + i) + k64 * (pc - plo));
-            else dst[i] = __ldg(src + i) + a.c.k_upd * (pc - plo);
+            const P plo = comp == 2 ? p_back : cur.plo[comp < 2 ? comp : 0];
+            if constexpr (std::is_same<P, double>::value) dst[i] = (float)((double)cur.src[comp] + k64 * (pc - plo));
+            else dst[i] = cur.src[comp] + a.c.k_upd * (pc - plo);
         }
         p_back = pc;
         s_back = sc;
+        cur = nxt;
     }
 }
 
@@ -927,17 +957,29 @@ __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restri
         const int ze = min(zb + planes, nz);
         float f_back = 0.f;
         if constexpr (DIM == 3) f_back = __ldg(a.w + idx3(x, y, zb, nx, ny));
+        // the cell's six faces always exist: a plane's five new faces and its
+        // flag are loaded one plane ahead, in flight across the plane before
+        struct Faces {
+            float t, b, r, l, f;
+            uint8_t fl;
+        };
+        auto fetch = [&](int z, Faces& F) {
+            F.t = __ldg(a.v + idx3(x, y + 1, z, nx, ny + 1));
+            F.b = __ldg(a.v + idx3(x, y, z, nx, ny + 1));
+            F.r = __ldg(a.u + idx3(x + 1, y, z, nx + 1, ny));
+            F.l = __ldg(a.u + idx3(x, y, z, nx + 1, ny));
+            F.f = DIM == 3 ? __ldg(a.w + idx3(x, y, z + 1, nx, ny)) : 0.f;
+            F.fl = __ldg(a.flags + idx3(x, y, z, nx, ny));
+        };
+        Faces cur;
+        fetch(zb, cur);
         for (int z = zb; z < ze; ++z) {
             const int c = idx3(x, y, z, nx, ny);
-            // the cell's six faces always exist: load them before the flag test
-            // so the loads do not wait for it
-            const float f_top = __ldg(a.v + idx3(x, y + 1, z, nx, ny + 1));
-            const float f_bottom = __ldg(a.v + idx3(x, y, z, nx, ny + 1));
-            const float f_right = __ldg(a.u + idx3(x + 1, y, z, nx + 1, ny));
-            const float f_left = __ldg(a.u + idx3(x, y, z, nx + 1, ny));
-            float f_front = 0.f;
-            if constexpr (DIM == 3) f_front = __ldg(a.w + idx3(x, y, z + 1, nx, ny));
-            const uint8_t fl = __ldg(a.flags + c);
+            Faces nxt = cur;
+            if (z + 1 < ze) fetch(z + 1, nxt);
+            const float f_top = cur.t, f_bottom = cur.b, f_right = cur.r, f_left = cur.l, f_front = cur.f;
+            const uint8_t fl = cur.fl;
+            cur = nxt;
             if (!(fl & F_SOLID)) {
                 const bool sv = a.sv0 != nullptr;
                 const float v_top = (fl & F_TOP) ? (sv ? a.sv1[c + nx] : 0.f) : f_top;
