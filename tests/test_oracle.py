@@ -1,7 +1,8 @@
 """CPU tests of the oracle (the checker): known answers the reference's
 algorithm must satisfy, FP32 vs FP64 agreement, and the reference quirks it
-restates.  The reference ships no tests or golden vectors (parity unpinned);
-tests/golden/ holds fixtures generated by this oracle (see make_golden.py)."""
+restates.  The reference ships no tests or golden vectors and its GLSL
+cannot run here (no OpenGL stack), so the oracle's parity is unpinned: these
+known-answer tests are what pins it."""
 import numpy as np
 import pytest
 
