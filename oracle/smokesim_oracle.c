@@ -957,10 +957,11 @@ static void og_coarse_matrix(og_sim* s, int L, const ss_mg_schedule* mg, real dt
         s->cm_iters = mg->n_coarse;
     }
     /* `parts` slices of i per value (the largest power of two <= 32 with
-     * parts * n <= 1024), each with eight round-robin partial sums added
-     * pairwise, the slices folded as a tree: v[q] += v[q + o], o = parts/2 .. 1 */
+     * parts * n <= 16384, the lanes of the GPU's 16-block cluster), each with
+     * eight round-robin partial sums added pairwise, the slices folded as a
+     * tree: v[q] += v[q + o], o = parts/2 .. 1 */
     size_t parts = 1;
-    while (parts < 32 && parts * 2 * n <= 1024) parts *= 2;
+    while (parts < 32 && parts * 2 * n <= 16384) parts *= 2;
     const size_t chunk = (n + parts - 1) / parts;
     for (size_t j = 0; j < n; ++j) {
         real v[32];

@@ -98,6 +98,7 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->cmat);
     cudaFree(s->cmat_alpha);
     cudaFree(s->cmat_state);
+    cudaFree(s->cmat_part);
     for (auto& g : s->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     cudaFree(s->d_scale);
@@ -209,6 +210,10 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     // dependent launch (each waits for the previous one to finish before it
     // is scheduled); the results are the same.
     if (const char* e = getenv("SMOKESIM_PDL")) s->pdl = atoi(e) ? 1 : 0;
+    // SMOKESIM_CLUSTER=0 runs the mixed solve's small coarse levels as one
+    // launch per level operation instead of one thread-block cluster launch;
+    // the results are the same.
+    if (const char* e = getenv("SMOKESIM_CLUSTER")) s->use_cluster = atoi(e) ? 1 : 0;
     s->nv[0] = (size_t)(s->nx + 1) * s->ny * s->nz;
     s->nv[1] = (size_t)s->nx * (s->ny + 1) * s->nz;
     s->nv[2] = s->dim == 3 ? (size_t)s->nx * s->ny * (s->nz + 1) : 0;
@@ -234,6 +239,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
         s->lv[l].hh = s->lv[l].h * s->lv[l].h;
     }
     s->bottom = bottom_start(s);
+    s->cluster_from = coarse_cluster_from(s);
 
     int rc = SS_OK;
     auto A = [&](void** p, size_t bytes) { if (rc == SS_OK) rc = dalloc(p, bytes); };
@@ -792,12 +798,14 @@ static int ensure_mixed(ss_sim* s, int prec, cudaStream_t st) {
             CU(cudaMalloc((void**)&s->cmat, (size_t)(nc * nc) * sizeof(float)), "cudaMalloc(coarse matrix)");
             CU(cudaMalloc((void**)&s->cmat_alpha, (size_t)nc * sizeof(float)), "cudaMalloc(coarse matrix)");
             CU(cudaMalloc((void**)&s->cmat_state, 2 * sizeof(int)), "cudaMalloc(coarse matrix)");
+            CU(cudaMalloc((void**)&s->cmat_part, kProductLanes * sizeof(float)), "cudaMalloc(coarse matrix)");
             CU(cudaMemsetAsync(s->cmat_state, 0xff, 2 * sizeof(int), st), "memset");
             s->cmat_n = (int)nc;
             s->cmat_dirty = 1;
             s->cmat_iters = -1;
         }
     }
+    TRY(coarse_cluster_setup(s));
     s->cstore = prec;
     return SS_OK;
 }
@@ -815,6 +823,7 @@ static int v_cycle_mixed(ss_sim* s, const StepConsts& c, const ss_mg_schedule& m
         TRY(launch_rb_prolong_mixed(s, prec, st));
         return launch_rb_sweep(s, mg.n_post, st, z);
     }
+    if (L == s->cluster_from && s->cluster_ctas > 0) return coarse_cluster(s, mg, L, prec, st);
     if (L >= s->bottom) return coarse_bottom(s, mg, L, prec, st);
     if (L == s->levels - 1) return coarse_smooth(s, c, L, mg.n_coarse, prec, st);
     TRY(coarse_smooth(s, c, L, mg.n_pre, prec, st));

@@ -9,8 +9,12 @@
 // pyramid as RGBA16F images).
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "ss_internal.h"
+
+namespace cg = cooperative_groups;
 
 namespace ss {
 
@@ -546,6 +550,7 @@ struct BottomArgsT {
     int n_pre, n_post, n_coarse, quirks;
     float oob_smooth, oob_resid;
     const float* cmat;   // coarsest level by its response matrix (mixed solve), or null: sweeps
+    float* cpart;        // the product's slice sums (kProductLanes floats)
 };
 
 template <typename T>
@@ -694,7 +699,10 @@ SS_D void bottom_smooth(const MGArgs& a, int iterations) {
 // ((i - i0) mod 8), added pairwise, so the oracle can repeat the order.  Two
 // rounds of eight independent loads are in flight per step (the matrix
 // streams from L2).
-SS_D float coarse_product(const float* __restrict__ E, const float* r, int n, int j, int i0, int i1) {
+// r: the level's right-hand side (shared-memory floats in the one-block
+// bottom solve, the level's global array with CG in the cluster form).
+template <bool CG = false, typename RT>
+SS_D float coarse_product(const float* __restrict__ E, const RT* r, int n, int j, int i0, int i1) {
     float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     const float* e = E + j;
     int i = i0;
@@ -703,20 +711,56 @@ SS_D float coarse_product(const float* __restrict__ E, const float* r, int n, in
 #pragma unroll
         for (int k = 0; k < 16; ++k) v[k] = __ldg(e + (size_t)(i + k) * n);
 #pragma unroll
-        for (int k = 0; k < 16; ++k) a[k & 7] += v[k] * r[i + k];
+        for (int k = 0; k < 16; ++k) a[k & 7] += v[k] * ldv<CG>(r + i + k);
     }
 #pragma unroll
     for (int k = 0; k < 16; ++k)
-        if (i + k < i1) a[k & 7] += __ldg(e + (size_t)(i + k) * n) * r[i + k];
+        if (i + k < i1) a[k & 7] += __ldg(e + (size_t)(i + k) * n) * ldv<CG>(r + i + k);
     return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
 }
 
-// Threads per coarse value in the bottom's matrix product: the largest power
-// of two (at most 32) with parts * n <= the block's 1024 threads.
+// Slices of i per coarse value in the matrix product: the largest power of
+// two (at most 32) with parts * n <= kProductLanes, a cluster's threads - so
+// the cluster form takes one slice (at most 16 terms at 8^3) per thread.  The
+// one-block bottom solve walks the same (slice, value) items in turns of its
+// 1024 threads, so both give the same sums in the same order.
 SS_D int coarse_parts(int n) {
     int parts = 1;
-    while (parts < 32 && parts * 2 * n <= 1024) parts *= 2;
+    while (parts < 32 && parts * 2 * n <= kProductLanes) parts *= 2;
     return parts;
+}
+
+// p_j = sum_i E[i n + j] r_i for every j of the coarsest level, in two phases
+// separated by a barrier of the caller's.  Phase 1: item t is slice
+// q = t / n of value j = t % n (adjacent lanes read adjacent j of a row of E,
+// coalesced); its sum goes to part[q n + j].  Phase 2: value j folds its
+// slices as a tree, v[q] += v[q + o] for o = parts/2 .. 1, rounds the result
+// as R and stores it as PT.  `part` holds parts * n <= kProductLanes floats.
+template <bool CG, typename RT>
+SS_D void coarse_matrix_partials(const float* __restrict__ E, const RT* r, float* part, int n, int tid,
+                                 int nthreads) {
+    const int parts = coarse_parts(n), chunk = (n + parts - 1) / parts;
+    for (int t = tid; t < parts * n; t += nthreads) {
+        const int q = t / n, j = t % n;
+        part[t] = coarse_product<CG>(E, r, n, j, q * chunk, min(n, (q + 1) * chunk));
+    }
+}
+
+template <bool CG, typename R, typename PT>
+SS_D void coarse_matrix_fold(const float* part, PT* p, int n, int tid, int nthreads) {
+    const int parts = coarse_parts(n);
+    for (int j = tid; j < n; j += nthreads) {
+        float v[32];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) v[q] = q < parts ? ldv<CG>(part + q * n + j) : 0.f;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1)
+            if (o < parts) {
+#pragma unroll
+                for (int q = 0; q < o; ++q) v[q] = v[q] + v[q + o];
+            }
+        p[j] = st<PT>(rnd<R>(v[0]));
+    }
 }
 
 template <int DIM, typename T, typename R>
@@ -780,18 +824,12 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgsT<T> b) {
     }
     // coarsest level
     if (b.cmat) {
-        // p = E r: `parts` adjacent lanes per value, each over a contiguous
-        // slice of i, their sums folded by a shuffle tree (lane q += lane q + o
-        // for o = parts/2 .. 1)
+        // p = E r (coarse_matrix_apply), the stores rounded as R
         const MGArgs ac = bottom_level(b, sp, sr, sa, b.nlev - 1, b.oob_smooth);
         const int n = ac.nx * ac.ny * ac.nz;
-        const int parts = coarse_parts(n), chunk = (n + parts - 1) / parts;
-        const int t = threadIdx.x, j = t / parts, part = t % parts;
-        const bool on = t < n * parts;
-        float v = 0.f;
-        if (on) v = coarse_product(b.cmat, ac.r, n, j, part * chunk, min(n, (part + 1) * chunk));
-        for (int o = parts / 2; o >= 1; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (on && part == 0) ac.p[j] = rnd<R>(v);
+        coarse_matrix_partials<false>(b.cmat, ac.r, b.cpart, n, (int)threadIdx.x, (int)blockDim.x);
+        __syncthreads();
+        coarse_matrix_fold<false, R>(b.cpart, ac.p, n, (int)threadIdx.x, (int)blockDim.x);
         __syncthreads();
     } else {
         bottom_smooth<DIM, R>(bottom_level(b, sp, sr, sa, b.nlev - 1, b.oob_smooth), b.n_coarse);
@@ -843,6 +881,116 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgsT<T> b) {
     }
 }
 
+// ------------------------------------------------ coarse levels in one cluster
+// The mixed solve's levels from cluster_from (the first of at most
+// kClusterCells cells) down to the coarsest and back up, in ONE launch of one
+// thread-block cluster of up to 16 CTAs x 1024 threads.  Every phase - a red
+// or black half-sweep of a level, a residual + restriction (which also sets
+// the next level's pressure to +0), a prolongation, the coarsest level's
+// matrix product - is spread over all the cluster's threads, and a cluster
+// barrier (barrier.cluster, release / acquire; about 0.3 us on B200) separates
+// it from the next, in place of a launch per phase.  The arrays stay in global
+// memory (L2-resident at these sizes): every value another CTA of the launch
+// may have written is read with ld.global.cg (L1 is not coherent across SMs),
+// the fixed solid fractions through L1.  The per-cell operations are those of
+// the per-level kernels, so the result is the same, bit for bit, as launching
+// them level by level.
+constexpr int kClusterCells = 32768;
+constexpr int kClusterThreads = 1024;
+
+template <typename T>
+struct ClusterArgsT {
+    int nlev;
+    int n[SS_MAX_LEVELS][3];
+    float hh[SS_MAX_LEVELS];
+    T* p[SS_MAX_LEVELS];
+    T* r[SS_MAX_LEVELS];
+    const float* alpha[SS_MAX_LEVELS];
+    int n_pre, n_post, n_coarse;
+    float oob_smooth, oob_resid;
+    const float* cmat;   // coarsest level by its response matrix, or null: sweeps
+    float* cpart;        // the product's slice sums (kProductLanes floats)
+};
+
+template <typename T>
+SS_D MGArgsT<T> cluster_level(const ClusterArgsT<T>& b, int l, float oobA) {
+    MGArgsT<T> a;
+    a.p = b.p[l];
+    a.r = b.r[l];
+    a.alpha = b.alpha[l];
+    a.flags = nullptr;
+    a.div0 = nullptr;
+    a.div0r = nullptr;
+    a.nx = b.n[l][0];
+    a.ny = b.n[l][1];
+    a.nz = b.n[l][2];
+    a.oobA = oobA;
+    a.hh = b.hh[l];
+    a.rho_h = 0.f;
+    a.dt = 1.f;
+    a.rho = 1.f;
+    a.dt_h = 1.f;
+    return a;
+}
+
+// `iterations` red-black sweeps of one level, cell (x, y, z) of each colour
+// as k_smooth numbers them, a cluster barrier after every half-sweep
+template <int DIM, typename T>
+SS_D void cluster_sweeps(const MGArgsT<T>& a, int iterations, int tid, int nthreads, cg::cluster_group& cl) {
+    const int hx = (a.nx + 1) / 2, m = hx * a.ny * a.nz;
+    for (int it = 0; it < 2 * iterations; ++it) {
+        const int parity = it & 1;
+        for (int i = tid; i < m; i += nthreads) {
+            const int xi = i % hx, t = i / hx, y = t % a.ny, z = t / a.ny;
+            const int x = 2 * xi + ((y + z + parity) & 1);
+            if (x < a.nx) smooth_cell<DIM, false, T, T, true>(a, x, y, z);
+        }
+        cl.sync();
+    }
+}
+
+template <int DIM, typename T>
+__global__ void __launch_bounds__(kClusterThreads, 1) k_coarse_cluster(ClusterArgsT<T> b) {
+    pdl_entry();
+    cg::cluster_group cl = cg::this_cluster();
+    const int nthreads = (int)(cl.num_blocks() * blockDim.x);
+    const int tid = (int)(cl.block_rank() * blockDim.x + threadIdx.x);
+    // down: pre-smoothing, residual + restriction (next level's p cleared)
+    for (int l = 0; l + 1 < b.nlev; ++l) {
+        cluster_sweeps<DIM, T>(cluster_level(b, l, b.oob_smooth), b.n_pre, tid, nthreads, cl);
+        const MGArgsT<T> ar = cluster_level(b, l, b.oob_resid);
+        const int cx = b.n[l + 1][0], cy = b.n[l + 1][1], cz = b.n[l + 1][2];
+        const int hx = (ar.nx + 1) / 2, hy = (ar.ny + 1) / 2, hz = DIM == 3 ? (ar.nz + 1) / 2 : 1;
+        for (int q = tid; q < hx * hy * hz; q += nthreads) {
+            const int X = q % hx, t = q / hx, Y = t % hy, Z = t / hy;
+            residual_restrict_cell<DIM, false, false, true, T, true>(ar, b.r[l + 1], cx, cy, cz, X, Y, Z, b.p[l + 1]);
+        }
+        cl.sync();
+    }
+    // coarsest level
+    const int lc = b.nlev - 1;
+    if (b.cmat) {
+        const int n = b.n[lc][0] * b.n[lc][1] * b.n[lc][2];
+        coarse_matrix_partials<true>(b.cmat, b.r[lc], b.cpart, n, tid, nthreads);
+        cl.sync();
+        coarse_matrix_fold<true, T>(b.cpart, b.p[lc], n, tid, nthreads);
+        cl.sync();
+    } else {
+        cluster_sweeps<DIM, T>(cluster_level(b, lc, b.oob_smooth), b.n_coarse, tid, nthreads, cl);
+    }
+    // up: prolongation + post-smoothing
+    for (int l = b.nlev - 2; l >= 0; --l) {
+        const int ax = b.n[l][0], ay = b.n[l][1], az = b.n[l][2];
+        for (int c = tid; c < ax * ay * az; c += nthreads) {
+            const int x = c % ax, t = c / ax, y = t % ay, z = t / ay;
+            prolong_cell<DIM, T, true>(b.p[l], ax, ay, az, b.p[l + 1], b.n[l + 1][0], b.n[l + 1][1], b.n[l + 1][2], x,
+                                       y, z);
+        }
+        cl.sync();
+        cluster_sweeps<DIM, T>(cluster_level(b, l, b.oob_smooth), b.n_post, tid, nthreads, cl);
+    }
+}
+
 int bottom_start(const ss_sim* s) {
     // finest level >= 1 from which the rest of the pyramid fits the block's shared memory
     long long cum = 0;
@@ -877,6 +1025,7 @@ static int launch_bottom_t(ss_sim* s, const ss_mg_schedule& mg, int L, T* const*
     b.oob_smooth = smooth_oob(s, mg.ref_quirks);
     b.oob_resid = resid_oob(s, mg.ref_quirks);
     b.cmat = sizeof(T) == 2 ? s->cmat : nullptr;   // the mixed solve's coarse storage
+    b.cpart = s->cmat_part;
     const size_t smem = (size_t)3 * off * sizeof(float);
     if (smem > (size_t)kBottomSmemBytes) return set_error(SS_E_INVALID, "bottom levels exceed shared memory");
     // the attribute is per function; setting it on every launch is cheap
@@ -1049,6 +1198,100 @@ int coarse_residual_restrict(ss_sim* s, const StepConsts& c, int L, int prec, cu
 int coarse_prolong(ss_sim* s, int L, int prec, cudaStream_t st) {
     if (prec == SS_PREC_MIXED) return coarse_prolong_t<__half>(s, L, (__half*)s->cp[L], (const __half*)s->cp[L + 1], st);
     return coarse_prolong_t<__nv_bfloat16>(s, L, (__nv_bfloat16*)s->cp[L], (const __nv_bfloat16*)s->cp[L + 1], st);
+}
+
+// ---------------------------------------------- coarse levels in one cluster
+// The first level >= 1 of at most kClusterCells cells (0: none).
+int coarse_cluster_from(const ss_sim* s) {
+    for (int l = 1; l < s->levels; ++l)
+        if ((long long)s->lv[l].n[0] * s->lv[l].n[1] * s->lv[l].n[2] <= kClusterCells) return l;
+    return 0;
+}
+
+template <int DIM, typename T>
+static cudaError_t cluster_config(int ctas, cudaLaunchConfig_t* cfg, cudaLaunchAttribute* at, int* active) {
+    cudaError_t e = cudaFuncSetAttribute(k_coarse_cluster<DIM, T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    *cfg = cudaLaunchConfig_t{};
+    cfg->gridDim = dim3(ctas);
+    cfg->blockDim = dim3(kClusterThreads);
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = ctas;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg->attrs = at;
+    cfg->numAttrs = 1;
+    return active ? cudaOccupancyMaxActiveClusters(active, k_coarse_cluster<DIM, T>, cfg) : cudaSuccess;
+}
+
+// Cluster size for this device: 16 CTAs when the GPU can place such a
+// cluster (non-portable size), else 8, else 0 (the per-level launches).
+// Called outside any stream capture.
+int coarse_cluster_setup(ss_sim* s) {
+    if (s->cluster_ctas >= 0) return SS_OK;
+    s->cluster_ctas = 0;
+    if (!s->use_cluster || !s->cluster_from) return SS_OK;
+    for (int ctas : {16, 8}) {
+        cudaLaunchConfig_t cfg;
+        cudaLaunchAttribute at[1];
+        int active = 0, a2 = 0;
+        cudaError_t e = s->dim == 3 ? cluster_config<3, __half>(ctas, &cfg, at, &active)
+                                    : cluster_config<2, __half>(ctas, &cfg, at, &active);
+        if (e == cudaSuccess)
+            e = s->dim == 3 ? cluster_config<3, __nv_bfloat16>(ctas, &cfg, at, &a2)
+                            : cluster_config<2, __nv_bfloat16>(ctas, &cfg, at, &a2);
+        if (e != cudaSuccess) {
+            cudaGetLastError();   // an unsupported size is not an error of the solve
+            continue;
+        }
+        if (active >= 1 && a2 >= 1) {
+            s->cluster_ctas = ctas;
+            break;
+        }
+    }
+    return SS_OK;
+}
+
+template <int DIM, typename T>
+static int launch_cluster_t(ss_sim* s, const ss_mg_schedule& mg, int L, T* const* p, T* const* r, cudaStream_t st) {
+    ClusterArgsT<T> b{};
+    b.nlev = s->levels - L;
+    for (int l = 0; l < b.nlev; ++l) {
+        const ss::Level& lv = s->lv[L + l];
+        b.n[l][0] = lv.n[0]; b.n[l][1] = lv.n[1]; b.n[l][2] = lv.n[2];
+        b.hh[l] = lv.hh;
+        b.p[l] = p[L + l];
+        b.r[l] = r[L + l];
+        b.alpha[l] = s->alpha[L + l];
+    }
+    b.n_pre = mg.n_pre; b.n_post = mg.n_post; b.n_coarse = mg.n_coarse;
+    b.oob_smooth = smooth_oob(s, 0);
+    b.oob_resid = resid_oob(s, 0);
+    b.cmat = s->cmat;
+    b.cpart = s->cmat_part;
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute at[2];
+    cudaError_t e = cluster_config<DIM, T>(s->cluster_ctas, &cfg, at, nullptr);
+    if (e != cudaSuccess) return check_cuda(e, "cluster attributes");
+    cfg.stream = st;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.numAttrs = s->pdl ? 2 : 1;
+    e = cudaLaunchKernelEx(&cfg, k_coarse_cluster<DIM, T>, b);
+    s->nlaunch += 1;
+    return check_cuda(e, "k_coarse_cluster");
+}
+
+int coarse_cluster(ss_sim* s, const ss_mg_schedule& mg, int L, int prec, cudaStream_t st) {
+    if (prec == SS_PREC_MIXED) {
+        __half* const* p = (__half* const*)s->cp;
+        __half* const* r = (__half* const*)s->cr;
+        return s->dim == 3 ? launch_cluster_t<3, __half>(s, mg, L, p, r, st) : launch_cluster_t<2, __half>(s, mg, L, p, r, st);
+    }
+    __nv_bfloat16* const* p = (__nv_bfloat16* const*)s->cp;
+    __nv_bfloat16* const* r = (__nv_bfloat16* const*)s->cr;
+    return s->dim == 3 ? launch_cluster_t<3, __nv_bfloat16>(s, mg, L, p, r, st)
+                       : launch_cluster_t<2, __nv_bfloat16>(s, mg, L, p, r, st);
 }
 
 int coarse_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, int prec, cudaStream_t st) {

@@ -144,6 +144,7 @@ struct ss_sim {
     float* cmat = nullptr;       // cmat_n^2: E[i n + j] = dp_j / dr_i
     float* cmat_alpha = nullptr; // solid fractions it was built for
     int* cmat_state = nullptr;   // device: [0] iteration count it was built for, [1] rebuild flag
+    float* cmat_part = nullptr;  // the product's slice sums (kProductLanes floats)
     int cmat_n = 0, cmat_iters = -1, cmat_dirty = 1;
     // The multigrid part of a solve recorded once as a CUDA graph and replayed
     // (api.cpp, run_graph): slot 0 fixed-count FP32 V-cycles, 1 one FP32
@@ -157,6 +158,12 @@ struct ss_sim {
     int use_graphs = 1;
     // programmatic dependent launch of the solve's kernel chain (SMOKESIM_PDL=0 sets 0)
     int pdl = 1;
+    // mixed solve: the levels from cluster_from down in one thread-block
+    // cluster launch (k_coarse_cluster) of cluster_ctas CTAs; -1 = not yet
+    // probed, 0 = per-level launches (SMOKESIM_CLUSTER=0 sets use_cluster 0)
+    int use_cluster = 1;
+    int cluster_from = 0;
+    int cluster_ctas = -1;
     int rb_active = 0;         // level-0 pressure currently lives colour-split in p_alt[0]
     std::vector<ss::TensorMapEntry> tmaps;
     cudaStream_t stream0 = nullptr;
@@ -220,6 +227,9 @@ int coarse_smooth(ss_sim* s, const StepConsts& c, int L, int iterations, int pre
 int coarse_residual_restrict(ss_sim* s, const StepConsts& c, int L, int prec, cudaStream_t st);
 int coarse_prolong(ss_sim* s, int L, int prec, cudaStream_t st);
 int coarse_bottom(ss_sim* s, const ss_mg_schedule& mg, int L, int prec, cudaStream_t st);
+int coarse_cluster_from(const ss_sim* s);
+int coarse_cluster_setup(ss_sim* s);
+int coarse_cluster(ss_sim* s, const ss_mg_schedule& mg, int L, int prec, cudaStream_t st);
 int launch_rb_residual_restrict_mixed(ss_sim* s, int prec, cudaStream_t st);
 
 int launch_rb_prolong_mixed(ss_sim* s, int prec, cudaStream_t st);
@@ -274,6 +284,9 @@ struct AdjScratch {
 };
 // coarsest levels up to this many cells get a response matrix (4 MiB)
 constexpr int kCoarseResponseMax = 1024;
+// lanes of the coarsest level's matrix product (k_mg.cu, coarse_parts): one
+// 16-block cluster of 1024 threads
+constexpr int kProductLanes = 16384;
 int launch_coarse_response(ss_sim* s, int iters, float* D, cudaStream_t st);
 int update_coarse_matrix(ss_sim* s, const ss_mg_schedule& mg, cudaStream_t st);
 // Scratch of the deterministic (owner-computes) adjoint scatters; a null
