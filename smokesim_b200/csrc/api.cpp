@@ -99,6 +99,7 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->cmat_alpha);
     cudaFree(s->cmat_state);
     cudaFree(s->cmat_part);
+    cudaFree(s->cluster_fine);
     for (auto& g : s->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     cudaFree(s->d_scale);

@@ -90,6 +90,18 @@ SS_D void smooth_cell(const MGArgsT<T>& a, int x, int y, int z) {
     const int c = idx3(x, y, z, nx, ny);
     float f_top, f_bottom, f_right, f_left, f_front = 0.f, f_back = 0.f;
     float r_c = 0.f;
+    float p_top, p_bottom, p_right, p_left, p_front = 0.f, p_back = 0.f;
+    auto load_p = [&]() {
+        const T* P = a.p;
+        p_top = y + 1 < ny ? ldv<CG>(P + c + nx) : 0.f;
+        p_bottom = y > 0 ? ldv<CG>(P + c - nx) : 0.f;
+        p_right = x + 1 < nx ? ldv<CG>(P + c + 1) : 0.f;
+        p_left = x > 0 ? ldv<CG>(P + c - 1) : 0.f;
+        if constexpr (DIM == 3) {
+            p_front = z + 1 < nz ? ldv<CG>(P + c + nx * ny) : 0.f;
+            p_back = z > 0 ? ldv<CG>(P + c - nx * ny) : 0.f;
+        }
+    };
     if constexpr (L0) {
         const uint8_t fl = a.flags[c];
         if (fl & F_SOLID) return;
@@ -116,6 +128,9 @@ SS_D void smooth_cell(const MGArgsT<T>& a, int x, int y, int z) {
             a_k = z > 0 ? a.alpha[c - nx * ny] : a.oobA;
         }
         r_c = ldv<CG>(a.r + c);
+        // the neighbours' pressures too: with CG they come from L2, and
+        // issuing them here keeps the cell to one memory round trip
+        load_p();
         if (a_c >= 1.f) return;
         f_top = 1.f - a_t;
         f_bottom = 1.f - a_b;
@@ -126,16 +141,7 @@ SS_D void smooth_cell(const MGArgsT<T>& a, int x, int y, int z) {
             f_back = 1.f - a_k;
         }
     }
-    const T* P = a.p;
-    const float p_top = y + 1 < ny ? ldv<CG>(P + c + nx) : 0.f;
-    const float p_bottom = y > 0 ? ldv<CG>(P + c - nx) : 0.f;
-    const float p_right = x + 1 < nx ? ldv<CG>(P + c + 1) : 0.f;
-    const float p_left = x > 0 ? ldv<CG>(P + c - 1) : 0.f;
-    float p_front = 0.f, p_back = 0.f;
-    if constexpr (DIM == 3) {
-        p_front = z + 1 < nz ? ldv<CG>(P + c + nx * ny) : 0.f;
-        p_back = z > 0 ? ldv<CG>(P + c - nx * ny) : 0.f;
-    }
+    if constexpr (L0) load_p();
     float f_sum = f_top + f_bottom + f_right + f_left;
     if constexpr (DIM == 3) f_sum = f_sum + f_front + f_back;
     if (f_sum == 0.f) return;
@@ -192,6 +198,19 @@ SS_D float residual_cell(const MGArgsT<T>& a, int x, int y, int z) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int c = idx3(x, y, z, nx, ny);
     float f_top, f_bottom, f_right, f_left, f_front = 0.f, f_back = 0.f;
+    float p_top, p_bottom, p_right, p_left, p_front = 0.f, p_back = 0.f, p_c, old;
+    const T* P = a.p;
+    auto load_p = [&]() {
+        p_top = y + 1 < ny ? ldv<CG>(P + c + nx) : 0.f;
+        p_bottom = y > 0 ? ldv<CG>(P + c - nx) : 0.f;
+        p_right = x + 1 < nx ? ldv<CG>(P + c + 1) : 0.f;
+        p_left = x > 0 ? ldv<CG>(P + c - 1) : 0.f;
+        if constexpr (DIM == 3) {
+            p_front = z + 1 < nz ? ldv<CG>(P + c + nx * ny) : 0.f;
+            p_back = z > 0 ? ldv<CG>(P + c - nx * ny) : 0.f;
+        }
+        p_c = ldv<CG>(P + c);
+    };
     if constexpr (L0) {
         const uint8_t fl = a.flags[c];
         if (fl & F_SOLID) return 0.f;
@@ -204,37 +223,43 @@ SS_D float residual_cell(const MGArgsT<T>& a, int x, int y, int z) {
             f_front = (fl & F_FRONT) ? 0.f : (z + 1 < nz ? 1.f : fo);
             f_back = (fl & F_BACK) ? 0.f : (z > 0 ? 1.f : fo);
         }
+        load_p();
+        old = a.rho * a.div0r[c] / a.dt_h;
     } else {
-        if (a.alpha[c] >= 1.f) return 0.f;
-        f_top = 1.f - (y + 1 < ny ? a.alpha[c + nx] : a.oobA);
-        f_bottom = 1.f - (y > 0 ? a.alpha[c - nx] : a.oobA);
-        f_right = 1.f - (x + 1 < nx ? a.alpha[c + 1] : a.oobA);
-        f_left = 1.f - (x > 0 ? a.alpha[c - 1] : a.oobA);
+        // every load of the cell (fractions, pressures, right-hand side) is
+        // issued before the solid test: one memory round trip a cell
+        const float a_c = a.alpha[c];
+        const float a_t = y + 1 < ny ? a.alpha[c + nx] : a.oobA;
+        const float a_b = y > 0 ? a.alpha[c - nx] : a.oobA;
+        const float a_r = x + 1 < nx ? a.alpha[c + 1] : a.oobA;
+        const float a_l = x > 0 ? a.alpha[c - 1] : a.oobA;
+        float a_f = 0.f, a_k = 0.f;
         if constexpr (DIM == 3) {
-            f_front = 1.f - (z + 1 < nz ? a.alpha[c + nx * ny] : a.oobA);
-            f_back = 1.f - (z > 0 ? a.alpha[c - nx * ny] : a.oobA);
+            a_f = z + 1 < nz ? a.alpha[c + nx * ny] : a.oobA;
+            a_k = z > 0 ? a.alpha[c - nx * ny] : a.oobA;
+        }
+        load_p();
+        old = ldv<CG>(a.r + c);
+        if (a_c >= 1.f) return 0.f;
+        f_top = 1.f - a_t;
+        f_bottom = 1.f - a_b;
+        f_right = 1.f - a_r;
+        f_left = 1.f - a_l;
+        if constexpr (DIM == 3) {
+            f_front = 1.f - a_f;
+            f_back = 1.f - a_k;
         }
     }
-    const T* P = a.p;
-    const float p_top = y + 1 < ny ? ldv<CG>(P + c + nx) : 0.f;
-    const float p_bottom = y > 0 ? ldv<CG>(P + c - nx) : 0.f;
-    const float p_right = x + 1 < nx ? ldv<CG>(P + c + 1) : 0.f;
-    const float p_left = x > 0 ? ldv<CG>(P + c - 1) : 0.f;
     float p_sum = p_top * f_top + p_bottom * f_bottom;
     p_sum = p_sum + p_right * f_right;
     p_sum = p_sum + p_left * f_left;
     float f_sum = f_top + f_bottom + f_right + f_left;
     if constexpr (DIM == 3) {
-        const float p_front = z + 1 < nz ? ldv<CG>(P + c + nx * ny) : 0.f;
-        const float p_back = z > 0 ? ldv<CG>(P + c - nx * ny) : 0.f;
         p_sum = p_sum + p_front * f_front;
         p_sum = p_sum + p_back * f_back;
         f_sum = f_sum + f_front + f_back;
     }
-    float old;
-    if constexpr (L0) old = a.rho * a.div0r[c] / a.dt_h;
-    else old = ldv<CG>(a.r + c);
-    return old - (p_sum - f_sum * ldv<CG>(P + c)) / a.hh;
+    return old - (p_sum - f_sum * p_c) / a.hh;
 }
 
 // One thread per coarse cell: residual of its 2^DIM children (written in place
@@ -910,7 +935,33 @@ struct ClusterArgsT {
     float oob_smooth, oob_resid;
     const float* cmat;   // coarsest level by its response matrix, or null: sweeps
     float* cpart;        // the product's slice sums (kProductLanes floats)
+    float* fine;         // a level's residuals (kClusterCells floats)
 };
+
+// restrict_residual of coarse cell (X, Y, Z) from the fine residuals of the
+// previous phase, in residual_restrict_cell's sum order (fine cells outside
+// the grid count 0)
+template <int DIM>
+SS_D float cluster_restrict(const float* fine, int nx, int ny, int nz, int X, int Y, int Z) {
+    float v[2][2][2];   // [dz][dy][dx]
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) {
+                const int x = 2 * X + dx, y = 2 * Y + dy, z = DIM == 3 ? 2 * Z + dz : 0;
+                v[dz][dy][dx] = (x < nx && y < ny && z < nz && (DIM == 3 || dz == 0))
+                                    ? __ldcg(fine + idx3(x, y, z, nx, ny)) : 0.f;
+            }
+    if constexpr (DIM == 3) {
+        const float bottom = v[0][0][0] + v[1][0][0] + v[0][0][1] + v[1][0][1];
+        const float top = v[0][1][0] + v[1][1][0] + v[0][1][1] + v[1][1][1];
+        return (bottom + top) / 8.f;
+    } else {
+        return (v[0][0][0] + v[0][0][1] + v[0][1][0] + v[0][1][1]) / 4.f;
+    }
+}
 
 template <typename T>
 SS_D MGArgsT<T> cluster_level(const ClusterArgsT<T>& b, int l, float oobA) {
@@ -958,12 +1009,20 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_coarse_cluster(ClusterAr
     // down: pre-smoothing, residual + restriction (next level's p cleared)
     for (int l = 0; l + 1 < b.nlev; ++l) {
         cluster_sweeps<DIM, T>(cluster_level(b, l, b.oob_smooth), b.n_pre, tid, nthreads, cl);
+        // residual of every fine cell (one a thread), then the restriction
+        // from those values; the next level's p is cleared beside it
         const MGArgsT<T> ar = cluster_level(b, l, b.oob_resid);
+        const int nf = ar.nx * ar.ny * ar.nz;
+        for (int c = tid; c < nf; c += nthreads) {
+            const int x = c % ar.nx, t = c / ar.nx, y = t % ar.ny, z = t / ar.ny;
+            b.fine[c] = residual_cell<DIM, false, T, true>(ar, x, y, z);
+        }
+        cl.sync();
         const int cx = b.n[l + 1][0], cy = b.n[l + 1][1], cz = b.n[l + 1][2];
-        const int hx = (ar.nx + 1) / 2, hy = (ar.ny + 1) / 2, hz = DIM == 3 ? (ar.nz + 1) / 2 : 1;
-        for (int q = tid; q < hx * hy * hz; q += nthreads) {
-            const int X = q % hx, t = q / hx, Y = t % hy, Z = t / hy;
-            residual_restrict_cell<DIM, false, false, true, T, true>(ar, b.r[l + 1], cx, cy, cz, X, Y, Z, b.p[l + 1]);
+        for (int q = tid; q < cx * cy * cz; q += nthreads) {
+            const int X = q % cx, t = q / cx, Y = t % cy, Z = t / cy;
+            b.r[l + 1][q] = st<T>(cluster_restrict<DIM>(b.fine, ar.nx, ar.ny, ar.nz, X, Y, Z));
+            b.p[l + 1][q] = st<T>(0.f);
         }
         cl.sync();
     }
@@ -1231,6 +1290,10 @@ int coarse_cluster_setup(ss_sim* s) {
     if (s->cluster_ctas >= 0) return SS_OK;
     s->cluster_ctas = 0;
     if (!s->use_cluster || !s->cluster_from) return SS_OK;
+    if (!s->cluster_fine) {
+        const cudaError_t e = cudaMalloc((void**)&s->cluster_fine, kClusterCells * sizeof(float));
+        if (e != cudaSuccess) return check_cuda(e, "cudaMalloc(cluster residuals)");
+    }
     for (int ctas : {16, 8}) {
         cudaLaunchConfig_t cfg;
         cudaLaunchAttribute at[1];
@@ -1269,6 +1332,7 @@ static int launch_cluster_t(ss_sim* s, const ss_mg_schedule& mg, int L, T* const
     b.oob_resid = resid_oob(s, 0);
     b.cmat = s->cmat;
     b.cpart = s->cmat_part;
+    b.fine = s->cluster_fine;
     cudaLaunchConfig_t cfg;
     cudaLaunchAttribute at[2];
     cudaError_t e = cluster_config<DIM, T>(s->cluster_ctas, &cfg, at, nullptr);

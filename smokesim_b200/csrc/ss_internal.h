@@ -164,6 +164,7 @@ struct ss_sim {
     int use_cluster = 1;
     int cluster_from = 0;
     int cluster_ctas = -1;
+    float* cluster_fine = nullptr;   // a cluster level's residuals (kClusterCells floats)
     int rb_active = 0;         // level-0 pressure currently lives colour-split in p_alt[0]
     std::vector<ss::TensorMapEntry> tmaps;
     cudaStream_t stream0 = nullptr;
