@@ -130,6 +130,10 @@ typedef struct ss_mg_schedule {
     double tol;             /* > 0: iterate until relative divergence <= tol */
     int ref_quirks;         /* 1: post-smoothing at level > 0 reads the in-place residual (reference) */
     int precision;          /* ss_precision */
+    int warm_start;         /* mixed-precision solve: 0 starts from the previous step's pressure (as the
+                               reference does); 1 from its linear extrapolation 2 p(n-1) - p(n-2) once two
+                               consecutive mixed solves exist (fewer refinement steps; forward runs only:
+                               ss_adjoint_forward rejects it) */
 } ss_mg_schedule;
 
 /* Physics constants: reference physics_settings (common/physics/physics.h:22-32). */

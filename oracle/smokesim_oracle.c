@@ -68,6 +68,8 @@ typedef struct og_sim {
      * store of the correction V-cycle */
     double* p64;
     int p64_valid;
+    double* p64_prev;   /* the extrapolated warm start's p(n-2) */
+    int prev_ok;        /* p64_prev holds the pressure the current p64 was solved from */
     int cround;
     real force[3];   /* control force on the faces inside active emitters */
     real* ff;        /* coarse control force field, 3 * ffn^3 (none: ffn == 0) */
@@ -249,6 +251,7 @@ void og_destroy(og_sim* s) {
     }
     free(s->em); free(s->ob); free(s->bx);
     free(s->p64);
+    free(s->p64_prev);
     free(s->cm);
     free(s->cm_alpha);
     free(s->ff);
@@ -1194,9 +1197,29 @@ static int og_mixed_pressure_solve(og_sim* s, const ss_mg_schedule* mg, real dt,
     ss_mg_schedule m2 = *mg;
     m2.ref_quirks = 0;
     if (!s->p64) s->p64 = (double*)calloc(s->ncell, sizeof(double));
+    int fresh = 0;
     if (!s->p64_valid) {
         for (size_t i = 0; i < s->ncell; ++i) s->p64[i] = (double)s->p[0][i];
         s->p64_valid = 1;
+        fresh = 1;
+    }
+    /* warm start: with warm_start 1 and the previous solve's starting (solved)
+     * pressure p(n-2) kept, start from 2 p(n-1) - p(n-2); keep p(n-1) either
+     * way.  A fresh p64, not solved by this path, starts no history. */
+    if (mg->warm_start == 1 && !fresh) {
+        if (!s->p64_prev) s->p64_prev = (double*)calloc(s->ncell, sizeof(double));
+        if (s->prev_ok) {
+            for (size_t i = 0; i < s->ncell; ++i) {
+                const double a = s->p64[i], c = s->p64_prev[i];
+                s->p64[i] = 2.0 * a - c;
+                s->p64_prev[i] = a;
+            }
+        } else {
+            memcpy(s->p64_prev, s->p64, s->ncell * sizeof(double));
+            s->prev_ok = 1;
+        }
+    } else {
+        s->prev_ok = 0;
     }
     real* e = (real*)malloc(sizeof(real) * s->ncell);
     real* rhs_s = (real*)malloc(sizeof(real) * s->ncell);

@@ -110,6 +110,7 @@ class MGSchedule(C.Structure):
         ("tol", C.c_double),
         ("ref_quirks", C.c_int),
         ("precision", C.c_int),
+        ("warm_start", C.c_int),
     ]
 
 
@@ -202,7 +203,7 @@ def reference_params():
 
 def make_params(dt=0.1, rho=1.0, t_ambient=0.0, alpha=0.05, beta=0.3, eps=0.2, wind=(0, 0, 0),
                 n_pre=2, n_post=2, n_coarse=80, n_vcycles=4, tol=0.0, ref_quirks=1,
-                precision=PREC_FP32, stage_mask=STAGE_ALL, current_time=0.0, collect_stats=1):
+                precision=PREC_FP32, stage_mask=STAGE_ALL, current_time=0.0, collect_stats=1, warm_start=0):
     p = Params()
     p.time_step = dt
     p.density = rho
@@ -221,6 +222,7 @@ def make_params(dt=0.1, rho=1.0, t_ambient=0.0, alpha=0.05, beta=0.3, eps=0.2, w
     p.mg.tol = tol
     p.mg.ref_quirks = ref_quirks
     p.mg.precision = precision
+    p.mg.warm_start = warm_start
     return p
 
 

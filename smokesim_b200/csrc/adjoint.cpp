@@ -157,6 +157,7 @@ static int restore_state(ss_sim* s, const State& S, cudaStream_t st) {
     if (S.p64_valid && s->p64) {
         TRY_ADJ(copy_d2d(s->p64, S.p64, s->ncell * sizeof(double), st));
         s->p64_valid = 1;
+        s->prev_ok = 0;
     }
     s->em = S.em;
     s->ob = S.ob;
@@ -180,6 +181,10 @@ static int check_adjoint_params(const ss_adjoint* A, const ss_params* p) {
         if (p->mg.precision != SS_PREC_FP32 && p->mg.precision != SS_PREC_MIXED &&
             p->mg.precision != SS_PREC_MIXED_BF16)
             return set_error(SS_E_INVALID, "unknown precision mode");
+        // the extrapolated warm start makes a step's pressure depend on the
+        // two before it; the reverse pass transposes the one-step warm start
+        if (p->mg.warm_start != 0)
+            return set_error(SS_E_UNSUPPORTED, "the adjoint needs warm_start = 0 (the previous step's pressure)");
     }
     return SS_OK;
 }

@@ -93,6 +93,7 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->rb_pw);
     cudaFree(s->p64);
     cudaFree(s->p64b);
+    cudaFree(s->p64c);
     cudaFree(s->render_buf);
     cudaFree(s->ffield);
     cudaFree(s->cmat);
@@ -834,6 +835,26 @@ static int v_cycle_mixed(ss_sim* s, const StepConsts& c, const ss_mg_schedule& m
     return coarse_smooth(s, c, L, mg.n_post, prec, st);
 }
 
+// Warm start of the mixed solve.  p64 holds the previous step's pressure
+// p(n-1).  With warm_start 1 and p64c holding p(n-2) - the solved pressure the
+// previous mixed solve started from - the solve starts from the linear
+// extrapolation 2 p(n-1) - p(n-2) and p64c takes p(n-1); otherwise p64c just
+// takes p(n-1), so that the next solve can extrapolate.  A fresh p64 (made
+// from the FP32 pressure, not solved by this path) starts no history.
+static int warm_start_p64(ss_sim* s, int mode, bool fresh, cudaStream_t st) {
+    if (mode != 1 || fresh) {
+        s->prev_ok = 0;
+        return SS_OK;
+    }
+    if (!s->p64c) CU(cudaMalloc((void**)&s->p64c, s->ncell * sizeof(double)), "cudaMalloc(p64c)");
+    if (!s->prev_ok) {
+        CU(cudaMemcpyAsync(s->p64c, s->p64, s->ncell * sizeof(double), cudaMemcpyDeviceToDevice, st), "warm start copy");
+        s->prev_ok = 1;
+        return SS_OK;
+    }
+    return launch_p64_extrapolate(s, st);
+}
+
 // Mixed-precision projection: iterative refinement of the FP64 pressure with
 // FP32 V-cycles on the FP64 residual (k_mixed.cu).  Each refinement step
 // counts as one V-cycle in the statistics.
@@ -848,7 +869,9 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
     const bool tol_mode = mg.tol > 0.0;
     const bool stats = p->collect_stats || tol_mode;
     TRY(launch_divergence(s, true, stats ? SLOT_DIV_BEFORE : -1, st));
-    if (!s->p64_valid) TRY(launch_p64_from_p0(s, st));
+    const bool fresh = !s->p64_valid;
+    if (fresh) TRY(launch_p64_from_p0(s, st));
+    TRY(warm_start_p64(s, mg.warm_start, fresh, st));
     const int cap = mg.n_vcycles > 0 ? mg.n_vcycles : 1;
     int done = 0;
     double db = 0.0, res = 0.0;
@@ -1003,6 +1026,7 @@ static int do_step(ss_sim* s, const ss_params* p, cudaStream_t st, StepSaves* sv
             // the pressure this step's solve produced in an earlier run
             if (f64) {
                 TRY(ensure_mixed(s, p->mg.precision, st));
+                s->prev_ok = 0;
                 CU(cudaMemcpyAsync(s->p64, sv->pres_restore, s->ncell * sizeof(double), cudaMemcpyDeviceToDevice, st),
                    "pressure restore");
                 s->p64_valid = 1;

@@ -110,6 +110,8 @@ struct ss_sim {
     // mixed-precision solve: FP64 level-0 pressure, FP16/BF16 coarse levels
     double* p64 = nullptr;
     double* p64b = nullptr;             // ping-pong partner of p64 (update + residual in one pass)
+    double* p64c = nullptr;             // the extrapolated warm start's p(n-2) (warm_start 1)
+    int prev_ok = 0;                    // p64c holds the pressure the current p64 was solved from
     int p64_parity = 0;                 // which of the two allocations p64 currently is
     int p64_valid = 0;                  // p64 holds the current pressure (else p[0] does)
     int cstore = 0;                     // storage type of cp/cr (SS_PREC_MIXED or SS_PREC_MIXED_BF16)
@@ -235,6 +237,7 @@ int launch_rb_residual_restrict_mixed(ss_sim* s, int prec, cudaStream_t st);
 
 int launch_rb_prolong_mixed(ss_sim* s, int prec, cudaStream_t st);
 int launch_p64_from_p0(ss_sim* s, cudaStream_t st);
+int launch_p64_extrapolate(ss_sim* s, cudaStream_t st);
 int launch_p0_from_p64(ss_sim* s, cudaStream_t st);
 int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate, cudaStream_t st);
 int launch_ir_accumulate(ss_sim* s, cudaStream_t st);

@@ -190,3 +190,52 @@ def test_mixed_coarse_sweeps_bitwise(monkeypatch, name, dim, n, nch, enc, mc):
         g.step(p)
         o.step(p)
         assert_same(g, o, dim, f"coarse sweeps step {k}")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,dim,n,nch,enc,mc", [MIXED_GRIDS[0], MIXED_GRIDS[1], MIXED_GRIDS[4], MIXED_GRIDS[5]])
+@pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_MIXED_BF16])
+def test_extrapolated_warm_start_bitwise(name, dim, n, nch, enc, mc, prec):
+    """warm_start = 1: from the third consecutive mixed solve on, the solve
+    starts from 2 p(n-1) - p(n-2).  Tolerance solves over six steps, then the
+    history is broken and rebuilt twice - a step with warm_start = 0, a new
+    pressure field - and each time the GPU follows the oracle bit for bit,
+    refinement-step counts included."""
+    g, o = make_pair(dim, n, nch, enc, seed=37, min_coarse=mc)
+    p = scene.workload_params(ref_quirks=0, precision=prec, tol=1e-6, n_vcycles=40, n_coarse=12, collect_stats=1,
+                              warm_start=1)
+    p0 = scene.workload_params(ref_quirks=0, precision=prec, tol=1e-6, n_vcycles=40, n_coarse=12, collect_stats=1)
+    rng = np.random.default_rng(5)
+
+    def both(params, label):
+        g.step(params)
+        o.step(params)
+        assert_same(g, o, dim, label)
+        assert g.stats().vcycles == o.stats().vcycles, (label, g.stats().vcycles, o.stats().vcycles)
+
+    for k in range(6):
+        both(p, f"extrapolated step {k}")
+    both(p0, "plain warm start")
+    for k in range(3):
+        both(p, f"after plain step {k}")
+    pr = (0.01 * rng.standard_normal(int(np.prod(g.shape(abi.FIELD_PRESSURE))))).astype(np.float32)
+    g.set_field(abi.FIELD_PRESSURE, pr)
+    o.set_field(abi.FIELD_PRESSURE, pr)
+    for k in range(3):
+        both(p, f"after a new pressure step {k}")
+
+
+@pytest.mark.gpu
+def test_adjoint_rejects_extrapolated_warm_start():
+    from smokesim_b200 import Sim, SmokeSimError
+    from smokesim_b200.adjoint import Rollout
+    sc = scene.rollout64(seed=1, n=16)
+    g = Sim(sc["desc"])
+    scene.apply(g, sc)
+    ro = Rollout(g, 2, 1)
+    p = scene.workload_params(ref_quirks=0, precision=abi.PREC_MIXED, n_vcycles=2, warm_start=1)
+    with pytest.raises(SmokeSimError) as e:
+        ro.forward(p, np.zeros((2, 3), np.float32))
+    assert e.value.code == abi.SS_E_UNSUPPORTED
+    ro.close()
+    g.close()

@@ -296,3 +296,27 @@ def test_render_known_answers(oracle_mod):
     img2 = o2.render(d)
     amb = np.round(np.array([0.678, 0.847, 0.902]) * 255).astype(np.uint8)
     assert (img2[..., :3] == amb).all() and (img2[..., 3] == 255).all()
+
+
+def test_extrapolated_warm_start_saves_refinement_steps(oracle_mod):
+    """The mixed solve to 1e-6 on the GRF plume at 32^3: once the start-up
+    transient is over, starting from 2 p(n-1) - p(n-2) (warm_start = 1) needs
+    fewer refinement steps than starting from p(n-1); the first two solves,
+    without a history, are the same."""
+    counts = {}
+    for ws in (0, 1):
+        sc = scene.grf256(seed=0, n=32)
+        sc.pop("rng", None)
+        o = oracle_mod.OracleSim(sc["desc"])
+        scene.apply(o, sc)
+        p = scene.workload_params(ref_quirks=0, precision=abi.PREC_MIXED, tol=1e-6, n_vcycles=40, collect_stats=1,
+                                  warm_start=ws)
+        vc = []
+        for _ in range(16):
+            o.step(p)
+            vc.append(o.stats().vcycles)
+            assert o.stats().converged == 1
+        counts[ws] = vc
+        o.close()
+    assert counts[0][:2] == counts[1][:2]
+    assert sum(counts[1][10:]) < sum(counts[0][10:]), counts
