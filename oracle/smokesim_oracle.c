@@ -1552,6 +1552,9 @@ int og_set_field(og_sim* s, int f, const float* src, size_t count) {
         real* d = field_ptr(s, f, c, &n);
         for (size_t i = 0; i < n; ++i) d[i] = (real)src[c * n + i];
     }
+    /* a new pressure is the mixed solve's next warm start (its FP64 copy and
+     * history are dropped), as the GPU path's ss_set_field does */
+    if (f == SS_FIELD_PRESSURE) s->p64_valid = 0;
     return 0;
 }
 int og_set_field_f64(og_sim* s, int f, const double* src, size_t count) {
@@ -1562,6 +1565,9 @@ int og_set_field_f64(og_sim* s, int f, const double* src, size_t count) {
         real* d = field_ptr(s, f, c, &n);
         for (size_t i = 0; i < n; ++i) d[i] = (real)src[c * n + i];
     }
+    /* a new pressure is the mixed solve's next warm start (its FP64 copy and
+     * history are dropped), as the GPU path's ss_set_field does */
+    if (f == SS_FIELD_PRESSURE) s->p64_valid = 0;
     return 0;
 }
 int og_get_field(og_sim* s, int f, float* dst, size_t count) {

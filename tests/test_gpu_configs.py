@@ -58,15 +58,19 @@ def test_plume3d_128_steps_bitwise():
     _step_and_compare(g, o, sc["params"], 2, "plume3d 128")
 
 
-@pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_MIXED_BF16])
-def test_grf128_mixed_tolerance_steps_bitwise(prec):
+@pytest.mark.parametrize("prec,warm_start,steps", [(abi.PREC_MIXED, 0, 2), (abi.PREC_MIXED_BF16, 0, 2),
+                                                   (abi.PREC_MIXED, 1, 4)])
+def test_grf128_mixed_tolerance_steps_bitwise(prec, warm_start, steps):
     """The benchmark's headline variant (mixed-precision projection to a
     projected divergence of 1e-6, cap 40) on its Gaussian-random-field scene
-    at 128^3: the same refinement steps and the same bits as the oracle."""
+    at 128^3: the same refinement steps and the same bits as the oracle.  With
+    warm_start = 1 the third and fourth solves start from the extrapolated
+    pressure 2 p(n-1) - p(n-2)."""
     sc = scene.grf256(seed=0, n=128, with_grf=True)
     g, o = _pair(sc)
-    p = scene.workload_params(ref_quirks=0, precision=prec, tol=1e-6, n_vcycles=40, collect_stats=1)
-    _step_and_compare(g, o, p, 2, f"grf128 mixed {prec}")
+    p = scene.workload_params(ref_quirks=0, precision=prec, tol=1e-6, n_vcycles=40, collect_stats=1,
+                              warm_start=warm_start)
+    _step_and_compare(g, o, p, steps, f"grf128 mixed {prec} warm start {warm_start}")
     assert g.stats().converged == 1
 
 

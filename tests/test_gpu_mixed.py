@@ -197,14 +197,15 @@ def test_mixed_coarse_sweeps_bitwise(monkeypatch, name, dim, n, nch, enc, mc):
 @pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_MIXED_BF16])
 def test_extrapolated_warm_start_bitwise(name, dim, n, nch, enc, mc, prec):
     """warm_start = 1: from the third consecutive mixed solve on, the solve
-    starts from 2 p(n-1) - p(n-2).  Tolerance solves over six steps, then the
+    starts from 2 p(n-1) - p(n-2).  Six steps of 4 refinement steps, then the
     history is broken and rebuilt twice - a step with warm_start = 0, a new
-    pressure field - and each time the GPU follows the oracle bit for bit,
-    refinement-step counts included."""
+    pressure field - and each time the GPU follows the oracle bit for bit.
+    (The random test state is not smooth in time, so a tolerance solve from an
+    extrapolated start can take many refinement steps here; the tolerance form
+    runs on the benchmark scene in test_gpu_configs.py.)"""
     g, o = make_pair(dim, n, nch, enc, seed=37, min_coarse=mc)
-    p = scene.workload_params(ref_quirks=0, precision=prec, tol=1e-6, n_vcycles=40, n_coarse=12, collect_stats=1,
-                              warm_start=1)
-    p0 = scene.workload_params(ref_quirks=0, precision=prec, tol=1e-6, n_vcycles=40, n_coarse=12, collect_stats=1)
+    p = scene.workload_params(ref_quirks=0, precision=prec, n_vcycles=4, n_coarse=12, collect_stats=1, warm_start=1)
+    p0 = scene.workload_params(ref_quirks=0, precision=prec, n_vcycles=4, n_coarse=12, collect_stats=1)
     rng = np.random.default_rng(5)
 
     def both(params, label):
