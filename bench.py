@@ -183,13 +183,16 @@ def cpu_step_rate(sc, steps, warmup):
     for _ in range(warmup):
         o.step(sc["params"])
     times = []
+    vcycles = []
     for _ in range(steps):
         t0 = time.perf_counter()
         o.step(sc["params"])
         times.append(time.perf_counter() - t0)
+        vcycles.append(o.stats().vcycles)
     n = sc["desc"].n
     cells = n[0] * n[1] * n[2]
     sec = statistics.median(times)
+    cpu_step_rate.vcycles = vcycles   # refinement steps (V-cycles) of the sampled steps
     return cells / sec / 1e6, sec, oracle.num_threads(), o
 
 
@@ -215,11 +218,13 @@ def run_reference(args):
         if time.perf_counter() - t_start > REFERENCE_BUDGET_S / 4:
             break
     times = []
+    vcycles = []
     t_timed = time.perf_counter()
     for _ in range(args.steps):
         t0 = time.perf_counter()
         o.step(sc["params"])
         times.append(time.perf_counter() - t0)
+        vcycles.append(o.stats().vcycles)
         if time.perf_counter() - t_start > REFERENCE_BUDGET_S:
             break
     total = time.perf_counter() - t_timed
@@ -239,6 +244,7 @@ def run_reference(args):
                          "sample": f"{k} consecutive full {args.n}^3 steps after {w} warm-up steps, from the "
                                    f"workload's initial state (the steps that fit in {REFERENCE_BUDGET_S:.0f} s)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "vcycles_mean": sum(vcycles) / max(1, len(vcycles)),
         "note": "the reference's own GLSL compute path needs an OpenGL 4.6 context: unavailable on this box; this "
                 "arm runs the C/OpenMP restatement of its compute shaders (oracle/) on all host threads, with the "
                 "same step as the GPU arm: the reference's stage order, boundary rules and red-black ordering, "
@@ -714,7 +720,9 @@ def main():
         cv, csec, threads, o = cpu_step_rate(sc, PARITY_STEPS, 0)
         line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"median of the first {PARITY_STEPS} full {args.n}^3 steps of the same "
-                                          f"variant from the initial state, C/OpenMP oracle"}
+                                          f"variant from the initial state, C/OpenMP oracle (start-up steps: "
+                                          f"more refinement steps than the timed GPU steps, see vcycles)",
+                                "vcycles": list(cpu_step_rate.vcycles)}
         line["parity"] = step_parity(sc, o, stream)
     if rank == 0:
         print(json.dumps(line), flush=True)
