@@ -560,37 +560,63 @@ __global__ void __launch_bounds__(kMT) k_vorticity_march(FluidArgs a, float inv_
         }
     };
     const float two_h = 2.f * a.c.vort_k;
+    // This thread's (at most two) cells of the |w| tile, fixed for the
+    // launch: halo index i = hy * kHW + hx.  The rows of the u / v, w rings
+    // are one / two floats wider than the tile's, so a cell's ring offsets
+    // are i + hy and i + 2 hy; only the ring slots change from plane to plane.
+    constexpr int kHN = kHW * kHH;
+    int hrow[2], fxy[2];
+    bool hin[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int i = tid + j * kMT;
+        hrow[j] = i / kHW;
+        const int hx = i - hrow[j] * kHW;
+        const int x = x0 - 1 + hx, y = y0 - 1 + hrow[j];
+        hin[j] = i < kHN && x >= 0 && y >= 0 && x < nx && y < ny;
+        fxy[j] = y * nx + x;
+    }
+    const int pl = nx * ny;
     // w and |w| of plane k from the rings (planes k-1 .. k+1 resident)
     auto vorticity_plane = [&](int k) {
         const int sm = (k + 3) & 3, s0 = (k + 4) & 3, sp = (k + 5) & 3;
-        for (int i = tid; i < kHW * kHH; i += kMT) {
-            const int hx = i % kHW, hy = i / kHW;
-            const int x = x0 - 1 + hx, y = y0 - 1 + hy;
+        const float* U0 = &S.u[s0][0][0];
+        const float* Um = &S.u[sm][0][0];
+        const float* Up = &S.u[sp][0][0];
+        const float* V0 = &S.v[s0][0][0];
+        const float* Vm = &S.v[sm][0][0];
+        const float* Vp = &S.v[sp][0][0];
+        const float* W0 = &S.w[s0][0][0];
+        const float* Wp = &S.w[sp][0][0];
+        float* M0 = &S.m[s0][0][0];
+        float* O = &S.o[k & 1][0][0][0];
+        const bool kin = k >= 0 && k < nz;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int i = tid + j * kMT;
+            if (i >= kHN) break;
+            const int hy = hrow[j], hx = i - hy * kHW;
+            const int ub = i + hy, vb = i + 2 * hy;
             float o0 = 0.f, o1 = 0.f, o2 = 0.f, m = 0.f;
-            if (x >= 0 && y >= 0 && k >= 0 && x < nx && y < ny && k < nz &&
-                !(a.flags[idx3(x, y, k, nx, ny)] & F_SOLID)) {
-#define CCX(SL, R, C) ((S.u[SL][R][C] + S.u[SL][R][(C) + 1]) * 0.5f)
-#define CCY(SL, R, C) ((S.v[SL][R][C] + S.v[SL][(R) + 1][C]) * 0.5f)
-#define CCZ(R, C) ((S.w[s0][R][C] + S.w[sp][R][C]) * 0.5f)
-                const float x1 = CCZ(hy + 2, hx + 1) - CCZ(hy, hx + 1);
-                const float x2 = CCY(sp, hy, hx + 1) - CCY(sm, hy, hx + 1);
-                const float y1 = CCX(sp, hy + 1, hx) - CCX(sm, hy + 1, hx);
-                const float y2 = CCZ(hy + 1, hx + 2) - CCZ(hy + 1, hx);
-                const float z1 = CCY(s0, hy, hx + 2) - CCY(s0, hy, hx);
-                const float z2 = CCX(s0, hy + 2, hx) - CCX(s0, hy, hx);
-#undef CCX
-#undef CCY
-#undef CCZ
+            if (hin[j] && kin && !(a.flags[k * pl + fxy[j]] & F_SOLID)) {
+                const float x1 = ((W0[vb + 2 * kWW + 1] + Wp[vb + 2 * kWW + 1]) * 0.5f) -
+                                 ((W0[vb + 1] + Wp[vb + 1]) * 0.5f);
+                const float x2 = ((Vp[vb + 1] + Vp[vb + kVW + 1]) * 0.5f) - ((Vm[vb + 1] + Vm[vb + kVW + 1]) * 0.5f);
+                const float y1 = ((Up[ub + kUW] + Up[ub + kUW + 1]) * 0.5f) - ((Um[ub + kUW] + Um[ub + kUW + 1]) * 0.5f);
+                const float y2 = ((W0[vb + kWW + 2] + Wp[vb + kWW + 2]) * 0.5f) - ((W0[vb + kWW] + Wp[vb + kWW]) * 0.5f);
+                const float z1 = ((V0[vb + 2] + V0[vb + kVW + 2]) * 0.5f) - ((V0[vb] + V0[vb + kVW]) * 0.5f);
+                const float z2 = ((U0[ub + 2 * kUW] + U0[ub + 2 * kUW + 1]) * 0.5f) - ((U0[ub] + U0[ub + 1]) * 0.5f);
                 o0 = POW2 ? (x1 - x2) * inv_2h : (x1 - x2) / two_h;
                 o1 = POW2 ? (y1 - y2) * inv_2h : (y1 - y2) / two_h;
                 o2 = POW2 ? (z1 - z2) * inv_2h : (z1 - z2) / two_h;
                 m = sqrtf(o0 * o0 + o1 * o1 + o2 * o2);
             }
-            S.m[s0][hy][hx] = m;
+            M0[i] = m;
             if (hx >= 1 && hy >= 1 && hx <= kMX && hy <= kMY) {
-                S.o[k & 1][0][hy - 1][hx - 1] = o0;
-                S.o[k & 1][1][hy - 1][hx - 1] = o1;
-                S.o[k & 1][2][hy - 1][hx - 1] = o2;
+                const int ob = i - 2 * hy - kMX - 1;   // (hy - 1) * kMX + hx - 1
+                O[ob] = o0;
+                O[kMT + ob] = o1;
+                O[2 * kMT + ob] = o2;
             }
         }
     };
@@ -607,6 +633,11 @@ __global__ void __launch_bounds__(kMT) k_vorticity_march(FluidArgs a, float inv_
     const int tx = tid % kMX, ty = tid / kMX;
     const int x = x0 + tx, y = y0 + ty;
     const float eps = 1e-20f;
+    // this thread's ring offsets and output indices in the x-y plane
+    const int mo = (ty + 1) * kHW + tx;
+    const int uo_s = (ty + 2) * kUW + tx + 1, vo_s = (ty + 1) * kVW + tx + 2, wo_s = (ty + 2) * kWW + tx + 2;
+    const int pu_o = (nx + 1) * ny, pv_o = nx * (ny + 1);
+    const int uxy = y * (nx + 1) + x, vxy = y * nx + x;
     for (int z = zb; z < ze; ++z) {
         store_plane(z + 2);
         if (z + 1 < ze) fetch_plane(z + 3);
@@ -615,29 +646,35 @@ __global__ void __launch_bounds__(kMT) k_vorticity_march(FluidArgs a, float inv_
         __syncthreads();
         if (x < nx && y < ny) {
             const int sm = (z + 3) & 3, s0 = (z + 4) & 3, sp = (z + 5) & 3;
-            const float dx = S.m[s0][ty + 1][tx + 2] - S.m[s0][ty + 1][tx];
-            const float dy = S.m[s0][ty + 2][tx + 1] - S.m[s0][ty][tx + 1];
-            const float dz = S.m[sp][ty + 1][tx + 1] - S.m[sm][ty + 1][tx + 1];
+            const float* M0 = &S.m[s0][0][0];
+            const float dx = M0[mo + 2] - M0[mo];
+            const float dy = M0[mo + kHW + 1] - M0[mo - kHW + 1];
+            const float dz = (&S.m[sp][0][0])[mo + 1] - (&S.m[sm][0][0])[mo + 1];
             const float gx = POW2 ? dx * inv_2h : dx / two_h;
             const float gy = POW2 ? dy * inv_2h : dy / two_h;
             const float gz = POW2 ? dz * inv_2h : dz / two_h;
             const float len = sqrtf(gx * gx + gy * gy + gz * gz) + eps;
             const float nxv = gx / len, nyv = gy / len, nzv = gz / len;
-            const float o0 = S.o[z & 1][0][ty][tx], o1 = S.o[z & 1][1][ty][tx], o2 = S.o[z & 1][2][ty][tx];
+            const float* O = &S.o[z & 1][0][0][0];
+            const float o0 = O[tid], o1 = O[kMT + tid], o2 = O[2 * kMT + tid];
             const float f0 = nyv * o2 - o1 * nzv, f1 = nzv * o0 - o2 * nxv, f2 = nxv * o1 - o0 * nyv;
             const float k = a.c.eps, vk = a.c.vort_k, dt = a.c.dt, rho = a.c.rho;
             auto term = [&](float f) {
                 const float t = f * 0.5f * k * vk * dt;
                 return POW2 ? t * inv_rho : t / rho;
             };
-            a.uo[idx3(x, y, z, nx + 1, ny)] = S.u[s0][ty + 2][tx + 1] + term(f0);
-            a.vo[idx3(x, y, z, nx, ny + 1)] = S.v[s0][ty + 1][tx + 2] + term(f1);
-            a.wo[idx3(x, y, z, nx, ny)] = S.w[s0][ty + 2][tx + 2] + term(f2);
+            const float* U0 = &S.u[s0][0][0];
+            const float* V0 = &S.v[s0][0][0];
+            const float* W0 = &S.w[s0][0][0];
+            const int ui = z * pu_o + uxy, vi = z * pv_o + vxy, wi = z * pl + vxy;
+            a.uo[ui] = U0[uo_s] + term(f0);
+            a.vo[vi] = V0[vo_s] + term(f1);
+            a.wo[wi] = W0[wo_s] + term(f2);
             // faces past the last cell: the force there is +0 (w = 0 outside the grid)
             const float zero_term = term(0.f);
-            if (x == nx - 1) a.uo[idx3(nx, y, z, nx + 1, ny)] = S.u[s0][ty + 2][tx + 2] + zero_term;
-            if (y == ny - 1) a.vo[idx3(x, ny, z, nx, ny + 1)] = S.v[s0][ty + 2][tx + 2] + zero_term;
-            if (z == nz - 1) a.wo[idx3(x, y, nz, nx, ny)] = S.w[sp][ty + 2][tx + 2] + zero_term;
+            if (x == nx - 1) a.uo[ui + 1] = U0[uo_s + 1] + zero_term;
+            if (y == ny - 1) a.vo[vi + nx] = V0[vo_s + kVW] + zero_term;
+            if (z == nz - 1) a.wo[wi + pl] = (&S.w[sp][0][0])[wo_s] + zero_term;
         }
     }
 }
