@@ -262,29 +262,77 @@ __global__ void __launch_bounds__(256) k_advect_velocity(FluidArgs a) {
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const float cfl = a.c.cfl;
+    // linear indices of position (x, y, z) in the cell / w array (c), the u
+    // array and the v array, and the plane sizes: every tap of the face
+    // averages below is one of these plus a fixed offset
+    const int zy = z * ny + y;
+    const int c = zy * nx + x;
+    const int iu = c + zy, iv = c + z * nx;
+    const int ux = nx + 1, pl = nx * ny, plu = ux * ny, plv = nx * (ny + 1);
+    const bool in_cell = x < nx && y < ny && z < nz;
     // solid flags of this cell and of its -x, -y, -z neighbours (out of grid = solid)
-    const bool s_c = solid_oob1(a.flags, x, y, z, nx, ny, nz);
+    const bool s_c = !in_cell || (a.flags[c] & F_SOLID);
     // every tap of the face velocities below lies inside the arrays
-    const bool interior = x >= 1 && y >= 1 && (DIM == 2 || z >= 1) && x < nx && y < ny && z < nz;
+    const bool interior = x >= 1 && y >= 1 && (DIM == 2 || z >= 1) && in_cell;
 #pragma unroll
     for (int comp = 0; comp < DIM; ++comp) {
         const int ax = nx + (comp == 0), ay = ny + (comp == 1), az = nz + (comp == 2);
         if (x >= ax || y >= ay || z >= az) continue;
         const float* __restrict__ src = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
         float* __restrict__ dst = comp == 0 ? a.uo : comp == 1 ? a.vo : a.wo;
-        const int i = idx3(x, y, z, ax, ay);
+        const int i = comp == 0 ? iu : comp == 1 ? iv : c;
         const int id = comp == 0 ? x : comp == 1 ? y : z;
+        // the cell on the face's low side: out of grid (id == 0) counts solid
+        const bool s_lo = id == 0 || (a.flags[c - (comp == 0 ? 1 : comp == 1 ? nx : pl)] & F_SOLID);
         float out;
         if (id == 0 && a.c.wind[comp] != 0.f) {
             out = a.c.wind[comp];
-        } else if (s_c || solid_oob1(a.flags, x - (comp == 0), y - (comp == 1), z - (comp == 2), nx, ny, nz)) {
+        } else if (s_c || s_lo) {
             out = 0.f;
         } else {
             float vel[3];
-            if (interior) vel_at_face_interior<DIM>(a.u, a.v, a.w, nx, ny, nz, comp, x, y, z, vel);
-            else if (comp == 0) vel_at_xface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
-            else if (comp == 1) vel_at_yface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
-            else vel_at_zface(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+            if (interior) {
+                // vel_at_face_interior's values, its taps addressed from i, c
+                if (comp == 0) {
+                    vel[0] = __ldg(a.u + iu);
+                    const float* pv = a.v + iv - 1;
+                    vel[1] = lerp_(lerp_(__ldg(pv), __ldg(pv + 1), 0.5f), lerp_(__ldg(pv + nx), __ldg(pv + nx + 1), 0.5f),
+                                   0.5f);
+                    if constexpr (DIM == 3) {
+                        const float* pw = a.w + c - 1;
+                        vel[2] = lerp_(lerp_(__ldg(pw), __ldg(pw + 1), 0.5f),
+                                       lerp_(__ldg(pw + pl), __ldg(pw + pl + 1), 0.5f), 0.5f);
+                    } else {
+                        vel[2] = 0.f;
+                    }
+                } else if (comp == 1) {
+                    const float* pu = a.u + iu - ux;
+                    vel[0] = lerp_(lerp_(__ldg(pu), __ldg(pu + 1), 0.5f), lerp_(__ldg(pu + ux), __ldg(pu + ux + 1), 0.5f),
+                                   0.5f);
+                    vel[1] = __ldg(a.v + iv);
+                    if constexpr (DIM == 3) {
+                        const float* pw = a.w + c - nx;
+                        vel[2] = lerp_(lerp_(__ldg(pw), __ldg(pw + nx), 0.5f),
+                                       lerp_(__ldg(pw + pl), __ldg(pw + pl + nx), 0.5f), 0.5f);
+                    } else {
+                        vel[2] = 0.f;
+                    }
+                } else {
+                    const float* pu = a.u + iu - plu;
+                    vel[0] = lerp_(lerp_(__ldg(pu), __ldg(pu + 1), 0.5f), lerp_(__ldg(pu + plu), __ldg(pu + plu + 1), 0.5f),
+                                   0.5f);
+                    const float* pv = a.v + iv - plv;
+                    vel[1] = lerp_(lerp_(__ldg(pv), __ldg(pv + nx), 0.5f), lerp_(__ldg(pv + plv), __ldg(pv + plv + nx), 0.5f),
+                                   0.5f);
+                    vel[2] = __ldg(a.w + c);
+                }
+            } else if (comp == 0) {
+                vel_at_xface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+            } else if (comp == 1) {
+                vel_at_yface<DIM>(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+            } else {
+                vel_at_zface(a.u, a.v, a.w, nx, ny, nz, x, y, z, vel);
+            }
             const float gx = (float)x + (comp == 0 ? 0.f : 0.5f);
             const float gy = (float)y + (comp == 1 ? 0.f : 0.5f);
             const float gz = DIM == 3 ? (float)z + (comp == 2 ? 0.f : 0.5f) : 0.f;
@@ -295,7 +343,10 @@ __global__ void __launch_bounds__(256) k_advect_velocity(FluidArgs a) {
         }
         if constexpr (BUOY) {
             if (comp == 1) {
-                if (solid_oob0(a.flags, x, y, z, nx, ny, nz) || solid_oob0(a.flags, x, y - 1, z, nx, ny, nz)) {
+                // the y face's two cells (out of grid = fluid)
+                const bool solid_hi = y < ny && in_cell && (a.flags[c] & F_SOLID);
+                const bool solid_lo = y > 0 && x < nx && z < nz && (a.flags[c - nx] & F_SOLID);
+                if (solid_hi || solid_lo) {
                     out = __ldg(src + i);
                 } else {
                     const size_t ncell = (size_t)nx * ny * nz;
@@ -854,15 +905,19 @@ __global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a, DivFold df, i
     const int zb = blockIdx.z * planes, ze = min(zb + planes, nz);
     const size_t ncell = (size_t)nx * ny * nz;
     double acc = 0.0;
+    // linear indices in the x-y plane; a plane adds pl (cells, w), plu (u), plv (v)
+    const int pl = nx * ny, plu = (nx + 1) * ny, plv = nx * (ny + 1);
+    const int cxy = y * nx + x, uxy = y * (nx + 1) + x;
     for (int z = zb; z < ze && x < nx && y < ny; ++z) {
-        const int c = idx3(x, y, z, nx, ny);
+        const int c = z * pl + cxy;
+        const int iu = z * plu + uxy, iv = z * plv + cxy;
         // the cell's faces always exist: loaded before the solid test
-        const float f_left = __ldg(a.u + idx3(x, y, z, nx + 1, ny)), f_right = __ldg(a.u + idx3(x + 1, y, z, nx + 1, ny));
-        const float f_bottom = __ldg(a.v + idx3(x, y, z, nx, ny + 1)), f_top = __ldg(a.v + idx3(x, y + 1, z, nx, ny + 1));
+        const float f_left = __ldg(a.u + iu), f_right = __ldg(a.u + iu + 1);
+        const float f_bottom = __ldg(a.v + iv), f_top = __ldg(a.v + iv + nx);
         float f_back = 0.f, f_front = 0.f;
         if constexpr (DIM == 3) {
-            f_back = __ldg(a.w + idx3(x, y, z, nx, ny));
-            f_front = __ldg(a.w + idx3(x, y, z + 1, nx, ny));
+            f_back = __ldg(a.w + c);
+            f_front = __ldg(a.w + c + pl);
         }
         // vel_at_centre's values
         const float vel[3] = {lerp_(f_left, f_right, 0.5f), lerp_(f_bottom, f_top, 0.5f),
@@ -881,7 +936,6 @@ __global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a, DivFold df, i
             const float v_left = (fl & F_LEFT) ? (sv ? a.sv0[c - 1] : 0.f) : f_left;
             float d = v_right - v_left + v_top - v_bottom;
             if constexpr (DIM == 3) {
-                const int pl = nx * ny;
                 const float v_front = (fl & F_FRONT) ? (sv ? a.sv2[c + pl] : 0.f) : f_front;
                 const float v_back = (fl & F_BACK) ? (sv ? a.sv2[c - pl] : 0.f) : f_back;
                 d = d + v_front - v_back;
@@ -892,9 +946,27 @@ __global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a, DivFold df, i
         const float cfl = a.c.cfl;
         const float bx = gx - vel[0] * cfl, by = gy - vel[1] * cfl, bz = gz - vel[2] * cfl;
         const Taps t = make_taps<DIM>(nx, ny, nz, bx - 0.5f, by - 0.5f, bz - 0.5f);
-        for (int ch = 0; ch < a.nch; ++ch)
-            a.dens_o[ch * ncell + c] = sample_taps_fast<DIM>(a.dens + ch * ncell, nx, ny, nz, t, 0.f);
-        a.temp_o[c] = sample_taps_fast<DIM>(a.temp, nx, ny, nz, t, a.c.t_amb);
+        // sample_taps_fast's values, its range test and base index formed once
+        // for every channel
+        const bool tin = t.x0 >= 0 && t.x0 + 1 < nx && t.y0 >= 0 && t.y0 + 1 < ny &&
+                         (DIM == 2 || (t.z0 >= 0 && t.z0 + 1 < nz));
+        const int tb = tin ? idx3(t.x0, t.y0, t.z0, nx, ny) : 0;
+        auto sample = [&](const float* __restrict__ f, float border) -> float {
+            if (!tin) return sample_taps<DIM>(f, nx, ny, nz, t, border);
+            const float* q = f + tb;
+            const float c00 = __ldg(q), c10 = __ldg(q + 1), c01 = __ldg(q + nx), c11 = __ldg(q + nx + 1);
+            if constexpr (DIM == 2) {
+                return lerp_(lerp_(c00, c10, t.wx), lerp_(c01, c11, t.wx), t.wy);
+            } else {
+                const float d00 = __ldg(q + pl), d10 = __ldg(q + pl + 1), d01 = __ldg(q + pl + nx),
+                            d11 = __ldg(q + pl + nx + 1);
+                const float c0 = lerp_(lerp_(c00, c10, t.wx), lerp_(c01, c11, t.wx), t.wy);
+                const float c1 = lerp_(lerp_(d00, d10, t.wx), lerp_(d01, d11, t.wx), t.wy);
+                return lerp_(c0, c1, t.wz);
+            }
+        };
+        for (int ch = 0; ch < a.nch; ++ch) a.dens_o[ch * ncell + c] = sample(a.dens + ch * ncell, 0.f);
+        a.temp_o[c] = sample(a.temp, a.c.t_amb);
     }
     if constexpr (DIV) {
         const double bs = block_sum(acc);
