@@ -115,7 +115,7 @@ static void free_sim(ss_sim* s) {
     cudaFree(s->d_em);
     cudaFree(s->d_ob);
     cudaFree(s->d_bx);
-    cudaFree(s->d_err);
+    if (s->chain_stream) cudaStreamDestroy(s->chain_stream);
     delete s;
 }
 
@@ -216,6 +216,11 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     // launch per level operation instead of one thread-block cluster launch;
     // the results are the same.
     if (const char* e = getenv("SMOKESIM_CLUSTER")) s->use_cluster = atoi(e) ? 1 : 0;
+    // SMOKESIM_DEVICE_LOOP=0 runs the mixed solve's tolerance loop on the
+    // host, reading the residual back after every refinement step, instead of
+    // as conditional graph nodes whose residual kernel tests convergence on
+    // the device; the results are the same.
+    if (const char* e = getenv("SMOKESIM_DEVICE_LOOP")) s->device_loop = atoi(e) ? 1 : 0;
     s->nv[0] = (size_t)(s->nx + 1) * s->ny * s->nz;
     s->nv[1] = (size_t)s->nx * (s->ny + 1) * s->nz;
     s->nv[2] = s->dim == 3 ? (size_t)s->nx * s->ny * (s->nz + 1) : 0;
@@ -277,7 +282,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
     s->red.stage2 = s->red.max_blocks / 1024 + 2;
     A((void**)&s->red.partial2, (size_t)2 * s->red.stage2 * sizeof(double));
     A((void**)&s->red.out, SLOT_COUNT * sizeof(double));
-    A((void**)&s->d_err, sizeof(int));
+    if (rc == SS_OK) s->d_err = reinterpret_cast<int*>(s->red.out + SLOT_ERR);
     A((void**)&s->red.ticket, sizeof(unsigned int));
     if (rc == SS_OK) {
         cudaError_t e = cudaMallocHost((void**)&s->red.host, SLOT_COUNT * sizeof(double));
@@ -299,7 +304,7 @@ int ss_create(const ss_desc* d, void* stream, ss_sim** out) {
         rc = check_cuda(cudaMemsetAsync(s->p[l], 0, n * 4, st), "memset");
         if (!rc) rc = check_cuda(cudaMemsetAsync(s->r[l], 0, n * 4, st), "memset");
     }
-    if (!rc) rc = check_cuda(cudaMemsetAsync(s->d_err, 0, sizeof(int), st), "memset");
+    if (!rc) rc = check_cuda(cudaMemsetAsync(s->red.out, 0, SLOT_COUNT * sizeof(double), st), "memset");
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->red.ticket, 0, sizeof(unsigned int), st), "memset");
     if (!rc) rc = check_cuda(cudaMemsetAsync(s->div0, 0, s->ncell * 4, st), "memset");
     if (!rc && s->div0r != s->div0) rc = check_cuda(cudaMemsetAsync(s->div0r, 0, s->ncell * 4, st), "memset");
@@ -666,13 +671,13 @@ static int v_cycle_rec(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg,
 
 // The device error word collects the bounded waits that gave up (bit 0: a
 // coarse-level sweep's TMA tile load did not arrive in time, so that sweep
-// skipped its cells).  It is read here - by every statistics read of a step,
-// ss_get_stats and ss_get_field - reported once and cleared, so the next
-// report concerns later launches only.
-static int check_device_error(ss_sim* s, cudaStream_t st) {
-    int err = 0;
-    CU(cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "error word");
-    CU(cudaStreamSynchronize(st), "error word sync");
+// skipped its cells).  Only those sweeps (the FP32 solve's coarse levels) set
+// it; a solve that may run them arms s->err_armed.  It is read - with the
+// statistics slots of a step, which hold it, and by ss_get_stats and
+// ss_get_field while armed - reported once and cleared, so the next report
+// concerns later launches only.
+static int report_device_error(ss_sim* s, int err, cudaStream_t st) {
+    s->err_armed = 0;
     if (err) {
         CU(cudaMemsetAsync(s->d_err, 0, sizeof(int), st), "error word clear");
         CU(cudaStreamSynchronize(st), "error word clear");
@@ -684,10 +689,20 @@ static int check_device_error(ss_sim* s, cudaStream_t st) {
     return SS_OK;
 }
 
+static int check_device_error(ss_sim* s, cudaStream_t st) {
+    int err = 0;
+    CU(cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "error word");
+    CU(cudaStreamSynchronize(st), "error word sync");
+    return report_device_error(s, err, st);
+}
+
+// the statistics slots and the error word, in one copy and one synchronisation
 static int read_slots(ss_sim* s, cudaStream_t st) {
     CU(cudaMemcpyAsync(s->red.host, s->red.out, SLOT_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st), "slots");
     CU(cudaStreamSynchronize(st), "slots sync");
-    return check_device_error(s, st);
+    int err = 0;
+    memcpy(&err, &s->red.host[SLOT_ERR], sizeof(int));
+    return report_device_error(s, err, st);
 }
 
 static int ensure_pyramid(ss_sim* s, cudaStream_t st) {
@@ -855,6 +870,131 @@ static int warm_start_p64(ss_sim* s, int mode, bool fresh, cudaStream_t st) {
     return launch_p64_extrapolate(s, st);
 }
 
+// ------------------------------------------------ device-side tolerance loop
+// The mixed solve's tolerance loop as one graph: the first residual, then
+// refinement step 1 as the body of a conditional (IF) graph node, step 2 as an
+// IF node inside step 1's body, and so on, depth steps deep.  The last block
+// of each residual launch applies the host loop's test (k_ir_residual,
+// IrDecide) and sets the condition of the next step, so the steps run back to
+// back with no host round trip between them.  A condition nobody set stays 0
+// (the default, restored at every launch of the graph) and ends the chain:
+// nothing in it can loop.  The steps alternate the FP64 buffers, so the chain
+// is recorded once per starting parity (graphs 4 and 5).
+constexpr int kChainDepth = 8;
+
+static int build_solve_chain(ss_sim* s, const StepConsts& c, const ss_mg_schedule& mg, int depth,
+                             ss_sim::SolveGraph& g) {
+    if (!s->chain_stream)
+        CU(cudaStreamCreateWithFlags(&s->chain_stream, cudaStreamNonBlocking), "cudaStreamCreate(chain)");
+    cudaStream_t cs = s->chain_stream;
+    double* const pa = s->p64;
+    double* const pb = s->p64b;
+    const int pdl = s->pdl;
+    s->pdl = 0;   // plain stream order inside the conditional bodies
+    cudaGraph_t top = nullptr;
+    int rc = check_cuda(cudaGraphCreate(&top, 0), "cudaGraphCreate(solve chain)");
+    cudaGraph_t cur = top;   // the graph that receives step k
+    for (int k = 0; k <= depth && rc == SS_OK; ++k) {
+        IrDecide d;
+        d.tol = mg.tol;
+        d.k = k;
+        d.more = k < depth ? 1 : 0;
+        d.active = 1;
+        if (d.more)
+            rc = check_cuda(cudaGraphConditionalHandleCreate(&d.next, cur, 0, cudaGraphCondAssignDefault),
+                            "cudaGraphConditionalHandleCreate");
+        if (rc == SS_OK)
+            rc = check_cuda(cudaStreamBeginCaptureToGraph(cs, cur, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed),
+                            "cudaStreamBeginCaptureToGraph");
+        if (rc != SS_OK) break;
+        const long long before = s->nlaunch;
+        if (k > 0) rc = v_cycle_mixed(s, c, mg, 0, mg.precision, cs);
+        if (rc == SS_OK) rc = launch_ir_residual(s, c, SLOT_RESIDUAL, k > 0, cs, &d);
+        (k == 0 ? g.launches : g.step_launches) = s->nlaunch - before;
+        cudaGraph_t next = nullptr;
+        if (rc == SS_OK && d.more) {
+            cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nd = 0;
+            rc = check_cuda(cudaStreamGetCaptureInfo(cs, &cst, nullptr, nullptr, &deps, &nd), "cudaStreamGetCaptureInfo");
+            if (rc == SS_OK) {
+                cudaGraphNodeParams np{};
+                np.type = cudaGraphNodeTypeConditional;
+                np.conditional.handle = d.next;
+                np.conditional.type = cudaGraphCondTypeIf;
+                np.conditional.size = 1;
+                cudaGraphNode_t node = nullptr;
+                rc = check_cuda(cudaGraphAddNode(&node, cur, deps, nd, &np), "cudaGraphAddNode(conditional)");
+                if (rc == SS_OK) next = np.conditional.phGraph_out[0];
+            }
+        }
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(cs, &captured);
+        if (rc == SS_OK) rc = check_cuda(ee, "cudaStreamEndCapture(solve chain)");
+        if (k > 0) std::swap(s->p64, s->p64b);
+        cur = next;
+    }
+    s->p64 = pa;
+    s->p64b = pb;
+    s->pdl = pdl;
+    if (rc == SS_OK) {
+        const cudaError_t ei = cudaGraphInstantiate(&g.exec, top, 0);
+        if (ei != cudaSuccess) g.exec = nullptr;
+        rc = check_cuda(ei, "cudaGraphInstantiate(solve chain)");
+    }
+    if (top) cudaGraphDestroy(top);
+    if (rc != SS_OK) {
+        cudaGetLastError();
+        return set_error(rc, g_err +
+                                 " (recording the device-side tolerance loop; SMOKESIM_DEVICE_LOOP=0 runs it on the host)");
+    }
+    return SS_OK;
+}
+
+// The device-side loop needs a stream that graphs can be launched on and that
+// is not being recorded by the caller.
+static bool chain_ok(ss_sim* s, cudaStream_t st) {
+    if (!s->device_loop || !s->use_graphs || st == nullptr) return false;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return false;
+    return cs == cudaStreamCaptureStatusNone;
+}
+
+// Runs up to depth refinement steps of the tolerance loop on the device and
+// reads the statistics slots once; *k = the steps it took.  The FP64 buffers
+// end swapped after an odd number of steps.
+static int run_solve_chain(ss_sim* s, const ss_params* p, const StepConsts& c, int depth, cudaStream_t st,
+                           int* k_out) {
+    const GraphKey key = graph_key(s, 4, s->p64_parity, SLOT_RESIDUAL, depth, p);
+    unsigned char kb[sizeof(s->graphs[0].key)] = {};
+    memcpy(kb, &key, sizeof(GraphKey));
+    ss_sim::SolveGraph& g = s->graphs[4 + s->p64_parity];
+    if (!g.exec || memcmp(g.key, kb, sizeof kb) != 0) {
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+        const long long n0 = s->nlaunch;
+        const int rc = build_solve_chain(s, c, p->mg, depth, g);
+        s->nlaunch = n0;
+        if (rc != SS_OK) return rc;
+        memcpy(g.key, kb, sizeof kb);
+    }
+    CU(cudaGraphLaunch(g.exec, st), "cudaGraphLaunch(solve chain)");
+    TRY(read_slots(s, st));
+    const double kd = s->red.host[SLOT_STEPS];
+    if (!(kd >= 0.0 && kd <= (double)depth))
+        return set_error(SS_E_CUDA, "the device-side tolerance loop reported an impossible step count");
+    const int k = (int)kd;
+    s->nlaunch += g.launches + (long long)k * g.step_launches;
+    if (k & 1) {
+        std::swap(s->p64, s->p64b);
+        s->p64_parity ^= 1;
+    }
+    *k_out = k;
+    return SS_OK;
+}
+
 // Mixed-precision projection: iterative refinement of the FP64 pressure with
 // FP32 V-cycles on the FP64 residual (k_mixed.cu).  Each refinement step
 // counts as one V-cycle in the statistics.
@@ -877,7 +1017,24 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
     double db = 0.0, res = 0.0;
     bool conv = true;
     bool pending = false;   // the last V-cycle's correction is not in p64 yet
-    for (;;) {
+    bool finished = false;
+    if (tol_mode && chain_ok(s, st)) {
+        // the first steps (all of them, as a rule) on the device; where the
+        // chain ends unconverged below the cap, the host loop carries on
+        TRY(run_solve_chain(s, p, c, std::min(cap, kChainDepth), st, &done));
+        db = sqrt(s->red.host[SLOT_DIV_BEFORE]);
+        res = sqrt(s->red.host[SLOT_RESIDUAL]);
+        if (res <= mg.tol * db) {
+            finished = true;
+        } else if (done == cap) {
+            conv = false;
+            finished = true;
+        } else {
+            pending = true;
+            ++done;
+        }
+    }
+    while (!finished) {
         const bool last = !tol_mode && done == cap;
         if (last && !stats) break;
         if (pending) {
@@ -927,6 +1084,7 @@ static int pressure_solve(ss_sim* s, const ss_params* p, const StepConsts& c, cu
     const ss_mg_schedule& mg = p->mg;
     if (mg.precision != SS_PREC_FP32) return pressure_solve_mixed(s, p, c, st, defer_p0);
     s->p64_valid = 0;
+    s->err_armed = 1;   // its coarse-level sweeps may take the bounded-wait TMA form
     const bool tol_mode = mg.tol > 0.0;
     const bool stats = p->collect_stats || tol_mode;
     TRY(ensure_pyramid(s, st));
@@ -1124,7 +1282,7 @@ int ss_set_force_field(ss_sim* s, int n, const float* field, void* stream) {
 int ss_get_stats(ss_sim* s, ss_stats* out) {
     if (!s || !out) return set_error(SS_E_INVALID, "NULL argument");
     *out = s->st;
-    return check_device_error(s, nullptr);
+    return s->err_armed ? check_device_error(s, nullptr) : SS_OK;
 }
 
 // ------------------------------------------------------------ single stages

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
     const float* __restrict__ div0, const uint8_t* __restrict__ fmask, int nx, int ny, int nz, double k,
     double inv_k, double inv_khh, float* __restrict__ rhs_s, float* __restrict__ rhs_r, double* __restrict__ psum,
     double* __restrict__ pmax, unsigned int* __restrict__ ticket, double* __restrict__ out, int slot,
-    float* __restrict__ scale, int planes) {
+    float* __restrict__ scale, int planes, IrDecide dec) {
     pdl_entry();
     __shared__ double sP[2][kIrTY + 2][kIrTX + 2];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kIrTX * ty;
@@ -233,6 +233,13 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
         scale[0] = (float)ldexp(1.0, -e);
         scale[1] = (float)ldexp(1.0, e);
         *ticket = 0u;
+        if (dec.active) {
+            // the host loop's test, on the same doubles: stop once
+            // sqrt(residual) <= tol sqrt(divergence before the solve)
+            out[SLOT_STEPS] = (double)dec.k;
+            const double res = sqrt(fs[0]), db = sqrt(out[SLOT_DIV_BEFORE]);
+            if (dec.more && !(res <= dec.tol * db)) cudaGraphSetConditional(dec.next, 1u);
+        }
     }
 }
 
@@ -279,7 +286,10 @@ int launch_p0_from_p64(ss_sim* s, cudaStream_t st) {
     return check_cuda(cudaGetLastError(), "k_f32_from_p64");
 }
 
-int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate, cudaStream_t st) {
+int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate, cudaStream_t st,
+                       const IrDecide* dec) {
+    const IrDecide d = dec ? *dec : IrDecide{};
+    if (d.active && slot != SLOT_RESIDUAL) return set_error(SS_E_INVALID, "the convergence test reads the residual slot");
     dim3 b(kIrTX, kIrTY, 1);
     const int tx = (s->nx + kIrTX - 1) / kIrTX, ty = (s->ny + kIrTY - 1) / kIrTY;
     const int planes = z_planes((long long)tx * ty, s->nz, kIrChunk);
@@ -295,7 +305,7 @@ int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate
     float* rhs_r = s->rhs_r_is_s ? nullptr : s->rhs_r;
 #define IR_ARGS(ACC) s->p64, s->p_alt[0], s->p64b, s->div0, s->fmask, s->nx, s->ny, s->nz, k, inv_k, inv_khh, \
                      s->rhs_s, rhs_r, s->red.partial, s->red.partial_max, s->red.ticket, s->red.out, slot, \
-                     s->d_scale, planes
+                     s->d_scale, planes, d
     if (s->dim == 3) {
         if (accumulate) launch_k(s->pdl, g, b, 0, st, k_ir_residual<3, true>, IR_ARGS(true));
         else launch_k(s->pdl, g, b, 0, st, k_ir_residual<3, false>, IR_ARGS(false));

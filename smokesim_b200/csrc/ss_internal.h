@@ -62,7 +62,24 @@ struct ReduceSlots {
     double* host;         // pinned mirror of out
     int max_blocks;
 };
-enum { SLOT_DIV_BEFORE = 0, SLOT_RESIDUAL = 1, SLOT_DIV_AFTER = 2, SLOT_AMAX = 3, SLOT_COUNT = 8 };
+// SLOT_STEPS: refinement steps a device-side tolerance loop took (a double);
+// SLOT_ERR: the device error word (an int at the start of the slot), so that
+// one copy of the slots brings both back
+enum { SLOT_DIV_BEFORE = 0, SLOT_RESIDUAL = 1, SLOT_DIV_AFTER = 2, SLOT_AMAX = 3, SLOT_STEPS = 4, SLOT_ERR = 7,
+       SLOT_COUNT = 8 };
+
+// Convergence test of the mixed solve's tolerance loop, folded into the last
+// block of the refinement residual (k_ir_residual): it records k, the
+// refinement steps done, in SLOT_STEPS and, where more is set and the
+// residual norm is above tol times the pre-solve divergence norm, sets the
+// condition of the graph node that runs the next refinement step.
+struct IrDecide {
+    cudaGraphConditionalHandle next = 0;
+    double tol = 0.0;
+    int k = 0;
+    int more = 0;
+    int active = 0;
+};
 
 struct TensorMapEntry {
     CUtensorMap map;
@@ -138,7 +155,8 @@ struct ss_sim {
 
     ss_stats st{};
     long long nlaunch = 0;     // kernels launched since the counter was reset
-    int* d_err = nullptr;      // device error word: bit 0 = a bounded barrier wait gave up
+    int* d_err = nullptr;      // device error word (in red.out[SLOT_ERR]): bit 0 = a bounded barrier wait gave up
+    int err_armed = 0;         // a kernel that can set the error word ran since the word was last read
     int use_tma = 1;           // TMA tile loads of the coarse-level tiled sweeps (0: per-thread loads)
     // mixed solve: the coarsest level by its response matrix instead of its
     // n_coarse sweeps (levels of at most kCoarseResponseMax cells)
@@ -150,14 +168,21 @@ struct ss_sim {
     int cmat_n = 0, cmat_iters = -1, cmat_dirty = 1;
     // The multigrid part of a solve recorded once as a CUDA graph and replayed
     // (api.cpp, run_graph): slot 0 fixed-count FP32 V-cycles, 1 one FP32
-    // tolerance cycle, 2/3 one mixed refinement step per FP64 buffer parity.
+    // tolerance cycle, 2/3 one mixed refinement step per FP64 buffer parity,
+    // 4/5 the mixed tolerance loop on the device per starting parity.
     struct SolveGraph {
         cudaGraphExec_t exec = nullptr;
         unsigned char key[96] = {};
-        long long launches = 0;
+        long long launches = 0;        // kernels of one replay (4/5: of the first residual)
+        long long step_launches = 0;   // 4/5: kernels of one refinement step
     };
-    SolveGraph graphs[4];
+    SolveGraph graphs[6];
     int use_graphs = 1;
+    // mixed solve to a tolerance: the first chain_depth refinement steps as
+    // nested conditional graph nodes, the convergence test on the device
+    // (SMOKESIM_DEVICE_LOOP=0 sets 0: a host round trip per step)
+    int device_loop = 1;
+    cudaStream_t chain_stream = nullptr;   // records the nested step graphs
     // programmatic dependent launch of the solve's kernel chain (SMOKESIM_PDL=0 sets 0)
     int pdl = 1;
     // mixed solve: the levels from cluster_from down in one thread-block
@@ -239,7 +264,8 @@ int launch_rb_prolong_mixed(ss_sim* s, int prec, cudaStream_t st);
 int launch_p64_from_p0(ss_sim* s, cudaStream_t st);
 int launch_p64_extrapolate(ss_sim* s, cudaStream_t st);
 int launch_p0_from_p64(ss_sim* s, cudaStream_t st);
-int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate, cudaStream_t st);
+int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate, cudaStream_t st,
+                       const IrDecide* dec = nullptr);
 int launch_ir_accumulate(ss_sim* s, cudaStream_t st);
 // p0_out: when given, the FP32 copy of the FP64 pressure is written there too
 int launch_update_velocities_p64(ss_sim* s, const StepConsts& c, cudaStream_t st, float* p0_out = nullptr);

@@ -46,12 +46,14 @@ def _scene_for(dim, n, rng):
     return em, ob, bx
 
 
-def make_pair(dim, n, nch, enclosed, seed=0, min_coarse=4, state=True, t_amb=0.0):
+def make_pair(dim, n, nch, enclosed, seed=0, min_coarse=4, state=True, t_amb=0.0, stream=None):
+    """stream: a CUDA stream handle for the library's simulation (the solve
+    records and replays CUDA graphs only on a stream of the caller's)."""
     from oracle.oracle import OracleSim
     from smokesim_b200 import Sim
     desc = abi.make_desc(dim, n, cell_size=1.0, density_channels=nch, enclosed=enclosed, min_coarse=min_coarse,
                          t_ambient=t_amb)
-    g = Sim(desc)
+    g = Sim(desc, stream=stream)
     o = OracleSim(desc)
     rng = scene.Rng(seed)
     em, ob, bx = _scene_for(dim, n, rng)
