@@ -302,16 +302,16 @@ SS_D double fold_sum(const double* p, unsigned int n, unsigned int tid, unsigned
 SS_D float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 SS_D float f4(const float4& v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
 
-// a / f for an integer count f in 1..6, value-identical to the IEEE quotient
-// (the same value; -0 may come back as +0): q0 = a*RN(1/f) followed by one
-// residual correction with fused multiply-adds - the FMA-based correctly
-// rounded division of P. Markstein, "Computation of elementary functions on
-// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990, with the
-// exact reciprocal of a small integer as its start value - verified
-// exhaustively against IEEE division over every finite float a for f = 1..5
-// (tests/division_check.c).
-// For f = 6 it divides a/2 by 3, exact except where a/2 is subnormal, which
-// takes the IEEE path.
+// a / f for an integer count f in 1..6, bit-identical to the IEEE quotient
+// for every finite a: q0 = a*RN(1/f) followed by one residual correction with
+// fused multiply-adds - the FMA-based correctly rounded division of P.
+// Markstein, "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990, with the reciprocal of a small
+// integer as its start value - verified exhaustively against IEEE division
+// over every finite float a for f = 1..6 (tests/division_check.c).  A zero a
+// is returned as it is (the correction would turn -0 into +0).  For f = 6 it
+// divides a/2 by 3, exact except where a/2 is subnormal: |a| < 2^-120 (zeros
+// included) takes the IEEE path.  An infinite a gives NaN.
 SS_D float div_by_count(float a, int f) {
     if (f == 6) {
         // the f = 3 steps below on a/2, written out so the interior cells'
@@ -322,6 +322,7 @@ SS_D float div_by_count(float a, int f) {
         const float r = __fmaf_rn(-3.0f, q0, h);
         return __fmaf_rn(r, 1.0f / 3.0f, q0);
     }
+    if (a == 0.f) return a;
     const float y = f == 1 ? 1.f : f == 2 ? 0.5f : f == 3 ? (1.0f / 3.0f) : f == 4 ? 0.25f : (1.0f / 5.0f);
     const float q0 = __fmul_rn(a, y);
     const float r = __fmaf_rn(-(float)f, q0, a);
