@@ -853,21 +853,24 @@ static int v_cycle_mixed(ss_sim* s, const StepConsts& c, const ss_mg_schedule& m
 // Warm start of the mixed solve.  p64 holds the previous step's pressure
 // p(n-1).  With warm_start 1 and p64c holding p(n-2) - the solved pressure the
 // previous mixed solve started from - the solve starts from the linear
-// extrapolation 2 p(n-1) - p(n-2) and p64c takes p(n-1); otherwise p64c just
-// takes p(n-1), so that the next solve can extrapolate.  A fresh p64 (made
-// from the FP32 pressure, not solved by this path) starts no history.
+// extrapolation 2 p(n-1) - p(n-2) and p64c takes p(n-1): the pre-solve
+// divergence pass does that in place (extrapolates(), k_divergence's ep/eq).
+// Otherwise p64c just takes p(n-1) (warm_start_p64), so that the next solve
+// can extrapolate.  A fresh p64 (made from the FP32 pressure, not solved by
+// this path) starts no history.
+static bool extrapolates(const ss_sim* s, int mode, bool fresh) {
+    return mode == 1 && !fresh && s->prev_ok && s->p64c;
+}
+
 static int warm_start_p64(ss_sim* s, int mode, bool fresh, cudaStream_t st) {
     if (mode != 1 || fresh) {
         s->prev_ok = 0;
         return SS_OK;
     }
     if (!s->p64c) CU(cudaMalloc((void**)&s->p64c, s->ncell * sizeof(double)), "cudaMalloc(p64c)");
-    if (!s->prev_ok) {
-        CU(cudaMemcpyAsync(s->p64c, s->p64, s->ncell * sizeof(double), cudaMemcpyDeviceToDevice, st), "warm start copy");
-        s->prev_ok = 1;
-        return SS_OK;
-    }
-    return launch_p64_extrapolate(s, st);
+    CU(cudaMemcpyAsync(s->p64c, s->p64, s->ncell * sizeof(double), cudaMemcpyDeviceToDevice, st), "warm start copy");
+    s->prev_ok = 1;
+    return SS_OK;
 }
 
 // ------------------------------------------------ device-side tolerance loop
@@ -1008,10 +1011,12 @@ static int pressure_solve_mixed(ss_sim* s, const ss_params* p, const StepConsts&
     TRY(update_coarse_matrix(s, mg, st));
     const bool tol_mode = mg.tol > 0.0;
     const bool stats = p->collect_stats || tol_mode;
-    TRY(launch_divergence(s, true, stats ? SLOT_DIV_BEFORE : -1, st));
     const bool fresh = !s->p64_valid;
+    const bool extrap = extrapolates(s, mg.warm_start, fresh);
+    TRY(launch_divergence(s, true, stats ? SLOT_DIV_BEFORE : -1, st, nullptr, -1, extrap ? s->p64 : nullptr,
+                          extrap ? s->p64c : nullptr));
     if (fresh) TRY(launch_p64_from_p0(s, st));
-    TRY(warm_start_p64(s, mg.warm_start, fresh, st));
+    if (!extrap) TRY(warm_start_p64(s, mg.warm_start, fresh, st));
     const int cap = mg.n_vcycles > 0 ? mg.n_vcycles : 1;
     int done = 0;
     double db = 0.0, res = 0.0;

@@ -252,10 +252,12 @@ SS_D void vel_at_centre(const float* __restrict__ u, const float* __restrict__ v
 
 // Border sample with a branch-free interior fast path: when all taps are in
 // range one base address serves the 8 (4) loads.
+// 0 <= v && v + 1 < n, as one unsigned comparison (v is a clamped tap index)
+SS_D bool tap_pair_in(int v, int n) { return (unsigned)v < (unsigned)(n - 1); }
+
 template <int DIM>
 SS_D float sample_taps_fast(const float* __restrict__ a, int ax, int ay, int az, const Taps& t, float border) {
-    const bool in = t.x0 >= 0 && t.x0 + 1 < ax && t.y0 >= 0 && t.y0 + 1 < ay &&
-                    (DIM == 2 || (t.z0 >= 0 && t.z0 + 1 < az));
+    const bool in = tap_pair_in(t.x0, ax) && tap_pair_in(t.y0, ay) && (DIM == 2 || tap_pair_in(t.z0, az));
     if (!in) return sample_taps<DIM>(a, ax, ay, az, t, border);
     const float* p = a + idx3(t.x0, t.y0, t.z0, ax, ay);
     const float c00 = __ldg(p), c10 = __ldg(p + 1), c01 = __ldg(p + ax), c11 = __ldg(p + ax + 1);

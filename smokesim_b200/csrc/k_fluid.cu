@@ -1054,9 +1054,13 @@ struct RhsOut {
 // loaded once), so a block reduces up to 256 * kDivPlanes cells.
 constexpr int kDivPlanes = 8;
 
+// ep / eq (optional): the mixed solve's extrapolated warm start, elementwise
+// over the same cells (ep = 2 ep - eq in FP64, eq = the old ep), riding on this
+// pass, whose own traffic leaves HBM bandwidth to spare.
 template <int DIM>
 __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restrict__ div0, float* __restrict__ div0r,
-                                                    double* __restrict__ partial, RhsOut ro, int planes) {
+                                                    double* __restrict__ partial, RhsOut ro, int planes,
+                                                    double* __restrict__ ep, double* __restrict__ eq) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int zb = blockIdx.z * planes;
@@ -1071,6 +1075,7 @@ __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restri
         struct Faces {
             float t, b, r, l, f;
             uint8_t fl;
+            double ep, eq;
         };
         auto fetch = [&](int z, Faces& F) {
             F.t = __ldg(a.v + idx3(x, y + 1, z, nx, ny + 1));
@@ -1079,6 +1084,10 @@ __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restri
             F.l = __ldg(a.u + idx3(x, y, z, nx + 1, ny));
             F.f = DIM == 3 ? __ldg(a.w + idx3(x, y, z + 1, nx, ny)) : 0.f;
             F.fl = __ldg(a.flags + idx3(x, y, z, nx, ny));
+            if (ep) {
+                F.ep = ep[idx3(x, y, z, nx, ny)];
+                F.eq = eq[idx3(x, y, z, nx, ny)];
+            }
         };
         Faces cur;
         fetch(zb, cur);
@@ -1088,6 +1097,10 @@ __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restri
             if (z + 1 < ze) fetch(z + 1, nxt);
             const float f_top = cur.t, f_bottom = cur.b, f_right = cur.r, f_left = cur.l, f_front = cur.f;
             const uint8_t fl = cur.fl;
+            if (ep) {
+                ep[c] = 2.0 * cur.ep - cur.eq;
+                eq[c] = cur.ep;
+            }
             cur = nxt;
             if (!(fl & F_SOLID)) {
                 const bool sv = a.sv0 != nullptr;
@@ -1136,7 +1149,8 @@ __global__ void __launch_bounds__(256) k_divergence(FluidArgs a, float* __restri
     }
 }
 
-int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st, const StepConsts* sc, int quirks) {
+int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st, const StepConsts* sc, int quirks,
+                      double* ep, double* eq) {
     StepConsts c{};
     FluidArgs a = fluid_args(s, c);
     RhsOut ro{};
@@ -1155,8 +1169,9 @@ int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st, const St
     float* d0 = write ? s->div0 : nullptr;
     float* d0r = (write && s->div0r != s->div0) ? s->div0r : nullptr;
     double* part = slot >= 0 ? s->red.partial : nullptr;
-    if (s->dim == 3) k_divergence<3><<<g, b, 0, st>>>(a, d0, d0r, part, ro, planes);
-    else k_divergence<2><<<g, b, 0, st>>>(a, d0, d0r, part, ro, planes);
+    if ((ep == nullptr) != (eq == nullptr)) return set_error(SS_E_INVALID, "extrapolation needs both buffers");
+    if (s->dim == 3) k_divergence<3><<<g, b, 0, st>>>(a, d0, d0r, part, ro, planes, ep, eq);
+    else k_divergence<2><<<g, b, 0, st>>>(a, d0, d0r, part, ro, planes, ep, eq);
     s->nlaunch += 1;
     int rc = check_cuda(cudaGetLastError(), "k_divergence");
     if (rc || slot < 0) return rc;

@@ -264,21 +264,6 @@ int launch_p64_from_p0(ss_sim* s, cudaStream_t st) {
     return check_cuda(cudaGetLastError(), "k_p64_from_f32");
 }
 
-// Extrapolated warm start, in place over every cell: p = 2 p - q, q = the old
-// p (the buffers keep their places, so recorded solve graphs stay valid)
-__global__ void k_p64_extrapolate(double* __restrict__ p, double* __restrict__ q, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const double a = p[i], c = q[i];
-        p[i] = 2.0 * a - c;
-        q[i] = a;
-    }
-}
-
-int launch_p64_extrapolate(ss_sim* s, cudaStream_t st) {
-    k_p64_extrapolate<<<4 * 148, 256, 0, st>>>(s->p64, s->p64c, s->ncell);
-    s->nlaunch += 1;
-    return check_cuda(cudaGetLastError(), "k_p64_extrapolate");
-}
 
 int launch_p0_from_p64(ss_sim* s, cudaStream_t st) {
     k_f32_from_p64<<<4 * 148, 256, 0, st>>>(s->p64, s->p[0], s->ncell);

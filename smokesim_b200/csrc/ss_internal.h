@@ -215,9 +215,11 @@ int launch_update_velocities(ss_sim* s, const StepConsts& c, cudaStream_t st);
 // into that statistics slot (the k_divergence operator, no right-hand sides)
 int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st, int div_slot = -1);
 // divergence of the current velocities into div0 (+div0r); optional ||div||^2 into slot
-// with sc and quirks >= 0 also the level-0 right-hand sides rhs_s / rhs_r of that boundary rule
+// with sc and quirks >= 0 also the level-0 right-hand sides rhs_s / rhs_r of that boundary rule;
+// with ep / eq also the extrapolated warm start of the mixed solve in the same pass
+// (every cell: ep = 2 ep - eq, eq = the old ep)
 int launch_divergence(ss_sim* s, bool write, int slot, cudaStream_t st, const StepConsts* sc = nullptr,
-                      int quirks = -1);
+                      int quirks = -1, double* ep = nullptr, double* eq = nullptr);
 
 // ---- multigrid kernels (k_mg.cu) ----
 int launch_smooth(ss_sim* s, const StepConsts& c, int L, int iterations, int quirks, cudaStream_t st);
@@ -262,7 +264,6 @@ int launch_rb_residual_restrict_mixed(ss_sim* s, int prec, cudaStream_t st);
 
 int launch_rb_prolong_mixed(ss_sim* s, int prec, cudaStream_t st);
 int launch_p64_from_p0(ss_sim* s, cudaStream_t st);
-int launch_p64_extrapolate(ss_sim* s, cudaStream_t st);
 int launch_p0_from_p64(ss_sim* s, cudaStream_t st);
 int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate, cudaStream_t st,
                        const IrDecide* dec = nullptr);
