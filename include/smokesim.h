@@ -127,7 +127,9 @@ typedef struct ss_mg_schedule {
     int n_post;             /* red-black sweeps after prolongation */
     int n_coarse;           /* sweeps on the coarsest level */
     int n_vcycles;          /* V-cycles per frame (tol == 0) or the cap (tol > 0) */
-    double tol;             /* > 0: iterate until relative divergence <= tol */
+    double tol;             /* > 0: iterate until relative divergence <= tol (mixed-precision solve on a
+                               caller's stream: the first 8 refinement steps run as conditional graph
+                               nodes with the test on the device; SMOKESIM_DEVICE_LOOP=0 tests on the host) */
     int ref_quirks;         /* 1: post-smoothing at level > 0 reads the in-place residual (reference) */
     int precision;          /* ss_precision */
     int warm_start;         /* mixed-precision solve: 0 starts from the previous step's pressure (as the
