@@ -75,7 +75,11 @@ __global__ void k_f32_from_p64(const double* __restrict__ p64, float* __restrict
 constexpr int kIrTX = 32, kIrTY = 8, kIrChunk = 16;   // largest z chunk
 constexpr int kIrRim = 2 * kIrTX + 2 * kIrTY;   // rim cells of a tile (no corners: 5/7-point stencil)
 
-template <int DIM, bool ACC>
+// DEC: the launch carries the device-side convergence test (IrDecide) of the
+// tolerance loop's graph.  Only those instantiations contain the call that
+// sets a graph condition; the others stay plain kernels (profilers skip graph
+// kernel nodes that can set conditions).
+template <int DIM, bool ACC, bool DEC = false>
 __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
     const double* __restrict__ p_in, const float* __restrict__ e, double* __restrict__ p_out,
     const float* __restrict__ div0, const uint8_t* __restrict__ fmask, int nx, int ny, int nz, double k,
@@ -233,7 +237,7 @@ __global__ void __launch_bounds__(kIrTX * kIrTY) k_ir_residual(
         scale[0] = (float)ldexp(1.0, -e);
         scale[1] = (float)ldexp(1.0, e);
         *ticket = 0u;
-        if (dec.active) {
+        if (DEC && dec.active) {
             // the host loop's test, on the same doubles: stop once
             // sqrt(residual) <= tol sqrt(divergence before the solve)
             out[SLOT_STEPS] = (double)dec.k;
@@ -292,11 +296,21 @@ int launch_ir_residual(ss_sim* s, const StepConsts& c, int slot, bool accumulate
                      s->rhs_s, rhs_r, s->red.partial, s->red.partial_max, s->red.ticket, s->red.out, slot, \
                      s->d_scale, planes, d
     if (s->dim == 3) {
-        if (accumulate) launch_k(s->pdl, g, b, 0, st, k_ir_residual<3, true>, IR_ARGS(true));
-        else launch_k(s->pdl, g, b, 0, st, k_ir_residual<3, false>, IR_ARGS(false));
+        if (d.active) {
+            if (accumulate) launch_k(s->pdl, g, b, 0, st, k_ir_residual<3, true, true>, IR_ARGS(true));
+            else launch_k(s->pdl, g, b, 0, st, k_ir_residual<3, false, true>, IR_ARGS(false));
+        } else {
+            if (accumulate) launch_k(s->pdl, g, b, 0, st, k_ir_residual<3, true>, IR_ARGS(true));
+            else launch_k(s->pdl, g, b, 0, st, k_ir_residual<3, false>, IR_ARGS(false));
+        }
     } else {
-        if (accumulate) launch_k(s->pdl, g, b, 0, st, k_ir_residual<2, true>, IR_ARGS(true));
-        else launch_k(s->pdl, g, b, 0, st, k_ir_residual<2, false>, IR_ARGS(false));
+        if (d.active) {
+            if (accumulate) launch_k(s->pdl, g, b, 0, st, k_ir_residual<2, true, true>, IR_ARGS(true));
+            else launch_k(s->pdl, g, b, 0, st, k_ir_residual<2, false, true>, IR_ARGS(false));
+        } else {
+            if (accumulate) launch_k(s->pdl, g, b, 0, st, k_ir_residual<2, true>, IR_ARGS(true));
+            else launch_k(s->pdl, g, b, 0, st, k_ir_residual<2, false>, IR_ARGS(false));
+        }
     }
 #undef IR_ARGS
     s->nlaunch += 1;
