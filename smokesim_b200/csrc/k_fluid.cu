@@ -929,18 +929,25 @@ __global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a, DivFold df, i
             continue;
         }
         if constexpr (DIV) {
-            const bool sv = a.sv0 != nullptr;
-            const float v_top = (fl & F_TOP) ? (sv ? a.sv1[c + nx] : 0.f) : f_top;
-            const float v_bottom = (fl & F_BOTTOM) ? (sv ? a.sv1[c - nx] : 0.f) : f_bottom;
-            const float v_right = (fl & F_RIGHT) ? (sv ? a.sv0[c + 1] : 0.f) : f_right;
-            const float v_left = (fl & F_LEFT) ? (sv ? a.sv0[c - 1] : 0.f) : f_left;
-            float d = v_right - v_left + v_top - v_bottom;
-            if constexpr (DIM == 3) {
-                const float v_front = (fl & F_FRONT) ? (sv ? a.sv2[c + pl] : 0.f) : f_front;
-                const float v_back = (fl & F_BACK) ? (sv ? a.sv2[c - pl] : 0.f) : f_back;
-                d = d + v_front - v_back;
+            if (!(fl & 0x7Eu)) {
+                // no face borders a solid: the faces as loaded, the same operations
+                float d = f_right - f_left + f_top - f_bottom;
+                if constexpr (DIM == 3) d = d + f_front - f_back;
+                acc += (double)d * (double)d;
+            } else {
+                const bool sv = a.sv0 != nullptr;
+                const float v_top = (fl & F_TOP) ? (sv ? a.sv1[c + nx] : 0.f) : f_top;
+                const float v_bottom = (fl & F_BOTTOM) ? (sv ? a.sv1[c - nx] : 0.f) : f_bottom;
+                const float v_right = (fl & F_RIGHT) ? (sv ? a.sv0[c + 1] : 0.f) : f_right;
+                const float v_left = (fl & F_LEFT) ? (sv ? a.sv0[c - 1] : 0.f) : f_left;
+                float d = v_right - v_left + v_top - v_bottom;
+                if constexpr (DIM == 3) {
+                    const float v_front = (fl & F_FRONT) ? (sv ? a.sv2[c + pl] : 0.f) : f_front;
+                    const float v_back = (fl & F_BACK) ? (sv ? a.sv2[c - pl] : 0.f) : f_back;
+                    d = d + v_front - v_back;
+                }
+                acc += (double)d * (double)d;
             }
-            acc += (double)d * (double)d;
         }
         const float gx = (float)x + 0.5f, gy = (float)y + 0.5f, gz = DIM == 3 ? (float)z + 0.5f : 0.f;
         const float cfl = a.c.cfl;
@@ -992,7 +999,10 @@ __global__ void __launch_bounds__(256) k_advect_smoke(FluidArgs a, DivFold df, i
 int launch_advect_smoke(ss_sim* s, const StepConsts& c, cudaStream_t st, int div_slot) {
     FluidArgs a = fluid_args(s, c);
     dim3 b(32, 8, 1);
-    const int planes = z_planes((long long)((s->nx + 31) / 32) * ((s->ny + 7) / 8), s->nz, kSmokePlanes);
+    // the divergence fold ends each block with a reduction: twice the planes
+    // a thread spread its barrier over twice the cells
+    const int planes = z_planes((long long)((s->nx + 31) / 32) * ((s->ny + 7) / 8), s->nz,
+                                div_slot >= 0 ? 2 * kSmokePlanes : kSmokePlanes);
     dim3 g = grid_for(s->nx, s->ny, (s->nz + planes - 1) / planes, b);
     DivFold df{s->red.partial, s->red.ticket, s->red.out, div_slot};
     if (div_slot >= 0 && (int)(g.x * g.y * g.z) > s->red.max_blocks)
