@@ -311,6 +311,7 @@ int launch_rbgs_sweep_tma(ss_sim* s, const StepConsts& c, int L, int quirks, boo
     const bool pow2 = is_pow2_float(a.hh);
     a.inv_hh = pow2 ? 1.f / a.hh : 0.f;
     a.err = s->d_err;
+    s->err_armed = 1;   // its bounded waits may set the error word
     a.p_out = s->p_alt[L];
     if (L == 0) return set_error(SS_E_UNSUPPORTED, "level 0 runs on the colour-split arrays");
     const float* rhs = s->r[L];
